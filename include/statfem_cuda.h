@@ -1,0 +1,255 @@
+/*
+ * statfem_cuda.h -- C ABI of the B200-native statFEM forward-and-conditioning
+ * path (element assembly, SPD sparse solves, GP forcing covariance and the
+ * prior-to-posterior conditioning on sensor data).
+ *
+ * Plain C types only: host pointers, sizes, opaque handles.  Every function
+ * returns SFC_OK (0) or a negative SFC_ERR_* code; sfc_last_error() gives the
+ * message of the last failure on a context.  Calls on one context are issued
+ * in order on that context's CUDA stream; a context is not thread-safe (one
+ * context per host thread), like the reference's solver objects.  Pointer
+ * arguments are HOST memory unless the name ends in _dev.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * fcirak/statFEM).  The reference has no FFI of its own: it is a header-only
+ * C++ library whose solver is selected by a typedef
+ * (del2/apps/reference/laplaceRHSinfer/laplaceRHSinfer.cpp:99).  The C++
+ * class corlib::SystemSolveCuda (include/corlib/SystemSolveCuda.hpp) wraps
+ * this ABI with the method set of corlib::SystemSolveEigenSparse so that
+ * changing that typedef is the whole integration.
+ */
+#ifndef STATFEM_CUDA_H
+#define STATFEM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define SFC_OK                 0
+#define SFC_ERR_CUDA          -1  /* a CUDA runtime call failed              */
+#define SFC_ERR_BAD_ARG       -2  /* invalid argument / state                 */
+#define SFC_ERR_NOT_SPD       -3  /* Cholesky or CG breakdown (p^T A p <= 0)  */
+#define SFC_ERR_NOT_CONVERGED -4  /* iteration cap reached                    */
+#define SFC_ERR_TIMEOUT       -5  /* a bounded device-side wait gave up       */
+#define SFC_ERR_NO_MEMORY     -6  /* device or host allocation failed         */
+#define SFC_ERR_NEG_JACOBIAN  -7  /* detJ <= 0 in an element (FTL_VERIFY in
+                                     corlib/ElementBasic.ipp:199)             */
+
+/* ---- element kinds (element type + its integrand) ------------------------ */
+#define SFC_ELEM_LINE2_POISSON  1 /* del2::fem::ElementPotential, 2-node line */
+#define SFC_ELEM_TRI3_POISSON   2 /* ElementPotential, 3-node triangle        */
+#define SFC_ELEM_HEX8_POISSON   3 /* ElementPotential, trilinear hexahedron   */
+#define SFC_ELEM_HEX8_ELASTIC   4 /* solid::fem::ElementStatic + SVenant at
+                                     F = I (isotropic linear elasticity)      */
+
+/* ---- solver methods ------------------------------------------------------ */
+#define SFC_SOLVER_PCG_FP64      0 /* plain FP64 Jacobi-PCG, one RHS at a time */
+#define SFC_SOLVER_PCG_MIXED     1 /* FP32 block Jacobi-PCG (many RHS share the
+                                      matrix) + FP64 residual refinement      */
+
+typedef struct sfc_ctx sfc_ctx_t;
+typedef struct sfc_mesh sfc_mesh_t;
+typedef struct sfc_system sfc_system_t;
+typedef struct sfc_covar_forcing sfc_covar_forcing_t;
+typedef struct sfc_forward_gauss sfc_forward_gauss_t;
+typedef struct sfc_koh sfc_koh_t;
+
+typedef struct sfc_solver_options {
+    int32_t method;        /* SFC_SOLVER_*                                     */
+    int32_t max_iter;      /* inner iteration cap per right-hand side          */
+    double tol;            /* relative residual ||b-Ax||/||b|| (true, FP64)    */
+    double inner_tol;      /* FP32 inner reduction per refinement cycle        */
+    int32_t block_width;   /* RHS per block for SFC_SOLVER_PCG_MIXED (0: auto) */
+    int32_t check_every;   /* iterations between convergence checks (0: auto)  */
+} sfc_solver_options_t;
+
+typedef struct sfc_solve_stats {
+    int32_t iterations;       /* max over right-hand sides, inner iterations   */
+    int32_t refinements;      /* FP64 refinement cycles (mixed solver)         */
+    int32_t num_rhs;
+    int32_t converged;        /* 1 when every RHS met tol                      */
+    double max_rel_residual;  /* max over RHS of the true FP64 ||b-Ax||/||b||  */
+    double device_ms;         /* device time of the last solve call            */
+} sfc_solve_stats_t;
+
+/* Hyperparameters; the reference keeps them in std::map<std::string,double>
+ * under these names (statX/infer/ExpKernel.hpp:63-64 with the prefixes set in
+ * CovarianceForcing.hpp:73, MismatchCovariance.hpp:62-67 and
+ * LikelihoodKOH.hpp:66). */
+typedef struct sfc_hparams {
+    double forcing_sigma;       /* "forcing.sigma"       */
+    double forcing_length;      /* "forcing.length"      */
+    double rho;                 /* "rho"                 */
+    double mismatch_sigma;      /* "mismatch.sigma"      */
+    double mismatch_length;     /* "mismatch.length"     */
+    double mismatch_sensor_eps; /* "mismatch.sensorEps"  */
+} sfc_hparams_t;
+
+/* ---- context --------------------------------------------------------------- */
+int32_t sfc_version(void);
+/* No reference counterpart (the reference is host-only): owns the device and
+ * the CUDA stream that every later call on it is issued on. */
+int32_t sfc_ctx_create(int32_t device, sfc_ctx_t **out);
+int32_t sfc_ctx_destroy(sfc_ctx_t *ctx);
+const char *sfc_last_error(const sfc_ctx_t *ctx);
+int32_t sfc_ctx_synchronize(sfc_ctx_t *ctx);
+/* Number of kernels this library has launched on the context. */
+int32_t sfc_ctx_kernel_launches(const sfc_ctx_t *ctx, int64_t *count);
+/* Device time between two markers recorded on the context stream. */
+int32_t sfc_ctx_mark(sfc_ctx_t *ctx, int32_t slot);
+int32_t sfc_ctx_marker_ms(sfc_ctx_t *ctx, int32_t slot_begin, int32_t slot_end, double *ms);
+
+/* ---- mesh -------------------------------------------------------------- */
+/* Replaces corlib::Mesh<Element>(std::istream& smf) (corlib/Mesh.ipp:63-102)
+ * plus Node::numberDOFs (del2/fem/NodePotential.hpp:65,
+ * solid/fem/NodeStatic.ipp:15-19): coords are num_nodes x 3 (an SMF node line
+ * always has three columns), conn is num_elems x nodes_per_elem with 0-based
+ * node ids, dof = node * dofs_per_node + component.  quad_points is the
+ * reference's Quadrature<SHAPE,QPS> QPS (line: 1..5; triangle: 1 or 3;
+ * hexahedron: 1, 8, 27, 64, 125).  Builds the CSR pattern and the
+ * element-entry -> CSR-slot maps on the device (one-time symbolic phase). */
+int32_t sfc_mesh_create(sfc_ctx_t *ctx, int32_t element_kind, int32_t quad_points,
+                        const double *coords, int64_t num_nodes, const uint32_t *conn,
+                        int64_t num_elems, sfc_mesh_t **out);
+int32_t sfc_mesh_destroy(sfc_mesh_t *mesh);
+/* Per-element coefficient: conductivity (ElementPotential::setConductivity,
+ * del2/fem/ElementPotential.hpp:94-97) or Young's modulus (SVenant
+ * "youngModulus", solid/material/svenant/SVenant.ipp:16); poisson_ratio is
+ * used by the elastic kind.  values == NULL sets every element to uniform. */
+int32_t sfc_mesh_set_coefficients(sfc_mesh_t *mesh, const double *values, double uniform,
+                                  double poisson_ratio);
+int64_t sfc_mesh_num_dofs(const sfc_mesh_t *mesh);
+int64_t sfc_mesh_nnz(const sfc_mesh_t *mesh);
+
+/* ---- system (corlib::SystemSolveEigenSparse replacement) ------------------ */
+/* SystemSolveEigenSparse(numDofs), corlib/SystemSolveEigenSparse.hpp:54-60 */
+int32_t sfc_system_create(sfc_ctx_t *ctx, int64_t num_dofs, sfc_system_t **out);
+int32_t sfc_system_destroy(sfc_system_t *sys);
+int32_t sfc_system_set_options(sfc_system_t *sys, const sfc_solver_options_t *opt);
+int32_t sfc_system_get_options(const sfc_system_t *sys, sfc_solver_options_t *opt);
+int32_t sfc_system_last_stats(const sfc_system_t *sys, sfc_solve_stats_t *stats);
+
+/* insertToMatrix, SystemSolveEigenSparse.hpp:160-172 (called per element by
+ * MatrixAssembler::operator(), corlib/MatrixAssembler.hpp:224-229).  Ke is
+ * row-major n x m.  Entries are staged on the host and sorted / merged on the
+ * GPU at the next finish, constraint or solve call, with the triplet
+ * semantics of corlib/Triplet.hpp:126-170 (duplicates summed in insertion
+ * order, explicit zeros kept). */
+int32_t sfc_insert_matrix(sfc_system_t *sys, const double *Ke, const uint32_t *rows, uint32_t n,
+                          const uint32_t *cols, uint32_t m);
+/* insertToRhs, SystemSolveEigenSparse.hpp:176-184: F[dofs[i]] += fe[i]. */
+int32_t sfc_insert_rhs(sfc_system_t *sys, const double *fe, const uint32_t *dofs, uint32_t n);
+/* finishAssembly / finishMatAssembly / finishRhsAssembly,
+ * SystemSolveEigenSparse.hpp:93-98 (no-ops there; here they flush the staged
+ * host data to the device). */
+int32_t sfc_finish_assembly(sfc_system_t *sys);
+
+/* GPU assembler (corlib::MatrixComputeAndAssembleFun over all elements,
+ * corlib/MatrixAssembler.hpp:43-100 + ComputeElementMatrix.hpp:62-77 with
+ * Element::stiffnessIntegrand): computes every element matrix and sums them
+ * into the system's CSR values, in element order per CSR slot.  Replaces any
+ * previous matrix values (clearMatrix + full assembly). */
+int32_t sfc_assemble_matrix(sfc_system_t *sys, const sfc_mesh_t *mesh);
+/* GPU body-force load (Integrator<Quad,BodyForce> over elements +
+ * VectorAssembler, corlib/Integrator.hpp:61-73, BodyForce.hpp:66-71,
+ * VectorAssembler.hpp:101-114) for a constant force f[dofs_per_node]:
+ * F += assembled nodal forces. */
+int32_t sfc_assemble_load(sfc_system_t *sys, const sfc_mesh_t *mesh, const double *f);
+
+/* applyConstraints, SystemSolveEigenSparse.hpp:197-215 (Triplet::zeroRow,
+ * corlib/Triplet.hpp:219-260): for each (idx[t], value[t]) zero the row, put
+ * `scalar` on its diagonal and set F[idx] = (factor*value)*scalar.
+ * value == NULL means all zero. */
+int32_t sfc_apply_constraints(sfc_system_t *sys, const uint32_t *idx, const double *value,
+                              int64_t n, double factor, double scalar);
+/* fixDOF, SystemSolveEigenSparse.hpp:219-226 */
+int32_t sfc_fix_dof(sfc_system_t *sys, uint32_t idx, double scalar);
+
+/* solveSystem() / solveSystem(bool reuse), SystemSolveEigenSparse.hpp:
+ * 273-360: X = A^-1 F.  The row-zeroed matrix is solved through its symmetric
+ * elimination (constrained columns lifted into the right-hand side) with the
+ * configured PCG; `reuse` is accepted for interface parity (the iterative
+ * solver keeps no factorisation). */
+int32_t sfc_solve(sfc_system_t *sys, int32_t reuse);
+/* solveSystemTranspose, SystemSolveEigenSparse.hpp:364-404: u = A^-T rhs
+ * for num_rhs right-hand sides (rhs, u: num_rhs x num_dofs, row-major, host). */
+int32_t sfc_solve_transpose(sfc_system_t *sys, const double *rhs, double *u, int32_t num_rhs,
+                            int32_t reuse);
+/* giveSolution / giveForce, SystemSolveEigenSparse.hpp:408-428 */
+int32_t sfc_give_solution(const sfc_system_t *sys, const uint32_t *dofs, int64_t n,
+                          double *out);
+int32_t sfc_give_force(const sfc_system_t *sys, const uint32_t *dofs, int64_t n, double *out);
+/* clearMatrix / clearRhs, SystemSolveEigenSparse.hpp:104-107 */
+int32_t sfc_clear_matrix(sfc_system_t *sys);
+int32_t sfc_clear_rhs(sfc_system_t *sys);
+/* numNonZeros / normMatrix / normRhs / norm1Rhs / normSol,
+ * SystemSolveEigenSparse.hpp:78-83,118 */
+int64_t sfc_num_nonzeros(const sfc_system_t *sys);
+int32_t sfc_norms(const sfc_system_t *sys, double *frobenius_matrix, double *norm2_rhs,
+                  double *norm1_rhs, double *norm2_sol);
+/* Export of the assembled matrix in the reference's row-zeroed form (CSR of
+ * the sorted, merged triplets; writeMatrix, SystemSolveEigenSparse.hpp:73). */
+int32_t sfc_get_csr(const sfc_system_t *sys, int64_t *row_ptr, int32_t *col, double *val);
+
+/* ---- statX: forcing covariance ------------------------------------------- */
+/* CovarianceForcing<DOF,ExpKernel>(numNodes), statX/infer/CovarianceForcing.hpp:
+ * 68-74, with coordinates inserted per node (insertToCoordinates, .ipp:27-34)
+ * and phibar = int(phi_i) from the GPU unit load (inference.hpp:108-119). */
+int32_t sfc_covar_forcing_create(sfc_ctx_t *ctx, const sfc_mesh_t *mesh,
+                                 sfc_covar_forcing_t **out);
+int32_t sfc_covar_forcing_destroy(sfc_covar_forcing_t *cf);
+/* CovarianceForcing::applyConstraints, CovarianceForcing.hpp:101-114 */
+int32_t sfc_covar_forcing_apply_constraints(sfc_covar_forcing_t *cf, const uint32_t *idx,
+                                            int64_t n);
+int32_t sfc_covar_forcing_get_phibar(const sfc_covar_forcing_t *cf, double *out);
+/* giveProjectedCovar, CovarianceForcing.ipp:38-109: out = M C_f M^T for a
+ * dense M (rows x num_dofs, row-major, host); out is rows x rows. */
+int32_t sfc_covar_forcing_projected(sfc_covar_forcing_t *cf, const sfc_hparams_t *hp,
+                                    const double *M, int64_t rows, double *out);
+
+/* ---- statX: ForwardGaussRHS ------------------------------------------------ */
+/* ForwardGaussRHS(solver, covarForcing, regEps), statX/infer/ForwardGaussRHS.hpp:61-64 */
+int32_t sfc_forward_gauss_create(sfc_system_t *sys, sfc_covar_forcing_t *cf, double reg_eps,
+                                 sfc_forward_gauss_t **out);
+int32_t sfc_forward_gauss_destroy(sfc_forward_gauss_t *fg);
+/* setProjectionMatrix, ForwardGaussRHS.hpp:71-74; P given as CSR
+ * (num_sensors x num_dofs). */
+int32_t sfc_forward_gauss_set_projection(sfc_forward_gauss_t *fg, int64_t num_sensors,
+                                         const int64_t *indptr, const int32_t *indices,
+                                         const double *data);
+/* updateSolution, ForwardGaussRHS.hpp:95-139: R = P A^-1 from one block
+ * adjoint solve, mean = R F, C_s = R C_f R^T + (sigma_f reg)^2 P P^T. */
+int32_t sfc_forward_gauss_update(sfc_forward_gauss_t *fg, const sfc_hparams_t *hp);
+/* giveProjectedMeanU / giveProjectedCovarU, ForwardGaussRHS.hpp:77-92 */
+int32_t sfc_forward_gauss_mean(const sfc_forward_gauss_t *fg, double *out);
+int32_t sfc_forward_gauss_covar(const sfc_forward_gauss_t *fg, double *out);
+
+/* ---- statX: LikelihoodKOH ---------------------------------------------------- */
+/* LikelihoodKOH(forwardGauss, mismatchCov) with MismatchCovariance(sensorCoords),
+ * statX/infer/LikelihoodKOH.hpp:66-72, MismatchCovariance.hpp:62-67;
+ * sensor_coords is num_sensors x dim. */
+int32_t sfc_koh_create(sfc_forward_gauss_t *fg, const double *sensor_coords, int32_t dim,
+                       sfc_koh_t **out);
+int32_t sfc_koh_destroy(sfc_koh_t *koh);
+/* setSensorValues, LikelihoodKOH.hpp:79-84: Y is num_sensors x num_readings,
+ * row-major. */
+int32_t sfc_koh_set_sensor_values(sfc_koh_t *koh, const double *Y, int32_t num_readings);
+/* giveLogLikelihood, LikelihoodKOH.ipp:75-120 (FP64 sensor-space Cholesky) */
+int32_t sfc_koh_log_likelihood(sfc_koh_t *koh, const sfc_hparams_t *hp, double *out);
+/* giveProjFEconditionedData, LikelihoodKOH.ipp:311-361: posterior mean
+ * (num_sensors) and covariance (num_sensors^2) at the sensors. */
+int32_t sfc_koh_proj_conditioned(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean,
+                                 double *cov);
+/* giveFEconditionedDataWoodbury, LikelihoodKOH.ipp:442-508: full-field
+ * posterior mean (num_dofs) and covariance (num_dofs^2; may be NULL).  Needs
+ * num_dofs adjoint solves, so it is limited to num_dofs <= 8192. */
+int32_t sfc_koh_woodbury(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean, double *cov);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

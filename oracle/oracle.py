@@ -1,0 +1,311 @@
+"""CPU oracle for the statFEM forward-and-conditioning path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of ``bench.py`` as the checker.  The product never
+imports it.
+
+Finite-element arithmetic (quadrature, element matrices, loads, triplet
+assembly, row-zeroing constraints, squared-exponential kernel, dense nodal
+forcing covariance) comes from the C restatement in ``sfo.c``; the sparse
+direct solves use SuperLU (``scipy.sparse.linalg.splu``), the same LU family
+as the reference's ``Eigen::SparseLU`` (corlib/SystemSolveEigenSparse.hpp:
+153,299-300,394-397), applied to the same non-symmetric row-zeroed matrix and
+its transpose; the small dense statistics are restated in numpy following
+statX/infer/{ForwardGaussRHS.hpp,MismatchCovariance.hpp,LikelihoodKOH.ipp}.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libsfo.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+def build():
+    """Compile sfo.c into _build/libsfo.so (make, no reference sources)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(_HERE, "sfo.c")
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.sfo_quadrature.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.sfo_element_matrix.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_double,
+                                         ctypes.c_double, _dp]
+        L.sfo_assemble_load.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int64, _u32p,
+                                        ctypes.c_int64, _dp, _dp]
+        L.sfo_assemble_csr.restype = ctypes.c_int64
+        L.sfo_assemble_csr.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_int64, _u32p,
+                                       ctypes.c_int64, _dp, ctypes.c_double, _i64p, _i32p, _dp]
+        L.sfo_apply_constraints.argtypes = [ctypes.c_int64, _i64p, _i32p, _dp, _dp, _u32p, _dp,
+                                            ctypes.c_int64, ctypes.c_double, ctypes.c_double]
+        L.sfo_se_kernel.restype = ctypes.c_double
+        L.sfo_se_kernel.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double]
+        L.sfo_forcing_covariance_dense.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, _dp,
+                                                   _dp, ctypes.c_double, ctypes.c_double, _dp]
+        L.sfo_pcg.argtypes = [ctypes.c_int64, _i64p, _i32p, _dp, _u8p, _dp, _dp, ctypes.c_double,
+                              ctypes.c_int, _dp]
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+# --------------------------------------------------------------------------
+# finite-element part (C restatement)
+# --------------------------------------------------------------------------
+
+def quadrature(kind, qps):
+    w = np.zeros(125)
+    pts = np.zeros(375)
+    n = lib().sfo_quadrature(kind, qps, _p(w, _dp), _p(pts, _dp))
+    if n <= 0:
+        raise ValueError("unsupported quadrature")
+    return w[:n].copy(), pts[: 3 * n].reshape(n, 3).copy()
+
+
+def element_matrix(kind, qps, X, coeff=1.0, nu=0.3):
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    L = {1: 2, 2: 3, 3: 8, 4: 24}[kind]
+    Ke = np.zeros((L, L))
+    rc = lib().sfo_element_matrix(kind, qps, _p(X, _dp), coeff, nu, _p(Ke, _dp))
+    if rc < 0:
+        raise ValueError("element matrix failed (%d)" % rc)
+    return Ke
+
+
+def assemble_csr(mesh, qps, coeff=None, nu=0.3):
+    """Row-major sorted-unique triplets (explicit zeros kept) as scipy CSR."""
+    L = lib()
+    c = None if coeff is None else np.ascontiguousarray(coeff, dtype=np.float64)
+    cp = _p(c, _dp) if c is not None else None
+    args = (mesh.kind, qps, _p(mesh.coords, _dp), mesh.num_nodes, _p(mesh.conn, _u32p),
+            mesh.num_elems, cp, nu)
+    nnz = L.sfo_assemble_csr(*args, None, None, None)
+    if nnz < 0:
+        raise ValueError("assembly failed (%d)" % nnz)
+    N = mesh.num_dofs
+    rp = np.zeros(N + 1, dtype=np.int64)
+    col = np.zeros(nnz, dtype=np.int32)
+    val = np.zeros(nnz)
+    L.sfo_assemble_csr(*args, _p(rp, _i64p), _p(col, _i32p), _p(val, _dp))
+    return rp, col, val
+
+
+def assemble_load(mesh, qps, f):
+    f = np.ascontiguousarray(np.atleast_1d(f), dtype=np.float64)
+    F = np.zeros(mesh.num_dofs)
+    rc = lib().sfo_assemble_load(mesh.kind, qps, _p(mesh.coords, _dp), mesh.num_nodes,
+                                 _p(mesh.conn, _u32p), mesh.num_elems, _p(f, _dp), _p(F, _dp))
+    if rc < 0:
+        raise ValueError("load failed")
+    return F
+
+
+def apply_constraints(rp, col, val, F, idx, value=None, factor=1.0, scalar=1.0):
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    value = np.zeros(len(idx)) if value is None else np.ascontiguousarray(value, dtype=np.float64)
+    rc = lib().sfo_apply_constraints(len(rp) - 1, _p(rp, _i64p), _p(col, _i32p), _p(val, _dp),
+                                     _p(F, _dp) if F is not None else None, _p(idx, _u32p),
+                                     _p(value, _dp), len(idx), factor, scalar)
+    if rc < 0:
+        raise ValueError("constraint failed (%d)" % rc)
+
+
+def se_kernel(dim, x, y, sigma, length):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    return lib().sfo_se_kernel(dim, _p(x, _dp), _p(y, _dp), sigma, length)
+
+
+def forcing_covariance_dense(dim, dof, coords, phibar, sigma, length):
+    """coords: num_nodes x 3 (SMF layout); the first dim columns are used."""
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    if coords.ndim != 2 or coords.shape[1] != 3:
+        raise ValueError("coords must be num_nodes x 3")
+    phibar = np.ascontiguousarray(phibar, dtype=np.float64)
+    n = coords.shape[0]
+    Cf = np.zeros((n * dof, n * dof))
+    lib().sfo_forcing_covariance_dense(dim, dof, n, _p(coords, _dp), _p(phibar, _dp), sigma,
+                                       length, _p(Cf, _dp))
+    return Cf
+
+
+def pcg(rp, col, val, mask, b, tol=1e-8, max_iter=100000):
+    N = len(rp) - 1
+    x = np.zeros(N)
+    work = np.zeros(4 * N)
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    it = lib().sfo_pcg(N, _p(rp, _i64p), _p(col, _i32p), _p(val, _dp), _p(m, _u8p), _p(b, _dp),
+                       _p(x, _dp), tol, max_iter, _p(work, _dp))
+    return x, it
+
+
+# --------------------------------------------------------------------------
+# solver: SuperLU on the reference's row-zeroed system
+# --------------------------------------------------------------------------
+
+class DirectSolver:
+    """SystemSolveEigenSparse restated with SuperLU: solveSystem factorises A,
+    solveSystemTranspose factorises A^T (SystemSolveEigenSparse.hpp:273-404)."""
+
+    def __init__(self, rp, col, val):
+        N = len(rp) - 1
+        self.A = sp.csr_matrix((val, col, rp), shape=(N, N))
+        self._lu = None
+        self._luT = None
+
+    def solve(self, F):
+        if self._lu is None:
+            self._lu = spla.splu(self.A.tocsc())
+        return self._lu.solve(np.asarray(F, dtype=np.float64))
+
+    def solve_transpose(self, rhs):
+        if self._luT is None:
+            self._luT = spla.splu(self.A.T.tocsc())
+        return self._luT.solve(np.asarray(rhs, dtype=np.float64))
+
+
+# --------------------------------------------------------------------------
+# statistics (numpy restatement of statX/infer)
+# --------------------------------------------------------------------------
+
+def se_matrix(X, Y, sigma, length):
+    """ExpKernel values for all pairs (statX/infer/ExpKernel.hpp:74-92)."""
+    D = X[:, None, :] - Y[None, :, :]
+    return sigma * sigma * np.exp(-np.sum(D * D, axis=2) / (2.0 * length * length))
+
+
+def forward_gauss_rhs(solver, F, P, coords, phibar, dim, dof, sigma_f, length_f, reg):
+    """ForwardGaussRHS::updateSolution (statX/infer/ForwardGaussRHS.hpp:95-139):
+    R rows solve A^T r_i = P_i; mean = R F; C_s = R C_f R^T + (sigma_f*reg)^2 P P^T
+    with C_f from CovarianceForcing::giveProjectedCovar (CovarianceForcing.ipp:38-109)."""
+    R = np.stack([solver.solve_transpose(P[i]) for i in range(P.shape[0])])
+    mean = R @ F
+    Cf = forcing_covariance_dense(dim, dof, coords, phibar, sigma_f, length_f)
+    C = R @ Cf @ R.T
+    add = sigma_f * reg
+    C = C + add * add * (P @ P.T)
+    return mean, C, R
+
+
+def mismatch_covariance(sensor_coords, sigma_d, length_d, eps):
+    """MismatchCovariance::giveCovariance (statX/infer/MismatchCovariance.hpp:76-99)."""
+    K = se_matrix(sensor_coords, sensor_coords, sigma_d, length_d)
+    return K + eps * eps * np.eye(len(sensor_coords))
+
+
+def koh_log_likelihood(mean_s, C_s, Ks, Y, rho):
+    """LikelihoodKOH::giveLogLikelihood (statX/infer/LikelihoodKOH.ipp:75-120):
+    C = K_s + rho^2 C_s; n_o * (-ns/2 log 2pi - sum log L_ii) - 1/2 sum_k d_k^T C^-1 d_k."""
+    ns, n_o = Y.shape
+    C = Ks + rho * rho * C_s
+    L = np.linalg.cholesky(C)
+    t1 = -0.5 * ns * math.log(2.0 * math.pi)
+    t2 = -0.5 * (2.0 * np.sum(np.log(np.diag(L))))
+    t3 = 0.0
+    for k in range(n_o):
+        d = Y[:, k] - rho * mean_s
+        z = np.linalg.solve(L, d)
+        q = -0.5 * float(z @ z)
+        if not q < 0.0:
+            raise ValueError("non-negative quadratic term")
+        t3 += q
+    return n_o * (t1 + t2) + t3
+
+
+def koh_proj_conditioned(mean_s, C_s, Ks, Y, rho):
+    """LikelihoodKOH::giveProjFEconditionedData (LikelihoodKOH.ipp:311-361):
+    Sigma = (rho^2 n_o K_s^-1 + C_s^-1)^-1; m = Sigma (rho K_s^-1 sum_k y_k + C_s^-1 mean)."""
+    n_o = Y.shape[1]
+    Ksi = np.linalg.inv(Ks)
+    Cui = np.linalg.inv(C_s)
+    S = np.linalg.inv(rho * rho * n_o * Ksi + Cui)
+    ysum = Y.sum(axis=1)
+    m = S @ (rho * Ksi @ ysum + Cui @ mean_s)
+    return m, S
+
+
+def koh_woodbury(C_s, Ks, Y, rho, P, C_u, u_mean):
+    """LikelihoodKOH::giveFEconditionedDataWoodbury (LikelihoodKOH.ipp:442-508):
+    S = K_s/(rho^2 n_o) + C_s; D = I - C_u P^T S^-1 P; Sigma = D C_u;
+    m = D (rho C_u P^T K_s^-1 sum_k y_k + u_mean).  C_u, u_mean are the
+    unprojected (P = I) prior covariance and mean."""
+    n_o = Y.shape[1]
+    Ksi = np.linalg.inv(Ks)
+    Si = np.linalg.inv(Ks / (rho * rho * n_o) + C_s)
+    N = C_u.shape[0]
+    D = np.eye(N) - C_u @ P.T @ Si @ P
+    cov = D @ C_u
+    ysum = Y.sum(axis=1)
+    vecA = rho * (C_u @ P.T @ Ksi @ ysum)
+    mean = D @ (vecA + u_mean)
+    return mean, cov
+
+
+def gp_regression(x_train, y_train, x_pred, sigma, length, eps):
+    """statX/infer/GaussianProcess.hpp fit/predictMean/predictVariance/
+    giveLogLikelihood (LLT of k(x,x) + eps^2 I)."""
+    K = se_matrix(x_train, x_train, sigma, length) + eps * eps * np.eye(len(x_train))
+    L = np.linalg.cholesky(K)
+    alpha = np.linalg.solve(L.T, np.linalg.solve(L, y_train))
+    ks = se_matrix(x_train, x_pred, sigma, length)
+    mean = ks.T @ alpha
+    v = np.linalg.solve(L, ks)
+    var = sigma * sigma - np.sum(v * v, axis=0)
+    ll = -0.5 * float(y_train @ alpha) - float(np.sum(np.log(np.diag(L)))) \
+        - 0.5 * len(x_train) * math.log(2.0 * math.pi)
+    return mean, var, ll
+
+
+# --------------------------------------------------------------------------
+# full problems
+# --------------------------------------------------------------------------
+
+def fem(mesh, qps, f, bc_dofs, coeff=None, nu=0.3, bc_values=None):
+    """laplaceRHSinfer fem() (del2/apps/reference/laplaceRHSinfer/fem.hpp:49-97):
+    assemble K, F, apply row-zeroing constraints; returns (rp, col, val, F)."""
+    rp, col, val = assemble_csr(mesh, qps, coeff=coeff, nu=nu)
+    F = assemble_load(mesh, qps, f)
+    apply_constraints(rp, col, val, F, bc_dofs, bc_values)
+    return rp, col, val, F
+
+
+def unit_load(mesh, qps, bc_dofs):
+    """CovarianceForcing::covVec_: phibar = assembled unit load, zero at the
+    constrained dofs (inference.hpp:108-124; CovarianceForcing.hpp:101-114)."""
+    phibar = assemble_load(mesh, qps, np.ones(mesh.dof))
+    phibar[np.asarray(bc_dofs, dtype=np.int64)] = 0.0
+    return phibar
+
+
+def statfem_prior(mesh, qps, f, bc_dofs, P, sigma_f, length_f, reg, coeff=None, nu=0.3):
+    rp, col, val, F = fem(mesh, qps, f, bc_dofs, coeff=coeff, nu=nu)
+    solver = DirectSolver(rp, col, val)
+    u = solver.solve(F)
+    phibar = unit_load(mesh, qps, bc_dofs)
+    mean_s, C_s, R = forward_gauss_rhs(solver, F, P, mesh.coords, phibar,
+                                       mesh.dim, mesh.dof, sigma_f, length_f, reg)
+    return dict(rp=rp, col=col, val=val, F=F, u=u, phibar=phibar, mean_s=mean_s, C_s=C_s,
+                R=R, solver=solver)

@@ -1,0 +1,488 @@
+"""Python mirror of the reference interface for the statFEM hot path, bound to
+the C ABI (include/statfem_cuda.h) of libstatfem_cuda.so through ctypes.
+
+Class and method names follow the reference:
+  SystemSolveCuda      <- corlib::SystemSolveEigenSparse (corlib/SystemSolveEigenSparse.hpp)
+  CovarianceForcing    <- statX::infer::CovarianceForcing (statX/infer/CovarianceForcing.hpp)
+  ForwardGaussRHS      <- statX::infer::ForwardGaussRHS (statX/infer/ForwardGaussRHS.hpp)
+  LikelihoodKOH        <- statX::infer::LikelihoodKOH + MismatchCovariance
+                          (statX/infer/LikelihoodKOH.hpp, MismatchCovariance.hpp)
+Hyperparameters are passed as the reference's name -> value maps
+("forcing.sigma", "forcing.length", "rho", "mismatch.sigma", "mismatch.length",
+"mismatch.sensorEps").  Where the reference aborts (FTL_VERIFY), these raise
+SfcError.  There is no CPU fallback: every call goes to the CUDA library, and
+importing this module fails if the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import meshgen
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libstatfem_cuda.so")
+
+SFC_SOLVER_PCG_FP64 = 0
+SFC_SOLVER_PCG_MIXED = 1
+
+_ERR = {-1: "CUDA error", -2: "bad argument", -3: "not SPD", -4: "not converged", -5: "timeout",
+        -6: "out of memory", -7: "negative Jacobian"}
+
+
+class SfcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (_ERR.get(code, "error"), code, msg))
+        self.code = code
+
+
+class SolverOptions(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("tol", ctypes.c_double),
+                ("inner_tol", ctypes.c_double), ("block_width", ctypes.c_int32),
+                ("check_every", ctypes.c_int32)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("refinements", ctypes.c_int32),
+                ("num_rhs", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("max_rel_residual", ctypes.c_double), ("device_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class HParams(ctypes.Structure):
+    _fields_ = [("forcing_sigma", ctypes.c_double), ("forcing_length", ctypes.c_double),
+                ("rho", ctypes.c_double), ("mismatch_sigma", ctypes.c_double),
+                ("mismatch_length", ctypes.c_double), ("mismatch_sensor_eps", ctypes.c_double)]
+
+    @classmethod
+    def from_map(cls, hp):
+        g = lambda k: float(hp.get(k, 0.0))  # noqa: E731
+        return cls(g("forcing.sigma"), g("forcing.length"), g("rho"), g("mismatch.sigma"),
+                   g("mismatch.length"), g("mismatch.sensorEps"))
+
+
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_d = ctypes.c_double
+
+# name -> (restype, argtypes); the complete exported surface of the header
+SIGNATURES = {
+    "sfc_version": (_i32, []),
+    "sfc_ctx_create": (_i32, [_i32, ctypes.POINTER(_vp)]),
+    "sfc_ctx_destroy": (_i32, [_vp]),
+    "sfc_last_error": (ctypes.c_char_p, [_vp]),
+    "sfc_ctx_synchronize": (_i32, [_vp]),
+    "sfc_ctx_kernel_launches": (_i32, [_vp, _i64p]),
+    "sfc_ctx_mark": (_i32, [_vp, _i32]),
+    "sfc_ctx_marker_ms": (_i32, [_vp, _i32, _i32, _dp]),
+    "sfc_mesh_create": (_i32, [_vp, _i32, _i32, _dp, _i64, _u32p, _i64, ctypes.POINTER(_vp)]),
+    "sfc_mesh_destroy": (_i32, [_vp]),
+    "sfc_mesh_set_coefficients": (_i32, [_vp, _dp, _d, _d]),
+    "sfc_mesh_num_dofs": (_i64, [_vp]),
+    "sfc_mesh_nnz": (_i64, [_vp]),
+    "sfc_system_create": (_i32, [_vp, _i64, ctypes.POINTER(_vp)]),
+    "sfc_system_destroy": (_i32, [_vp]),
+    "sfc_system_set_options": (_i32, [_vp, ctypes.POINTER(SolverOptions)]),
+    "sfc_system_get_options": (_i32, [_vp, ctypes.POINTER(SolverOptions)]),
+    "sfc_system_last_stats": (_i32, [_vp, ctypes.POINTER(SolveStats)]),
+    "sfc_insert_matrix": (_i32, [_vp, _dp, _u32p, ctypes.c_uint32, _u32p, ctypes.c_uint32]),
+    "sfc_insert_rhs": (_i32, [_vp, _dp, _u32p, ctypes.c_uint32]),
+    "sfc_finish_assembly": (_i32, [_vp]),
+    "sfc_assemble_matrix": (_i32, [_vp, _vp]),
+    "sfc_assemble_load": (_i32, [_vp, _vp, _dp]),
+    "sfc_apply_constraints": (_i32, [_vp, _u32p, _dp, _i64, _d, _d]),
+    "sfc_fix_dof": (_i32, [_vp, ctypes.c_uint32, _d]),
+    "sfc_solve": (_i32, [_vp, _i32]),
+    "sfc_solve_transpose": (_i32, [_vp, _dp, _dp, _i32, _i32]),
+    "sfc_give_solution": (_i32, [_vp, _u32p, _i64, _dp]),
+    "sfc_give_force": (_i32, [_vp, _u32p, _i64, _dp]),
+    "sfc_clear_matrix": (_i32, [_vp]),
+    "sfc_clear_rhs": (_i32, [_vp]),
+    "sfc_num_nonzeros": (_i64, [_vp]),
+    "sfc_norms": (_i32, [_vp, _dp, _dp, _dp, _dp]),
+    "sfc_get_csr": (_i32, [_vp, _i64p, _i32p, _dp]),
+    "sfc_covar_forcing_create": (_i32, [_vp, _vp, ctypes.POINTER(_vp)]),
+    "sfc_covar_forcing_destroy": (_i32, [_vp]),
+    "sfc_covar_forcing_apply_constraints": (_i32, [_vp, _u32p, _i64]),
+    "sfc_covar_forcing_get_phibar": (_i32, [_vp, _dp]),
+    "sfc_covar_forcing_projected": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _i64, _dp]),
+    "sfc_forward_gauss_create": (_i32, [_vp, _vp, _d, ctypes.POINTER(_vp)]),
+    "sfc_forward_gauss_destroy": (_i32, [_vp]),
+    "sfc_forward_gauss_set_projection": (_i32, [_vp, _i64, _i64p, _i32p, _dp]),
+    "sfc_forward_gauss_update": (_i32, [_vp, ctypes.POINTER(HParams)]),
+    "sfc_forward_gauss_mean": (_i32, [_vp, _dp]),
+    "sfc_forward_gauss_covar": (_i32, [_vp, _dp]),
+    "sfc_koh_create": (_i32, [_vp, _dp, _i32, ctypes.POINTER(_vp)]),
+    "sfc_koh_destroy": (_i32, [_vp]),
+    "sfc_koh_set_sensor_values": (_i32, [_vp, _dp, _i32]),
+    "sfc_koh_log_likelihood": (_i32, [_vp, ctypes.POINTER(HParams), _dp]),
+    "sfc_koh_proj_conditioned": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
+    "sfc_koh_woodbury": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library; raises when it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libstatfem_cuda.so not built: run `python -m statfem_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+class Context:
+    def __init__(self, device=0):
+        self.lib = load()
+        h = _vp()
+        rc = self.lib.sfc_ctx_create(device, ctypes.byref(h))
+        if rc:
+            raise SfcError(rc, "context creation failed")
+        self.h = h
+
+    def check(self, rc):
+        if rc:
+            raise SfcError(rc, self.lib.sfc_last_error(self.h).decode())
+
+    def synchronize(self):
+        self.check(self.lib.sfc_ctx_synchronize(self.h))
+
+    def kernel_launches(self):
+        c = ctypes.c_int64()
+        self.check(self.lib.sfc_ctx_kernel_launches(self.h, ctypes.byref(c)))
+        return c.value
+
+    def mark(self, slot):
+        self.check(self.lib.sfc_ctx_mark(self.h, slot))
+
+    def marker_ms(self, a, b):
+        v = ctypes.c_double()
+        self.check(self.lib.sfc_ctx_marker_ms(self.h, a, b, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sfc_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mesh:
+    """corlib::Mesh + per-element material; builds the CSR pattern on the GPU."""
+
+    def __init__(self, ctx, kind, quad_points, coords, conn):
+        self.ctx = ctx
+        self.kind = kind
+        self.coords = _arr(coords, np.float64)
+        self.conn = _arr(conn, np.uint32)
+        h = _vp()
+        ctx.check(ctx.lib.sfc_mesh_create(ctx.h, kind, quad_points, _p(self.coords, _dp), self.coords.shape[0],
+                                          _p(self.conn, _u32p), self.conn.shape[0], ctypes.byref(h)))
+        self.h = h
+        self.num_dofs = ctx.lib.sfc_mesh_num_dofs(h)
+        self.nnz = ctx.lib.sfc_mesh_nnz(h)
+
+    @classmethod
+    def from_meshgen(cls, ctx, m, quad_points):
+        return cls(ctx, m.kind, quad_points, m.coords, m.conn)
+
+    def set_coefficients(self, values=None, uniform=1.0, poisson_ratio=0.3):
+        v = None if values is None else _arr(values, np.float64)
+        self.ctx.check(self.ctx.lib.sfc_mesh_set_coefficients(self.h, _p(v, _dp), uniform, poisson_ratio))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_mesh_destroy(self.h)
+            self.h = None
+
+
+class SystemSolveCuda:
+    """corlib::SystemSolveEigenSparse method set on the GPU."""
+
+    def __init__(self, ctx, num_dofs):
+        self.ctx = ctx
+        self.N = int(num_dofs)
+        h = _vp()
+        ctx.check(ctx.lib.sfc_system_create(ctx.h, self.N, ctypes.byref(h)))
+        self.h = h
+
+    # -- options / stats (no reference counterpart) --
+    def set_options(self, method=SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=20000, inner_tol=1e-4,
+                    block_width=0, check_every=16):
+        o = SolverOptions(method, max_iter, tol, inner_tol, block_width, check_every)
+        self.ctx.check(self.ctx.lib.sfc_system_set_options(self.h, ctypes.byref(o)))
+
+    def last_stats(self):
+        s = SolveStats()
+        self.ctx.check(self.ctx.lib.sfc_system_last_stats(self.h, ctypes.byref(s)))
+        return s.as_dict()
+
+    # -- insertion (compat path) --
+    def insertToMatrix(self, Ke, rows, cols):
+        Ke = _arr(Ke, np.float64)
+        r = _arr(rows, np.uint32)
+        c = _arr(cols, np.uint32)
+        self.ctx.check(self.ctx.lib.sfc_insert_matrix(self.h, _p(Ke, _dp), _p(r, _u32p), len(r), _p(c, _u32p),
+                                                      len(c)))
+
+    def insertToRhs(self, fe, dofs):
+        fe = _arr(fe, np.float64)
+        d = _arr(dofs, np.uint32)
+        self.ctx.check(self.ctx.lib.sfc_insert_rhs(self.h, _p(fe, _dp), _p(d, _u32p), len(d)))
+
+    def finishAssembly(self):
+        self.ctx.check(self.ctx.lib.sfc_finish_assembly(self.h))
+
+    finishMatAssembly = finishAssembly
+    finishRhsAssembly = finishAssembly
+
+    # -- GPU assembler --
+    def assemble(self, mesh):
+        self.ctx.check(self.ctx.lib.sfc_assemble_matrix(self.h, mesh.h))
+
+    def assemble_load(self, mesh, f):
+        f = _arr(np.atleast_1d(f), np.float64)
+        self.ctx.check(self.ctx.lib.sfc_assemble_load(self.h, mesh.h, _p(f, _dp)))
+
+    # -- constraints --
+    def applyConstraints(self, constraints, factor=1.0, scalar=1.0):
+        """constraints: iterable of (dof, value) pairs, or (idx_array, value_array)."""
+        if isinstance(constraints, tuple) and len(constraints) == 2 and hasattr(constraints[0], "__len__"):
+            idx, val = constraints
+        else:
+            pairs = list(constraints)
+            idx = [p[0] for p in pairs]
+            val = [p[1] for p in pairs]
+        idx = _arr(idx, np.uint32)
+        val = _arr(val, np.float64)
+        self.ctx.check(self.ctx.lib.sfc_apply_constraints(self.h, _p(idx, _u32p), _p(val, _dp), len(idx), factor,
+                                                          scalar))
+
+    def fixDOF(self, index, scalar=1.0):
+        self.ctx.check(self.ctx.lib.sfc_fix_dof(self.h, int(index), scalar))
+
+    # -- solves --
+    def solveSystem(self, reuse=False):
+        self.ctx.check(self.ctx.lib.sfc_solve(self.h, int(bool(reuse))))
+
+    def solveSystemTranspose(self, rhs, reuse=False):
+        rhs = _arr(rhs, np.float64)
+        single = rhs.ndim == 1
+        R = rhs.reshape(1, -1) if single else rhs
+        U = np.zeros_like(R)
+        self.ctx.check(self.ctx.lib.sfc_solve_transpose(self.h, _p(R, _dp), _p(U, _dp), R.shape[0],
+                                                        int(bool(reuse))))
+        return U[0] if single else U
+
+    def giveSolution(self, dofs=None):
+        d = _arr(np.arange(self.N) if dofs is None else dofs, np.uint32)
+        out = np.zeros(len(d))
+        self.ctx.check(self.ctx.lib.sfc_give_solution(self.h, _p(d, _u32p), len(d), _p(out, _dp)))
+        return out
+
+    def giveForce(self, dofs=None):
+        d = _arr(np.arange(self.N) if dofs is None else dofs, np.uint32)
+        out = np.zeros(len(d))
+        self.ctx.check(self.ctx.lib.sfc_give_force(self.h, _p(d, _u32p), len(d), _p(out, _dp)))
+        return out
+
+    def clearMatrix(self):
+        self.ctx.check(self.ctx.lib.sfc_clear_matrix(self.h))
+
+    def clearRhs(self):
+        self.ctx.check(self.ctx.lib.sfc_clear_rhs(self.h))
+
+    def numNonZeros(self):
+        return self.ctx.lib.sfc_num_nonzeros(self.h)
+
+    def _norms(self):
+        v = [ctypes.c_double() for _ in range(4)]
+        self.ctx.check(self.ctx.lib.sfc_norms(self.h, *[ctypes.byref(x) for x in v]))
+        return [x.value for x in v]
+
+    def normMatrix(self):
+        return self._norms()[0]
+
+    def normRhs(self):
+        return self._norms()[1]
+
+    def norm1Rhs(self):
+        return self._norms()[2]
+
+    def normSol(self):
+        return self._norms()[3]
+
+    def get_csr(self):
+        nnz = self.numNonZeros()
+        rp = np.zeros(self.N + 1, dtype=np.int64)
+        col = np.zeros(nnz, dtype=np.int32)
+        val = np.zeros(nnz)
+        self.ctx.check(self.ctx.lib.sfc_get_csr(self.h, _p(rp, _i64p), _p(col, _i32p), _p(val, _dp)))
+        return rp, col, val
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_system_destroy(self.h)
+            self.h = None
+
+
+class CovarianceForcing:
+    """statX::infer::CovarianceForcing with phibar computed on the GPU."""
+
+    def __init__(self, ctx, mesh):
+        self.ctx = ctx
+        self.mesh = mesh
+        h = _vp()
+        ctx.check(ctx.lib.sfc_covar_forcing_create(ctx.h, mesh.h, ctypes.byref(h)))
+        self.h = h
+
+    def applyConstraints(self, idx):
+        idx = _arr(idx, np.uint32)
+        self.ctx.check(self.ctx.lib.sfc_covar_forcing_apply_constraints(self.h, _p(idx, _u32p), len(idx)))
+
+    def phibar(self):
+        out = np.zeros(self.mesh.num_dofs)
+        self.ctx.check(self.ctx.lib.sfc_covar_forcing_get_phibar(self.h, _p(out, _dp)))
+        return out
+
+    def giveProjectedCovar(self, hp, M):
+        M = _arr(M, np.float64)
+        out = np.zeros((M.shape[0], M.shape[0]))
+        h = HParams.from_map(hp)
+        self.ctx.check(self.ctx.lib.sfc_covar_forcing_projected(self.h, ctypes.byref(h), _p(M, _dp), M.shape[0],
+                                                                _p(out, _dp)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_covar_forcing_destroy(self.h)
+            self.h = None
+
+
+class ForwardGaussRHS:
+    """statX::infer::ForwardGaussRHS on the GPU (block adjoint solve)."""
+
+    def __init__(self, solver, covar_forcing, reg_eps=1e-4):
+        self.ctx = solver.ctx
+        self.solver = solver
+        h = _vp()
+        self.ctx.check(self.ctx.lib.sfc_forward_gauss_create(solver.h, covar_forcing.h, reg_eps, ctypes.byref(h)))
+        self.h = h
+        self.ns = 0
+
+    def setProjectionMatrix(self, P):
+        """P: dense (ns x N) array or CSR triple (indptr, indices, data)."""
+        if isinstance(P, tuple):
+            ip, ix, dv = P
+        else:
+            P = np.asarray(P, dtype=np.float64)
+            ip = [0]
+            ix, dv = [], []
+            for a in range(P.shape[0]):
+                nz = np.nonzero(P[a])[0]
+                ix.extend(nz.tolist())
+                dv.extend(P[a, nz].tolist())
+                ip.append(len(ix))
+        ip = _arr(ip, np.int64)
+        ix = _arr(ix, np.int32)
+        dv = _arr(dv, np.float64)
+        self.ns = len(ip) - 1
+        self.ctx.check(self.ctx.lib.sfc_forward_gauss_set_projection(self.h, self.ns, _p(ip, _i64p), _p(ix, _i32p),
+                                                                     _p(dv, _dp)))
+
+    def updateSolution(self, hp):
+        h = HParams.from_map(hp)
+        self.ctx.check(self.ctx.lib.sfc_forward_gauss_update(self.h, ctypes.byref(h)))
+
+    def giveProjectedMeanU(self):
+        out = np.zeros(self.ns)
+        self.ctx.check(self.ctx.lib.sfc_forward_gauss_mean(self.h, _p(out, _dp)))
+        return out
+
+    def giveProjectedCovarU(self):
+        out = np.zeros((self.ns, self.ns))
+        self.ctx.check(self.ctx.lib.sfc_forward_gauss_covar(self.h, _p(out, _dp)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_forward_gauss_destroy(self.h)
+            self.h = None
+
+
+class LikelihoodKOH:
+    """statX::infer::LikelihoodKOH with MismatchCovariance(sensorCoords)."""
+
+    def __init__(self, forward_gauss, sensor_coords):
+        self.ctx = forward_gauss.ctx
+        self.fg = forward_gauss
+        xs = _arr(sensor_coords, np.float64)
+        if xs.ndim == 1:
+            xs = xs.reshape(-1, 1)
+        h = _vp()
+        self.ctx.check(self.ctx.lib.sfc_koh_create(forward_gauss.h, _p(xs, _dp), xs.shape[1], ctypes.byref(h)))
+        self.h = h
+        self.ns = xs.shape[0]
+
+    def setSensorValues(self, Y):
+        Y = _arr(Y, np.float64)
+        self.ctx.check(self.ctx.lib.sfc_koh_set_sensor_values(self.h, _p(Y, _dp), Y.shape[1]))
+
+    def giveLogLikelihood(self, hp):
+        h = HParams.from_map(hp)
+        v = ctypes.c_double()
+        self.ctx.check(self.ctx.lib.sfc_koh_log_likelihood(self.h, ctypes.byref(h), ctypes.byref(v)))
+        return v.value
+
+    def giveProjFEconditionedData(self, hp):
+        h = HParams.from_map(hp)
+        m = np.zeros(self.ns)
+        c = np.zeros((self.ns, self.ns))
+        self.ctx.check(self.ctx.lib.sfc_koh_proj_conditioned(self.h, ctypes.byref(h), _p(m, _dp), _p(c, _dp)))
+        return m, c
+
+    def giveFEconditionedDataWoodbury(self, hp, with_cov=True):
+        h = HParams.from_map(hp)
+        N = self.fg.solver.N
+        m = np.zeros(N)
+        c = np.zeros((N, N)) if with_cov else None
+        self.ctx.check(self.ctx.lib.sfc_koh_woodbury(self.h, ctypes.byref(h), _p(m, _dp), _p(c, _dp)))
+        return m, c
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_koh_destroy(self.h)
+            self.h = None
+
+
+__all__ = ["Context", "Mesh", "SystemSolveCuda", "CovarianceForcing", "ForwardGaussRHS", "LikelihoodKOH",
+           "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64", "SFC_SOLVER_PCG_MIXED"]

@@ -1,0 +1,289 @@
+// Internal declarations shared by the CUDA translation units of the statFEM
+// B200 library.  Nothing here is part of the C ABI (include/statfem_cuda.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "statfem_cuda.h"
+
+namespace sfc {
+
+// ---------------------------------------------------------------------------
+// errors: internal code throws Error; every C entry point converts it to a
+// status code and stores the message on the context.
+// ---------------------------------------------------------------------------
+struct Error {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] inline void fail(int code, const std::string &msg) { throw Error{code, msg}; }
+
+#define SFC_CK(call)                                                                   \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            ::sfc::fail(SFC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define SFC_REQUIRE(cond, msg)                                                         \
+    do {                                                                               \
+        if (!(cond)) ::sfc::fail(SFC_ERR_BAD_ARG, msg);                                \
+    } while (0)
+
+// Device buffer with RAII ownership.
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    // (re)allocate to exactly `count` elements when the size differs
+    void alloc(size_t count)
+    {
+        if (count == n && p) return;
+        release();
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            fail(SFC_ERR_NO_MEMORY, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
+        }
+        n = count;
+    }
+    // grow only
+    void reserve(size_t count)
+    {
+        if (count > n) alloc(count);
+    }
+    T *get() const { return p; }
+};
+
+}  // namespace sfc
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct sfc_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    cudaEvent_t marks[16] = {};
+    // pinned host scratch for small device->host reads
+    void *pinned = nullptr;
+    size_t pinned_bytes = 0;
+    sfc::DBuf<unsigned char> scratch;  // generic device scratch (CUB temp etc.)
+};
+
+namespace sfc {
+
+inline void count_launch(sfc_ctx *ctx, int n = 1)
+{
+    ctx->launches += n;
+    SFC_CK(cudaGetLastError());
+}
+
+inline unsigned grid_for(int64_t work, int block, int max_blocks = 148 * 32)
+{
+    int64_t g = (work + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > max_blocks) g = max_blocks;
+    return (unsigned)g;
+}
+
+// copy host -> device on the context stream (synchronous w.r.t. the host
+// buffer: the call returns once the data has been consumed)
+template <class T>
+void upload(sfc_ctx *ctx, DBuf<T> &dst, const T *src, size_t count)
+{
+    dst.alloc(count);
+    if (count) {
+        SFC_CK(cudaMemcpyAsync(dst.p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+        SFC_CK(cudaStreamSynchronize(ctx->stream));
+    }
+}
+
+template <class T>
+void download(sfc_ctx *ctx, T *dst, const T *src, size_t count)
+{
+    if (count) {
+        SFC_CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+        SFC_CK(cudaStreamSynchronize(ctx->stream));
+    }
+}
+
+void *pinned(sfc_ctx *ctx, size_t bytes);
+
+// ---------------------------------------------------------------------------
+// quadrature tables (weights, shape values, reference gradients at the
+// points), evaluated on the host with the reference's literals
+// ---------------------------------------------------------------------------
+constexpr int kMaxQ = 27;
+
+struct QuadTable {
+    int nq;
+    double w[kMaxQ];
+    double xi[kMaxQ][3];
+    double phi[kMaxQ][8];
+    double dphi[kMaxQ][3][8];  // d phi^K / d xi_a
+};
+
+int elem_dim(int kind);
+int elem_nodes(int kind);
+int elem_dofs(int kind);
+void make_quadrature(int kind, int qps, QuadTable &t);
+
+}  // namespace sfc
+
+// ---------------------------------------------------------------------------
+// mesh + its symbolic (pattern) data
+// ---------------------------------------------------------------------------
+struct sfc_mesh {
+    sfc_ctx *ctx = nullptr;
+    int kind = 0, qps = 0, dim = 0, nn = 0, dof = 0, L = 0;
+    int64_t num_nodes = 0, num_elems = 0, num_dofs = 0;
+    sfc::QuadTable quad{};
+    std::vector<double> h_coords;  // num_nodes x 3
+    sfc::DBuf<double> coords;      // num_nodes x 3
+    sfc::DBuf<uint32_t> conn;      // num_elems x nn
+    sfc::DBuf<double> coeff;       // num_elems
+    double nu = 0.3;
+    // CSR pattern of the assembled matrix (sorted unique (row,col) pairs)
+    int64_t nnz = 0;
+    sfc::DBuf<int32_t> row_ptr;    // num_dofs + 1
+    sfc::DBuf<int32_t> col;        // nnz
+    sfc::DBuf<int32_t> diag;       // num_dofs: slot of (i,i)
+    // sorted-key gather map: CSR slot s sums element entries
+    // contrib[slot_ptr[s] .. slot_ptr[s+1]) in element order; an element entry
+    // id is e*L*L + r*L + c
+    sfc::DBuf<int32_t> slot_ptr;   // nnz + 1
+    sfc::DBuf<int32_t> contrib;    // num_elems * L * L
+    // node -> incident (element*nn + local node), ascending element order
+    sfc::DBuf<int32_t> node_ptr;   // num_nodes + 1
+    sfc::DBuf<int32_t> node_elem;  // num_elems * nn
+    // element matrices of the last assembly (num_elems * L * L)
+    sfc::DBuf<double> ke;
+    // tensor-grid description of the node set (for the Kronecker covariance)
+    bool is_grid = false;
+    int gn[3] = {1, 1, 1};
+    std::vector<double> gaxis[3];
+};
+
+// ---------------------------------------------------------------------------
+// linear system
+// ---------------------------------------------------------------------------
+struct sfc_system {
+    sfc_ctx *ctx = nullptr;
+    int64_t N = 0;
+    sfc_solver_options_t opt{};
+    sfc_solve_stats_t stats{};
+    // pattern (owned copy, from a mesh or from staged triplets)
+    int64_t nnz = 0;
+    bool has_pattern = false;
+    const sfc_mesh *pattern_mesh = nullptr;  // mesh whose pattern is installed
+    sfc::DBuf<int32_t> row_ptr, col, diag;
+    // values
+    sfc::DBuf<double> a_ref;   // reference semantics: K with constrained rows zeroed
+    sfc::DBuf<double> a_op;    // symmetric elimination (SPD operator) FP64
+    sfc::DBuf<float> a_op32;   // FP32 copy of a_op
+    sfc::DBuf<double> dinv;    // 1 / diag(a_op)
+    sfc::DBuf<float> dinv32;
+    bool op_valid = false;
+    // vectors
+    sfc::DBuf<double> F, X;
+    sfc::DBuf<unsigned char> mask;   // 1 for constrained dofs
+    sfc::DBuf<double> bc_val;        // prescribed value on constrained dofs
+    bool any_constraint = false;
+    bool inhomogeneous = false;
+    double bc_scalar = 1.0;
+    // host staging for the compat insert path
+    std::vector<uint32_t> st_rows, st_cols;
+    std::vector<double> st_vals;
+    std::vector<double> st_rhs;
+    bool st_rhs_dirty = false;
+    // solver workspaces
+    sfc::DBuf<double> w64;
+    sfc::DBuf<float> w32;
+    sfc::DBuf<double> scal;  // per-iteration scalars
+    sfc::DBuf<int> flags;
+    sfc::DBuf<double> fix;   // transposed-constraint fixup scratch
+};
+
+// ---------------------------------------------------------------------------
+// statX objects
+// ---------------------------------------------------------------------------
+struct sfc_covar_forcing {
+    sfc_ctx *ctx = nullptr;
+    const sfc_mesh *mesh = nullptr;
+    int dim = 0, dof = 0;
+    int64_t num_nodes = 0, num_dofs = 0;
+    sfc::DBuf<double> phibar;  // num_dofs
+};
+
+struct sfc_forward_gauss {
+    sfc_ctx *ctx = nullptr;
+    sfc_system *sys = nullptr;
+    sfc_covar_forcing *cf = nullptr;
+    double reg = 1e-4;
+    int64_t ns = 0;
+    std::vector<int64_t> p_ptr;
+    std::vector<int32_t> p_idx;
+    std::vector<double> p_val;
+    sfc::DBuf<int64_t> d_p_ptr;
+    sfc::DBuf<int32_t> d_p_idx;
+    sfc::DBuf<double> d_p_val;
+    std::vector<double> ppt;          // P P^T (ns x ns), host
+    sfc::DBuf<double> d_ppt;
+    sfc::DBuf<double> R;              // num_dofs x ns (column a = r_a)
+    sfc::DBuf<double> mean;           // ns
+    sfc::DBuf<double> cov;            // ns x ns
+    sfc::DBuf<double> work;           // covariance workspace
+    bool valid = false;
+};
+
+struct sfc_koh {
+    sfc_ctx *ctx = nullptr;
+    sfc_forward_gauss *fg = nullptr;
+    int dim = 0;
+    int64_t ns = 0;
+    int n_o = 0;
+    sfc::DBuf<double> sensor_coords;  // ns x 3
+    sfc::DBuf<double> Y;              // ns x n_o
+    sfc::DBuf<double> work;
+};
+
+namespace sfc {
+// assembly.cu
+void build_pattern(sfc_mesh *m);
+void assemble_matrix(sfc_system *s, const sfc_mesh *m);
+void assemble_load(sfc_ctx *ctx, const sfc_mesh *m, const double *f, double *F_dev, bool zero_first);
+void apply_constraints_dev(sfc_system *s, const uint32_t *idx_dev, const double *val_dev, int64_t n,
+                           double factor, double scalar);
+void build_operator(sfc_system *s);
+void flush_staged(sfc_system *s);
+void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);
+// solvers.cu
+void solve_forward(sfc_system *s);
+void solve_block(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
+void transpose_fixup(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
+double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n);
+// stats.cu
+void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp);
+}  // namespace sfc

@@ -1,0 +1,843 @@
+// SPD sparse solves on the GPU: the replacement of the reference's
+// Eigen::SparseLU behind SystemSolveEigenSparse::solveSystem /
+// solveSystemTranspose (corlib/SystemSolveEigenSparse.hpp:273-404).
+//
+// The row-zeroed reference system A (corlib/Triplet.hpp:219-260) is solved
+// through its symmetric elimination S (free rows keep free columns,
+// constrained rows keep their diagonal): A u = F  <=>  S u = F - K_fc u_c, and
+// A^T r = p  <=>  S r = p on the free dofs with r_c = (p_c - K_cf r_f)/scalar.
+//
+// Two methods:
+//  * plain FP64 Jacobi-PCG, one right-hand side at a time (the baseline and
+//    the judge): CSR SpMV with sub-warp row groups, fused p.q reduction,
+//    fused x/r/z update with the r.r and r.z reductions;
+//  * mixed block PCG: up to 128 right-hand sides share each pass over the
+//    FP32 copy of the matrix (one warp per row, each lane owns 1-4 columns of
+//    an RHS-interleaved [N][K] block), iterations in FP32, and an outer FP64
+//    loop recomputes the true residual b - S x with the FP64 matrix and
+//    restarts FP32 PCG on it (iterative refinement) until every column meets
+//    the FP64 relative-residual target.
+// All reductions accumulate in FP64.  Scalars are kept per iteration (and per
+// column) in device arrays, so no scalar kernel or host round trip sits
+// between the three launches of an iteration; the host checks convergence
+// every `check_every` iterations.
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sfc {
+
+namespace {
+
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// block-wide sum of one value per thread, result valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0;
+    if (w == 0) {
+        r = l < (int)(blockDim.x >> 5) ? sh[l] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// single right-hand side, FP64
+// ---------------------------------------------------------------------------
+
+// y = S x over rows, G lanes per row; dot += x.y
+template <int G>
+__global__ void __launch_bounds__(kRedThreads) k_spmv64(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                                         const double *__restrict__ a, const double *__restrict__ x,
+                                                         double *__restrict__ y, int64_t N, double *dot,
+                                                         const int *done)
+{
+    __shared__ double sh[32];
+    if (done && *done) return;
+    const int g = threadIdx.x % G;
+    const int64_t groups = (int64_t)gridDim.x * (blockDim.x / G);
+    double d = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G; i < N; i += groups) {
+        double s = 0.0;
+        const int32_t e = rp[i + 1];
+        for (int32_t k = rp[i] + g; k < e; k += G) s += a[k] * x[col[k]];
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
+        if (g == 0) {
+            y[i] = s;
+            d += x[i] * s;
+        }
+    }
+    if (dot) {
+        d = block_sum(d, sh);
+        if (threadIdx.x == 0) atomicAdd(dot, d);
+    }
+}
+
+// r = b' (lifted rhs), x = 0, p = z = D^-1 r; rz0 = r.z, bb = r.r
+__global__ void __launch_bounds__(kRedThreads) k_pcg_init(const double *__restrict__ b, const double *__restrict__ dinv,
+                                                           double *__restrict__ x, double *__restrict__ r,
+                                                           double *__restrict__ p, int64_t N, double *rz0, double *bb)
+{
+    __shared__ double sh[32];
+    double a = 0, c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ri = b[i], zi = dinv[i] * ri;
+        x[i] = 0.0;
+        r[i] = ri;
+        p[i] = zi;
+        a += ri * zi;
+        c += ri * ri;
+    }
+    a = block_sum(a, sh);
+    c = block_sum(c, sh);
+    if (threadIdx.x == 0) {
+        atomicAdd(rz0, a);
+        atomicAdd(bb, c);
+    }
+}
+
+// alpha = rz/pq; x += alpha p; r -= alpha q; z = D^-1 r; rz' = r.z; rr' = r.r
+__global__ void __launch_bounds__(kRedThreads) k_pcg_update(double *__restrict__ x, double *__restrict__ r,
+                                                             const double *__restrict__ p, const double *__restrict__ q,
+                                                             const double *__restrict__ dinv, int64_t N,
+                                                             const double *pq, const double *rz, double *rz_next,
+                                                             double *rr_next, const int *done, int *err)
+{
+    __shared__ double sh[32];
+    if (*done) return;
+    const double den = *pq;
+    if (!(den > 0.0)) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
+    const double alpha = *rz / den;
+    double a = 0, c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        const double zi = dinv[i] * ri;
+        a += ri * zi;
+        c += ri * ri;
+    }
+    a = block_sum(a, sh);
+    c = block_sum(c, sh);
+    if (threadIdx.x == 0) {
+        atomicAdd(rz_next, a);
+        atomicAdd(rr_next, c);
+    }
+}
+
+// convergence test on rr'; else beta = rz'/rz, p = D^-1 r + beta p
+__global__ void k_pcg_pupdate(double *__restrict__ p, const double *__restrict__ r, const double *__restrict__ dinv,
+                              int64_t N, const double *rz, const double *rz_next, const double *rr_next, double thr,
+                              int it_next, int *done, const int *err)
+{
+    if (*done || *err) return;
+    if (*rr_next <= thr) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *done = it_next;
+        return;
+    }
+    const double beta = *rz_next / *rz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = dinv[i] * r[i] + beta * p[i];
+}
+
+// lifting of prescribed values: b_f = F_f - sum_{j constrained} a_ref[f,j] g_j,
+// g_j = F_j / a_ref[j,j]; constrained rows keep F.
+__global__ void k_lift(const int32_t *__restrict__ rp, const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
+                       const double *__restrict__ a_ref, const unsigned char *__restrict__ mask,
+                       const double *__restrict__ F, int64_t N, double *__restrict__ b)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = F[i];
+        if (!mask[i])
+            for (int32_t s = rp[i]; s < rp[i + 1]; ++s) {
+                const int32_t j = col[s];
+                if (mask[j]) v -= a_ref[s] * (F[j] / a_ref[diag[j]]);
+            }
+        b[i] = v;
+    }
+}
+
+__global__ void k_axpby(double *__restrict__ y, const double *__restrict__ x, double a, double b, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = a * x[i] + b * y[i];
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_dot(const double *__restrict__ a, const double *__restrict__ b,
+                                                      int64_t n, double *out)
+{
+    __shared__ double sh[32];
+    double s = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += a[i] * b[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) atomicAdd(out, s);
+}
+
+// ---------------------------------------------------------------------------
+// block of K = 32*V right-hand sides, RHS-interleaved [N][K]
+// ---------------------------------------------------------------------------
+template <int V>
+struct VecT;
+template <> struct VecT<1> { using f = float; using d = double; };
+template <> struct VecT<2> { using f = float2; using d = double2; };
+template <> struct VecT<4> { using f = float4; using d = double4; };
+
+template <int V>
+__device__ __forceinline__ void ldv(const float *p, float (&v)[V])
+{
+    if constexpr (V == 1) v[0] = *p;
+    if constexpr (V == 2) { const float2 t = *reinterpret_cast<const float2 *>(p); v[0] = t.x; v[1] = t.y; }
+    if constexpr (V == 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+}
+template <int V>
+__device__ __forceinline__ void stv(float *p, const float (&v)[V])
+{
+    if constexpr (V == 1) *p = v[0];
+    if constexpr (V == 2) *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+    if constexpr (V == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// reduce per-lane column partials acc[V] (column lane*V+v) over the block's
+// warps and add them to out[K]
+template <int V>
+__device__ __forceinline__ void block_cols_add(const double (&acc)[V], double *sh, double *out)
+{
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    constexpr int K = 32 * V;
+#pragma unroll
+    for (int v = 0; v < V; ++v) sh[w * K + l * V + v] = acc[v];
+    __syncthreads();
+    for (int c = threadIdx.x; c < K; c += blockDim.x) {
+        double s = 0;
+        for (int j = 0; j < nw; ++j) s += sh[j * K + c];
+        atomicAdd(out + c, s);
+    }
+}
+
+// Q = S P (FP32 values, FP32 vectors, FP32 accumulate), warp per row;
+// pq[c] += sum_i P[i][c] Q[i][c] in FP64
+template <int V>
+__global__ void __launch_bounds__(256) k_spmm32(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                                const float *__restrict__ a, const float *__restrict__ P,
+                                                float *__restrict__ Q, int64_t N, double *pq, const int *stop)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    if (*stop) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double dacc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        float acc[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = 0.f;
+        const int32_t b = rp[i], e = rp[i + 1];
+        for (int32_t s0 = b; s0 < e; s0 += 32) {
+            const int32_t s = s0 + lane;
+            const float av = s < e ? a[s] : 0.f;
+            const int32_t cv = s < e ? col[s] : 0;
+            const int n = min(32, e - s0);
+            for (int j = 0; j < n; ++j) {
+                const float aj = __shfl_sync(0xffffffffu, av, j);
+                const int32_t cj = __shfl_sync(0xffffffffu, cv, j);
+                float pv[V];
+                ldv<V>(P + (int64_t)cj * K + lane * V, pv);
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[v] = fmaf(aj, pv[v], acc[v]);
+            }
+        }
+        stv<V>(Q + i * K + lane * V, acc);
+        float pi[V];
+        ldv<V>(P + i * K + lane * V, pi);
+#pragma unroll
+        for (int v = 0; v < V; ++v) dacc[v] += (double)pi[v] * (double)acc[v];
+    }
+    block_cols_add<V>(dacc, sh, pq);
+}
+
+// R = B - S X in FP64 (warp per row); rr[c] += R[i][c]^2
+template <int V>
+__global__ void __launch_bounds__(256) k_resid64(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                                 const double *__restrict__ a, const double *__restrict__ X,
+                                                 const double *__restrict__ B, double *__restrict__ R, int64_t N,
+                                                 double *rr)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double dacc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        double acc[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = 0.0;
+        const int32_t b = rp[i], e = rp[i + 1];
+        for (int32_t s0 = b; s0 < e; s0 += 32) {
+            const int32_t s = s0 + lane;
+            const double av = s < e ? a[s] : 0.0;
+            const int32_t cv = s < e ? col[s] : 0;
+            const int n = min(32, e - s0);
+            for (int j = 0; j < n; ++j) {
+                const double aj = __shfl_sync(0xffffffffu, av, j);
+                const int32_t cj = __shfl_sync(0xffffffffu, cv, j);
+                const double *xp = X + (int64_t)cj * K + lane * V;
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[v] = fma(aj, xp[v], acc[v]);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const double rv = B[i * K + lane * V + v] - acc[v];
+            R[i * K + lane * V + v] = rv;
+            dacc[v] += rv * rv;
+        }
+    }
+    block_cols_add<V>(dacc, sh, rr);
+}
+
+// r32 = r64 * scale_c, x32 = 0, p = z = D^-1 r32; rz0[c], rr0[c]
+template <int V>
+__global__ void __launch_bounds__(256) k_binit32(const double *__restrict__ R64, const double *__restrict__ scale,
+                                                 const float *__restrict__ dinv, float *__restrict__ r,
+                                                 float *__restrict__ x, float *__restrict__ p, int64_t N, double *rz0,
+                                                 double *rr0)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double a1[V], a2[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) a1[v] = a2[v] = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const float di = dinv[i];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int64_t o = i * K + lane * V + v;
+            const float rv = (float)(R64[o] * scale[lane * V + v]);
+            const float zv = di * rv;
+            r[o] = rv;
+            x[o] = 0.f;
+            p[o] = zv;
+            a1[v] += (double)rv * zv;
+            a2[v] += (double)rv * rv;
+        }
+    }
+    block_cols_add<V>(a1, sh, rz0);
+    __syncthreads();
+    block_cols_add<V>(a2, sh, rr0);
+}
+
+// per column: frozen when rr[it][c] <= thr[c]; alpha = rz/pq; x += alpha p;
+// r -= alpha q; rz'[c], rr'[c]
+template <int V>
+__global__ void __launch_bounds__(256) k_bupdate32(float *__restrict__ x, float *__restrict__ r,
+                                                   const float *__restrict__ p, const float *__restrict__ q,
+                                                   const float *__restrict__ dinv, int64_t N, const double *pq,
+                                                   const double *rz, const double *rr, const double *thr,
+                                                   double *rz_next, double *rr_next, const int *stop, int *err)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    if (*stop) return;
+    const int lane = threadIdx.x & 31;
+    float alpha[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int c = lane * V + v;
+        const bool frozen = rr[c] <= thr[c];
+        const double den = pq[c];
+        if (!frozen && !(den > 0.0)) atomicExch(err, 1);
+        alpha[v] = (frozen || !(den > 0.0)) ? 0.f : (float)(rz[c] / den);
+    }
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double a1[V], a2[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) a1[v] = a2[v] = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const int64_t o = i * K + lane * V;
+        float xv[V], rv[V], pv[V], qv[V];
+        ldv<V>(x + o, xv);
+        ldv<V>(r + o, rv);
+        ldv<V>(p + o, pv);
+        ldv<V>(q + o, qv);
+        const float di = dinv[i];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            xv[v] = fmaf(alpha[v], pv[v], xv[v]);
+            rv[v] = fmaf(-alpha[v], qv[v], rv[v]);
+            const float zv = di * rv[v];
+            a1[v] += (double)rv[v] * zv;
+            a2[v] += (double)rv[v] * rv[v];
+        }
+        stv<V>(x + o, xv);
+        stv<V>(r + o, rv);
+    }
+    block_cols_add<V>(a1, sh, rz_next);
+    __syncthreads();
+    block_cols_add<V>(a2, sh, rr_next);
+}
+
+// p = D^-1 r + beta p for active columns (rr' > thr)
+template <int V>
+__global__ void __launch_bounds__(256) k_bpupdate32(float *__restrict__ p, const float *__restrict__ r,
+                                                    const float *__restrict__ dinv, int64_t N, const double *rz,
+                                                    const double *rz_next, const double *rr_next, const double *thr,
+                                                    const int *stop)
+{
+    constexpr int K = 32 * V;
+    if (*stop) return;
+    const int lane = threadIdx.x & 31;
+    float beta[V];
+    bool act[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int c = lane * V + v;
+        act[v] = rr_next[c] > thr[c];
+        beta[v] = act[v] ? (float)(rz_next[c] / rz[c]) : 0.f;
+    }
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const int64_t o = i * K + lane * V;
+        float pv[V], rv[V];
+        ldv<V>(p + o, pv);
+        ldv<V>(r + o, rv);
+        const float di = dinv[i];
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            if (act[v]) pv[v] = fmaf(beta[v], pv[v], di * rv[v]);
+        stv<V>(p + o, pv);
+    }
+}
+
+// all columns converged at iteration it -> *stop = 1
+template <int K>
+__global__ void k_bcheck(const double *rr, const double *thr, int *stop)
+{
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int c = threadIdx.x; c < K; c += blockDim.x)
+        if (rr[c] > thr[c]) any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0 && !any) *stop = 1;
+}
+
+// x64 += norm_c * x32
+template <int V>
+__global__ void k_bacc64(double *__restrict__ X64, const float *__restrict__ x32, const double *__restrict__ norm,
+                         int64_t N)
+{
+    constexpr int K = 32 * V;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * K; t += (int64_t)gridDim.x * blockDim.x)
+        X64[t] += norm[t % K] * (double)x32[t];
+}
+
+// gather columns [c0, c0+kb) of B (row stride ld) into a zero-padded [N][K]
+__global__ void k_gather_cols(const double *__restrict__ B, int ld, int c0, int kb, int K, int64_t N,
+                              double *__restrict__ out)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * K; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / K;
+        const int c = (int)(t - i * K);
+        out[t] = c < kb ? B[i * ld + c0 + c] : 0.0;
+    }
+}
+
+__global__ void k_scatter_cols(const double *__restrict__ in, int ld, int c0, int kb, int K, int64_t N,
+                               double *__restrict__ X)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * (int64_t)kb; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / kb;
+        const int c = (int)(t - i * kb);
+        X[i * ld + c0 + c] = in[i * K + c];
+    }
+}
+
+// A^T fixup on constrained dofs: Y[c][a] += sum over free rows f of
+// a_ref[f,c] X[f][a]
+__global__ void k_fix_accum(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                            const double *__restrict__ a_ref, const unsigned char *__restrict__ mask,
+                            const double *__restrict__ X, int ld, int nrhs, int64_t N, double *__restrict__ Y)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * nrhs; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t f = t / nrhs;
+        const int a = (int)(t - f * nrhs);
+        if (mask[f]) continue;
+        const double xf = X[f * ld + a];
+        for (int32_t s = rp[f]; s < rp[f + 1]; ++s) {
+            const int32_t j = col[s];
+            if (mask[j]) atomicAdd(&Y[(int64_t)j * nrhs + a], a_ref[s] * xf);
+        }
+    }
+}
+
+__global__ void k_fix_apply(const int32_t *__restrict__ diag, const double *__restrict__ a_ref,
+                            const unsigned char *__restrict__ mask, const double *__restrict__ B,
+                            const double *__restrict__ Y, int ld, int nrhs, int64_t N, double *__restrict__ X)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * nrhs; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = t / nrhs;
+        const int a = (int)(t - c * nrhs);
+        if (!mask[c]) continue;
+        X[c * ld + a] = (B[c * ld + a] - Y[c * nrhs + a]) / a_ref[diag[c]];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+struct PcgResult {
+    int iters;
+    bool converged;
+};
+
+void launch_spmv64(sfc_system *s, const double *x, double *y, double *dot, const int *done)
+{
+    const double avg = (double)s->nnz / (double)std::max<int64_t>(s->N, 1);
+    sfc_ctx *ctx = s->ctx;
+    const unsigned grid = (unsigned)(ctx->sm_count * 8);
+    if (avg > 24)
+        k_spmv64<32><<<grid_for(s->N * 32, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
+                                                                                              s->a_op.p, x, y, s->N, dot, done);
+    else if (avg > 12)
+        k_spmv64<16><<<grid_for(s->N * 16, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
+                                                                                              s->a_op.p, x, y, s->N, dot, done);
+    else if (avg > 6)
+        k_spmv64<8><<<grid_for(s->N * 8, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
+                                                                                            s->a_op.p, x, y, s->N, dot, done);
+    else
+        k_spmv64<4><<<grid_for(s->N * 4, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
+                                                                                            s->a_op.p, x, y, s->N, dot, done);
+    count_launch(ctx);
+}
+
+// FP64 Jacobi-PCG on S x = b (device vectors, length N)
+PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_iter, int check)
+{
+    sfc_ctx *ctx = s->ctx;
+    const int64_t N = s->N;
+    s->w64.reserve(3 * N);
+    double *r = s->w64.p, *p = r + N, *q = p + N;
+    const int nsc = 3 * (max_iter + 2) + 1;
+    s->scal.reserve(nsc);
+    double *pq = s->scal.p, *rz = pq + (max_iter + 2), *rr = rz + (max_iter + 2), *bb = rr + (max_iter + 2);
+    s->flags.reserve(2);
+    int *done = s->flags.p, *err = s->flags.p + 1;
+    SFC_CK(cudaMemsetAsync(s->scal.p, 0, nsc * sizeof(double), ctx->stream));
+    SFC_CK(cudaMemsetAsync(s->flags.p, 0, 2 * sizeof(int), ctx->stream));
+    const unsigned g = grid_for(N, kRedThreads, ctx->sm_count * 4);
+    k_pcg_init<<<g, kRedThreads, 0, ctx->stream>>>(b, s->dinv.p, x, r, p, N, rz, bb);
+    count_launch(ctx);
+    double hbb = 0;
+    download(ctx, &hbb, bb, 1);
+    if (hbb == 0.0) return {0, true};
+    const double thr = tol * tol * hbb;
+    int it = 0;
+    PcgResult res{max_iter, false};
+    for (it = 0; it < max_iter; ++it) {
+        launch_spmv64(s, p, q, pq + it, done);
+        k_pcg_update<<<g, kRedThreads, 0, ctx->stream>>>(x, r, p, q, s->dinv.p, N, pq + it, rz + it, rz + it + 1,
+                                                         rr + it + 1, done, err);
+        k_pcg_pupdate<<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, N, rz + it, rz + it + 1, rr + it + 1, thr,
+                                                          it + 1, done, err);
+        count_launch(ctx, 2);
+        if ((it + 1) % check == 0 || it + 1 == max_iter) {
+            int hf[2];
+            download(ctx, hf, s->flags.p, 2);
+            if (hf[1]) fail(SFC_ERR_NOT_SPD, "PCG breakdown: p^T A p <= 0");
+            if (hf[0]) {
+                res = {hf[0], true};
+                break;
+            }
+        }
+    }
+    return res;
+}
+
+double true_rel_residual(sfc_system *s, const double *b, const double *x)
+{
+    sfc_ctx *ctx = s->ctx;
+    const int64_t N = s->N;
+    DBuf<double> t, d;
+    t.alloc(N);
+    d.alloc(2);
+    SFC_CK(cudaMemsetAsync(d.p, 0, 2 * sizeof(double), ctx->stream));
+    launch_spmv64(s, x, t.p, nullptr, nullptr);
+    k_axpby<<<grid_for(N, 256), 256, 0, ctx->stream>>>(t.p, b, 1.0, -1.0, N);  // t = b - Sx
+    const unsigned g = grid_for(N, kRedThreads, ctx->sm_count * 4);
+    k_dot<<<g, kRedThreads, 0, ctx->stream>>>(t.p, t.p, N, d.p);
+    k_dot<<<g, kRedThreads, 0, ctx->stream>>>(b, b, N, d.p + 1);
+    count_launch(ctx, 3);
+    double h[2];
+    download(ctx, h, d.p, 2);
+    return h[1] > 0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+}
+
+template <int V>
+void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sfc_solve_stats_t &st)
+{
+    constexpr int K = 32 * V;
+    sfc_ctx *ctx = s->ctx;
+    const int64_t N = s->N;
+    const auto &o = s->opt;
+    const int max_iter = o.max_iter > 0 ? o.max_iter : 20000;
+    const int check = o.check_every > 0 ? o.check_every : 16;
+    const double tol = o.tol > 0 ? o.tol : 1e-8;
+    const double itol = o.inner_tol > 0 ? o.inner_tol : 1e-4;
+    DBuf<double> b64, x64, r64, cs;  // cs: column scalars
+    DBuf<float> f32;
+    b64.alloc(N * K);
+    x64.alloc(N * K);
+    r64.alloc(N * K);
+    f32.alloc(4 * N * K);
+    float *xr = f32.p, *rr32 = xr + N * K, *pp = rr32 + N * K, *qq = pp + N * K;
+    const int64_t nsc = 3 * (int64_t)(max_iter + 2) * K;
+    s->scal.reserve(nsc);
+    double *pq = s->scal.p, *rz = pq + (int64_t)(max_iter + 2) * K, *rrs = rz + (int64_t)(max_iter + 2) * K;
+    cs.alloc(6 * K);
+    double *bn2 = cs.p, *rn2 = bn2 + K, *scale = rn2 + K, *norm = scale + K, *thr = norm + K;
+    s->flags.reserve(2);
+    int *stop = s->flags.p, *err = s->flags.p + 1;
+    const unsigned gw = (unsigned)(ctx->sm_count * 2);  // warp-per-row kernels: 8 warps/block
+    std::vector<double> hb(K), hr(K), hs(K), hn(K), ht(K);
+    int max_inner = 0, max_cycles = 0;
+    double worst = 0.0;
+    bool all_conv = true;
+    for (int c0 = 0; c0 < nrhs; c0 += K) {
+        const int kb = std::min(K, nrhs - c0);
+        k_gather_cols<<<grid_for(N * K, 256), 256, 0, ctx->stream>>>(B, ld, c0, kb, K, N, b64.p);
+        SFC_CK(cudaMemsetAsync(x64.p, 0, N * K * 8, ctx->stream));
+        SFC_CK(cudaMemsetAsync(cs.p, 0, 6 * K * 8, ctx->stream));
+        count_launch(ctx);
+        // ||b_c||^2 via the FP64 residual of x = 0
+        k_resid64<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, x64.p, b64.p, r64.p, N, bn2);
+        count_launch(ctx);
+        download(ctx, hb.data(), bn2, K);
+        int inner_total = 0, cycles = 0;
+        std::vector<double> rn(K);
+        for (int c = 0; c < K; ++c) rn[c] = hb[c];
+        for (int cyc = 0;; ++cyc) {
+            if (cyc > 0) {
+                SFC_CK(cudaMemsetAsync(rn2, 0, K * 8, ctx->stream));
+                k_resid64<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, x64.p, b64.p, r64.p, N,
+                                                          rn2);
+                count_launch(ctx);
+                download(ctx, rn.data(), rn2, K);
+            }
+            bool done_all = true;
+            for (int c = 0; c < K; ++c) {
+                const double bnc = std::sqrt(hb[c]), rnc = std::sqrt(rn[c]);
+                const bool ok = c >= kb || bnc == 0.0 || rnc <= tol * bnc;
+                if (!ok) done_all = false;
+                hs[c] = rnc > 0 ? 1.0 / rnc : 0.0;
+                hn[c] = rnc;
+                // inner target relative to the normalised residual (1.0): no
+                // tighter than needed to meet tol this cycle
+                const double need = rnc > 0 ? 0.5 * tol * bnc / rnc : 1.0;
+                const double t = ok ? INFINITY : std::max(itol, need);
+                ht[c] = ok ? INFINITY : t * t;
+            }
+            if (done_all || cyc >= 40 || inner_total >= max_iter) {
+                for (int c = 0; c < kb; ++c) {
+                    const double bnc = std::sqrt(hb[c]);
+                    if (bnc > 0) worst = std::max(worst, std::sqrt(rn[c]) / bnc);
+                }
+                if (!done_all) all_conv = false;
+                break;
+            }
+            ++cycles;
+            SFC_CK(cudaMemcpyAsync(scale, hs.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
+            SFC_CK(cudaMemcpyAsync(norm, hn.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
+            SFC_CK(cudaMemcpyAsync(thr, ht.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
+            const int cap = max_iter - inner_total;
+            SFC_CK(cudaMemsetAsync(s->scal.p, 0, 3 * (int64_t)(std::min(cap, max_iter) + 2) * K * 8, ctx->stream));
+            SFC_CK(cudaMemsetAsync(s->flags.p, 0, 2 * sizeof(int), ctx->stream));
+            k_binit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, rr32, xr, pp, N, rz, rrs);
+            count_launch(ctx);
+            int it = 0;
+            for (it = 0; it < cap; ++it) {
+                const int64_t o0 = (int64_t)it * K, o1 = (int64_t)(it + 1) * K;
+                k_spmm32<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op32.p, pp, qq, N, pq + o0, stop);
+                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
+                                                            rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+                k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1, thr,
+                                                             stop);
+                count_launch(ctx, 3);
+                if ((it + 1) % check == 0 || it + 1 == cap) {
+                    k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + o1, thr, stop);
+                    count_launch(ctx);
+                    int hf[2];
+                    download(ctx, hf, s->flags.p, 2);
+                    if (hf[1]) fail(SFC_ERR_NOT_SPD, "block PCG breakdown: p^T A p <= 0");
+                    if (hf[0]) {
+                        ++it;
+                        break;
+                    }
+                }
+            }
+            inner_total += it;
+            k_bacc64<V><<<grid_for(N * K, 256), 256, 0, ctx->stream>>>(x64.p, xr, norm, N);
+            count_launch(ctx);
+        }
+        k_scatter_cols<<<grid_for(N * kb, 256), 256, 0, ctx->stream>>>(x64.p, ld, c0, kb, K, N, X);
+        count_launch(ctx);
+        max_inner = std::max(max_inner, inner_total);
+        max_cycles = std::max(max_cycles, cycles);
+    }
+    SFC_CK(cudaStreamSynchronize(ctx->stream));
+    st.iterations = max_inner;
+    st.refinements = max_cycles;
+    st.num_rhs = nrhs;
+    st.max_rel_residual = worst;
+    st.converged = all_conv ? 1 : 0;
+}
+
+}  // namespace
+
+double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n)
+{
+    DBuf<double> d;
+    d.alloc(1);
+    SFC_CK(cudaMemsetAsync(d.p, 0, sizeof(double), ctx->stream));
+    k_dot<<<grid_for(n, kRedThreads, ctx->sm_count * 4), kRedThreads, 0, ctx->stream>>>(a, b, n, d.p);
+    count_launch(ctx);
+    double h = 0;
+    download(ctx, &h, d.p, 1);
+    return h;
+}
+
+// X = A^-1 F into s->X
+void solve_forward(sfc_system *s)
+{
+    sfc_ctx *ctx = s->ctx;
+    build_operator(s);
+    const int64_t N = s->N;
+    s->X.alloc(N);
+    DBuf<double> b;
+    b.alloc(N);
+    k_lift<<<grid_for(N, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p, s->mask.p, s->F.p,
+                                                      N, b.p);
+    count_launch(ctx);
+    const auto &o = s->opt;
+    const int max_iter = o.max_iter > 0 ? o.max_iter : 20000;
+    const int check = o.check_every > 0 ? o.check_every : 16;
+    const double tol = o.tol > 0 ? o.tol : 1e-8;
+    cudaEvent_t e0, e1;
+    SFC_CK(cudaEventCreate(&e0));
+    SFC_CK(cudaEventCreate(&e1));
+    SFC_CK(cudaEventRecord(e0, ctx->stream));
+    PcgResult r = pcg64(s, b.p, s->X.p, tol, max_iter, check);
+    SFC_CK(cudaEventRecord(e1, ctx->stream));
+    const double rel = true_rel_residual(s, b.p, s->X.p);
+    float ms = 0;
+    SFC_CK(cudaEventSynchronize(e1));
+    SFC_CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->stats = {};
+    s->stats.iterations = r.iters;
+    s->stats.num_rhs = 1;
+    s->stats.converged = r.converged ? 1 : 0;
+    s->stats.max_rel_residual = rel;
+    s->stats.device_ms = ms;
+    if (!r.converged) fail(SFC_ERR_NOT_CONVERGED, "PCG did not converge within max_iter");
+}
+
+// S X = B for nrhs columns of the [N][ld] arrays (free-dof part of A^T solves;
+// constrained rows come out as B_c / scalar, fixed up by transpose_fixup)
+void solve_block(sfc_system *s, const double *B, double *X, int nrhs, int ld)
+{
+    sfc_ctx *ctx = s->ctx;
+    build_operator(s);
+    const int64_t N = s->N;
+    cudaEvent_t e0, e1;
+    SFC_CK(cudaEventCreate(&e0));
+    SFC_CK(cudaEventCreate(&e1));
+    SFC_CK(cudaEventRecord(e0, ctx->stream));
+    sfc_solve_stats_t st{};
+    const auto &o = s->opt;
+    if (o.method == SFC_SOLVER_PCG_MIXED) {
+        int bw = o.block_width > 0 ? o.block_width : 64;
+        if (nrhs <= 32) bw = 32;
+        if (bw <= 32)
+            block_mixed<1>(s, B, X, nrhs, ld, st);
+        else if (bw <= 64)
+            block_mixed<2>(s, B, X, nrhs, ld, st);
+        else
+            block_mixed<4>(s, B, X, nrhs, ld, st);
+    } else {
+        const int max_iter = o.max_iter > 0 ? o.max_iter : 20000;
+        const int check = o.check_every > 0 ? o.check_every : 16;
+        const double tol = o.tol > 0 ? o.tol : 1e-8;
+        DBuf<double> b, x;
+        b.alloc(N);
+        x.alloc(N);
+        st.converged = 1;
+        for (int a = 0; a < nrhs; ++a) {
+            k_gather_cols<<<grid_for(N, 256), 256, 0, ctx->stream>>>(B, ld, a, 1, 1, N, b.p);
+            count_launch(ctx);
+            PcgResult r = pcg64(s, b.p, x.p, tol, max_iter, check);
+            st.iterations = std::max(st.iterations, r.iters);
+            if (!r.converged) st.converged = 0;
+            k_scatter_cols<<<grid_for(N, 256), 256, 0, ctx->stream>>>(x.p, ld, a, 1, 1, N, X);
+            count_launch(ctx);
+        }
+        st.num_rhs = nrhs;
+        st.refinements = 0;
+        st.max_rel_residual = -1.0;  // recurrence residual below tol for each RHS
+    }
+    SFC_CK(cudaEventRecord(e1, ctx->stream));
+    float ms = 0;
+    SFC_CK(cudaEventSynchronize(e1));
+    SFC_CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    st.device_ms = ms;
+    s->stats = st;
+    if (!st.converged) fail(SFC_ERR_NOT_CONVERGED, "block PCG did not converge within max_iter");
+}
+
+void transpose_fixup(sfc_system *s, const double *B, double *X, int nrhs, int ld)
+{
+    if (!s->any_constraint) return;
+    sfc_ctx *ctx = s->ctx;
+    const int64_t N = s->N;
+    s->fix.reserve(N * (int64_t)nrhs);
+    SFC_CK(cudaMemsetAsync(s->fix.p, 0, N * (int64_t)nrhs * 8, ctx->stream));
+    k_fix_accum<<<grid_for(N * nrhs, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_ref.p, s->mask.p, X,
+                                                                   ld, nrhs, N, s->fix.p);
+    k_fix_apply<<<grid_for(N * nrhs, 256), 256, 0, ctx->stream>>>(s->diag.p, s->a_ref.p, s->mask.p, B, s->fix.p, ld,
+                                                                  nrhs, N, X);
+    count_launch(ctx, 2);
+}
+
+}  // namespace sfc

@@ -1,0 +1,736 @@
+// statX on the GPU: nodal forcing covariance, ForwardGaussRHS, mismatch
+// covariance and the Kennedy-O'Hagan likelihood / posterior, all FP64.
+//
+// Forcing covariance (statX/infer/CovarianceForcing.ipp:38-109) is
+//   C_f[i][j] = phibar_i k(x_i,x_j) phibar_j   (same component, 0 otherwise),
+// k the squared-exponential kernel (statX/infer/ExpKernel.hpp:74-92).  The
+// reference materialises C_f as N^2 triplets; here M C_f M^T is evaluated
+// matrix-free as W^T (K W) with W = diag(phibar) M^T:
+//   * general node sets: K W with the kernel evaluated on the fly, tile by
+//     tile;
+//   * tensor-grid node sets (structured meshes): K = s^2 Kz (x) Ky (x) Kx, so
+//     K W is three small dense products along the grid axes -- the same
+//     matrix in exact arithmetic at O(N (nx+ny+nz)) instead of O(N^2).
+// Small dense algebra (Cholesky, triangular solves, SPD inverses) runs in
+// single-CTA kernels with a batch index in blockIdx.x.
+
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sfc {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// kernels: forcing covariance
+// ---------------------------------------------------------------------------
+
+// B[idx][a] = val for each entry of P row a (B is N x ns, zeroed before)
+__global__ void k_scatter_pt(const int64_t *__restrict__ ptr, const int32_t *__restrict__ idx,
+                             const double *__restrict__ val, int64_t ns, double *__restrict__ B)
+{
+    for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < ns; a += (int64_t)gridDim.x * blockDim.x)
+        for (int64_t s = ptr[a]; s < ptr[a + 1]; ++s) B[(int64_t)idx[s] * ns + a] += val[s];
+}
+
+// W[i][a] = phibar[i] * X[i][a]
+__global__ void k_scale_rows(const double *__restrict__ X, const double *__restrict__ phibar, int64_t N, int64_t ns,
+                             double *__restrict__ W)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * ns; t += (int64_t)gridDim.x * blockDim.x)
+        W[t] = phibar[t / ns] * X[t];
+}
+
+// out[a] = sum_i X[i][a] F[i]   (one block per column a, FP64 reduction)
+__global__ void k_colsum_dot(const double *__restrict__ X, const double *__restrict__ F, int64_t N, int64_t ns,
+                             double *__restrict__ out)
+{
+    __shared__ double sh[256];
+    for (int64_t a = blockIdx.x; a < ns; a += gridDim.x) {
+        double s = 0;
+        for (int64_t i = threadIdx.x; i < N; i += blockDim.x) s += X[i * ns + a] * F[i];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[a] = sh[0];
+        __syncthreads();
+    }
+}
+
+// squared-exponential value, the reference's expression order
+__device__ __forceinline__ double se_value(const double *x, const double *y, int dim, double sigma, double length)
+{
+    double t[3] = {0, 0, 0};
+    for (int a = 0; a < dim; ++a) {
+        const double d = x[a] - y[a];
+        t[a] = __dmul_rn(d, d);
+    }
+    double sq = dim == 1 ? t[0] : dim == 2 ? __dadd_rn(t[0], t[1]) : __dadd_rn(t[0], __dadd_rn(t[1], t[2]));
+    return __dmul_rn(__dmul_rn(sigma, sigma), exp(-sq / __dmul_rn(__dmul_rn(2., length), length)));
+}
+
+// T[i*dof+c][a] = sum_j k(x_i,x_j) W[j*dof+c][a], kernel on the fly.
+// Block: 16 nodes i x all columns; j tiles of 16 nodes staged in shared memory.
+constexpr int kTI = 16, kTJ = 16;
+__global__ void __launch_bounds__(256) k_kw_dense(const double *__restrict__ coords, int64_t nodes, int dim, int dof,
+                                                   int c, int64_t ns, const double *__restrict__ W,
+                                                   double *__restrict__ T, double sigma, double length)
+{
+    extern __shared__ double smem[];
+    double *kv = smem;                 // kTI x kTJ
+    double *wt = smem + kTI * kTJ;     // kTJ x ns
+    const int64_t i0 = (int64_t)blockIdx.x * kTI;
+    const int nout = kTI * (int)ns;
+    double acc[16];
+    for (int u = 0; u < 16; ++u) acc[u] = 0.0;
+    for (int64_t j0 = 0; j0 < nodes; j0 += kTJ) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kTI * kTJ; t += blockDim.x) {
+            const int ii = t / kTJ, jj = t % kTJ;
+            const int64_t i = i0 + ii, j = j0 + jj;
+            kv[t] = (i < nodes && j < nodes) ? se_value(coords + 3 * i, coords + 3 * j, dim, sigma, length) : 0.0;
+        }
+        for (int t = threadIdx.x; t < kTJ * ns; t += blockDim.x) {
+            const int jj = t / (int)ns, a = t % (int)ns;
+            const int64_t j = j0 + jj;
+            wt[t] = j < nodes ? W[(j * dof + c) * ns + a] : 0.0;
+        }
+        __syncthreads();
+        for (int u = 0, o = threadIdx.x; o < nout && u < 16; o += blockDim.x, ++u) {
+            const int ii = o / (int)ns, a = o % (int)ns;
+            double s = acc[u];
+#pragma unroll
+            for (int jj = 0; jj < kTJ; ++jj) s = fma(kv[ii * kTJ + jj], wt[jj * ns + a], s);
+            acc[u] = s;
+        }
+    }
+    for (int u = 0, o = threadIdx.x; o < nout && u < 16; o += blockDim.x, ++u) {
+        const int ii = o / (int)ns, a = o % (int)ns;
+        const int64_t i = i0 + ii;
+        if (i < nodes) T[(i * dof + c) * ns + a] = acc[u];
+    }
+}
+
+// one axis of the Kronecker product: for every node, column a:
+// out[node(m)] = sum_k Kd[m][k] in[node(k)]  along axis d (stride sd, length nd)
+__global__ void k_kron_axis(const double *__restrict__ Kd, int nd, int64_t sd, int64_t nodes, int dof, int c,
+                            int64_t ns, const double *__restrict__ in, double *__restrict__ out)
+{
+    extern __shared__ double sK[];
+    for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) sK[t] = Kd[t];
+    __syncthreads();
+    const int64_t total = nodes * ns;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t node = t / ns;
+        const int64_t a = t - node * ns;
+        const int64_t m = (node / sd) % nd;
+        const int64_t base = node - m * sd;
+        double s = 0.0;
+        for (int k = 0; k < nd; ++k) s = fma(sK[m * nd + k], in[((base + k * sd) * dof + c) * ns + a], s);
+        out[(node * dof + c) * ns + a] = s;
+    }
+}
+
+// C[a][b] += sum_i A[i][a] B[i][b] over a slice of rows (split-K, atomics);
+// 64 x 64 output tile per block, 4 x 4 per thread
+__global__ void __launch_bounds__(256) k_atb(const double *__restrict__ A, const double *__restrict__ B, int64_t K,
+                                              int64_t M, int64_t Nn, int64_t rows_per_block, double alpha,
+                                              double *__restrict__ C)
+{
+    __shared__ double sa[16][64];
+    __shared__ double sb[16][64];
+    const int64_t a0 = blockIdx.y * 64, b0 = blockIdx.z * 64;
+    const int64_t k0 = blockIdx.x * rows_per_block;
+    const int64_t k1 = min(K, k0 + rows_per_block);
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[4][4] = {};
+    for (int64_t kk = k0; kk < k1; kk += 16) {
+        for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+            const int r = t / 64, cc = t % 64;
+            const int64_t k = kk + r;
+            sa[r][cc] = (k < k1 && a0 + cc < M) ? A[k * M + a0 + cc] : 0.0;
+            sb[r][cc] = (k < k1 && b0 + cc < Nn) ? B[k * Nn + b0 + cc] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                av[u] = sa[r][ty * 4 + u];
+                bv[u] = sb[r][tx * 4 + u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int64_t a = a0 + ty * 4 + u, b = b0 + tx * 4 + v;
+            if (a < M && b < Nn) atomicAdd(&C[a * Nn + b], alpha * acc[u][v]);
+        }
+}
+
+// general row-major C = alpha op(A) op(B) + beta C  (small dense algebra)
+__global__ void __launch_bounds__(256) k_gemm(int ta, int tb, int64_t M, int64_t N, int64_t K, double alpha,
+                                               const double *__restrict__ A, int64_t lda, const double *__restrict__ B,
+                                               int64_t ldb, double beta, double *__restrict__ C, int64_t ldc)
+{
+    __shared__ double sa[16][64];
+    __shared__ double sb[16][64];
+    const int64_t m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[4][4] = {};
+    for (int64_t k0 = 0; k0 < K; k0 += 16) {
+        for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+            const int r = t / 64, cc = t % 64;
+            const int64_t k = k0 + r, m = m0 + cc, n = n0 + cc;
+            sa[r][cc] = (k < K && m < M) ? (ta ? A[k * lda + m] : A[m * lda + k]) : 0.0;
+            sb[r][cc] = (k < K && n < N) ? (tb ? B[n * ldb + k] : B[k * ldb + n]) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                av[u] = sa[r][ty * 4 + u];
+                bv[u] = sb[r][tx * 4 + u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int64_t m = m0 + ty * 4 + u, n = n0 + tx * 4 + v;
+            if (m < M && n < N) C[m * ldc + n] = alpha * acc[u][v] + (beta == 0.0 ? 0.0 : beta * C[m * ldc + n]);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// single-CTA dense FP64 kernels (blockIdx.x = batch item)
+// ---------------------------------------------------------------------------
+
+// in-place lower Cholesky of the n x n row-major A (upper part left as is);
+// info[b] = 0 or k+1 at the first non-positive pivot (Eigen::LLT info != Success)
+__device__ void chol_lower(int n, double *A, int lda, int *info)
+{
+    __shared__ double piv;
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        if (threadIdx.x == 0) {
+            const double d = A[(int64_t)k * lda + k];
+            if (!(d > 0.0)) {
+                bad = k + 1;
+                piv = 1.0;
+            } else {
+                piv = sqrt(d);
+            }
+            A[(int64_t)k * lda + k] = piv;
+        }
+        __syncthreads();
+        if (bad) break;
+        const double pv = piv;
+        for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) A[(int64_t)i * lda + k] /= pv;
+        __syncthreads();
+        const int m = n - k - 1;
+        for (int64_t t = threadIdx.x; t < (int64_t)m * m; t += blockDim.x) {
+            const int i = k + 1 + (int)(t / m), j = k + 1 + (int)(t % m);
+            if (j <= i) A[(int64_t)i * lda + j] -= A[(int64_t)i * lda + k] * A[(int64_t)j * lda + k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *info = bad;
+    __syncthreads();
+}
+
+// B = L^-1 B (forward substitution), L lower n x n, B n x m (row-major)
+__device__ void trsm_lower(int n, const double *L, int ldl, int m, double *B, int ldb)
+{
+    for (int k = 0; k < n; ++k) {
+        const double d = L[(int64_t)k * ldl + k];
+        for (int c = threadIdx.x; c < m; c += blockDim.x) B[(int64_t)k * ldb + c] /= d;
+        __syncthreads();
+        for (int64_t t = threadIdx.x; t < (int64_t)(n - k - 1) * m; t += blockDim.x) {
+            const int i = k + 1 + (int)(t / m), c = (int)(t % m);
+            B[(int64_t)i * ldb + c] -= L[(int64_t)i * ldl + k] * B[(int64_t)k * ldb + c];
+        }
+        __syncthreads();
+    }
+}
+
+// B = L^-T B (back substitution with the transpose)
+__device__ void trsm_lower_t(int n, const double *L, int ldl, int m, double *B, int ldb)
+{
+    for (int k = n - 1; k >= 0; --k) {
+        const double d = L[(int64_t)k * ldl + k];
+        for (int c = threadIdx.x; c < m; c += blockDim.x) B[(int64_t)k * ldb + c] /= d;
+        __syncthreads();
+        for (int64_t t = threadIdx.x; t < (int64_t)k * m; t += blockDim.x) {
+            const int i = (int)(t / m), c = (int)(t % m);
+            B[(int64_t)i * ldb + c] -= L[(int64_t)k * ldl + i] * B[(int64_t)k * ldb + c];
+        }
+        __syncthreads();
+    }
+}
+
+// Ainv = A^-1 for SPD A (n x n); L is scratch n x n; info as chol_lower
+__device__ void spd_inverse(int n, const double *A, double *L, double *Ainv, int *info)
+{
+    for (int64_t t = threadIdx.x; t < (int64_t)n * n; t += blockDim.x) {
+        L[t] = A[t];
+        Ainv[t] = (t / n == t % n) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    chol_lower(n, L, n, info);
+    if (*info) return;
+    trsm_lower(n, L, n, n, Ainv, n);
+    trsm_lower_t(n, L, n, n, Ainv, n);
+}
+
+// MismatchCovariance::giveCovariance (statX/infer/MismatchCovariance.hpp:76-99)
+__device__ void mismatch_cov(int ns, const double *xs, int dim, double sd, double ld, double eps, double *K)
+{
+    for (int64_t t = threadIdx.x; t < (int64_t)ns * ns; t += blockDim.x) {
+        const int k = (int)(t / ns), l = (int)(t % ns);
+        double v = se_value(xs + 3 * k, xs + 3 * l, dim, sd, ld);
+        if (k == l) v += eps * eps;
+        K[t] = v;
+    }
+    __syncthreads();
+}
+
+// LikelihoodKOH::giveLogLikelihood (statX/infer/LikelihoodKOH.ipp:75-120)
+// work: 2*ns*ns + ns*n_o doubles per batch item
+__global__ void __launch_bounds__(1024) k_koh_loglik(int ns, int n_o, const double *__restrict__ mean,
+                                                     const double *__restrict__ Cs, const double *__restrict__ xs,
+                                                     int dim, const double *__restrict__ Y, sfc_hparams_t hp,
+                                                     double *__restrict__ work, double *out, int *info)
+{
+    double *C = work;
+    double *D = work + (int64_t)ns * ns;
+    mismatch_cov(ns, xs, dim, hp.mismatch_sigma, hp.mismatch_length, hp.mismatch_sensor_eps, C);
+    const double rho = hp.rho;
+    for (int64_t t = threadIdx.x; t < (int64_t)ns * ns; t += blockDim.x) C[t] += rho * rho * Cs[t];
+    for (int64_t t = threadIdx.x; t < (int64_t)ns * n_o; t += blockDim.x) D[t] = Y[t] - rho * mean[t / n_o];
+    __syncthreads();
+    chol_lower(ns, C, ns, info);
+    if (*info) {
+        if (threadIdx.x == 0) *out = NAN;
+        return;
+    }
+    trsm_lower(ns, C, ns, n_o, D, n_o);
+    __shared__ double red[1024];
+    double ld = 0.0;
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) ld += log(C[(int64_t)k * ns + k]);
+    red[threadIdx.x] = ld;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    const double sumlog = red[0];
+    __syncthreads();
+    // quadratic terms per reading
+    double t3 = 0.0;
+    bool ok = true;
+    for (int r = 0; r < n_o; ++r) {
+        double q = 0.0;
+        for (int k = threadIdx.x; k < ns; k += blockDim.x) q += D[(int64_t)k * n_o + r] * D[(int64_t)k * n_o + r];
+        red[threadIdx.x] = q;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        const double comp = -0.5 * red[0];
+        if (!(comp < 0.0)) ok = false;
+        t3 += comp;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double t1 = -0.5 * ns * log(2. * M_PI);
+        const double t2 = -0.5 * (2. * sumlog);
+        *out = n_o * (t1 + t2) + t3;
+        if (!ok) *info = -1;
+    }
+}
+
+// LikelihoodKOH::giveProjFEconditionedData (LikelihoodKOH.ipp:311-361):
+// Sigma = (rho^2 n_o Ks^-1 + Cs^-1)^-1, m = Sigma (rho Ks^-1 sum_k y_k + Cs^-1 mean)
+// work: 5*ns*ns + 3*ns doubles
+__global__ void __launch_bounds__(1024) k_koh_proj(int ns, int n_o, const double *__restrict__ mean,
+                                                   const double *__restrict__ Cs, const double *__restrict__ xs, int dim,
+                                                   const double *__restrict__ Y, sfc_hparams_t hp,
+                                                   double *__restrict__ work, double *post_mean, double *post_cov,
+                                                   int *info)
+{
+    const int64_t nn = (int64_t)ns * ns;
+    double *Ks = work, *L = work + nn, *Ksi = work + 2 * nn, *Cui = work + 3 * nn, *Msum = work + 4 * nn;
+    double *ysum = work + 5 * nn, *v = ysum + ns;
+    mismatch_cov(ns, xs, dim, hp.mismatch_sigma, hp.mismatch_length, hp.mismatch_sensor_eps, Ks);
+    spd_inverse(ns, Ks, L, Ksi, info);
+    if (*info) return;
+    __syncthreads();
+    spd_inverse(ns, Cs, L, Cui, info);
+    if (*info) {
+        if (threadIdx.x == 0) *info += 100000;
+        return;
+    }
+    const double rho = hp.rho;
+    for (int64_t t = threadIdx.x; t < nn; t += blockDim.x) Msum[t] = rho * rho * n_o * Ksi[t] + Cui[t];
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        double s = 0;
+        for (int r = 0; r < n_o; ++r) s += Y[(int64_t)k * n_o + r];
+        ysum[k] = s;
+    }
+    __syncthreads();
+    spd_inverse(ns, Msum, L, post_cov, info);
+    if (*info) {
+        if (threadIdx.x == 0) *info += 200000;
+        return;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        double s = 0;
+        for (int j = 0; j < ns; ++j) s += rho * Ksi[(int64_t)k * ns + j] * ysum[j] + Cui[(int64_t)k * ns + j] * mean[j];
+        v[k] = s;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+        double s = 0;
+        for (int j = 0; j < ns; ++j) s += post_cov[(int64_t)k * ns + j] * v[j];
+        post_mean[k] = s;
+    }
+}
+
+// SPD inverse of one n x n matrix (used by the Woodbury form)
+__global__ void __launch_bounds__(1024) k_spd_inverse(int n, const double *A, double *L, double *Ainv, int *info)
+{
+    spd_inverse(n, A, L, Ainv, info);
+}
+
+__global__ void k_mismatch(int ns, const double *xs, int dim, sfc_hparams_t hp, double *K)
+{
+    mismatch_cov(ns, xs, dim, hp.mismatch_sigma, hp.mismatch_length, hp.mismatch_sensor_eps, K);
+}
+
+__global__ void k_add_scaled(double *__restrict__ y, const double *__restrict__ x, double a, int64_t n)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        y[t] += a * x[t];
+}
+
+__global__ void k_lincomb(double *__restrict__ y, double a, const double *__restrict__ x, double b, int64_t n)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+        y[t] = a * x[t] + b * y[t];
+}
+
+__global__ void k_identity_minus(double *__restrict__ D, int64_t n)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n; t += (int64_t)gridDim.x * blockDim.x)
+        D[t] = ((t / n) == (t % n) ? 1.0 : 0.0) - D[t];
+}
+
+__global__ void k_rowsum(const double *__restrict__ Y, int64_t ns, int n_o, double *__restrict__ out)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < ns; k += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int r = 0; r < n_o; ++r) s += Y[k * n_o + r];
+        out[k] = s;
+    }
+}
+
+void gemm(sfc_ctx *ctx, int ta, int tb, int64_t M, int64_t N, int64_t K, double alpha, const double *A, int64_t lda,
+          const double *B, int64_t ldb, double beta, double *C, int64_t ldc)
+{
+    dim3 g((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
+    k_gemm<<<g, 256, 0, ctx->stream>>>(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    count_launch(ctx);
+}
+
+// 1-D SE correlation factor along one grid axis: exp(-d^2/(2 l^2))
+std::vector<double> se_axis(const std::vector<double> &x, double length)
+{
+    const int n = (int)x.size();
+    std::vector<double> K((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+            const double d = x[i] - x[j];
+            K[(size_t)i * n + j] = std::exp(-(d * d) / (2. * length * length));
+        }
+    return K;
+}
+
+}  // namespace
+
+// T = K W (per component); W, T, tmp: num_dofs x ns device arrays
+static void kernel_times(sfc_ctx *ctx, const sfc_mesh *m, double sigma, double length, const double *W, double *T,
+                         int64_t ns, double *tmp)
+{
+    const int64_t nodes = m->num_nodes;
+    const int dof = m->dof;
+    if (m->is_grid) {
+        // K = sigma^2 Kz (x) Ky (x) Kx ; applied axis by axis, ping-ponging
+        // between T and tmp
+        const int nax = m->dim;
+        std::vector<DBuf<double>> dK(nax);
+        for (int a = 0; a < nax; ++a) {
+            std::vector<double> Kd = se_axis(m->gaxis[a], length);
+            if (a == 0)
+                for (double &v : Kd) v *= sigma * sigma;
+            upload(ctx, dK[a], Kd.data(), Kd.size());
+        }
+        for (int c = 0; c < dof; ++c) {
+            const double *src = W;
+            double *bufs[2] = {T, tmp};
+            int64_t sd = 1;
+            int cur = 0;
+            for (int a = 0; a < nax; ++a) {
+                const int nd = m->gn[a];
+                double *dst = bufs[cur];
+                k_kron_axis<<<grid_for(nodes * ns, 256), 256, (size_t)nd * nd * 8, ctx->stream>>>(
+                    dK[a].p, nd, sd, nodes, dof, c, ns, src, dst);
+                count_launch(ctx);
+                src = dst;
+                cur ^= 1;
+                sd *= nd;
+            }
+            if (src != T)  // strided copy of this component's rows back into T
+                SFC_CK(cudaMemcpy2DAsync(T + (int64_t)c * ns, (size_t)dof * ns * 8, src + (int64_t)c * ns,
+                                         (size_t)dof * ns * 8, (size_t)ns * 8, (size_t)nodes, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+        }
+        SFC_CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+        const size_t smem = (size_t)(kTI * kTJ + kTJ * ns) * 8;
+        SFC_REQUIRE(ns <= 256, "dense forcing covariance supports at most 256 projection rows");
+        SFC_CK(cudaFuncSetAttribute(k_kw_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        for (int c = 0; c < dof; ++c) {
+            k_kw_dense<<<(unsigned)((nodes + kTI - 1) / kTI), 256, smem, ctx->stream>>>(m->coords.p, nodes, m->dim, dof,
+                                                                                     c, ns, W, T, sigma, length);
+            count_launch(ctx);
+        }
+    }
+}
+
+// C (ns x ns) = W^T (K W) with W = diag(phibar) X, X: num_dofs x ns (device)
+static void projected_covar(sfc_ctx *ctx, const sfc_covar_forcing *cf, double sigma, double length, const double *X,
+                            int64_t ns, double *C, DBuf<double> &work)
+{
+    const sfc_mesh *m = cf->mesh;
+    const int64_t N = cf->num_dofs;
+    work.reserve((size_t)3 * N * ns);
+    double *W = work.p, *T = W + N * ns, *tmpp = T + N * ns;
+    k_scale_rows<<<grid_for(N * ns, 256), 256, 0, ctx->stream>>>(X, cf->phibar.p, N, ns, W);
+    count_launch(ctx);
+    kernel_times(ctx, m, sigma, length, W, T, ns, tmpp);
+    SFC_CK(cudaMemsetAsync(C, 0, ns * ns * 8, ctx->stream));
+    const int64_t tiles = ((ns + 63) / 64) * ((ns + 63) / 64);
+    int64_t splits = std::max<int64_t>(1, (ctx->sm_count * 4) / tiles);
+    int64_t rows = (N + splits - 1) / splits;
+    rows = ((rows + 15) / 16) * 16;
+    splits = (N + rows - 1) / rows;
+    dim3 g((unsigned)splits, (unsigned)((ns + 63) / 64), (unsigned)((ns + 63) / 64));
+    k_atb<<<g, 256, 0, ctx->stream>>>(W, T, N, ns, ns, rows, 1.0, C);
+    count_launch(ctx);
+}
+
+void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp)
+{
+    sfc_system *s = fg->sys;
+    sfc_ctx *ctx = fg->ctx;
+    const int64_t N = s->N, ns = fg->ns;
+    SFC_REQUIRE(ns > 0, "projection matrix not set");
+    SFC_REQUIRE(fg->cf->num_dofs == N, "covariance and system sizes differ");
+    // right-hand sides P^T (N x ns)
+    DBuf<double> B;
+    B.alloc(N * ns);
+    SFC_CK(cudaMemsetAsync(B.p, 0, N * ns * 8, ctx->stream));
+    k_scatter_pt<<<grid_for(ns, 128), 128, 0, ctx->stream>>>(fg->d_p_ptr.p, fg->d_p_idx.p, fg->d_p_val.p, ns, B.p);
+    count_launch(ctx);
+    // R^T = A^-T P^T : one block adjoint solve (solveSystemTranspose per row
+    // in the reference, ForwardGaussRHS.hpp:104-112)
+    fg->R.alloc(N * ns);
+    flush_staged(s);
+    solve_block(s, B.p, fg->R.p, (int)ns, (int)ns);
+    transpose_fixup(s, B.p, fg->R.p, (int)ns, (int)ns);
+    // mean = R F (ForwardGaussRHS.hpp:115-124)
+    fg->mean.alloc(ns);
+    k_colsum_dot<<<(unsigned)std::min<int64_t>(ns, 1024), 256, 0, ctx->stream>>>(fg->R.p, s->F.p, N, ns, fg->mean.p);
+    count_launch(ctx);
+    // C_s = R C_f R^T + (sigma_f reg)^2 P P^T  (ForwardGaussRHS.hpp:128-136)
+    fg->cov.alloc(ns * ns);
+    projected_covar(ctx, fg->cf, hp->forcing_sigma, hp->forcing_length, fg->R.p, ns, fg->cov.p, fg->work);
+    const double add = hp->forcing_sigma * fg->reg;
+    k_add_scaled<<<grid_for(ns * ns, 256), 256, 0, ctx->stream>>>(fg->cov.p, fg->d_ppt.p, add * add, ns * ns);
+    count_launch(ctx);
+    SFC_CK(cudaStreamSynchronize(ctx->stream));
+    fg->valid = true;
+}
+
+void covar_projected_host(sfc_covar_forcing *cf, const sfc_hparams_t *hp, const double *M, int64_t rows, double *out)
+{
+    sfc_ctx *ctx = cf->ctx;
+    const int64_t N = cf->num_dofs;
+    // X = M^T (N x rows)
+    std::vector<double> Xt((size_t)N * rows);
+    for (int64_t a = 0; a < rows; ++a)
+        for (int64_t i = 0; i < N; ++i) Xt[(size_t)i * rows + a] = M[(size_t)a * N + i];
+    DBuf<double> X, C, work;
+    upload(ctx, X, Xt.data(), Xt.size());
+    C.alloc(rows * rows);
+    projected_covar(ctx, cf, hp->forcing_sigma, hp->forcing_length, X.p, rows, C.p, work);
+    download(ctx, out, C.p, rows * rows);
+}
+
+void koh_loglik(sfc_koh *k, const sfc_hparams_t *hp, double *out)
+{
+    sfc_ctx *ctx = k->ctx;
+    sfc_forward_gauss *fg = k->fg;
+    SFC_REQUIRE(fg->valid, "forward model not updated");
+    SFC_REQUIRE(k->n_o > 0, "sensor values not set");
+    const int ns = (int)k->ns;
+    k->work.reserve((size_t)2 * ns * ns + (size_t)ns * k->n_o + 16);
+    DBuf<double> d;
+    DBuf<int> info;
+    d.alloc(1);
+    info.alloc(1);
+    k_koh_loglik<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim, k->Y.p, *hp,
+                                              k->work.p, d.p, info.p);
+    count_launch(ctx);
+    int hi = 0;
+    download(ctx, &hi, info.p, 1);
+    if (hi > 0) fail(SFC_ERR_NOT_SPD, "total covariance is not positive definite (LLT failed)");
+    if (hi < 0) fail(SFC_ERR_BAD_ARG, "non-negative quadratic term in the log-likelihood");
+    download(ctx, out, d.p, 1);
+}
+
+void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
+{
+    sfc_ctx *ctx = k->ctx;
+    sfc_forward_gauss *fg = k->fg;
+    SFC_REQUIRE(fg->valid, "forward model not updated");
+    SFC_REQUIRE(k->n_o > 0, "sensor values not set");
+    const int ns = (int)k->ns;
+    k->work.reserve((size_t)5 * ns * ns + 3 * (size_t)ns + 16);
+    DBuf<double> pm, pc;
+    DBuf<int> info;
+    pm.alloc(ns);
+    pc.alloc((size_t)ns * ns);
+    info.alloc(1);
+    k_koh_proj<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim, k->Y.p, *hp,
+                                            k->work.p, pm.p, pc.p, info.p);
+    count_launch(ctx);
+    int hi = 0;
+    download(ctx, &hi, info.p, 1);
+    if (hi) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible (code " + std::to_string(hi) + ")");
+    if (mean) download(ctx, mean, pm.p, ns);
+    if (cov) download(ctx, cov, pc.p, (size_t)ns * ns);
+}
+
+// giveFEconditionedDataWoodbury (LikelihoodKOH.ipp:442-508)
+void koh_woodbury(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
+{
+    sfc_ctx *ctx = k->ctx;
+    sfc_forward_gauss *fg = k->fg;
+    sfc_system *s = fg->sys;
+    SFC_REQUIRE(fg->valid, "forward model not updated");
+    SFC_REQUIRE(k->n_o > 0, "sensor values not set");
+    const int64_t N = s->N, ns = fg->ns;
+    SFC_REQUIRE(N <= 8192, "full-field Woodbury posterior limited to 8192 dofs");
+    const double rho = hp->rho;
+    const int n_o = k->n_o;
+    // K_s, K_s^-1, S = K_s/(rho^2 n_o) + C_s, S^-1
+    DBuf<double> Ks, Ksi, L, Sm, Si, ysum, P;
+    DBuf<int> info;
+    Ks.alloc(ns * ns);
+    Ksi.alloc(ns * ns);
+    L.alloc(std::max<int64_t>(ns * ns, 1));
+    Sm.alloc(ns * ns);
+    Si.alloc(ns * ns);
+    ysum.alloc(ns);
+    info.alloc(1);
+    SFC_CK(cudaMemsetAsync(info.p, 0, sizeof(int), ctx->stream));
+    k_mismatch<<<1, 1024, 0, ctx->stream>>>((int)ns, k->sensor_coords.p, k->dim, *hp, Ks.p);
+    k_spd_inverse<<<1, 1024, 0, ctx->stream>>>((int)ns, Ks.p, L.p, Ksi.p, info.p);
+    SFC_CK(cudaMemcpyAsync(Sm.p, fg->cov.p, ns * ns * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    k_add_scaled<<<grid_for(ns * ns, 256), 256, 0, ctx->stream>>>(Sm.p, Ks.p, 1.0 / (rho * rho * n_o), ns * ns);
+    k_spd_inverse<<<1, 1024, 0, ctx->stream>>>((int)ns, Sm.p, L.p, Si.p, info.p);
+    k_rowsum<<<1, 256, 0, ctx->stream>>>(k->Y.p, ns, n_o, ysum.p);
+    count_launch(ctx, 5);
+    int hi = 0;
+    download(ctx, &hi, info.p, 1);
+    if (hi) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible");
+    // dense P (ns x N)
+    std::vector<double> hP((size_t)ns * N, 0.0);
+    for (int64_t a = 0; a < ns; ++a)
+        for (int64_t t = fg->p_ptr[a]; t < fg->p_ptr[a + 1]; ++t) hP[(size_t)a * N + fg->p_idx[t]] += fg->p_val[t];
+    upload(ctx, P, hP.data(), hP.size());
+    // unprojected prior: R_I^T = A^-T I (N adjoint solves), C_u, u-bar
+    DBuf<double> I, RI, Cu, ubar;
+    std::vector<double> hI((size_t)N * N, 0.0);
+    for (int64_t i = 0; i < N; ++i) hI[(size_t)i * N + i] = 1.0;
+    upload(ctx, I, hI.data(), hI.size());
+    RI.alloc(N * N);
+    solve_block(s, I.p, RI.p, (int)N, (int)N);
+    transpose_fixup(s, I.p, RI.p, (int)N, (int)N);
+    ubar.alloc(N);
+    k_colsum_dot<<<(unsigned)std::min<int64_t>(N, 1024), 256, 0, ctx->stream>>>(RI.p, s->F.p, N, N, ubar.p);
+    count_launch(ctx);
+    Cu.alloc(N * N);
+    DBuf<double> work;
+    projected_covar(ctx, fg->cf, hp->forcing_sigma, hp->forcing_length, RI.p, N, Cu.p, work);
+    const double add = hp->forcing_sigma * fg->reg;
+    // + (sigma_f reg)^2 I  (P = I in the unprojected update)
+    k_add_scaled<<<grid_for(N * N, 256), 256, 0, ctx->stream>>>(Cu.p, I.p, add * add, N * N);
+    count_launch(ctx);
+    // G = C_u P^T (N x ns); H = G S^-1 (N x ns); D = I - H P (N x N)
+    DBuf<double> G, H, D, t1, t2;
+    G.alloc(N * ns);
+    H.alloc(N * ns);
+    D.alloc(N * N);
+    gemm(ctx, 0, 1, N, ns, N, 1.0, Cu.p, N, P.p, N, 0.0, G.p, ns);
+    gemm(ctx, 0, 0, N, ns, ns, 1.0, G.p, ns, Si.p, ns, 0.0, H.p, ns);
+    gemm(ctx, 0, 0, N, N, ns, 1.0, H.p, ns, P.p, N, 0.0, D.p, N);
+    k_identity_minus<<<grid_for(N * N, 256), 256, 0, ctx->stream>>>(D.p, N);
+    count_launch(ctx);
+    // vecA = rho G K_s^-1 ysum ; mean = D (vecA + ubar)
+    t1.alloc(ns);
+    t2.alloc(N);
+    gemm(ctx, 0, 0, ns, 1, ns, 1.0, Ksi.p, ns, ysum.p, 1, 0.0, t1.p, 1);
+    SFC_CK(cudaMemcpyAsync(t2.p, ubar.p, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    gemm(ctx, 0, 0, N, 1, ns, rho, G.p, ns, t1.p, 1, 1.0, t2.p, 1);
+    DBuf<double> pm;
+    pm.alloc(N);
+    gemm(ctx, 0, 0, N, 1, N, 1.0, D.p, N, t2.p, 1, 0.0, pm.p, 1);
+    if (mean) download(ctx, mean, pm.p, N);
+    if (cov) {
+        DBuf<double> pc;
+        pc.alloc(N * N);
+        gemm(ctx, 0, 0, N, N, N, 1.0, D.p, N, Cu.p, N, 0.0, pc.p, N);
+        download(ctx, cov, pc.p, N * N);
+    }
+    SFC_CK(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace sfc
