@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""statFEM posterior solves/s on B200.
+
+Default workload (the configuration the headline metric is quoted on that
+fits one GPU): 3-D linear elasticity statFEM on the unit cube, 48^3 trilinear
+hex8 elements with 2x2x2 Gauss quadrature (352,947 dofs, 27,437,625
+nonzeros), Young's modulus lognormal (log-GP squared-exponential sigma 0.3,
+length 0.25, sampled exactly on the element-centre grid), nu = 0.3, face x=0
+clamped, body force mean (0,0,-1) with a squared-exponential GP
+(sigma_f 0.05, length 0.3), 256 seeded sensors (one displacement component
+each, cycling x/y/z), sensor noise 1e-4, relative residual 1e-8.  Synthetic,
+seeded inputs; no dataset is involved.
+
+One step = one posterior solve on the GPU: assemble A and F, apply the
+Dirichlet constraints, solve A u = F, the 256 adjoint solves A^T R^T = P^T
+(one block solve), C_s = R C_f R^T + (sigma_f reg)^2 P P^T, the KOH
+log-likelihood and the posterior mean / covariance at the sensors.
+
+`--impl reference` times the CPU path instead (the oracle's C restatement
+of the reference's assembly and a CPU FP64 Jacobi-PCG standing in for the
+reference's Eigen SparseLU, which cannot run at this size), on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from statfem_b200 import meshgen as mg  # noqa: E402
+
+HP = {"forcing.sigma": 0.05, "forcing.length": 0.3, "rho": 1.0, "mismatch.sigma": 0.0,
+      "mismatch.length": 0.25, "mismatch.sensorEps": 1e-4}
+REG = 0.001
+
+
+def make_workload(config, seed):
+    rng = np.random.default_rng(seed)
+    if config == "c2":
+        n, ns = 48, 256
+        mesh = mg.unit_cube_hex(n, mg.HEX8_ELASTIC)
+        ax = mg.cell_centre_axes(n)
+        g = mg.se_field_tensor(rng, [ax, ax, ax], 0.3, 0.25)
+        coeff = np.exp(g)
+        bc = mg.dirichlet_dofs(mesh, "x0")
+        pts = mg.interior_points(rng, ns, 3, margin=0.02)
+        comps = np.arange(ns) % 3
+        P = mg.projection_matrix(mesh, pts, comps)
+        f = np.array([0.0, 0.0, -1.0])
+        hp = dict(HP)
+        desc = "3-D elasticity statFEM, 48^3 hex8 (352,947 dofs), 256 sensors, rel. residual 1e-8"
+        qps = 8
+    elif config == "c1":
+        n, ns = 64, 16
+        mesh = mg.unit_square_tri(n)
+        coeff = np.ones(mesh.num_elems)
+        bc = mg.dirichlet_dofs(mesh, "all")
+        pts = mg.interior_points(rng, ns, 2, margin=0.02)
+        P = mg.projection_matrix(mesh, pts)
+        f = np.array([1.0])
+        hp = dict(HP, **{"forcing.sigma": 0.1, "forcing.length": 0.2, "mismatch.sensorEps": 1e-3})
+        desc = "2-D Poisson statFEM, 64^2 cells x 2 P1 triangles (4,225 dofs), 16 sensors, rel. residual 1e-8"
+        qps = 3
+    else:
+        raise SystemExit("unknown config " + config)
+    return dict(mesh=mesh, coeff=coeff, bc=bc, pts=pts, P=P, f=f, hp=hp, desc=desc, qps=qps, ns=ns, rng=rng)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cuda_sync(ws):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+    except ImportError:
+        pass
+
+
+# ---------------------------------------------------------------------------
+# our GPU arm
+# ---------------------------------------------------------------------------
+class GpuStatFEM:
+    def __init__(self, wl, device, method):
+        from statfem_b200 import api
+        self.api = api
+        self.wl = wl
+        self.ctx = api.Context(device)
+        m = wl["mesh"]
+        self.gm = api.Mesh(self.ctx, m.kind, wl["qps"], m.coords, m.conn)
+        self.gm.set_coefficients(wl["coeff"])
+        self.s = api.SystemSolveCuda(self.ctx, m.num_dofs)
+        self.s.set_options(method=method, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=64,
+                           check_every=32)
+        self.cf = api.CovarianceForcing(self.ctx, self.gm)
+        self.cf.applyConstraints(wl["bc"])
+        self.fg = api.ForwardGaussRHS(self.s, self.cf, REG)
+        self.fg.setProjectionMatrix(wl["P"])
+        self.bc_vals = np.zeros(len(wl["bc"]))
+        self.koh = api.LikelihoodKOH(self.fg, wl["pts"])
+        # observations drawn from the prior plus noise (giveTypicalReadings),
+        # generated once with this GPU pipeline
+        self.prior_step()
+        mean, cov = self.fg.giveProjectedMeanU(), self.fg.giveProjectedCovarU()
+        hp = wl["hp"]
+        ns = wl["ns"]
+        C = hp["mismatch.sensorEps"] ** 2 * np.eye(ns) + hp["rho"] ** 2 * cov
+        L = np.linalg.cholesky(C)
+        self.Y = hp["rho"] * mean[:, None] + L @ wl["rng"].standard_normal((ns, 1))
+        self.koh.setSensorValues(self.Y)
+
+    def prior_step(self):
+        wl = self.wl
+        self.s.assemble(self.gm)
+        self.s.clearRhs()
+        self.s.assemble_load(self.gm, wl["f"])
+        self.s.applyConstraints((wl["bc"], self.bc_vals))
+        self.s.solveSystem()
+        self.fg.updateSolution(wl["hp"])
+
+    def step(self, e2e=False):
+        """One posterior solve.  e2e: the step's inputs come from host memory
+        (coefficient field, sensor values) and the results go back to it."""
+        if e2e:
+            self.gm.set_coefficients(self.wl["coeff"])
+            self.koh.setSensorValues(self.Y)
+        self.prior_step()
+        ll = self.koh.giveLogLikelihood(self.wl["hp"])
+        pm, pc = self.koh.giveProjFEconditionedData(self.wl["hp"])
+        return ll, pm, pc
+
+
+def run_ours(args, ws, rank, local):
+    from statfem_b200 import api
+    method = api.SFC_SOLVER_PCG_MIXED if args.method == "mixed" else api.SFC_SOLVER_PCG_FP64
+    wl = make_workload(args.config, seed=1234 + rank)
+    g = GpuStatFEM(wl, local, method)
+    ctx = g.ctx
+    for _ in range(args.warmup):
+        g.step()
+    g.s.solveSystem()
+    stats_fwd = g.s.last_stats()
+    g.fwd_iters = stats_fwd["iterations"]
+    # ---- device-resident timed region ----
+    barrier(ws)
+    cuda_sync(ws)
+    ctx.synchronize()
+    l0 = ctx.kernel_launches()
+    ctx.set_profiling(True)
+    with ClockSampler(local) as clk:
+        ctx.mark(0)
+        for _ in range(args.steps):
+            ll, pm, pc = g.step()
+        ctx.mark(1)
+        ctx.synchronize()
+    ctx.set_profiling(False)
+    cuda_sync(ws)
+    barrier(ws)
+    ms = ctx.marker_ms(0, 1)
+    launches = ctx.kernel_launches() - l0
+    prof = ctx.profile_report()
+    block_stats = g.s.last_stats()
+    ms_max = max_over_ranks(ws, ms)
+    value = ws * args.steps / (ms_max / 1e3)
+    # ---- end-to-end through the public API with host buffers ----
+    barrier(ws)
+    cuda_sync(ws)
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    ctx.mark(2)
+    e2e_steps = max(1, args.steps)
+    for _ in range(e2e_steps):
+        g.step(e2e=True)
+    ctx.mark(3)
+    ctx.synchronize()
+    e2e_wall = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(ws, ctx.marker_ms(2, 3))
+    ns = wl["ns"]
+    h2d = wl["coeff"].nbytes + g.Y.nbytes + wl["bc"].nbytes + g.bc_vals.nbytes
+    d2h = 8 * (1 + ns + ns * ns)
+    # ---- roofline of the dominant kernel ----
+    peak, peak_kind = peaks()
+    top = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    if top:
+        name, (cnt, tms, tbytes) = top
+        per_launch_bytes = tbytes / cnt
+        per_launch_s = tms / 1e3 / cnt
+        achieved = per_launch_bytes / per_launch_s / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                "bytes_per_launch": per_launch_bytes, "avg_launch_us": round(per_launch_s * 1e6, 2),
+                "launches": cnt, "share_of_step": round(tms / ms, 4)}
+    out = {
+        "metric": "posterior solves/s at rel. residual 1e-8 (learned+batched vs plain PCG, 1xB200)",
+        "value": round(value, 4), "unit": "posterior solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["desc"], "method": "mixed block Jacobi-PCG" if args.method == "mixed"
+                   else "plain FP64 Jacobi-PCG", "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (matrix 220+ MB)"},
+        "e2e": {"value": round(ws * e2e_steps / (e2e_ms / 1e3), 4), "unit": "posterior solves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "wall_s": round(e2e_wall, 3)},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "kernels": {k: {"launches": v[0], "ms": round(v[1], 3), "GBps": round(v[2] / max(v[1], 1e-9) / 1e6, 1)}
+                    for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "solver": {"forward": stats_fwd, "adjoint_block": block_stats},
+        "clocks": clk.summary(),
+        "loglik": ll,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args, wl, g, sample_iters=args.cpu_iters)
+    if rank == 0:
+        print(json.dumps(out))
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (oracle port)
+# ---------------------------------------------------------------------------
+def cpu_solve_rate(wl, rp, col, val, mask, F, iters_per_solve, sample_iters):
+    """Posterior solves/s of the CPU path, from a bounded sample: the time of
+    `sample_iters` FP64 Jacobi-PCG iterations on the full matrix, times
+    (1 + ns) solves of `iters_per_solve` iterations."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    O.pcg(rp, col, val, mask, F, tol=1e-300, max_iter=sample_iters)
+    dt = time.perf_counter() - t0
+    per_iter = dt / sample_iters
+    per_posterior = (1 + wl["ns"]) * iters_per_solve * per_iter
+    return 1.0 / per_posterior, per_iter
+
+
+def cpu_baseline(args, wl, g, sample_iters):
+    from oracle import oracle as O
+    rp, col, val = g.s.get_csr()
+    F = g.s.giveForce()
+    mask = np.zeros(len(rp) - 1, dtype=np.uint8)
+    mask[wl["bc"]] = 1
+    # iterations to 1e-8 of the same FP64 Jacobi-PCG, taken from the GPU
+    # forward solve on the identical matrix (avoids a minutes-long CPU solve)
+    its = int(g.fwd_iters)
+    rate, per_iter = cpu_solve_rate(wl, rp, col, val, mask, F, its, sample_iters)
+    threads = 1  # the C port is single-threaded, like the reference path
+    return {"value": round(rate, 6), "unit": "posterior solves/s", "cores": threads, "kind": "port",
+            "sample": "oracle C FP64 Jacobi-PCG on the same assembled matrix: %d iterations timed "
+                      "(%.2f ms/iter), x (1+%d) solves x %d iterations/solve (forward solve to 1e-8 on "
+                      "the CPU); assembly and covariance not counted" % (sample_iters, per_iter * 1e3,
+                                                                         wl["ns"], its)}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    wl = make_workload(args.config, seed=1234)
+    mesh = wl["mesh"]
+    t0 = time.perf_counter()
+    rp, col, val, F = O.fem(mesh, wl["qps"], wl["f"], wl["bc"], coeff=wl["coeff"], nu=0.3)
+    t_asm = time.perf_counter() - t0
+    mask = np.zeros(mesh.num_dofs, dtype=np.uint8)
+    mask[wl["bc"]] = 1
+    x, its = O.pcg(rp, col, val, mask, F, tol=1e-8, max_iter=60000)
+    rates = []
+    for k in range(args.warmup + args.steps):
+        r, per_iter = cpu_solve_rate(wl, rp, col, val, mask, F, its, args.cpu_iters)
+        if k >= args.warmup:
+            rates.append(r)
+    value = float(np.mean(rates))
+    threads = 1  # the C port is single-threaded, like the reference path
+    out = {"impl": "reference", "metric": "posterior solves/s at rel. residual 1e-8 (learned+batched vs plain "
+           "PCG, 1xB200)", "value": round(value, 6), "unit": "posterior solves/s", "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+           "config": {"workload": wl["desc"], "method": "CPU FP64 Jacobi-PCG (oracle port)"},
+           "cpu_baseline": {"value": round(value, 6), "unit": "posterior solves/s", "cores": threads,
+                            "kind": "port",
+                            "sample": "per step: %d PCG iterations timed on the full matrix, scaled to (1+%d) "
+                                      "solves x %d iterations; oracle assembly took %.1f s (not counted)"
+                                      % (args.cpu_iters, wl["ns"], its, t_asm)},
+           "e2e": {"value": round(value, 6), "unit": "posterior solves/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cpu-iters", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

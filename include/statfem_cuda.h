@@ -103,6 +103,14 @@ int32_t sfc_ctx_kernel_launches(const sfc_ctx_t *ctx, int64_t *count);
 int32_t sfc_ctx_mark(sfc_ctx_t *ctx, int32_t slot);
 int32_t sfc_ctx_marker_ms(sfc_ctx_t *ctx, int32_t slot_begin, int32_t slot_end, double *ms);
 
+/* Kernel timing (no reference counterpart; the reference has no tracing):
+ * when enabled, the hot kernels are bracketed by CUDA events on the context
+ * stream.  The report writes one line per kernel name,
+ * "name launches total_ms algorithmic_bytes", into buf (NUL-terminated) and
+ * clears the records. */
+int32_t sfc_ctx_set_profiling(sfc_ctx_t *ctx, int32_t enable);
+int32_t sfc_ctx_profile_report(sfc_ctx_t *ctx, char *buf, int64_t buflen);
+
 /* ---- mesh -------------------------------------------------------------- */
 /* Replaces corlib::Mesh<Element>(std::istream& smf) (corlib/Mesh.ipp:63-102)
  * plus Node::numberDOFs (del2/fem/NodePotential.hpp:65,

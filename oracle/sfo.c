@@ -591,6 +591,7 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
     int it;
     for (it = 1; it <= max_iter; ++it) {
         double pq = 0, rr = 0, rz2 = 0;
+#pragma omp parallel for reduction(+ : pq) schedule(static)
         for (int64_t i = 0; i < N; ++i) {
             double acc = 0;
             if (mask[i]) {
@@ -603,6 +604,7 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
             pq += p[i] * acc;
         }
         double alpha = rz / pq;
+#pragma omp parallel for reduction(+ : rr, rz2) schedule(static)
         for (int64_t i = 0; i < N; ++i) {
             x[i] += alpha * p[i];
             r[i] -= alpha * q[i];
@@ -613,6 +615,7 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
         if (rr <= tol * tol * bb) break;
         double beta = rz2 / rz;
         rz = rz2;
+#pragma omp parallel for schedule(static)
         for (int64_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
     }
     free(dinv);

@@ -84,6 +84,8 @@ SIGNATURES = {
     "sfc_ctx_kernel_launches": (_i32, [_vp, _i64p]),
     "sfc_ctx_mark": (_i32, [_vp, _i32]),
     "sfc_ctx_marker_ms": (_i32, [_vp, _i32, _i32, _dp]),
+    "sfc_ctx_set_profiling": (_i32, [_vp, _i32]),
+    "sfc_ctx_profile_report": (_i32, [_vp, ctypes.c_char_p, _i64]),
     "sfc_mesh_create": (_i32, [_vp, _i32, _i32, _dp, _i64, _u32p, _i64, ctypes.POINTER(_vp)]),
     "sfc_mesh_destroy": (_i32, [_vp]),
     "sfc_mesh_set_coefficients": (_i32, [_vp, _dp, _d, _d]),
@@ -183,6 +185,19 @@ class Context:
         v = ctypes.c_double()
         self.check(self.lib.sfc_ctx_marker_ms(self.h, a, b, ctypes.byref(v)))
         return v.value
+
+    def set_profiling(self, enable=True):
+        self.check(self.lib.sfc_ctx_set_profiling(self.h, int(bool(enable))))
+
+    def profile_report(self):
+        """{kernel name: (launches, total_ms, algorithmic_bytes)}; clears the records."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.check(self.lib.sfc_ctx_profile_report(self.h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, n, ms, b = line.split()
+            out[name] = (int(n), float(ms), float(b))
+        return out
 
     def close(self):
         if getattr(self, "h", None):

@@ -3,6 +3,7 @@
 // status code plus a message stored on the context (the reference aborts via
 // FTL_VERIFY instead, corlib/verify.hpp:61-70).
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -97,6 +98,7 @@ int32_t sfc_ctx_destroy(sfc_ctx_t *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto &e : ctx->marks)
         if (e) cudaEventDestroy(e);
+    for (auto &e : ctx->ev_pool) cudaEventDestroy(e);
     ctx->scratch.release();
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -133,6 +135,50 @@ int32_t sfc_ctx_marker_ms(sfc_ctx_t *ctx, int32_t a, int32_t b, double *ms)
         float f = 0;
         SFC_CK(cudaEventElapsedTime(&f, ctx->marks[a], ctx->marks[b]));
         *ms = f;
+    });
+}
+
+int32_t sfc_ctx_set_profiling(sfc_ctx_t *ctx, int32_t enable)
+{
+    if (!ctx) return SFC_ERR_BAD_ARG;
+    ctx->prof = enable != 0;
+    return SFC_OK;
+}
+
+int32_t sfc_ctx_profile_report(sfc_ctx_t *ctx, char *buf, int64_t buflen)
+{
+    if (!ctx || !buf || buflen <= 0) return SFC_ERR_BAD_ARG;
+    return guard(ctx, [&] {
+        SFC_CK(cudaStreamSynchronize(ctx->stream));
+        std::vector<std::string> names;
+        std::vector<double> ms, bytes;
+        std::vector<long> cnt;
+        for (auto &r : ctx->prof_recs) {
+            float f = 0;
+            SFC_CK(cudaEventElapsedTime(&f, r.a, r.b));
+            size_t k = 0;
+            while (k < names.size() && names[k] != r.name) ++k;
+            if (k == names.size()) {
+                names.emplace_back(r.name);
+                ms.push_back(0);
+                bytes.push_back(0);
+                cnt.push_back(0);
+            }
+            ms[k] += f;
+            bytes[k] += r.bytes;
+            cnt[k] += 1;
+        }
+        std::string out;
+        char line[256];
+        for (size_t k = 0; k < names.size(); ++k) {
+            snprintf(line, sizeof line, "%s %ld %.6f %.1f\n", names[k].c_str(), cnt[k], ms[k], bytes[k]);
+            out += line;
+        }
+        ctx->prof_recs.clear();
+        ctx->ev_used = 0;
+        const size_t n = std::min<size_t>(out.size(), (size_t)buflen - 1);
+        std::memcpy(buf, out.data(), n);
+        buf[n] = 0;
     });
 }
 

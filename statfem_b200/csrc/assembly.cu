@@ -795,6 +795,8 @@ void assemble_matrix(sfc_system *s, const sfc_mesh *mc)
     DBuf<int> err;
     err.alloc(1);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
+    ProfScope ps_elem(ctx, "element_matrices",
+                      (double)E * (m->nn * 4 + m->nn * 24 + 8) + (double)E * m->L * m->L * 8);
     switch (m->kind) {
     case SFC_ELEM_LINE2_POISSON:
         k_elem_poisson<1, 2><<<grid_for(E, 128), 128, 0, ctx->stream>>>(m->coords.p, m->conn.p, m->coeff.p, m->quad,
@@ -817,8 +819,12 @@ void assemble_matrix(sfc_system *s, const sfc_mesh *mc)
         fail(SFC_ERR_BAD_ARG, "unknown element kind");
     }
     count_launch(ctx);
-    k_gather<<<grid_for(s->nnz, 256), 256, 0, ctx->stream>>>(m->slot_ptr.p, m->contrib.p, m->ke.p, s->nnz,
-                                                             s->a_ref.p);
+    {
+        const double M = (double)E * m->L * m->L;
+        ProfScope ps(ctx, "csr_gather", (double)s->nnz * 12 + M * 12);
+        k_gather<<<grid_for(s->nnz, 256), 256, 0, ctx->stream>>>(m->slot_ptr.p, m->contrib.p, m->ke.p, s->nnz,
+                                                                 s->a_ref.p);
+    }
     count_launch(ctx);
     int h_err = 0;
     download(ctx, &h_err, err.p, 1);

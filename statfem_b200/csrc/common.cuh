@@ -90,6 +90,16 @@ struct sfc_ctx {
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
     sfc::DBuf<unsigned char> scratch;  // generic device scratch (CUB temp etc.)
+    // kernel timing (off by default): an event pair around each profiled launch
+    bool prof = false;
+    struct ProfRec {
+        const char *name;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<ProfRec> prof_recs;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
 };
 
 namespace sfc {
@@ -99,6 +109,32 @@ inline void count_launch(sfc_ctx *ctx, int n = 1)
     ctx->launches += n;
     SFC_CK(cudaGetLastError());
 }
+
+// Records a CUDA event before and after the launches in its scope when the
+// context's profiling is on; the report sums device time and algorithmic
+// bytes per kernel name.
+struct ProfScope {
+    sfc_ctx *ctx;
+    long idx = -1;
+    ProfScope(sfc_ctx *c, const char *name, double bytes) : ctx(c)
+    {
+        if (!ctx->prof) return;
+        while (ctx->ev_pool.size() < ctx->ev_used + 2) {
+            cudaEvent_t e;
+            SFC_CK(cudaEventCreate(&e));
+            ctx->ev_pool.push_back(e);
+        }
+        cudaEvent_t a = ctx->ev_pool[ctx->ev_used], b = ctx->ev_pool[ctx->ev_used + 1];
+        ctx->ev_used += 2;
+        SFC_CK(cudaEventRecord(a, ctx->stream));
+        idx = (long)ctx->prof_recs.size();
+        ctx->prof_recs.push_back({name, a, b, bytes});
+    }
+    ~ProfScope()
+    {
+        if (idx >= 0) cudaEventRecord(ctx->prof_recs[idx].b, ctx->stream);
+    }
+};
 
 inline unsigned grid_for(int64_t work, int block, int max_blocks = 148 * 32)
 {

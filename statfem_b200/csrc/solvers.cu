@@ -70,16 +70,24 @@ __global__ void __launch_bounds__(kRedThreads) k_spmv64(const int32_t *__restric
 {
     __shared__ double sh[32];
     if (done && *done) return;
-    const int g = threadIdx.x % G;
-    const int64_t groups = (int64_t)gridDim.x * (blockDim.x / G);
+    // The row loop runs over a warp-uniform base so that every lane of a warp
+    // takes the same number of trips and reaches each full-mask shuffle.
+    const int lane = threadIdx.x & 31, g = lane % G;
+    constexpr int kRowsPerWarp = 32 / G;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     double d = 0.0;
-    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G; i < N; i += groups) {
+    for (int64_t base = warp * kRowsPerWarp; base < N; base += stride) {
+        const int64_t i = base + lane / G;
+        const bool valid = i < N;
         double s = 0.0;
-        const int32_t e = rp[i + 1];
-        for (int32_t k = rp[i] + g; k < e; k += G) s += a[k] * x[col[k]];
+        if (valid) {
+            const int32_t e = rp[i + 1];
+            for (int32_t k = rp[i] + g; k < e; k += G) s += a[k] * x[col[k]];
+        }
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, G);
-        if (g == 0) {
+        if (valid && g == 0) {
             y[i] = s;
             d += x[i] * s;
         }
@@ -524,6 +532,7 @@ void launch_spmv64(sfc_system *s, const double *x, double *y, double *dot, const
 {
     const double avg = (double)s->nnz / (double)std::max<int64_t>(s->N, 1);
     sfc_ctx *ctx = s->ctx;
+    ProfScope ps(ctx, "spmv64", (double)s->nnz * 12 + 4.0 * (s->N + 1) + 16.0 * s->N);
     const unsigned grid = (unsigned)(ctx->sm_count * 8);
     if (avg > 24)
         k_spmv64<32><<<grid_for(s->N * 32, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
@@ -565,10 +574,16 @@ PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_i
     PcgResult res{max_iter, false};
     for (it = 0; it < max_iter; ++it) {
         launch_spmv64(s, p, q, pq + it, done);
-        k_pcg_update<<<g, kRedThreads, 0, ctx->stream>>>(x, r, p, q, s->dinv.p, N, pq + it, rz + it, rz + it + 1,
-                                                         rr + it + 1, done, err);
-        k_pcg_pupdate<<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, N, rz + it, rz + it + 1, rr + it + 1, thr,
-                                                          it + 1, done, err);
+        {
+            ProfScope ps(ctx, "pcg_update", 56.0 * N);
+            k_pcg_update<<<g, kRedThreads, 0, ctx->stream>>>(x, r, p, q, s->dinv.p, N, pq + it, rz + it, rz + it + 1,
+                                                             rr + it + 1, done, err);
+        }
+        {
+            ProfScope ps(ctx, "pcg_pupdate", 32.0 * N);
+            k_pcg_pupdate<<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, N, rz + it, rz + it + 1, rr + it + 1,
+                                                              thr, it + 1, done, err);
+        }
         count_launch(ctx, 2);
         if ((it + 1) % check == 0 || it + 1 == max_iter) {
             int hf[2];
@@ -648,6 +663,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         for (int cyc = 0;; ++cyc) {
             if (cyc > 0) {
                 SFC_CK(cudaMemsetAsync(rn2, 0, K * 8, ctx->stream));
+                ProfScope ps(ctx, "resid64", (double)s->nnz * 12 + 4.0 * (N + 1) + 3.0 * N * K * 8);
                 k_resid64<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, x64.p, b64.p, r64.p, N,
                                                           rn2);
                 count_launch(ctx);
@@ -686,11 +702,21 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             int it = 0;
             for (it = 0; it < cap; ++it) {
                 const int64_t o0 = (int64_t)it * K, o1 = (int64_t)(it + 1) * K;
-                k_spmm32<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op32.p, pp, qq, N, pq + o0, stop);
-                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
-                                                            rrs + o0, thr, rz + o1, rrs + o1, stop, err);
-                k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1, thr,
+                {
+                    ProfScope ps(ctx, "spmm32", (double)s->nnz * 8 + 4.0 * (N + 1) + 2.0 * N * K * 4);
+                    k_spmm32<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op32.p, pp, qq, N, pq + o0,
                                                              stop);
+                }
+                {
+                    ProfScope ps(ctx, "bupdate32", 6.0 * N * K * 4 + 4.0 * N);
+                    k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
+                                                                rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+                }
+                {
+                    ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + 4.0 * N);
+                    k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
+                                                                 thr, stop);
+                }
                 count_launch(ctx, 3);
                 if ((it + 1) % check == 0 || it + 1 == cap) {
                     k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + o1, thr, stop);

@@ -508,6 +508,7 @@ static void kernel_times(sfc_ctx *ctx, const sfc_mesh *m, double sigma, double l
             for (int a = 0; a < nax; ++a) {
                 const int nd = m->gn[a];
                 double *dst = bufs[cur];
+                ProfScope ps(ctx, "kron_axis", 2.0 * nodes * ns * 8);
                 k_kron_axis<<<grid_for(nodes * ns, 256), 256, (size_t)nd * nd * 8, ctx->stream>>>(
                     dK[a].p, nd, sd, nodes, dof, c, ns, src, dst);
                 count_launch(ctx);
@@ -551,6 +552,7 @@ static void projected_covar(sfc_ctx *ctx, const sfc_covar_forcing *cf, double si
     rows = ((rows + 15) / 16) * 16;
     splits = (N + rows - 1) / rows;
     dim3 g((unsigned)splits, (unsigned)((ns + 63) / 64), (unsigned)((ns + 63) / 64));
+    ProfScope ps(ctx, "covar_atb", 2.0 * N * ns * 8);
     k_atb<<<g, 256, 0, ctx->stream>>>(W, T, N, ns, ns, rows, 1.0, C);
     count_launch(ctx);
 }
