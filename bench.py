@@ -176,7 +176,7 @@ def cuda_sync(ws):
 # our GPU arm
 # ---------------------------------------------------------------------------
 class GpuStatFEM:
-    def __init__(self, wl, device, method):
+    def __init__(self, wl, device, method, block_width=64):
         from statfem_b200 import api
         self.api = api
         self.wl = wl
@@ -185,7 +185,8 @@ class GpuStatFEM:
         self.gm = api.Mesh(self.ctx, m.kind, wl["qps"], m.coords, m.conn)
         self.gm.set_coefficients(wl["coeff"])
         self.s = api.SystemSolveCuda(self.ctx, m.num_dofs)
-        self.s.set_options(method=method, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=64,
+        self.block_width = block_width
+        self.s.set_options(method=method, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=block_width,
                            check_every=32)
         self.cf = api.CovarianceForcing(self.ctx, self.gm)
         self.cf.applyConstraints(wl["bc"])
@@ -229,7 +230,7 @@ def run_ours(args, ws, rank, local):
     from statfem_b200 import api
     method = api.SFC_SOLVER_PCG_MIXED if args.method == "mixed" else api.SFC_SOLVER_PCG_FP64
     wl = make_workload(args.config, seed=1234 + rank)
-    g = GpuStatFEM(wl, local, method)
+    g = GpuStatFEM(wl, local, method, args.block_width)
     ctx = g.ctx
     for _ in range(args.warmup):
         g.step()
@@ -241,21 +242,32 @@ def run_ours(args, ws, rank, local):
     cuda_sync(ws)
     ctx.synchronize()
     l0 = ctx.kernel_launches()
-    ctx.set_profiling(True)
     with ClockSampler(local) as clk:
         ctx.mark(0)
         for _ in range(args.steps):
             ll, pm, pc = g.step()
         ctx.mark(1)
         ctx.synchronize()
-    ctx.set_profiling(False)
     cuda_sync(ws)
     barrier(ws)
     ms = ctx.marker_ms(0, 1)
     launches = ctx.kernel_launches() - l0
-    prof = ctx.profile_report()
     block_stats = g.s.last_stats()
     ms_max = max_over_ranks(ws, ms)
+    # kernel timing: the same steps again with an event pair around every hot
+    # kernel (kept out of the timed region above, whose value they would lower)
+    ctx.set_profiling(True)
+    ctx.mark(4)
+    for _ in range(args.prof_steps):
+        g.step()
+    ctx.mark(5)
+    ctx.synchronize()
+    ctx.set_profiling(False)
+    prof_ms = ctx.marker_ms(4, 5)
+    prof_all = ctx.profile_report()
+    phases = {k.split(":", 1)[1]: round(v[1] / max(args.prof_steps, 1), 3) for k, v in prof_all.items()
+              if k.startswith("phase:")}
+    prof = {k: v for k, v in prof_all.items() if not k.startswith("phase:")}
     value = ws * args.steps / (ms_max / 1e3)
     # ---- end-to-end through the public API with host buffers ----
     barrier(ws)
@@ -263,7 +275,7 @@ def run_ours(args, ws, rank, local):
     ctx.synchronize()
     t0 = time.perf_counter()
     ctx.mark(2)
-    e2e_steps = max(1, args.steps)
+    e2e_steps = 0 if args.no_e2e else max(1, args.steps)
     for _ in range(e2e_steps):
         g.step(e2e=True)
     ctx.mark(3)
@@ -285,31 +297,63 @@ def run_ours(args, ws, rank, local):
         roof = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
                 "bytes_per_launch": per_launch_bytes, "avg_launch_us": round(per_launch_s * 1e6, 2),
-                "launches": cnt, "share_of_step": round(tms / ms, 4)}
+                "launches": cnt, "share_of_step": round(tms / max(prof_ms, 1e-9), 4),
+                "timed_over": "%d profiled steps after the timed region" % args.prof_steps}
     out = {
         "metric": "posterior solves/s at rel. residual 1e-8 (learned+batched vs plain PCG, 1xB200)",
         "value": round(value, 4), "unit": "posterior solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals)",
         "data": "synthetic (seeded)",
-        "config": {"workload": wl["desc"], "method": "mixed block Jacobi-PCG" if args.method == "mixed"
+        "config": {"workload": wl["desc"], "block_width": args.block_width,
+                   "method": "mixed block Jacobi-PCG" if args.method == "mixed"
                    else "plain FP64 Jacobi-PCG", "parallelism": "replicas" if ws > 1 else "single GPU",
                    "l2": "inputs larger than L2 (matrix 220+ MB)"},
-        "e2e": {"value": round(ws * e2e_steps / (e2e_ms / 1e3), 4), "unit": "posterior solves/s",
-                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                "wall_s": round(e2e_wall, 3)},
+        "e2e": ({"value": round(ws * e2e_steps / (e2e_ms / 1e3), 4), "unit": "posterior solves/s",
+                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                 "wall_s": round(e2e_wall, 3)} if e2e_steps else None),
         "gpu_launches": int(launches),
         "roofline": roof,
         "kernels": {k: {"launches": v[0], "ms": round(v[1], 3), "GBps": round(v[2] / max(v[1], 1e-9) / 1e6, 1)}
                     for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "phases_ms_per_step": phases,
         "solver": {"forward": stats_fwd, "adjoint_block": block_stats},
         "clocks": clk.summary(),
         "loglik": ll,
     }
+    if args.plain_sample > 0 and args.method == "mixed":
+        out["plain_fp64"] = plain_fp64_estimate(g, wl, ms / args.steps, block_stats, stats_fwd, args.plain_sample)
+        out["speedup_vs_plain_fp64"] = round(out["value"] / ws / out["plain_fp64"]["value"], 2)
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, wl, g, sample_iters=args.cpu_iters)
     if rank == 0:
         print(json.dumps(out))
+
+
+def plain_fp64_estimate(g, wl, step_ms, block_stats, fwd_stats, sample):
+    """Posterior solves/s of the plain method on the same GPU: FP64 Jacobi-PCG,
+    one right-hand side at a time.  The forward solve is measured in full;
+    `sample` of the ns adjoint solves are measured and scaled to ns; the
+    non-solve part of the step (assembly, covariance, likelihood, posterior)
+    is taken from the mixed run's step."""
+    from statfem_b200 import api
+    ns = wl["ns"]
+    ip, ix, dv = wl["P"]
+    rows = np.zeros((sample, wl["mesh"].num_dofs))
+    pick = np.linspace(0, ns - 1, sample).astype(int)
+    for k, a in enumerate(pick):
+        rows[k, ix[ip[a]:ip[a + 1]]] = dv[ip[a]:ip[a + 1]]
+    g.s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=30000, check_every=32)
+    g.s.solveSystemTranspose(rows)
+    st = g.s.last_stats()
+    g.s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=g.block_width,
+                    check_every=32)
+    other_ms = max(0.0, step_ms - block_stats["device_ms"] - fwd_stats["device_ms"])
+    plain_ms = fwd_stats["device_ms"] + st["device_ms"] * ns / sample + other_ms
+    return {"value": round(1e3 / plain_ms, 5), "unit": "posterior solves/s", "ms_per_step": round(plain_ms, 1),
+            "sample": "FP64 Jacobi-PCG one RHS at a time: forward solve measured (%d it), %d of %d adjoint "
+                      "solves measured (%.1f ms, max %d it) and scaled; non-solve work from the timed step"
+                      % (fwd_stats["iterations"], sample, ns, st["device_ms"], st["iterations"])}
 
 
 # ---------------------------------------------------------------------------
@@ -389,6 +433,10 @@ def main():
     ap.add_argument("--config", default="c2", choices=["c2", "c1"])
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cpu-iters", type=int, default=100)
+    ap.add_argument("--plain-sample", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--prof-steps", type=int, default=1)
+    ap.add_argument("--block-width", type=int, default=64, choices=[32, 64, 128])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),

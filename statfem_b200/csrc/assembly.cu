@@ -886,6 +886,8 @@ void apply_constraints_dev(sfc_system *s, const uint32_t *idx_dev, const double 
     s->op_valid = false;
 }
 
+static void build_bsr(sfc_system *s);
+
 void build_operator(sfc_system *s)
 {
     if (s->op_valid) return;
@@ -913,7 +915,75 @@ void build_operator(sfc_system *s)
     download(ctx, &h, err.p, 1);
     if (h == 4) fail(SFC_ERR_BAD_ARG, "a row has no diagonal entry");
     if (h == 5) fail(SFC_ERR_NOT_SPD, "non-positive diagonal entry: the operator is not SPD");
+    build_bsr(s);
     s->op_valid = true;
+}
+
+// ---------------------------------------------------------------------------
+// node-block (3 x 3) view of the operator for 3-dof meshes.  The three rows of
+// node i have the same columns, grouped node by node (every component couples
+// to every component of each neighbour, and the triplet pattern keeps explicit
+// zeros), so block t of node i is read off rows 3i..3i+2 at offset 3t.
+// ---------------------------------------------------------------------------
+__global__ void k_bsr_ptr(const int32_t *__restrict__ row_ptr, int64_t nodes, int32_t *__restrict__ bptr, int *err)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i <= nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t r0 = row_ptr[3 * i];
+        if (r0 % 9) atomicExch(err, 1);
+        bptr[i] = r0 / 9;
+        if (i < nodes) {
+            const int32_t len = row_ptr[3 * i + 1] - r0;
+            if (row_ptr[3 * i + 2] - row_ptr[3 * i + 1] != len || row_ptr[3 * i + 3] - row_ptr[3 * i + 2] != len ||
+                len % 3)
+                atomicExch(err, 1);
+        }
+    }
+}
+
+__global__ void k_bsr_fill(const int32_t *__restrict__ row_ptr, const int32_t *__restrict__ col,
+                           const double *__restrict__ a_op, const int32_t *__restrict__ bptr, int64_t nodes,
+                           int32_t *__restrict__ bcol, float *__restrict__ b32, double *__restrict__ b64, int *err)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t r0 = row_ptr[3 * i];
+        const int32_t nb = bptr[i + 1] - bptr[i];
+        for (int32_t t = 0; t < nb; ++t) {
+            const int64_t b = bptr[i] + t;
+            const int32_t j = col[r0 + 3 * t] / 3;
+            bcol[b] = j;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) {
+                    const int32_t s = r0 + r * 3 * nb + 3 * t + c;
+                    if (col[s] != 3 * j + c) atomicExch(err, 1);
+                    b64[b * 9 + r * 3 + c] = a_op[s];
+                    b32[b * 9 + r * 3 + c] = (float)a_op[s];
+                }
+        }
+    }
+}
+
+static void build_bsr(sfc_system *s)
+{
+    sfc_ctx *ctx = s->ctx;
+    s->has_bsr = false;
+    if (!s->pattern_mesh || s->pattern_mesh->dof != 3 || s->N % 3) return;
+    const int64_t nodes = s->N / 3, nb = s->nnz / 9;
+    s->nodes = nodes;
+    s->nblocks = nb;
+    s->bptr.alloc(nodes + 1);
+    s->bcol.alloc(nb);
+    s->bval32.alloc(nb * 9);
+    s->bval64.alloc(nb * 9);
+    DBuf<int> err;
+    err.alloc(1);
+    SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
+    k_bsr_ptr<<<grid_for(nodes + 1, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, nodes, s->bptr.p, err.p);
+    k_bsr_fill<<<grid_for(nodes, 128), 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, s->bptr.p, nodes,
+                                                              s->bcol.p, s->bval32.p, s->bval64.p, err.p);
+    count_launch(ctx, 2);
+    int h = 0;
+    download(ctx, &h, err.p, 1);
+    s->has_bsr = (h == 0);
 }
 
 // ---------------------------------------------------------------------------

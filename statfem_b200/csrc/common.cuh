@@ -242,6 +242,13 @@ struct sfc_system {
     sfc::DBuf<double> dinv;    // 1 / diag(a_op)
     sfc::DBuf<float> dinv32;
     bool op_valid = false;
+    // node-block (3 x 3) view of the operator for 3-dof meshes: block row of
+    // node i is [bptr[i], bptr[i+1]); bval holds the row-major 3x3 blocks
+    bool has_bsr = false;
+    int64_t nodes = 0, nblocks = 0;
+    sfc::DBuf<int32_t> bptr, bcol;
+    sfc::DBuf<float> bval32;
+    sfc::DBuf<double> bval64;
     // vectors
     sfc::DBuf<double> F, X;
     sfc::DBuf<unsigned char> mask;   // 1 for constrained dofs

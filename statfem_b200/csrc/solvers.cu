@@ -24,6 +24,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -289,6 +291,148 @@ __global__ void __launch_bounds__(256) k_spmm32(const int32_t *__restrict__ rp, 
     block_cols_add<V>(dacc, sh, pq);
 }
 
+// Q = S P for 3-dof meshes through the node-block view: one warp per node
+// (three rows).  A chunk of up to 32 blocks (column node + 3x3 values) is
+// staged in shared memory; for each block the warp loads the column node's
+// three P rows (3*K contiguous floats) once and updates all three output rows,
+// so every gathered row of P feeds three rows of Q.
+template <int V>
+__global__ void __launch_bounds__(256) k_bspmm32(const int32_t *__restrict__ bptr, const int32_t *__restrict__ bcol,
+                                                 const float *__restrict__ bval, const float *__restrict__ P,
+                                                 float *__restrict__ Q, int64_t nodes, double *pq, const int *stop)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    __shared__ float sv[8][32 * 9];
+    __shared__ int sc[8][32];
+    if (*stop) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double dacc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nodes; i += warps) {
+        float acc[3][V];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[r][v] = 0.f;
+        const int32_t b0 = bptr[i], b1 = bptr[i + 1];
+        for (int32_t bb = b0; bb < b1; bb += 32) {
+            const int nbk = min(32, b1 - bb);
+            __syncwarp();
+            if (lane < nbk) sc[w][lane] = bcol[bb + lane];
+            for (int t = lane; t < 9 * nbk; t += 32) sv[w][t] = bval[(int64_t)bb * 9 + t];
+            __syncwarp();
+            // groups of U blocks: all 3U row loads are issued before the FMAs
+            // so that several gathers are in flight per warp
+            constexpr int U = V >= 4 ? 2 : 4;
+            int t = 0;
+            for (; t + U <= nbk; t += U) {
+                float pv[U][3][V];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const float *pj = P + (int64_t)(3 * sc[w][t + u]) * K + lane * V;
+                    ldv<V>(pj, pv[u][0]);
+                    ldv<V>(pj + K, pv[u][1]);
+                    ldv<V>(pj + 2 * K, pv[u][2]);
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const float *bv = &sv[w][(t + u) * 9];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) {
+                        const float a0 = bv[3 * r], a1 = bv[3 * r + 1], a2 = bv[3 * r + 2];
+#pragma unroll
+                        for (int v = 0; v < V; ++v)
+                            acc[r][v] =
+                                fmaf(a2, pv[u][2][v], fmaf(a1, pv[u][1][v], fmaf(a0, pv[u][0][v], acc[r][v])));
+                    }
+                }
+            }
+            for (; t < nbk; ++t) {
+                const float *pj = P + (int64_t)(3 * sc[w][t]) * K + lane * V;
+                float p0[V], p1[V], p2[V];
+                ldv<V>(pj, p0);
+                ldv<V>(pj + K, p1);
+                ldv<V>(pj + 2 * K, p2);
+                const float *bv = &sv[w][t * 9];
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const float a0 = bv[3 * r], a1 = bv[3 * r + 1], a2 = bv[3 * r + 2];
+#pragma unroll
+                    for (int v = 0; v < V; ++v)
+                        acc[r][v] = fmaf(a2, p2[v], fmaf(a1, p1[v], fmaf(a0, p0[v], acc[r][v])));
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            const int64_t o = (3 * i + r) * K + lane * V;
+            stv<V>(Q + o, acc[r]);
+            float pi[V];
+            ldv<V>(P + o, pi);
+#pragma unroll
+            for (int v = 0; v < V; ++v) dacc[v] += (double)pi[v] * (double)acc[r][v];
+        }
+    }
+    block_cols_add<V>(dacc, sh, pq);
+}
+
+// R = B - S X in FP64 through the node-block view (see k_bspmm32)
+template <int V>
+__global__ void __launch_bounds__(256) k_bresid64(const int32_t *__restrict__ bptr, const int32_t *__restrict__ bcol,
+                                                  const double *__restrict__ bval, const double *__restrict__ X,
+                                                  const double *__restrict__ B, double *__restrict__ R, int64_t nodes,
+                                                  double *rr)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    __shared__ double sv[8][32 * 9];
+    __shared__ int sc[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double dacc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nodes; i += warps) {
+        double acc[3][V];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[r][v] = 0.0;
+        const int32_t b0 = bptr[i], b1 = bptr[i + 1];
+        for (int32_t bb = b0; bb < b1; bb += 32) {
+            const int nbk = min(32, b1 - bb);
+            __syncwarp();
+            if (lane < nbk) sc[w][lane] = bcol[bb + lane];
+            for (int t = lane; t < 9 * nbk; t += 32) sv[w][t] = bval[(int64_t)bb * 9 + t];
+            __syncwarp();
+            for (int t = 0; t < nbk; ++t) {
+                const double *xj = X + (int64_t)(3 * sc[w][t]) * K + lane * V;
+                const double *bv = &sv[w][t * 9];
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    const double x0 = xj[v], x1 = xj[K + v], x2 = xj[2 * K + v];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+                        acc[r][v] = fma(bv[3 * r + 2], x2, fma(bv[3 * r + 1], x1, fma(bv[3 * r], x0, acc[r][v])));
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const int64_t o = (3 * i + r) * K + lane * V + v;
+                const double rv = B[o] - acc[r][v];
+                R[o] = rv;
+                dacc[v] += rv * rv;
+            }
+    }
+    block_cols_add<V>(dacc, sh, rr);
+}
+
 // R = B - S X in FP64 (warp per row); rr[c] += R[i][c]^2
 template <int V>
 __global__ void __launch_bounds__(256) k_resid64(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
@@ -331,12 +475,12 @@ __global__ void __launch_bounds__(256) k_resid64(const int32_t *__restrict__ rp,
     block_cols_add<V>(dacc, sh, rr);
 }
 
-// r32 = r64 * scale_c, x32 = 0, p = z = D^-1 r32; rz0[c], rr0[c]
+// r32 = r64 * scale_c, x32 = 0, p = z = D^-1 r32 for restarted columns; rz0[c], rr0[c]
 template <int V>
 __global__ void __launch_bounds__(256) k_binit32(const double *__restrict__ R64, const double *__restrict__ scale,
-                                                 const float *__restrict__ dinv, float *__restrict__ r,
-                                                 float *__restrict__ x, float *__restrict__ p, int64_t N, double *rz0,
-                                                 double *rr0)
+                                                 const float *__restrict__ dinv, const int *__restrict__ restart,
+                                                 float *__restrict__ r, float *__restrict__ x, float *__restrict__ p,
+                                                 int64_t N, double *rz0, double *rr0)
 {
     constexpr int K = 32 * V;
     __shared__ double sh[8 * K];
@@ -354,7 +498,7 @@ __global__ void __launch_bounds__(256) k_binit32(const double *__restrict__ R64,
             const float zv = di * rv;
             r[o] = rv;
             x[o] = 0.f;
-            p[o] = zv;
+            if (restart[lane * V + v]) p[o] = zv;
             a1[v] += (double)rv * zv;
             a2[v] += (double)rv * rv;
         }
@@ -381,9 +525,9 @@ __global__ void __launch_bounds__(256) k_bupdate32(float *__restrict__ x, float 
 #pragma unroll
     for (int v = 0; v < V; ++v) {
         const int c = lane * V + v;
-        const bool frozen = rr[c] <= thr[c];
+        const bool frozen = rr[c] <= thr[c] || err[c];
         const double den = pq[c];
-        if (!frozen && !(den > 0.0)) atomicExch(err, 1);
+        if (!frozen && !(den > 0.0)) err[c] = 1;  // per-column breakdown: the column restarts
         alpha[v] = (frozen || !(den > 0.0)) ? 0.f : (float)(rz[c] / den);
     }
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -419,7 +563,7 @@ template <int V>
 __global__ void __launch_bounds__(256) k_bpupdate32(float *__restrict__ p, const float *__restrict__ r,
                                                     const float *__restrict__ dinv, int64_t N, const double *rz,
                                                     const double *rz_next, const double *rr_next, const double *thr,
-                                                    const int *stop)
+                                                    const int *stop, const int *brk)
 {
     constexpr int K = 32 * V;
     if (*stop) return;
@@ -429,7 +573,7 @@ __global__ void __launch_bounds__(256) k_bpupdate32(float *__restrict__ p, const
 #pragma unroll
     for (int v = 0; v < V; ++v) {
         const int c = lane * V + v;
-        act[v] = rr_next[c] > thr[c];
+        act[v] = rr_next[c] > thr[c] && !brk[c];
         beta[v] = act[v] ? (float)(rz_next[c] / rz[c]) : 0.f;
     }
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -640,11 +784,49 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     double *pq = s->scal.p, *rz = pq + (int64_t)(max_iter + 2) * K, *rrs = rz + (int64_t)(max_iter + 2) * K;
     cs.alloc(6 * K);
     double *bn2 = cs.p, *rn2 = bn2 + K, *scale = rn2 + K, *norm = scale + K, *thr = norm + K;
-    s->flags.reserve(2);
+    // flags[0]: all columns below their thresholds; flags[1 + c]: breakdown
+    // (p^T A p <= 0) in column c
+    s->flags.reserve(1 + K);
     int *stop = s->flags.p, *err = s->flags.p + 1;
-    const unsigned gw = (unsigned)(ctx->sm_count * 2);  // warp-per-row kernels: 8 warps/block
-    std::vector<double> hb(K), hr(K), hs(K), hn(K), ht(K);
-    int max_inner = 0, max_cycles = 0;
+    std::vector<int> hflags(1 + K), nbreak(K);
+    const bool debug = std::getenv("SFC_DEBUG_SOLVER") != nullptr;
+    const unsigned gw = (unsigned)(ctx->sm_count * 8);  // warp-per-row kernels: 8 warps/block
+    const bool bsr = s->has_bsr;
+    // R = B - S X (FP64) and Q = S P (FP32), node-block kernels for 3-dof meshes
+    auto resid = [&](const double *X, const double *Bm, double *R, double *out) {
+        ProfScope ps(ctx, "resid64",
+                     bsr ? (double)s->nblocks * 76 + 4.0 * (s->nodes + 1) + 3.0 * N * K * 8
+                         : (double)s->nnz * 12 + 4.0 * (N + 1) + 3.0 * N * K * 8);
+        if (bsr)
+            k_bresid64<V><<<gw, 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval64.p, X, Bm, R, s->nodes, out);
+        else
+            k_resid64<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, X, Bm, R, N, out);
+        count_launch(ctx);
+    };
+    auto spmm = [&](const float *Pm, float *Qm, double *out) {
+        ProfScope ps(ctx, "spmm32",
+                     bsr ? (double)s->nblocks * 40 + 4.0 * (s->nodes + 1) + 2.0 * N * K * 4
+                         : (double)s->nnz * 8 + 4.0 * (N + 1) + 2.0 * N * K * 4);
+        if (bsr)
+            k_bspmm32<V><<<gw, 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval32.p, Pm, Qm, s->nodes, out, stop);
+        else
+            k_spmm32<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op32.p, Pm, Qm, N, out, stop);
+        count_launch(ctx);
+    };
+    // Reliable-update mixed-precision block PCG.  Each column is scaled to
+    // ||b|| = 1 and iterated in FP32; whenever every active column's recurrence
+    // residual has dropped by a decade since the last update (or has fallen
+    // below its freeze threshold), x32 is folded into the FP64 solution, the
+    // true residual b - S x is recomputed in FP64 and replaces r in the FP32
+    // iteration while the search direction p is kept (no Krylov restart).
+    // Columns whose true residual meets tol are frozen; a column whose
+    // recurrence fell below its threshold while the true residual did not
+    // restarts from p = z with a tighter threshold.
+    std::vector<double> hb(K), hs(K), hn(K), ht(K), rr_last(K), rr_now(K), rn(K);
+    std::vector<int> hrestart(K);
+    DBuf<int> restart;
+    restart.alloc(K);
+    int max_inner = 0, max_updates = 0;
     double worst = 0.0;
     bool all_conv = true;
     for (int c0 = 0; c0 < nrhs; c0 += K) {
@@ -652,96 +834,130 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         k_gather_cols<<<grid_for(N * K, 256), 256, 0, ctx->stream>>>(B, ld, c0, kb, K, N, b64.p);
         SFC_CK(cudaMemsetAsync(x64.p, 0, N * K * 8, ctx->stream));
         SFC_CK(cudaMemsetAsync(cs.p, 0, 6 * K * 8, ctx->stream));
+        SFC_CK(cudaMemsetAsync(s->scal.p, 0, nsc * 8, ctx->stream));
+        SFC_CK(cudaMemsetAsync(s->flags.p, 0, (1 + K) * sizeof(int), ctx->stream));
+        std::fill(nbreak.begin(), nbreak.end(), 0);
         count_launch(ctx);
-        // ||b_c||^2 via the FP64 residual of x = 0
-        k_resid64<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, x64.p, b64.p, r64.p, N, bn2);
-        count_launch(ctx);
+        resid(x64.p, b64.p, r64.p, bn2);  // r64 = b, ||b_c||^2
         download(ctx, hb.data(), bn2, K);
-        int inner_total = 0, cycles = 0;
-        std::vector<double> rn(K);
-        for (int c = 0; c < K; ++c) rn[c] = hb[c];
-        for (int cyc = 0;; ++cyc) {
-            if (cyc > 0) {
-                SFC_CK(cudaMemsetAsync(rn2, 0, K * 8, ctx->stream));
-                ProfScope ps(ctx, "resid64", (double)s->nnz * 12 + 4.0 * (N + 1) + 3.0 * N * K * 8);
-                k_resid64<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, x64.p, b64.p, r64.p, N,
-                                                          rn2);
-                count_launch(ctx);
-                download(ctx, rn.data(), rn2, K);
-            }
-            bool done_all = true;
-            for (int c = 0; c < K; ++c) {
-                const double bnc = std::sqrt(hb[c]), rnc = std::sqrt(rn[c]);
-                const bool ok = c >= kb || bnc == 0.0 || rnc <= tol * bnc;
-                if (!ok) done_all = false;
-                hs[c] = rnc > 0 ? 1.0 / rnc : 0.0;
-                hn[c] = rnc;
-                // inner target relative to the normalised residual (1.0): no
-                // tighter than needed to meet tol this cycle
-                const double need = rnc > 0 ? 0.5 * tol * bnc / rnc : 1.0;
-                const double t = ok ? INFINITY : std::max(itol, need);
-                ht[c] = ok ? INFINITY : t * t;
-            }
-            if (done_all || cyc >= 40 || inner_total >= max_iter) {
-                for (int c = 0; c < kb; ++c) {
-                    const double bnc = std::sqrt(hb[c]);
-                    if (bnc > 0) worst = std::max(worst, std::sqrt(rn[c]) / bnc);
-                }
-                if (!done_all) all_conv = false;
-                break;
-            }
-            ++cycles;
+        std::vector<bool> active(K);
+        int nactive = 0;
+        for (int c = 0; c < K; ++c) {
+            const double bn = std::sqrt(hb[c]);
+            active[c] = c < kb && bn > 0.0;
+            nactive += active[c];
+            hs[c] = active[c] ? 1.0 / bn : 0.0;
+            hn[c] = active[c] ? bn : 0.0;
+            ht[c] = active[c] ? (0.1 * tol) * (0.1 * tol) : INFINITY;
+            rr_last[c] = 1.0;
+            rn[c] = active[c] ? bn : 0.0;
+            hrestart[c] = 1;
+        }
+        int it = 0, updates = 0;
+        if (nactive > 0) {
             SFC_CK(cudaMemcpyAsync(scale, hs.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(norm, hn.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(thr, ht.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
-            const int cap = max_iter - inner_total;
-            SFC_CK(cudaMemsetAsync(s->scal.p, 0, 3 * (int64_t)(std::min(cap, max_iter) + 2) * K * 8, ctx->stream));
-            SFC_CK(cudaMemsetAsync(s->flags.p, 0, 2 * sizeof(int), ctx->stream));
-            k_binit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, rr32, xr, pp, N, rz, rrs);
-            count_launch(ctx);
-            int it = 0;
-            for (it = 0; it < cap; ++it) {
-                const int64_t o0 = (int64_t)it * K, o1 = (int64_t)(it + 1) * K;
-                {
-                    ProfScope ps(ctx, "spmm32", (double)s->nnz * 8 + 4.0 * (N + 1) + 2.0 * N * K * 4);
-                    k_spmm32<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op32.p, pp, qq, N, pq + o0,
-                                                             stop);
-                }
-                {
-                    ProfScope ps(ctx, "bupdate32", 6.0 * N * K * 4 + 4.0 * N);
-                    k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
-                                                                rrs + o0, thr, rz + o1, rrs + o1, stop, err);
-                }
-                {
-                    ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + 4.0 * N);
-                    k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
-                                                                 thr, stop);
-                }
-                count_launch(ctx, 3);
-                if ((it + 1) % check == 0 || it + 1 == cap) {
-                    k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + o1, thr, stop);
-                    count_launch(ctx);
-                    int hf[2];
-                    download(ctx, hf, s->flags.p, 2);
-                    if (hf[1]) fail(SFC_ERR_NOT_SPD, "block PCG breakdown: p^T A p <= 0");
-                    if (hf[0]) {
-                        ++it;
-                        break;
-                    }
-                }
-            }
-            inner_total += it;
-            k_bacc64<V><<<grid_for(N * K, 256), 256, 0, ctx->stream>>>(x64.p, xr, norm, N);
+            SFC_CK(cudaMemcpyAsync(restart.p, hrestart.data(), K * 4, cudaMemcpyHostToDevice, ctx->stream));
+            k_binit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, restart.p, rr32, xr, pp, N, rz, rrs);
             count_launch(ctx);
         }
+        while (nactive > 0) {
+            const int64_t o0 = (int64_t)it * K, o1 = (int64_t)(it + 1) * K;
+            spmm(pp, qq, pq + o0);
+            {
+                ProfScope ps(ctx, "bupdate32", 6.0 * N * K * 4 + 4.0 * N);
+                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
+                                                            rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+            }
+            {
+                ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + 4.0 * N);
+                k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
+                                                             thr, stop, err);
+            }
+            count_launch(ctx, 2);
+            ++it;
+            const bool at_cap = it >= max_iter;
+            if (it % check != 0 && !at_cap) continue;
+            k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + o1, thr, stop);
+            count_launch(ctx);
+            download(ctx, hflags.data(), s->flags.p, 1 + K);
+            download(ctx, rr_now.data(), rrs + o1, K);
+            bool update = hflags[0] || at_cap;
+            for (int c = 0; c < K; ++c)
+                if (active[c] && hflags[1 + c]) {
+                    // a breakdown restarts the column at the next update; a
+                    // column that keeps breaking down is not SPD in FP32
+                    if (++nbreak[c] > 4) fail(SFC_ERR_NOT_SPD, "block PCG breakdown: p^T A p <= 0");
+                    update = true;
+                }
+            if (!update) {
+                update = true;
+                for (int c = 0; c < K; ++c)
+                    if (active[c] && rr_now[c] > ht[c] && rr_now[c] > 1e-2 * rr_last[c]) update = false;
+            }
+            if (!update) continue;
+            // reliable update: x64 += ||b|| x32, true FP64 residual
+            k_bacc64<V><<<grid_for(N * K, 256), 256, 0, ctx->stream>>>(x64.p, xr, norm, N);
+            count_launch(ctx);
+            SFC_CK(cudaMemsetAsync(rn2, 0, K * 8, ctx->stream));
+            resid(x64.p, b64.p, r64.p, rn2);
+            download(ctx, rn.data(), rn2, K);
+            ++updates;
+            if (debug) {
+                double wr = 0, wrec = 0;
+                int nb = 0;
+                for (int c = 0; c < K; ++c)
+                    if (active[c]) {
+                        wr = std::max(wr, std::sqrt(rn[c]) / hn[c]);
+                        wrec = std::max(wrec, std::sqrt(rr_now[c]));
+                        nb += hflags[1 + c];
+                    }
+                std::fprintf(stderr, "[sfc block %d] it %d update %d: max true rel %.3e max recurrence %.3e breakdowns %d\n",
+                             c0, it, updates, wr, wrec, nb);
+            }
+            nactive = 0;
+            for (int c = 0; c < K; ++c) {
+                hrestart[c] = 0;
+                if (!active[c]) continue;
+                const double bn = hn[c], r = std::sqrt(rn[c]);
+                if (r <= tol * bn) {
+                    active[c] = false;
+                    ht[c] = INFINITY;
+                    continue;
+                }
+                ++nactive;
+                if (rr_now[c] <= ht[c]) {  // recurrence converged, true residual not
+                    ht[c] = std::max(ht[c] * 1e-2, 1e-30);
+                    hrestart[c] = 1;
+                }
+                if (hflags[1 + c]) hrestart[c] = 1;
+                rr_last[c] = (r / bn) * (r / bn);
+            }
+            if (nactive == 0 || at_cap) break;
+            SFC_CK(cudaMemcpyAsync(thr, ht.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
+            SFC_CK(cudaMemcpyAsync(restart.p, hrestart.data(), K * 4, cudaMemcpyHostToDevice, ctx->stream));
+            SFC_CK(cudaMemsetAsync(rz + o1, 0, K * 8, ctx->stream));
+            SFC_CK(cudaMemsetAsync(rrs + o1, 0, K * 8, ctx->stream));
+            SFC_CK(cudaMemsetAsync(s->flags.p, 0, (1 + K) * sizeof(int), ctx->stream));
+            // r32 <- scaled true residual, x32 <- 0, p kept (restarted columns: p = z)
+            k_binit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, restart.p, rr32, xr, pp, N, rz + o1,
+                                                      rrs + o1);
+            count_launch(ctx);
+        }
+        for (int c = 0; c < kb; ++c) {
+            const double bn = std::sqrt(hb[c]);
+            if (bn > 0) worst = std::max(worst, std::sqrt(rn[c]) / bn);
+        }
+        if (nactive > 0) all_conv = false;
         k_scatter_cols<<<grid_for(N * kb, 256), 256, 0, ctx->stream>>>(x64.p, ld, c0, kb, K, N, X);
         count_launch(ctx);
-        max_inner = std::max(max_inner, inner_total);
-        max_cycles = std::max(max_cycles, cycles);
+        max_inner = std::max(max_inner, it);
+        max_updates = std::max(max_updates, updates);
     }
     SFC_CK(cudaStreamSynchronize(ctx->stream));
     st.iterations = max_inner;
-    st.refinements = max_cycles;
+    st.refinements = max_updates;
     st.num_rhs = nrhs;
     st.max_rel_residual = worst;
     st.converged = all_conv ? 1 : 0;
@@ -781,7 +997,11 @@ void solve_forward(sfc_system *s)
     SFC_CK(cudaEventCreate(&e0));
     SFC_CK(cudaEventCreate(&e1));
     SFC_CK(cudaEventRecord(e0, ctx->stream));
-    PcgResult r = pcg64(s, b.p, s->X.p, tol, max_iter, check);
+    PcgResult r;
+    {
+        ProfScope ps(ctx, "phase:forward_solve", 0.0);
+        r = pcg64(s, b.p, s->X.p, tol, max_iter, check);
+    }
     SFC_CK(cudaEventRecord(e1, ctx->stream));
     const double rel = true_rel_residual(s, b.p, s->X.p);
     float ms = 0;

@@ -574,8 +574,12 @@ void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp)
     // in the reference, ForwardGaussRHS.hpp:104-112)
     fg->R.alloc(N * ns);
     flush_staged(s);
-    solve_block(s, B.p, fg->R.p, (int)ns, (int)ns);
-    transpose_fixup(s, B.p, fg->R.p, (int)ns, (int)ns);
+    {
+        ProfScope ps(ctx, "phase:adjoint_solve", 0.0);
+        solve_block(s, B.p, fg->R.p, (int)ns, (int)ns);
+        transpose_fixup(s, B.p, fg->R.p, (int)ns, (int)ns);
+    }
+    ProfScope ps_cov(ctx, "phase:mean_and_covariance", 0.0);
     // mean = R F (ForwardGaussRHS.hpp:115-124)
     fg->mean.alloc(ns);
     k_colsum_dot<<<(unsigned)std::min<int64_t>(ns, 1024), 256, 0, ctx->stream>>>(fg->R.p, s->F.p, N, ns, fg->mean.p);
@@ -617,8 +621,11 @@ void koh_loglik(sfc_koh *k, const sfc_hparams_t *hp, double *out)
     DBuf<int> info;
     d.alloc(1);
     info.alloc(1);
-    k_koh_loglik<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim, k->Y.p, *hp,
-                                              k->work.p, d.p, info.p);
+    {
+        ProfScope ps(ctx, "phase:koh_loglik", 0.0);
+        k_koh_loglik<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim,
+                                                  k->Y.p, *hp, k->work.p, d.p, info.p);
+    }
     count_launch(ctx);
     int hi = 0;
     download(ctx, &hi, info.p, 1);
@@ -640,8 +647,11 @@ void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
     pm.alloc(ns);
     pc.alloc((size_t)ns * ns);
     info.alloc(1);
-    k_koh_proj<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim, k->Y.p, *hp,
-                                            k->work.p, pm.p, pc.p, info.p);
+    {
+        ProfScope ps(ctx, "phase:koh_posterior", 0.0);
+        k_koh_proj<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim, k->Y.p,
+                                                *hp, k->work.p, pm.p, pc.p, info.p);
+    }
     count_launch(ctx);
     int hi = 0;
     download(ctx, &hi, info.p, 1);

@@ -13,7 +13,8 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def compile_driver(tmp_path):
-    lib = build.build()
+    from statfem_b200 import api
+    lib = api.LIB_PATH if os.path.exists(api.LIB_PATH) else build.build()
     exe = str(tmp_path / "laplace_rhs_infer")
     subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
                     os.path.join(ROOT, "tests", "cpp", "laplace_rhs_infer.cpp"), "-o", exe,
