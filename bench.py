@@ -436,7 +436,7 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--prof-steps", type=int, default=1)
-    ap.add_argument("--block-width", type=int, default=64, choices=[32, 64, 128])
+    ap.add_argument("--block-width", type=int, default=128, choices=[32, 64, 128])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),

@@ -932,6 +932,12 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                     hrestart[c] = 1;
                 }
                 if (hflags[1 + c]) hrestart[c] = 1;
+                // Keeping p after the residual replacement is only consistent
+                // when the FP32 recurrence still tracks the true residual; when
+                // they have drifted apart (fast convergence between checks),
+                // the column restarts from p = z instead.
+                const double rec = std::sqrt(rr_now[c]), tru = r / bn;
+                if (!(tru <= 1.5 * rec && rec <= 1.5 * tru)) hrestart[c] = 1;
                 rr_last[c] = (r / bn) * (r / bn);
             }
             if (nactive == 0 || at_cap) break;
@@ -1032,7 +1038,7 @@ void solve_block(sfc_system *s, const double *B, double *X, int nrhs, int ld)
     sfc_solve_stats_t st{};
     const auto &o = s->opt;
     if (o.method == SFC_SOLVER_PCG_MIXED) {
-        int bw = o.block_width > 0 ? o.block_width : 64;
+        int bw = o.block_width > 0 ? o.block_width : (nrhs > 64 ? 128 : 64);
         if (nrhs <= 32) bw = 32;
         if (bw <= 32)
             block_mixed<1>(s, B, X, nrhs, ld, st);
