@@ -176,7 +176,7 @@ def cuda_sync(ws):
 # our GPU arm
 # ---------------------------------------------------------------------------
 class GpuStatFEM:
-    def __init__(self, wl, device, method, block_width=64):
+    def __init__(self, wl, device, method, block_width=128, precond=0):
         from statfem_b200 import api
         self.api = api
         self.wl = wl
@@ -186,8 +186,9 @@ class GpuStatFEM:
         self.gm.set_coefficients(wl["coeff"])
         self.s = api.SystemSolveCuda(self.ctx, m.num_dofs)
         self.block_width = block_width
+        self.precond = precond
         self.s.set_options(method=method, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=block_width,
-                           check_every=32)
+                           check_every=32, precond=precond)
         self.cf = api.CovarianceForcing(self.ctx, self.gm)
         self.cf.applyConstraints(wl["bc"])
         self.fg = api.ForwardGaussRHS(self.s, self.cf, REG)
@@ -230,7 +231,8 @@ def run_ours(args, ws, rank, local):
     from statfem_b200 import api
     method = api.SFC_SOLVER_PCG_MIXED if args.method == "mixed" else api.SFC_SOLVER_PCG_FP64
     wl = make_workload(args.config, seed=1234 + rank)
-    g = GpuStatFEM(wl, local, method, args.block_width)
+    precond = api.SFC_PRECOND_BLOCK_JACOBI if args.precond == "block-jacobi" else api.SFC_PRECOND_JACOBI
+    g = GpuStatFEM(wl, local, method, args.block_width, precond)
     ctx = g.ctx
     for _ in range(args.warmup):
         g.step()
@@ -305,7 +307,7 @@ def run_ours(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals)",
         "data": "synthetic (seeded)",
-        "config": {"workload": wl["desc"], "block_width": args.block_width,
+        "config": {"workload": wl["desc"], "block_width": args.block_width, "precond": args.precond,
                    "method": "mixed block Jacobi-PCG" if args.method == "mixed"
                    else "plain FP64 Jacobi-PCG", "parallelism": "replicas" if ws > 1 else "single GPU",
                    "l2": "inputs larger than L2 (matrix 220+ MB)"},
@@ -347,7 +349,7 @@ def plain_fp64_estimate(g, wl, step_ms, block_stats, fwd_stats, sample):
     g.s.solveSystemTranspose(rows)
     st = g.s.last_stats()
     g.s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=g.block_width,
-                    check_every=32)
+                    check_every=32, precond=g.precond)
     other_ms = max(0.0, step_ms - block_stats["device_ms"] - fwd_stats["device_ms"])
     plain_ms = fwd_stats["device_ms"] + st["device_ms"] * ns / sample + other_ms
     return {"value": round(1e3 / plain_ms, 5), "unit": "posterior solves/s", "ms_per_step": round(plain_ms, 1),
@@ -437,6 +439,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--prof-steps", type=int, default=1)
     ap.add_argument("--block-width", type=int, default=128, choices=[32, 64, 128])
+    ap.add_argument("--precond", default="block-jacobi", choices=["jacobi", "block-jacobi"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),

@@ -65,7 +65,13 @@ typedef struct sfc_solver_options {
     double inner_tol;      /* FP32 inner reduction per refinement cycle        */
     int32_t block_width;   /* RHS per block for SFC_SOLVER_PCG_MIXED (0: auto) */
     int32_t check_every;   /* iterations between convergence checks (0: auto)  */
+    int32_t precond;       /* SFC_PRECOND_* for SFC_SOLVER_PCG_MIXED          */
 } sfc_solver_options_t;
+
+/* preconditioners of the mixed solver (the FP64 solver is always Jacobi) */
+#define SFC_PRECOND_JACOBI        0 /* point Jacobi                            */
+#define SFC_PRECOND_BLOCK_JACOBI  1 /* nodal 3x3 block Jacobi on 3-dof meshes,
+                                       point Jacobi otherwise                  */
 
 typedef struct sfc_solve_stats {
     int32_t iterations;       /* max over right-hand sides, inner iterations   */

@@ -27,6 +27,8 @@ LIB_PATH = os.path.join(_HERE, "libstatfem_cuda.so")
 
 SFC_SOLVER_PCG_FP64 = 0
 SFC_SOLVER_PCG_MIXED = 1
+SFC_PRECOND_JACOBI = 0
+SFC_PRECOND_BLOCK_JACOBI = 1
 
 _ERR = {-1: "CUDA error", -2: "bad argument", -3: "not SPD", -4: "not converged", -5: "timeout",
         -6: "out of memory", -7: "negative Jacobian"}
@@ -41,7 +43,7 @@ class SfcError(RuntimeError):
 class SolverOptions(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("tol", ctypes.c_double),
                 ("inner_tol", ctypes.c_double), ("block_width", ctypes.c_int32),
-                ("check_every", ctypes.c_int32)]
+                ("check_every", ctypes.c_int32), ("precond", ctypes.c_int32)]
 
 
 class SolveStats(ctypes.Structure):
@@ -252,8 +254,8 @@ class SystemSolveCuda:
 
     # -- options / stats (no reference counterpart) --
     def set_options(self, method=SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=20000, inner_tol=1e-4,
-                    block_width=0, check_every=16):
-        o = SolverOptions(method, max_iter, tol, inner_tol, block_width, check_every)
+                    block_width=0, check_every=16, precond=SFC_PRECOND_JACOBI):
+        o = SolverOptions(method, max_iter, tol, inner_tol, block_width, check_every, precond)
         self.ctx.check(self.ctx.lib.sfc_system_set_options(self.h, ctypes.byref(o)))
 
     def last_stats(self):

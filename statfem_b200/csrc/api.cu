@@ -82,6 +82,8 @@ int32_t sfc_ctx_create(int32_t device, sfc_ctx_t **out)
         SFC_CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
         SFC_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
         for (auto &e : ctx->marks) SFC_CK(cudaEventCreate(&e));
+        ctx->ierr.alloc(16);
+        ctx->dsmall.alloc(16);
     });
     if (rc != SFC_OK) {
         delete ctx;
@@ -100,6 +102,8 @@ int32_t sfc_ctx_destroy(sfc_ctx_t *ctx)
         if (e) cudaEventDestroy(e);
     for (auto &e : ctx->ev_pool) cudaEventDestroy(e);
     ctx->scratch.release();
+    ctx->ierr.release();
+    ctx->dsmall.release();
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -261,6 +265,7 @@ int32_t sfc_system_create(sfc_ctx_t *ctx, int64_t num_dofs, sfc_system_t **out)
         s->opt.inner_tol = 1e-4;
         s->opt.block_width = 0;
         s->opt.check_every = 16;
+        s->opt.precond = SFC_PRECOND_JACOBI;
         ensure_vectors(s);
         s->st_rhs.assign(num_dofs, 0.0);
     });
@@ -284,6 +289,10 @@ int32_t sfc_system_destroy(sfc_system_t *s)
 int32_t sfc_system_set_options(sfc_system_t *s, const sfc_solver_options_t *o)
 {
     if (!s || !o) return SFC_ERR_BAD_ARG;
+    if (o->precond != SFC_PRECOND_JACOBI && o->precond != SFC_PRECOND_BLOCK_JACOBI) {
+        s->ctx->err = "unknown preconditioner";
+        return SFC_ERR_BAD_ARG;
+    }
     if (o->method != SFC_SOLVER_PCG_FP64 && o->method != SFC_SOLVER_PCG_MIXED) {
         s->ctx->err = "unknown solver method";
         return SFC_ERR_BAD_ARG;
@@ -368,15 +377,13 @@ int32_t sfc_apply_constraints(sfc_system_t *s, const uint32_t *idx, const double
     return guard(s->ctx, [&] {
         flush_staged(s);
         if (n == 0) return;
-        DBuf<uint32_t> di;
-        DBuf<double> dv;
-        upload(s->ctx, di, idx, n);
+        upload(s->ctx, s->cidx, idx, n);
         if (value) {
-            upload(s->ctx, dv, value, n);
+            upload(s->ctx, s->cval, value, n);
             for (int64_t t = 0; t < n; ++t)
                 if (value[t] != 0.0) s->inhomogeneous = true;
         }
-        apply_constraints_dev(s, di.p, value ? dv.p : nullptr, n, factor, scalar);
+        apply_constraints_dev(s, s->cidx.p, value ? s->cval.p : nullptr, n, factor, scalar);
         SFC_CK(cudaStreamSynchronize(s->ctx->stream));
     });
 }

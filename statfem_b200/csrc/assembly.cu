@@ -792,8 +792,7 @@ void assemble_matrix(sfc_system *s, const sfc_mesh *mc)
     ensure_pattern_from_mesh(s, m);
     const int64_t E = m->num_elems;
     m->ke.alloc(E * m->L * m->L);
-    DBuf<int> err;
-    err.alloc(1);
+    DevInt err = status_word(ctx);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
     ProfScope ps_elem(ctx, "element_matrices",
                       (double)E * (m->nn * 4 + m->nn * 24 + 8) + (double)E * m->L * m->L * 8);
@@ -870,8 +869,7 @@ void apply_constraints_dev(sfc_system *s, const uint32_t *idx_dev, const double 
         SFC_CK(cudaMemsetAsync(s->bc_val.p, 0, s->N * 8, ctx->stream));
     }
     if (n == 0) return;
-    DBuf<int> err;
-    err.alloc(1);
+    DevInt err = status_word(ctx);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
     k_constraints<<<grid_for(n, 128), 128, 0, ctx->stream>>>(idx_dev, val_dev, n, s->row_ptr.p, s->col.p, s->a_ref.p,
                                                              s->F.p, s->mask.p, s->bc_val.p, factor, scalar, s->N,
@@ -904,8 +902,7 @@ void build_operator(sfc_system *s)
     s->a_op32.alloc(s->nnz);
     s->dinv.alloc(s->N);
     s->dinv32.alloc(s->N);
-    DBuf<int> err;
-    err.alloc(1);
+    DevInt err = status_word(ctx);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
     k_build_op<<<grid_for(s->N, 128), 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p,
                                                              s->mask.p, s->N, s->a_op.p, s->a_op32.p, s->dinv.p,
@@ -962,6 +959,32 @@ __global__ void k_bsr_fill(const int32_t *__restrict__ row_ptr, const int32_t *_
     }
 }
 
+// inverse of node i's diagonal 3x3 block (FP64 cofactors, stored FP32)
+__global__ void k_bsr_dinv(const int32_t *__restrict__ bptr, const int32_t *__restrict__ bcol,
+                           const double *__restrict__ b64, int64_t nodes, float *__restrict__ dinv, int *err)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t d = -1;
+        for (int32_t b = bptr[i]; b < bptr[i + 1]; ++b)
+            if (bcol[b] == i) d = b;
+        if (d < 0) {
+            atomicExch(err, 1);
+            continue;
+        }
+        const double *m = b64 + 9 * d;
+        const double c00 = m[4] * m[8] - m[5] * m[7], c01 = m[5] * m[6] - m[3] * m[8], c02 = m[3] * m[7] - m[4] * m[6];
+        const double det = m[0] * c00 + m[1] * c01 + m[2] * c02;
+        if (!(det > 0.0)) {
+            atomicExch(err, 1);
+            continue;
+        }
+        const double inv[9] = {c00, m[2] * m[7] - m[1] * m[8], m[1] * m[5] - m[2] * m[4],
+                               c01, m[0] * m[8] - m[2] * m[6], m[2] * m[3] - m[0] * m[5],
+                               c02, m[1] * m[6] - m[0] * m[7], m[0] * m[4] - m[1] * m[3]};
+        for (int k = 0; k < 9; ++k) dinv[9 * i + k] = (float)(inv[k] / det);
+    }
+}
+
 static void build_bsr(sfc_system *s)
 {
     sfc_ctx *ctx = s->ctx;
@@ -974,8 +997,7 @@ static void build_bsr(sfc_system *s)
     s->bcol.alloc(nb);
     s->bval32.alloc(nb * 9);
     s->bval64.alloc(nb * 9);
-    DBuf<int> err;
-    err.alloc(1);
+    DevInt err = status_word(ctx);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
     k_bsr_ptr<<<grid_for(nodes + 1, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, nodes, s->bptr.p, err.p);
     k_bsr_fill<<<grid_for(nodes, 128), 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, s->bptr.p, nodes,
@@ -984,6 +1006,15 @@ static void build_bsr(sfc_system *s)
     int h = 0;
     download(ctx, &h, err.p, 1);
     s->has_bsr = (h == 0);
+    s->bdinv32.release();
+    if (s->has_bsr) {
+        s->bdinv32.alloc(nodes * 9);
+        k_bsr_dinv<<<grid_for(nodes, 128), 128, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval64.p, nodes,
+                                                                  s->bdinv32.p, err.p);
+        count_launch(ctx);
+        download(ctx, &h, err.p, 1);
+        if (h) s->bdinv32.release();  // block Jacobi unavailable: point Jacobi is used
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -90,6 +90,11 @@ struct sfc_ctx {
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
     sfc::DBuf<unsigned char> scratch;  // generic device scratch (CUB temp etc.)
+    // small persistent device scratch (status words, scalars): per-call
+    // allocations would put cudaMalloc/cudaFree (and their implicit device
+    // synchronisation) on the repeated-solve path
+    sfc::DBuf<int> ierr;       // >= 16 ints
+    sfc::DBuf<double> dsmall;  // >= 16 doubles
     // kernel timing (off by default): an event pair around each profiled launch
     bool prof = false;
     struct ProfRec {
@@ -149,7 +154,7 @@ inline unsigned grid_for(int64_t work, int block, int max_blocks = 148 * 32)
 template <class T>
 void upload(sfc_ctx *ctx, DBuf<T> &dst, const T *src, size_t count)
 {
-    dst.alloc(count);
+    dst.reserve(count);
     if (count) {
         SFC_CK(cudaMemcpyAsync(dst.p, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
         SFC_CK(cudaStreamSynchronize(ctx->stream));
@@ -166,6 +171,12 @@ void download(sfc_ctx *ctx, T *dst, const T *src, size_t count)
 }
 
 void *pinned(sfc_ctx *ctx, size_t bytes);
+
+// a status word in the context's persistent scratch (callers memset it)
+struct DevInt {
+    int *p;
+};
+inline DevInt status_word(sfc_ctx *ctx, int k = 0) { return DevInt{ctx->ierr.p + k}; }
 
 // ---------------------------------------------------------------------------
 // quadrature tables (weights, shape values, reference gradients at the
@@ -249,6 +260,7 @@ struct sfc_system {
     sfc::DBuf<int32_t> bptr, bcol;
     sfc::DBuf<float> bval32;
     sfc::DBuf<double> bval64;
+    sfc::DBuf<float> bdinv32;  // inverse of each node's 3x3 diagonal block
     // vectors
     sfc::DBuf<double> F, X;
     sfc::DBuf<unsigned char> mask;   // 1 for constrained dofs
@@ -267,6 +279,14 @@ struct sfc_system {
     sfc::DBuf<double> scal;  // per-iteration scalars
     sfc::DBuf<int> flags;
     sfc::DBuf<double> fix;   // transposed-constraint fixup scratch
+    // persistent workspaces of the block solver and the forward solve
+    sfc::DBuf<double> blk64;   // b, x, r : 3 x N x K
+    sfc::DBuf<float> blk32;    // x, r, p, q : 4 x N x K
+    sfc::DBuf<double> colsc;   // per-column scalars
+    sfc::DBuf<int> restart;    // per-column restart flags
+    sfc::DBuf<double> tmpN, tmpN2;
+    sfc::DBuf<uint32_t> cidx;  // constraint upload buffers
+    sfc::DBuf<double> cval;
 };
 
 // ---------------------------------------------------------------------------
@@ -278,6 +298,7 @@ struct sfc_covar_forcing {
     int dim = 0, dof = 0;
     int64_t num_nodes = 0, num_dofs = 0;
     sfc::DBuf<double> phibar;  // num_dofs
+    sfc::DBuf<double> kron[3]; // 1-D SE factors along the grid axes
 };
 
 struct sfc_forward_gauss {
@@ -298,6 +319,7 @@ struct sfc_forward_gauss {
     sfc::DBuf<double> mean;           // ns
     sfc::DBuf<double> cov;            // ns x ns
     sfc::DBuf<double> work;           // covariance workspace
+    sfc::DBuf<double> B;              // adjoint right-hand sides P^T (N x ns)
     bool valid = false;
 };
 
@@ -310,6 +332,8 @@ struct sfc_koh {
     sfc::DBuf<double> sensor_coords;  // ns x 3
     sfc::DBuf<double> Y;              // ns x n_o
     sfc::DBuf<double> work;
+    sfc::DBuf<double> outv;           // posterior mean / covariance / log-likelihood
+    sfc::DBuf<int> info;
 };
 
 namespace sfc {

@@ -590,6 +590,156 @@ __global__ void __launch_bounds__(256) k_bpupdate32(float *__restrict__ p, const
     }
 }
 
+// ---- nodal 3x3 block-Jacobi variants of the three vector kernels -------------
+// One warp per node (rows 3n..3n+2); z = Dinv_n r with the inverse of the
+// node's diagonal block (row-major, FP32).
+template <int V>
+__device__ __forceinline__ void bj_apply(const float *__restrict__ D, const float (&r)[3][V], float (&z)[3][V])
+{
+    float d[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) d[k] = D[k];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int v = 0; v < V; ++v) z[i][v] = fmaf(d[3 * i + 2], r[2][v], fmaf(d[3 * i + 1], r[1][v], d[3 * i] * r[0][v]));
+}
+
+template <int V>
+__global__ void __launch_bounds__(256) k_ninit32(const double *__restrict__ R64, const double *__restrict__ scale,
+                                                 const float *__restrict__ bdinv, const int *__restrict__ restart,
+                                                 float *__restrict__ r, float *__restrict__ x, float *__restrict__ p,
+                                                 int64_t nodes, double *rz0, double *rr0)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double a1[V], a2[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) a1[v] = a2[v] = 0.0;
+    for (int64_t n = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; n < nodes; n += warps) {
+        float rv[3][V], zv[3][V];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int v = 0; v < V; ++v) rv[i][v] = (float)(R64[(3 * n + i) * K + lane * V + v] * scale[lane * V + v]);
+        bj_apply<V>(bdinv + 9 * n, rv, zv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t o = (3 * n + i) * K + lane * V;
+            float zero[V], pv[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) zero[v] = 0.f;
+            stv<V>(r + o, rv[i]);
+            stv<V>(x + o, zero);
+            ldv<V>(p + o, pv);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                if (restart[lane * V + v]) pv[v] = zv[i][v];
+                a1[v] += (double)rv[i][v] * zv[i][v];
+                a2[v] += (double)rv[i][v] * rv[i][v];
+            }
+            stv<V>(p + o, pv);
+        }
+    }
+    block_cols_add<V>(a1, sh, rz0);
+    __syncthreads();
+    block_cols_add<V>(a2, sh, rr0);
+}
+
+template <int V>
+__global__ void __launch_bounds__(256) k_nupdate32(float *__restrict__ x, float *__restrict__ r,
+                                                   const float *__restrict__ p, const float *__restrict__ q,
+                                                   const float *__restrict__ bdinv, int64_t nodes, const double *pq,
+                                                   const double *rz, const double *rr, const double *thr,
+                                                   double *rz_next, double *rr_next, const int *stop, int *err)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    if (*stop) return;
+    const int lane = threadIdx.x & 31;
+    float alpha[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int c = lane * V + v;
+        const bool frozen = rr[c] <= thr[c] || err[c];
+        const double den = pq[c];
+        if (!frozen && !(den > 0.0)) err[c] = 1;
+        alpha[v] = (frozen || !(den > 0.0)) ? 0.f : (float)(rz[c] / den);
+    }
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double a1[V], a2[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) a1[v] = a2[v] = 0.0;
+    for (int64_t n = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; n < nodes; n += warps) {
+        float rv[3][V], zv[3][V];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t o = (3 * n + i) * K + lane * V;
+            float xv[V], pv[V], qv[V];
+            ldv<V>(x + o, xv);
+            ldv<V>(r + o, rv[i]);
+            ldv<V>(p + o, pv);
+            ldv<V>(q + o, qv);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                xv[v] = fmaf(alpha[v], pv[v], xv[v]);
+                rv[i][v] = fmaf(-alpha[v], qv[v], rv[i][v]);
+            }
+            stv<V>(x + o, xv);
+            stv<V>(r + o, rv[i]);
+        }
+        bj_apply<V>(bdinv + 9 * n, rv, zv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                a1[v] += (double)rv[i][v] * zv[i][v];
+                a2[v] += (double)rv[i][v] * rv[i][v];
+            }
+    }
+    block_cols_add<V>(a1, sh, rz_next);
+    __syncthreads();
+    block_cols_add<V>(a2, sh, rr_next);
+}
+
+template <int V>
+__global__ void __launch_bounds__(256) k_npupdate32(float *__restrict__ p, const float *__restrict__ r,
+                                                    const float *__restrict__ bdinv, int64_t nodes, const double *rz,
+                                                    const double *rz_next, const double *rr_next, const double *thr,
+                                                    const int *stop, const int *brk)
+{
+    constexpr int K = 32 * V;
+    if (*stop) return;
+    const int lane = threadIdx.x & 31;
+    float beta[V];
+    bool act[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int c = lane * V + v;
+        act[v] = rr_next[c] > thr[c] && !brk[c];
+        beta[v] = act[v] ? (float)(rz_next[c] / rz[c]) : 0.f;
+    }
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t n = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; n < nodes; n += warps) {
+        float rv[3][V], zv[3][V];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) ldv<V>(r + (3 * n + i) * K + lane * V, rv[i]);
+        bj_apply<V>(bdinv + 9 * n, rv, zv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t o = (3 * n + i) * K + lane * V;
+            float pv[V];
+            ldv<V>(p + o, pv);
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                if (act[v]) pv[v] = fmaf(beta[v], pv[v], zv[i][v]);
+            stv<V>(p + o, pv);
+        }
+    }
+}
+
 // all columns converged at iteration it -> *stop = 1
 template <int K>
 __global__ void k_bcheck(const double *rr, const double *thr, int *stop)
@@ -746,9 +896,11 @@ double true_rel_residual(sfc_system *s, const double *b, const double *x)
 {
     sfc_ctx *ctx = s->ctx;
     const int64_t N = s->N;
-    DBuf<double> t, d;
-    t.alloc(N);
-    d.alloc(2);
+    s->tmpN2.reserve(N);
+    DBuf<double> &t = s->tmpN2;
+    struct {
+        double *p;
+    } d{ctx->dsmall.p};
     SFC_CK(cudaMemsetAsync(d.p, 0, 2 * sizeof(double), ctx->stream));
     launch_spmv64(s, x, t.p, nullptr, nullptr);
     k_axpby<<<grid_for(N, 256), 256, 0, ctx->stream>>>(t.p, b, 1.0, -1.0, N);  // t = b - Sx
@@ -772,17 +924,17 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     const int check = o.check_every > 0 ? o.check_every : 16;
     const double tol = o.tol > 0 ? o.tol : 1e-8;
     const double itol = o.inner_tol > 0 ? o.inner_tol : 1e-4;
-    DBuf<double> b64, x64, r64, cs;  // cs: column scalars
-    DBuf<float> f32;
-    b64.alloc(N * K);
-    x64.alloc(N * K);
-    r64.alloc(N * K);
-    f32.alloc(4 * N * K);
-    float *xr = f32.p, *rr32 = xr + N * K, *pp = rr32 + N * K, *qq = pp + N * K;
+    // persistent workspaces (grown, never freed per call)
+    s->blk64.reserve(3 * N * K);
+    s->blk32.reserve(4 * N * K);
+    s->colsc.reserve(6 * K);
+    struct {
+        double *p;
+    } b64{s->blk64.p}, x64{s->blk64.p + N * K}, r64{s->blk64.p + 2 * N * K}, cs{s->colsc.p};
+    float *xr = s->blk32.p, *rr32 = xr + N * K, *pp = rr32 + N * K, *qq = pp + N * K;
     const int64_t nsc = 3 * (int64_t)(max_iter + 2) * K;
     s->scal.reserve(nsc);
     double *pq = s->scal.p, *rz = pq + (int64_t)(max_iter + 2) * K, *rrs = rz + (int64_t)(max_iter + 2) * K;
-    cs.alloc(6 * K);
     double *bn2 = cs.p, *rn2 = bn2 + K, *scale = rn2 + K, *norm = scale + K, *thr = norm + K;
     // flags[0]: all columns below their thresholds; flags[1 + c]: breakdown
     // (p^T A p <= 0) in column c
@@ -792,6 +944,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     const bool debug = std::getenv("SFC_DEBUG_SOLVER") != nullptr;
     const unsigned gw = (unsigned)(ctx->sm_count * 8);  // warp-per-row kernels: 8 warps/block
     const bool bsr = s->has_bsr;
+    const bool bj = bsr && o.precond == SFC_PRECOND_BLOCK_JACOBI && s->bdinv32.p;
     // R = B - S X (FP64) and Q = S P (FP32), node-block kernels for 3-dof meshes
     auto resid = [&](const double *X, const double *Bm, double *R, double *out) {
         ProfScope ps(ctx, "resid64",
@@ -813,6 +966,18 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             k_spmm32<V><<<gw, 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op32.p, Pm, Qm, N, out, stop);
         count_launch(ctx);
     };
+    s->restart.reserve(K);
+    DBuf<int> &restart = s->restart;
+    // r32 = scaled r64, x32 = 0, p = z for restarted columns; rz, rr into the slots
+    auto init32 = [&](double *rz_slot, double *rr_slot) {
+        if (bj)
+            k_ninit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->bdinv32.p, restart.p, rr32, xr, pp, s->nodes,
+                                                      rz_slot, rr_slot);
+        else
+            k_binit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, restart.p, rr32, xr, pp, N, rz_slot,
+                                                      rr_slot);
+        count_launch(ctx);
+    };
     // Reliable-update mixed-precision block PCG.  Each column is scaled to
     // ||b|| = 1 and iterated in FP32; whenever every active column's recurrence
     // residual has dropped by a decade since the last update (or has fallen
@@ -824,8 +989,6 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     // restarts from p = z with a tighter threshold.
     std::vector<double> hb(K), hs(K), hn(K), ht(K), rr_last(K), rr_now(K), rn(K);
     std::vector<int> hrestart(K);
-    DBuf<int> restart;
-    restart.alloc(K);
     int max_inner = 0, max_updates = 0;
     double worst = 0.0;
     bool all_conv = true;
@@ -859,21 +1022,28 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             SFC_CK(cudaMemcpyAsync(norm, hn.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(thr, ht.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(restart.p, hrestart.data(), K * 4, cudaMemcpyHostToDevice, ctx->stream));
-            k_binit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, restart.p, rr32, xr, pp, N, rz, rrs);
-            count_launch(ctx);
+            init32(rz, rrs);
         }
         while (nactive > 0) {
             const int64_t o0 = (int64_t)it * K, o1 = (int64_t)(it + 1) * K;
             spmm(pp, qq, pq + o0);
             {
-                ProfScope ps(ctx, "bupdate32", 6.0 * N * K * 4 + 4.0 * N);
-                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
-                                                            rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+                ProfScope ps(ctx, "bupdate32", 6.0 * N * K * 4 + (bj ? 12.0 : 4.0) * N);
+                if (bj)
+                    k_nupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pq + o0,
+                                                                rz + o0, rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+                else
+                    k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
+                                                                rrs + o0, thr, rz + o1, rrs + o1, stop, err);
             }
             {
-                ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + 4.0 * N);
-                k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
-                                                             thr, stop, err);
+                ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + (bj ? 12.0 : 4.0) * N);
+                if (bj)
+                    k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz + o0, rz + o1,
+                                                                 rrs + o1, thr, stop, err);
+                else
+                    k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
+                                                                 thr, stop, err);
             }
             count_launch(ctx, 2);
             ++it;
@@ -947,9 +1117,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             SFC_CK(cudaMemsetAsync(rrs + o1, 0, K * 8, ctx->stream));
             SFC_CK(cudaMemsetAsync(s->flags.p, 0, (1 + K) * sizeof(int), ctx->stream));
             // r32 <- scaled true residual, x32 <- 0, p kept (restarted columns: p = z)
-            k_binit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, restart.p, rr32, xr, pp, N, rz + o1,
-                                                      rrs + o1);
-            count_launch(ctx);
+            init32(rz + o1, rrs + o1);
         }
         for (int c = 0; c < kb; ++c) {
             const double bn = std::sqrt(hb[c]);
@@ -973,8 +1141,9 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
 
 double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n)
 {
-    DBuf<double> d;
-    d.alloc(1);
+    struct {
+        double *p;
+    } d{ctx->dsmall.p + 4};
     SFC_CK(cudaMemsetAsync(d.p, 0, sizeof(double), ctx->stream));
     k_dot<<<grid_for(n, kRedThreads, ctx->sm_count * 4), kRedThreads, 0, ctx->stream>>>(a, b, n, d.p);
     count_launch(ctx);
@@ -990,8 +1159,8 @@ void solve_forward(sfc_system *s)
     build_operator(s);
     const int64_t N = s->N;
     s->X.alloc(N);
-    DBuf<double> b;
-    b.alloc(N);
+    s->tmpN.reserve(N);
+    DBuf<double> &b = s->tmpN;
     k_lift<<<grid_for(N, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p, s->mask.p, s->F.p,
                                                       N, b.p);
     count_launch(ctx);
@@ -1050,9 +1219,9 @@ void solve_block(sfc_system *s, const double *B, double *X, int nrhs, int ld)
         const int max_iter = o.max_iter > 0 ? o.max_iter : 20000;
         const int check = o.check_every > 0 ? o.check_every : 16;
         const double tol = o.tol > 0 ? o.tol : 1e-8;
-        DBuf<double> b, x;
-        b.alloc(N);
-        x.alloc(N);
+        s->tmpN.reserve(N);
+        s->blk64.reserve(N);
+        DBuf<double> &b = s->tmpN, &x = s->blk64;
         st.converged = 1;
         for (int a = 0; a < nrhs; ++a) {
             k_gather_cols<<<grid_for(N, 256), 256, 0, ctx->stream>>>(B, ld, a, 1, 1, N, b.p);

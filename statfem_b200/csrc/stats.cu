@@ -484,16 +484,17 @@ std::vector<double> se_axis(const std::vector<double> &x, double length)
 }  // namespace
 
 // T = K W (per component); W, T, tmp: num_dofs x ns device arrays
-static void kernel_times(sfc_ctx *ctx, const sfc_mesh *m, double sigma, double length, const double *W, double *T,
-                         int64_t ns, double *tmp)
+static void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *W,
+                         double *T, int64_t ns, double *tmp)
 {
+    const sfc_mesh *m = cf->mesh;
     const int64_t nodes = m->num_nodes;
     const int dof = m->dof;
     if (m->is_grid) {
         // K = sigma^2 Kz (x) Ky (x) Kx ; applied axis by axis, ping-ponging
         // between T and tmp
         const int nax = m->dim;
-        std::vector<DBuf<double>> dK(nax);
+        DBuf<double> *dK = cf->kron;
         for (int a = 0; a < nax; ++a) {
             std::vector<double> Kd = se_axis(m->gaxis[a], length);
             if (a == 0)
@@ -535,16 +536,15 @@ static void kernel_times(sfc_ctx *ctx, const sfc_mesh *m, double sigma, double l
 }
 
 // C (ns x ns) = W^T (K W) with W = diag(phibar) X, X: num_dofs x ns (device)
-static void projected_covar(sfc_ctx *ctx, const sfc_covar_forcing *cf, double sigma, double length, const double *X,
+static void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *X,
                             int64_t ns, double *C, DBuf<double> &work)
 {
-    const sfc_mesh *m = cf->mesh;
     const int64_t N = cf->num_dofs;
     work.reserve((size_t)3 * N * ns);
     double *W = work.p, *T = W + N * ns, *tmpp = T + N * ns;
     k_scale_rows<<<grid_for(N * ns, 256), 256, 0, ctx->stream>>>(X, cf->phibar.p, N, ns, W);
     count_launch(ctx);
-    kernel_times(ctx, m, sigma, length, W, T, ns, tmpp);
+    kernel_times(ctx, cf, sigma, length, W, T, ns, tmpp);
     SFC_CK(cudaMemsetAsync(C, 0, ns * ns * 8, ctx->stream));
     const int64_t tiles = ((ns + 63) / 64) * ((ns + 63) / 64);
     int64_t splits = std::max<int64_t>(1, (ctx->sm_count * 4) / tiles);
@@ -565,8 +565,8 @@ void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp)
     SFC_REQUIRE(ns > 0, "projection matrix not set");
     SFC_REQUIRE(fg->cf->num_dofs == N, "covariance and system sizes differ");
     // right-hand sides P^T (N x ns)
-    DBuf<double> B;
-    B.alloc(N * ns);
+    fg->B.reserve(N * ns);
+    DBuf<double> &B = fg->B;
     SFC_CK(cudaMemsetAsync(B.p, 0, N * ns * 8, ctx->stream));
     k_scatter_pt<<<grid_for(ns, 128), 128, 0, ctx->stream>>>(fg->d_p_ptr.p, fg->d_p_idx.p, fg->d_p_val.p, ns, B.p);
     count_launch(ctx);
@@ -617,10 +617,10 @@ void koh_loglik(sfc_koh *k, const sfc_hparams_t *hp, double *out)
     SFC_REQUIRE(k->n_o > 0, "sensor values not set");
     const int ns = (int)k->ns;
     k->work.reserve((size_t)2 * ns * ns + (size_t)ns * k->n_o + 16);
-    DBuf<double> d;
-    DBuf<int> info;
-    d.alloc(1);
-    info.alloc(1);
+    k->outv.reserve(1);
+    k->info.reserve(1);
+    DBuf<double> &d = k->outv;
+    DBuf<int> &info = k->info;
     {
         ProfScope ps(ctx, "phase:koh_loglik", 0.0);
         k_koh_loglik<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim,
@@ -642,22 +642,21 @@ void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
     SFC_REQUIRE(k->n_o > 0, "sensor values not set");
     const int ns = (int)k->ns;
     k->work.reserve((size_t)5 * ns * ns + 3 * (size_t)ns + 16);
-    DBuf<double> pm, pc;
-    DBuf<int> info;
-    pm.alloc(ns);
-    pc.alloc((size_t)ns * ns);
-    info.alloc(1);
+    k->outv.reserve((size_t)ns + (size_t)ns * ns);
+    k->info.reserve(1);
+    double *pm = k->outv.p, *pc = k->outv.p + ns;
+    DBuf<int> &info = k->info;
     {
         ProfScope ps(ctx, "phase:koh_posterior", 0.0);
         k_koh_proj<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim, k->Y.p,
-                                                *hp, k->work.p, pm.p, pc.p, info.p);
+                                                *hp, k->work.p, pm, pc, info.p);
     }
     count_launch(ctx);
     int hi = 0;
     download(ctx, &hi, info.p, 1);
     if (hi) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible (code " + std::to_string(hi) + ")");
-    if (mean) download(ctx, mean, pm.p, ns);
-    if (cov) download(ctx, cov, pc.p, (size_t)ns * ns);
+    if (mean) download(ctx, mean, pm, ns);
+    if (cov) download(ctx, cov, pc, (size_t)ns * ns);
 }
 
 // giveFEconditionedDataWoodbury (LikelihoodKOH.ipp:442-508)

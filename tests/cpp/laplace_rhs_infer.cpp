@@ -61,7 +61,7 @@ int main(int argc, char **argv)
     for (auto &n : nodes) n.dof = numDofs++;
 
     corlib::SystemSolveCuda sysmat(numDofs);
-    sfc_solver_options_t opt{SFC_SOLVER_PCG_FP64, 20000, 1e-13, 1e-4, 0, 16};
+    sfc_solver_options_t opt{SFC_SOLVER_PCG_FP64, 20000, 1e-13, 1e-4, 0, 16, SFC_PRECOND_JACOBI};
     sysmat.setOptions(opt);
 
     // fem(): constraints from x == 0 or x == 1 (fem.hpp:35-40), element matrices, body force
