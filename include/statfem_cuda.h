@@ -38,6 +38,7 @@ extern "C" {
 #define SFC_ERR_NO_MEMORY     -6  /* device or host allocation failed         */
 #define SFC_ERR_NEG_JACOBIAN  -7  /* detJ <= 0 in an element (FTL_VERIFY in
                                      corlib/ElementBasic.ipp:199)             */
+#define SFC_ERR_TOO_LARGE     -8  /* problem exceeds a fixed-size scratch area */
 
 /* ---- element kinds (element type + its integrand) ------------------------ */
 #define SFC_ELEM_LINE2_POISSON  1 /* del2::fem::ElementPotential, 2-node line */
@@ -262,6 +263,34 @@ int32_t sfc_koh_proj_conditioned(sfc_koh_t *koh, const sfc_hparams_t *hp, double
  * posterior mean (num_dofs) and covariance (num_dofs^2; may be NULL).  Needs
  * num_dofs adjoint solves, so it is limited to num_dofs <= 8192. */
 int32_t sfc_koh_woodbury(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean, double *cov);
+
+/* ---- allocation-free log-likelihood ----------------------------------------- */
+/* No counterpart in the reference.  The same quantity as
+ * sfc_koh_log_likelihood (LikelihoodKOH::giveLogLikelihood), for callers that
+ * cannot allocate device memory while they run: an MCMC loop on a stream it
+ * owns, where cudaMalloc / cudaFree would synchronise the whole device, or an
+ * application that gives this library a fixed memory budget at start-up.
+ * Everything is caller-owned DEVICE memory on the current device:
+ *   mean_dev          num_sensors          prior mean at the sensors
+ *   cov_dev           num_sensors^2        prior covariance C_s (row-major)
+ *   sensor_coords_dev num_sensors x 3      sensor coordinates (first dim used)
+ *   y_dev             num_sensors x num_readings readings (row-major)
+ *   loglik_dev        1                    result
+ *   info_dev          1                    0, k+1 if the Cholesky pivot k failed,
+ *                                          -1 for a non-negative quadratic term
+ * The kernel is launched on `stream` (a cudaStream_t, NULL = default stream)
+ * and nothing is allocated: the scratch is a fixed device array of
+ * 2*128*128 + 128*64 doubles (320 KiB, held by every device that loads the
+ * library until exit), so num_sensors <= 128 and num_readings <= 64, else
+ * SFC_ERR_TOO_LARGE.  The first call on a device looks up that array's device
+ * address (with the device current); make it before any stream capture.  All
+ * calls share the array: calls that can overlap on the GPU race and must be
+ * ordered by the caller. */
+int32_t sfc_koh_log_likelihood_noalloc(const double *mean_dev, const double *cov_dev,
+                                       const double *sensor_coords_dev, int32_t dim,
+                                       const double *y_dev, int32_t num_sensors,
+                                       int32_t num_readings, const sfc_hparams_t *hp,
+                                       double *loglik_dev, int32_t *info_dev, void *stream);
 
 #ifdef __cplusplus
 }

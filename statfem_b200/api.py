@@ -31,7 +31,7 @@ SFC_PRECOND_JACOBI = 0
 SFC_PRECOND_BLOCK_JACOBI = 1
 
 _ERR = {-1: "CUDA error", -2: "bad argument", -3: "not SPD", -4: "not converged", -5: "timeout",
-        -6: "out of memory", -7: "negative Jacobian"}
+        -6: "out of memory", -7: "negative Jacobian", -8: "too large for the fixed scratch"}
 
 
 class SfcError(RuntimeError):
@@ -131,6 +131,8 @@ SIGNATURES = {
     "sfc_koh_log_likelihood": (_i32, [_vp, ctypes.POINTER(HParams), _dp]),
     "sfc_koh_proj_conditioned": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
     "sfc_koh_woodbury": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
+    "sfc_koh_log_likelihood_noalloc": (_i32, [_vp, _vp, _vp, _i32, _vp, _i32, _i32, ctypes.POINTER(HParams), _vp,
+                                              _vp, _vp]),
 }
 
 _lib = None
