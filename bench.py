@@ -123,6 +123,20 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def ncu_traffic(kernel, block_width):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, when
+    it was captured at this block width."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            d = json.load(f)
+        e = d.get(kernel)
+        if e and e.get("block_width") == block_width:
+            return float(e["traffic_bytes"])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -297,7 +311,9 @@ def run_ours(args, ws, rank, local):
         per_launch_s = tms / 1e3 / cnt
         achieved = per_launch_bytes / per_launch_s / 1e9
         roof = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "peak_source": peak_kind,
+                "frac": round(achieved / peak, 4), "traffic": ncu_traffic(name, args.block_width),
+                "traffic_source": "profiles/ncu_traffic.json (ncu --set full, same workload)",
+                "peak_source": peak_kind,
                 "bytes_per_launch": per_launch_bytes, "avg_launch_us": round(per_launch_s * 1e6, 2),
                 "launches": cnt, "share_of_step": round(tms / max(prof_ms, 1e-9), 4),
                 "timed_over": "%d profiled steps after the timed region" % args.prof_steps}
