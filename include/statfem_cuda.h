@@ -51,6 +51,9 @@ extern "C" {
 #define SFC_SOLVER_PCG_FP64      0 /* plain FP64 Jacobi-PCG, one RHS at a time */
 #define SFC_SOLVER_PCG_MIXED     1 /* FP32 block Jacobi-PCG (many RHS share the
                                       matrix) + FP64 residual refinement      */
+#define SFC_SOLVER_FCG_MPNN      2 /* flexible CG (FP64) preconditioned by the
+                                      learned message-passing network set with
+                                      sfc_system_set_mpnn (forward solves)    */
 
 typedef struct sfc_ctx sfc_ctx_t;
 typedef struct sfc_mesh sfc_mesh_t;
@@ -291,6 +294,57 @@ int32_t sfc_koh_log_likelihood_noalloc(const double *mean_dev, const double *cov
                                        const double *y_dev, int32_t num_sensors,
                                        int32_t num_readings, const sfc_hparams_t *hp,
                                        double *loglik_dev, int32_t *info_dev, void *stream);
+
+/* ---- learned preconditioner ------------------------------------------------- */
+/* No counterpart in the reference (it factorises with Eigen::SparseLU,
+ * SystemSolveEigenSparse.hpp).  A message-passing network on the matrix
+ * graph: encoder (2 -> 64), 3 layers h' = relu(W [h ; Ahat h] + b) with
+ * W 64 x 128 in BF16 on tensor cores (FP32 accumulate), linear decoder, where
+ * Ahat = D^-1/2 S D^-1/2 is the unit-diagonal scaling of the system's
+ * symmetric operator.  M(r) = D^-1 r + |D^-1/2 r| D^-1/2 y(r): Jacobi plus a
+ * learned correction (the untrained network is exactly Jacobi).  Parameters
+ * are FP32 masters of sfc_mpnn_num_params() floats, trained with Adam on
+ * residual/error pairs (S e = r) from Jacobi-PCG iterates, loss = the S-norm
+ * of the error of M(r), scaled by 1/|D^-1/2 r|^2.  The system passed to the
+ * calls below must have its matrix assembled and constraints applied. */
+typedef struct sfc_mpnn sfc_mpnn_t;
+int64_t sfc_mpnn_num_params(void);
+int32_t sfc_mpnn_create(sfc_ctx_t *ctx, uint64_t seed, sfc_mpnn_t **out);
+int32_t sfc_mpnn_destroy(sfc_mpnn_t *net);
+int32_t sfc_mpnn_get_params(const sfc_mpnn_t *net, float *params, int64_t n);
+int32_t sfc_mpnn_set_params(sfc_mpnn_t *net, const float *params, int64_t n);
+/* Checkpoint: parameters and Adam moments (binary, this library's format). */
+int32_t sfc_mpnn_save(const sfc_mpnn_t *net, const char *path);
+int32_t sfc_mpnn_load(sfc_mpnn_t *net, const char *path);
+/* Loss and its parameter gradient (n = sfc_mpnn_num_params floats; grad may
+ * be NULL) for one pair of host vectors r, e of length num_dofs. */
+int32_t sfc_mpnn_loss_grad(sfc_mpnn_t *net, sfc_system_t *sys, const double *r, const double *e,
+                           double *loss, float *grad);
+/* z = M(r) for host vectors of length num_dofs. */
+int32_t sfc_mpnn_apply(sfc_mpnn_t *net, sfc_system_t *sys, const double *r, double *z);
+/* Training on the GPU.  Pairs come from Jacobi-PCG on the system's current
+ * right-hand side: the initial residual and the iterates after k iterations,
+ * k spaced geometrically up to the iteration where |r_k|/|b| first drops
+ * below pair_floor, against the solution converged to 1e-12 (later iterates
+ * carry too few digits of their error).  Each Adam step sums the loss
+ * gradients of `batch` pairs drawn at random (seeded); with normalize, a
+ * pair's loss is divided by the loss of plain Jacobi on it, so the loss
+ * reads as the fraction of Jacobi's error energy left (1.0 = no gain). */
+typedef struct sfc_mpnn_train_options {
+    int32_t steps;      /* Adam steps                                          */
+    int32_t batch;      /* pairs per step                                      */
+    int32_t max_pairs;  /* pairs from the PCG run (1..64)                      */
+    int32_t normalize;  /* 1: loss relative to Jacobi's (see above)            */
+    double lr;          /* Adam learning rate                                  */
+    double pair_floor;  /* last iterate: |r_k|/|b| >= pair_floor, in (0, 1)    */
+    uint64_t seed;      /* pair sampling                                       */
+} sfc_mpnn_train_options_t;
+int32_t sfc_mpnn_default_train_options(sfc_mpnn_train_options_t *opt);
+/* loss_history (may be NULL): opt->steps doubles, the batch loss per step. */
+int32_t sfc_mpnn_train(sfc_mpnn_t *net, sfc_system_t *sys, const sfc_mpnn_train_options_t *opt,
+                       double *loss_history);
+/* Attach (net != NULL) or detach the network used by SFC_SOLVER_FCG_MPNN. */
+int32_t sfc_system_set_mpnn(sfc_system_t *sys, sfc_mpnn_t *net);
 
 #ifdef __cplusplus
 }

@@ -27,6 +27,7 @@ LIB_PATH = os.path.join(_HERE, "libstatfem_cuda.so")
 
 SFC_SOLVER_PCG_FP64 = 0
 SFC_SOLVER_PCG_MIXED = 1
+SFC_SOLVER_FCG_MPNN = 2
 SFC_PRECOND_JACOBI = 0
 SFC_PRECOND_BLOCK_JACOBI = 1
 
@@ -67,8 +68,15 @@ class HParams(ctypes.Structure):
                    g("mismatch.length"), g("mismatch.sensorEps"))
 
 
+class MpnnTrainOptions(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int32), ("batch", ctypes.c_int32), ("max_pairs", ctypes.c_int32),
+                ("normalize", ctypes.c_int32), ("lr", ctypes.c_double), ("pair_floor", ctypes.c_double),
+                ("seed", ctypes.c_uint64)]
+
+
 _vp = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -133,6 +141,18 @@ SIGNATURES = {
     "sfc_koh_woodbury": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
     "sfc_koh_log_likelihood_noalloc": (_i32, [_vp, _vp, _vp, _i32, _vp, _i32, _i32, ctypes.POINTER(HParams), _vp,
                                               _vp, _vp]),
+    "sfc_mpnn_num_params": (_i64, []),
+    "sfc_mpnn_create": (_i32, [_vp, ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    "sfc_mpnn_destroy": (_i32, [_vp]),
+    "sfc_mpnn_get_params": (_i32, [_vp, _fp, _i64]),
+    "sfc_mpnn_set_params": (_i32, [_vp, _fp, _i64]),
+    "sfc_mpnn_save": (_i32, [_vp, ctypes.c_char_p]),
+    "sfc_mpnn_load": (_i32, [_vp, ctypes.c_char_p]),
+    "sfc_mpnn_loss_grad": (_i32, [_vp, _vp, _dp, _dp, _dp, _fp]),
+    "sfc_mpnn_apply": (_i32, [_vp, _vp, _dp, _dp]),
+    "sfc_mpnn_default_train_options": (_i32, [ctypes.POINTER(MpnnTrainOptions)]),
+    "sfc_mpnn_train": (_i32, [_vp, _vp, ctypes.POINTER(MpnnTrainOptions), _dp]),
+    "sfc_system_set_mpnn": (_i32, [_vp, _vp]),
 }
 
 _lib = None
@@ -503,5 +523,72 @@ class LikelihoodKOH:
             self.h = None
 
 
+class LearnedPreconditioner:
+    """Message-passing network M(r) ~ S^-1 r used by flexible CG
+    (SFC_SOLVER_FCG_MPNN); no counterpart in the reference, which factorises
+    with Eigen::SparseLU."""
+
+    def __init__(self, ctx, seed=0):
+        self.ctx = ctx
+        h = _vp()
+        ctx.check(ctx.lib.sfc_mpnn_create(ctx.h, int(seed), ctypes.byref(h)))
+        self.h = h
+        self.num_params = int(ctx.lib.sfc_mpnn_num_params())
+
+    def get_params(self):
+        out = np.zeros(self.num_params, dtype=np.float32)
+        self.ctx.check(self.ctx.lib.sfc_mpnn_get_params(self.h, _p(out, _fp), self.num_params))
+        return out
+
+    def set_params(self, params):
+        p = _arr(params, np.float32)
+        if p.size != self.num_params:
+            raise ValueError("expected %d parameters" % self.num_params)
+        self.ctx.check(self.ctx.lib.sfc_mpnn_set_params(self.h, _p(p, _fp), self.num_params))
+
+    def save(self, path):
+        self.ctx.check(self.ctx.lib.sfc_mpnn_save(self.h, str(path).encode()))
+
+    def load(self, path):
+        self.ctx.check(self.ctx.lib.sfc_mpnn_load(self.h, str(path).encode()))
+
+    def loss_grad(self, system, r, e):
+        r = _arr(r, np.float64)
+        e = _arr(e, np.float64)
+        loss = ctypes.c_double()
+        g = np.zeros(self.num_params, dtype=np.float32)
+        self.ctx.check(self.ctx.lib.sfc_mpnn_loss_grad(self.h, system.h, _p(r, _dp), _p(e, _dp), ctypes.byref(loss),
+                                                       _p(g, _fp)))
+        return loss.value, g
+
+    def apply(self, system, r):
+        r = _arr(r, np.float64)
+        z = np.zeros_like(r)
+        self.ctx.check(self.ctx.lib.sfc_mpnn_apply(self.h, system.h, _p(r, _dp), _p(z, _dp)))
+        return z
+
+    def train(self, system, **opts):
+        """Adam on pairs from Jacobi-PCG on `system` (options: steps, batch,
+        max_pairs, normalize, lr, pair_floor, seed); returns the loss per step."""
+        o = MpnnTrainOptions()
+        self.ctx.check(self.ctx.lib.sfc_mpnn_default_train_options(ctypes.byref(o)))
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise TypeError("unknown training option %r" % k)
+            setattr(o, k, v)
+        hist = np.zeros(max(o.steps, 1))
+        self.ctx.check(self.ctx.lib.sfc_mpnn_train(self.h, system.h, ctypes.byref(o), _p(hist, _dp)))
+        return hist[: o.steps]
+
+    def attach(self, system):
+        self.ctx.check(self.ctx.lib.sfc_system_set_mpnn(system.h, self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_mpnn_destroy(self.h)
+            self.h = None
+
+
 __all__ = ["Context", "Mesh", "SystemSolveCuda", "CovarianceForcing", "ForwardGaussRHS", "LikelihoodKOH",
-           "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64", "SFC_SOLVER_PCG_MIXED"]
+           "LearnedPreconditioner", "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64",
+           "SFC_SOLVER_PCG_MIXED", "SFC_SOLVER_FCG_MPNN"]

@@ -293,7 +293,7 @@ int32_t sfc_system_set_options(sfc_system_t *s, const sfc_solver_options_t *o)
         s->ctx->err = "unknown preconditioner";
         return SFC_ERR_BAD_ARG;
     }
-    if (o->method != SFC_SOLVER_PCG_FP64 && o->method != SFC_SOLVER_PCG_MIXED) {
+    if (o->method != SFC_SOLVER_PCG_FP64 && o->method != SFC_SOLVER_PCG_MIXED && o->method != SFC_SOLVER_FCG_MPNN) {
         s->ctx->err = "unknown solver method";
         return SFC_ERR_BAD_ARG;
     }

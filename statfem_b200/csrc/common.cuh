@@ -287,6 +287,7 @@ struct sfc_system {
     sfc::DBuf<double> tmpN, tmpN2;
     sfc::DBuf<uint32_t> cidx;  // constraint upload buffers
     sfc::DBuf<double> cval;
+    struct sfc_mpnn *mpnn = nullptr;  // learned preconditioner for SFC_SOLVER_FCG_MPNN
 };
 
 // ---------------------------------------------------------------------------
@@ -351,6 +352,15 @@ void solve_forward(sfc_system *s);
 void solve_block(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
 void transpose_fixup(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
 double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n);
+void spmv_op64(sfc_system *s, const double *x, double *y);
+void lifted_rhs(sfc_system *s, double *b);
+struct PcgStats {
+    int iters;
+    bool converged;
+};
+PcgStats pcg64_public(sfc_system *s, const double *b, double *x, double tol, int max_iter, int check);
+// mpnn.cu
+void solve_forward_fcg(sfc_system *s);
 // stats.cu
 void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp);
 }  // namespace sfc

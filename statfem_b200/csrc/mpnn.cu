@@ -1,0 +1,998 @@
+// Learned preconditioner: a message-passing network on the mesh graph, its
+// training on residual/error pairs from plain Jacobi-PCG, and flexible CG.
+// (No reference counterpart: the reference solves with Eigen::SparseLU.)
+//
+// Scaled operator  Ahat = D^-1/2 S D^-1/2  (unit diagonal, FP32 CSR values on
+// the matrix pattern; S is the symmetric elimination used by every solver).
+// For a residual r:  rhat = D^-1/2 r,  s = rms(rhat),  x0 = rhat / s,
+//   H0 = relu(E [x0, Ahat x0] + e)                    encoder, 2 -> 64
+//   Hl = relu(Wl [H(l-1) ; Ahat H(l-1)] + bl)         l = 1..3, 128 -> 64
+//   y  = w . H3 + c                                   decoder, 64 -> 1
+//   M(r) = s D^-1/2 (x0 + y) = D^-1 r + s D^-1/2 y    Jacobi + learned correction
+// (y = 0 on constrained dofs, whose rows of S are diagonal: Jacobi is exact).
+// The RMS normalisation keeps the node features O(1) whatever the mesh size.
+// The aggregation Ahat H is a 64-column SpMM on the operator's pattern; the
+// dense transforms run on BF16 tensor-core fragments (mma.sync m16n8k16,
+// FP32 accumulate) with the inputs rounded to BF16 on the fly; activations,
+// master weights, gradients and Adam state are FP32.
+//
+// Training pair (r, e) with S e = r: target t = D^1/2 e / s, d = x0 + y - t,
+// loss L = d^T Ahat d / N (the S-norm of the error of M(r) scaled by 1/(N s^2)).
+// Pairs come from x_k of Jacobi-PCG started at 0: r_k = b - S x_k,
+// e_k = x* - x_k, x* the converged solution.
+
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <new>
+#include <random>
+#include <vector>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int H = 64;                 // hidden width
+constexpr int LAYERS = 3;             // message-passing layers
+constexpr int OFF_EW = 0;             // encoder weights [64][2]
+constexpr int OFF_EB = OFF_EW + 2 * H;
+constexpr int OFF_L = OFF_EB + H;     // layer l: W [64][128] then b [64]
+constexpr int LSZ = H * 2 * H + H;
+constexpr int OFF_DW = OFF_L + LAYERS * LSZ;
+constexpr int OFF_DB = OFF_DW + H;
+constexpr int NPARAM = OFF_DB + 1;
+
+}  // namespace
+
+struct sfc_mpnn {
+    sfc_ctx *ctx = nullptr;
+    int64_t step = 0;
+    sfc::DBuf<float> params, grads, adam_m, adam_v;
+    sfc::DBuf<__nv_bfloat16> wbf;  // LAYERS x [64][128] BF16 copies
+    // operator-dependent data (for the system the network was last used on)
+    const sfc_system *op_sys = nullptr;
+    int64_t N = 0;
+    sfc::DBuf<float> ahat, sdinv;
+    // activations and gradients
+    sfc::DBuf<float> x0, ax0, yhat, tgt, dvec, qvec, H[LAYERS + 1], Y[LAYERS + 1], dH0, dH1, dY;
+    sfc::DBuf<double> scal;  // [0]: N s^2 = |D^-1/2 r|^2, [1]: loss
+    // training pairs (FP64, N each)
+    sfc::DBuf<double> pr, pe;
+    std::vector<double> pw;  // per-pair loss weights
+    int npairs = 0;
+};
+
+namespace sfc {
+namespace {
+
+__device__ __forceinline__ float warp_sumf(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // .x (low half) = lo
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+// D (16x8, f32) += A (16x16, bf16, row) * B (16x8, bf16, col)
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// ---- operator scaling --------------------------------------------------------
+__global__ void k_scale_op(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                           const int32_t *__restrict__ diag, const double *__restrict__ a, int64_t N,
+                           float *__restrict__ ahat, float *__restrict__ sdinv)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const double si = 1.0 / sqrt(a[diag[i]]);
+        sdinv[i] = (float)si;
+        for (int32_t s = rp[i]; s < rp[i + 1]; ++s) {
+            const int32_t j = col[s];
+            ahat[s] = (float)(a[s] * si / sqrt(a[diag[j]]));
+        }
+    }
+}
+
+// y = Ahat x (one column), warp per row
+__global__ void k_spmv32(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                         const float *__restrict__ v, const float *__restrict__ x, float *__restrict__ y, int64_t N)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        float s = 0.f;
+        for (int32_t k = rp[i] + lane; k < rp[i + 1]; k += 32) s = fmaf(v[k], x[col[k]], s);
+        s = warp_sumf(s);
+        if (lane == 0) y[i] = s;
+    }
+}
+
+// Y (+)= Ahat X for 64 feature columns, warp per row, two features per lane
+__global__ void k_agg64(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                        const float *__restrict__ v, const float *__restrict__ X, float *__restrict__ Y, int64_t N,
+                        int accumulate)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        float2 acc = make_float2(0.f, 0.f);
+        const int32_t b = rp[i], e = rp[i + 1];
+        for (int32_t s0 = b; s0 < e; s0 += 32) {
+            const int32_t s = s0 + lane;
+            const float av = s < e ? v[s] : 0.f;
+            const int32_t cv = s < e ? col[s] : 0;
+            const int n = min(32, e - s0);
+            for (int j = 0; j < n; ++j) {
+                const float aj = __shfl_sync(0xffffffffu, av, j);
+                const int32_t cj = __shfl_sync(0xffffffffu, cv, j);
+                const float2 xv = *reinterpret_cast<const float2 *>(X + (int64_t)cj * H + 2 * lane);
+                acc.x = fmaf(aj, xv.x, acc.x);
+                acc.y = fmaf(aj, xv.y, acc.y);
+            }
+        }
+        float2 *out = reinterpret_cast<float2 *>(Y + i * H + 2 * lane);
+        if (accumulate) {
+            const float2 o = *out;
+            acc.x += o.x;
+            acc.y += o.y;
+        }
+        *out = acc;
+    }
+}
+
+// x0 = D^-1/2 r / s  (N s^2 in scal[0])
+__global__ void k_x0(const double *__restrict__ r, const float *__restrict__ sdinv, const double *scal, int64_t N,
+                     float *__restrict__ x0)
+{
+    const double inv = scal[0] > 0 ? 1.0 / sqrt(scal[0] / (double)N) : 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        x0[i] = (float)(r[i] * (double)sdinv[i] * inv);
+}
+
+// scal[slot] += sum (D^-1/2 v)^2
+__global__ void k_scaled_norm2(const double *__restrict__ v, const float *__restrict__ sdinv, int64_t N, double *out)
+{
+    __shared__ double sh[32];
+    double s = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const double t = v[i] * (double)sdinv[i];
+        s += t * t;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) atomicAdd(out, s);
+    }
+}
+
+__global__ void k_encoder(const float *__restrict__ x0, const float *__restrict__ ax0, const float *__restrict__ P,
+                          int64_t N, float *__restrict__ H0)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * H; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / H;
+        const int k = (int)(t - i * H);
+        const float z = fmaf(P[OFF_EW + 2 * k], x0[i], fmaf(P[OFF_EW + 2 * k + 1], ax0[i], P[OFF_EB + k]));
+        H0[t] = fmaxf(z, 0.f);
+    }
+}
+
+// Hout = relu([Hin | Yin] W^T + b), 16 nodes per warp, BF16 mma, FP32 accumulate
+__global__ void __launch_bounds__(256) k_dense_fwd(const float *__restrict__ Hin, const float *__restrict__ Yin,
+                                                   const __nv_bfloat16 *__restrict__ W, const float *__restrict__ bias,
+                                                   int64_t N, float *__restrict__ Hout)
+{
+    __shared__ __align__(16) __nv_bfloat16 sW[H * 2 * H];
+    for (int t = threadIdx.x; t < H * 2 * H; t += blockDim.x) sW[t] = W[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int64_t tiles = (N + 15) / 16;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t tile = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; tile < tiles; tile += warps) {
+        const int64_t r0 = tile * 16 + gid, r1 = r0 + 8;
+        float acc[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+            const float *src = ks < 4 ? Hin : Yin;
+            const int c0 = (ks & 3) * 16 + tig * 2, c1 = c0 + 8;
+            float2 v00 = make_float2(0.f, 0.f), v01 = v00, v10 = v00, v11 = v00;
+            if (r0 < N) {
+                v00 = *reinterpret_cast<const float2 *>(src + r0 * H + c0);
+                v01 = *reinterpret_cast<const float2 *>(src + r0 * H + c1);
+            }
+            if (r1 < N) {
+                v10 = *reinterpret_cast<const float2 *>(src + r1 * H + c0);
+                v11 = *reinterpret_cast<const float2 *>(src + r1 * H + c1);
+            }
+            const uint32_t a[4] = {pack_bf16(v00.x, v00.y), pack_bf16(v10.x, v10.y), pack_bf16(v01.x, v01.y),
+                                   pack_bf16(v11.x, v11.y)};
+            const int k = ks * 16 + tig * 2;
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int n = nt * 8 + gid;
+                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&sW[n * 2 * H + k]);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&sW[n * 2 * H + k + 8]);
+                mma16816(acc[nt], a, b0, b1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+            const int c = nt * 8 + tig * 2;
+            const float b0 = bias[c], b1 = bias[c + 1];
+            if (r0 < N)
+                *reinterpret_cast<float2 *>(Hout + r0 * H + c) =
+                    make_float2(fmaxf(acc[nt][0] + b0, 0.f), fmaxf(acc[nt][1] + b1, 0.f));
+            if (r1 < N)
+                *reinterpret_cast<float2 *>(Hout + r1 * H + c) =
+                    make_float2(fmaxf(acc[nt][2] + b0, 0.f), fmaxf(acc[nt][3] + b1, 0.f));
+        }
+    }
+}
+
+// yhat = x0 + (w . H3 + c) on free dofs, x0 on constrained ones; warp per node
+__global__ void k_decoder(const float *__restrict__ H3, const float *__restrict__ P, const float *__restrict__ x0,
+                          const unsigned char *__restrict__ mask, int64_t N, float *__restrict__ yhat)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const float w0 = P[OFF_DW + 2 * lane], w1 = P[OFF_DW + 2 * lane + 1], c = P[OFF_DB];
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const float2 h = *reinterpret_cast<const float2 *>(H3 + i * H + 2 * lane);
+        const float s = warp_sumf(fmaf(w0, h.x, w1 * h.y));
+        if (lane == 0) yhat[i] = mask[i] ? x0[i] : x0[i] + s + c;
+    }
+}
+
+// z = s D^-1/2 yhat  (FP64 output; N s^2 in scal[0])
+__global__ void k_unscale(const float *__restrict__ yhat, const float *__restrict__ sdinv, const double *scal,
+                          int64_t N, double *__restrict__ z)
+{
+    const double s = sqrt(scal[0] / (double)N);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        z[i] = s * (double)sdinv[i] * (double)yhat[i];
+}
+
+// target t = D^1/2 e / s
+__global__ void k_target(const double *__restrict__ e, const float *__restrict__ sdinv, const double *scal, int64_t N,
+                         float *__restrict__ t)
+{
+    const double inv = scal[0] > 0 ? 1.0 / sqrt(scal[0] / (double)N) : 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        t[i] = (float)(e[i] / (double)sdinv[i] * inv);
+}
+
+__global__ void k_sub(const float *__restrict__ a, const float *__restrict__ b, int64_t N, float *__restrict__ d)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = a[i] - b[i];
+}
+
+// loss += w d . q / N ; g = 2 w q / N (in place)
+__global__ void k_loss(const float *__restrict__ d, float *__restrict__ q, int64_t N, double w, double *loss)
+{
+    __shared__ double sh[32];
+    double s = 0;
+    const float g2 = (float)(2.0 * w / (double)N);
+    const double invn = w / (double)N;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        s += (double)d[i] * (double)q[i] * invn;
+        q[i] *= g2;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) atomicAdd(loss, s);
+    }
+}
+
+// decoder backward: dH3 = g w ; dw += sum_i g_i H3_i ; dc += sum g_i
+__global__ void k_decoder_bwd(const float *__restrict__ g, const float *__restrict__ H3, const float *__restrict__ P,
+                              const unsigned char *__restrict__ mask, int64_t N, float *__restrict__ dH3,
+                              float *__restrict__ G)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const float w0 = P[OFF_DW + 2 * lane], w1 = P[OFF_DW + 2 * lane + 1];
+    float a0 = 0.f, a1 = 0.f, ac = 0.f;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const float gi = mask[i] ? 0.f : g[i];
+        const float2 h = *reinterpret_cast<const float2 *>(H3 + i * H + 2 * lane);
+        *reinterpret_cast<float2 *>(dH3 + i * H + 2 * lane) = make_float2(gi * w0, gi * w1);
+        a0 = fmaf(gi, h.x, a0);
+        a1 = fmaf(gi, h.y, a1);
+        ac += gi;
+    }
+    atomicAdd(&G[OFF_DW + 2 * lane], a0);
+    atomicAdd(&G[OFF_DW + 2 * lane + 1], a1);
+    if (lane == 0) atomicAdd(&G[OFF_DB], ac);
+}
+
+// input gradient of a dense layer: dZ = dH * (Hl > 0) (BF16),
+// [dHprev | dY] = dZ W  (16 nodes per warp, mma, FP32 accumulate)
+__global__ void __launch_bounds__(256) k_dense_bwd_x(const float *__restrict__ dH, const float *__restrict__ Hl,
+                                                     const __nv_bfloat16 *__restrict__ W, int64_t N,
+                                                     float *__restrict__ dHprev, float *__restrict__ dY)
+{
+    __shared__ __align__(16) __nv_bfloat16 sW[H * 2 * H];
+    for (int t = threadIdx.x; t < H * 2 * H; t += blockDim.x) sW[t] = W[t];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int64_t tiles = (N + 15) / 16;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t tile = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; tile < tiles; tile += warps) {
+        const int64_t r0 = tile * 16 + gid, r1 = r0 + 8;
+        float acc[16][4];
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+            const int c0 = ks * 16 + tig * 2, c1 = c0 + 8;
+            float v[4][2] = {};
+            if (r0 < N) {
+                const float2 d0 = *reinterpret_cast<const float2 *>(dH + r0 * H + c0);
+                const float2 d1 = *reinterpret_cast<const float2 *>(dH + r0 * H + c1);
+                const float2 h0 = *reinterpret_cast<const float2 *>(Hl + r0 * H + c0);
+                const float2 h1 = *reinterpret_cast<const float2 *>(Hl + r0 * H + c1);
+                v[0][0] = h0.x > 0.f ? d0.x : 0.f;
+                v[0][1] = h0.y > 0.f ? d0.y : 0.f;
+                v[2][0] = h1.x > 0.f ? d1.x : 0.f;
+                v[2][1] = h1.y > 0.f ? d1.y : 0.f;
+            }
+            if (r1 < N) {
+                const float2 d0 = *reinterpret_cast<const float2 *>(dH + r1 * H + c0);
+                const float2 d1 = *reinterpret_cast<const float2 *>(dH + r1 * H + c1);
+                const float2 h0 = *reinterpret_cast<const float2 *>(Hl + r1 * H + c0);
+                const float2 h1 = *reinterpret_cast<const float2 *>(Hl + r1 * H + c1);
+                v[1][0] = h0.x > 0.f ? d0.x : 0.f;
+                v[1][1] = h0.y > 0.f ? d0.y : 0.f;
+                v[3][0] = h1.x > 0.f ? d1.x : 0.f;
+                v[3][1] = h1.y > 0.f ? d1.y : 0.f;
+            }
+            const uint32_t a[4] = {pack_bf16(v[0][0], v[0][1]), pack_bf16(v[1][0], v[1][1]),
+                                   pack_bf16(v[2][0], v[2][1]), pack_bf16(v[3][0], v[3][1])};
+            const int k = ks * 16 + tig * 2;  // output-feature index of W rows
+#pragma unroll
+            for (int nt = 0; nt < 16; ++nt) {
+                const int n = nt * 8 + gid;  // input-feature index (0..127)
+                const uint32_t b0 = (uint32_t) * reinterpret_cast<const uint16_t *>(&sW[k * 2 * H + n]) |
+                                    ((uint32_t) * reinterpret_cast<const uint16_t *>(&sW[(k + 1) * 2 * H + n]) << 16);
+                const uint32_t b1 =
+                    (uint32_t) * reinterpret_cast<const uint16_t *>(&sW[(k + 8) * 2 * H + n]) |
+                    ((uint32_t) * reinterpret_cast<const uint16_t *>(&sW[(k + 9) * 2 * H + n]) << 16);
+                mma16816(acc[nt], a, b0, b1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 16; ++nt) {
+            const int c = nt * 8 + tig * 2;
+            float *dst = c < H ? dHprev : dY;
+            const int cc = c < H ? c : c - H;
+            if (r0 < N) *reinterpret_cast<float2 *>(dst + r0 * H + cc) = make_float2(acc[nt][0], acc[nt][1]);
+            if (r1 < N) *reinterpret_cast<float2 *>(dst + r1 * H + cc) = make_float2(acc[nt][2], acc[nt][3]);
+        }
+    }
+}
+
+// weight gradient of a dense layer: dW[o][j] += sum_i dZ[i][o] Xc[i][j] with
+// dZ and Xc = [Hin | Yin] rounded to BF16 (the operands of the tensor-core
+// products), db[o] += sum_i dZ[i][o] unrounded; FP32 accumulate
+constexpr int kTN = 32;
+__global__ void __launch_bounds__(256) k_dense_bwd_w(const float *__restrict__ dH, const float *__restrict__ Hl,
+                                                     const float *__restrict__ Hin, const float *__restrict__ Yin,
+                                                     int64_t N, float *__restrict__ GW, float *__restrict__ Gb)
+{
+    __shared__ float sZ[kTN][H];
+    __shared__ float sX[kTN][2 * H + 1];
+    const int o = threadIdx.x >> 2, jq = threadIdx.x & 3;  // 64 outputs x 4 interleaved input groups
+    float acc[32];
+#pragma unroll
+    for (int u = 0; u < 32; ++u) acc[u] = 0.f;
+    float accb = 0.f;
+    for (int64_t n0 = (int64_t)blockIdx.x * kTN; n0 < N; n0 += (int64_t)gridDim.x * kTN) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < kTN * H; t += blockDim.x) {
+            const int ii = t / H, k = t % H;
+            const int64_t i = n0 + ii;
+            float z = 0.f;
+            if (i < N) z = Hl[i * H + k] > 0.f ? dH[i * H + k] : 0.f;
+            sZ[ii][k] = z;
+        }
+        for (int t = threadIdx.x; t < kTN * 2 * H; t += blockDim.x) {
+            const int ii = t / (2 * H), j = t % (2 * H);
+            const int64_t i = n0 + ii;
+            float x = 0.f;
+            if (i < N) x = j < H ? Hin[i * H + j] : Yin[i * H + j - H];
+            sX[ii][j] = bf16r(x);
+        }
+        __syncthreads();
+        for (int ii = 0; ii < kTN; ++ii) {
+            const float z0 = sZ[ii][o], z = bf16r(z0);
+            if (jq == 0) accb += z0;
+#pragma unroll
+            for (int u = 0; u < 32; ++u) acc[u] = fmaf(z, sX[ii][u * 4 + jq], acc[u]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 32; ++u) atomicAdd(&GW[o * 2 * H + u * 4 + jq], acc[u]);
+    if (jq == 0) atomicAdd(&Gb[o], accb);
+}
+
+__global__ void k_encoder_bwd(const float *__restrict__ dH0, const float *__restrict__ H0, const float *__restrict__ x0,
+                              const float *__restrict__ ax0, int64_t N, float *__restrict__ G)
+{
+    // thread owns feature k = threadIdx.x & 63 for its node stride
+    const int k = threadIdx.x & (H - 1);
+    float a0 = 0.f, a1 = 0.f, ab = 0.f;
+    const int64_t lanes = (int64_t)gridDim.x * (blockDim.x / H);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / H; i < N; i += lanes) {
+        const float z = H0[i * H + k] > 0.f ? dH0[i * H + k] : 0.f;
+        a0 = fmaf(z, x0[i], a0);
+        a1 = fmaf(z, ax0[i], a1);
+        ab += z;
+    }
+    atomicAdd(&G[OFF_EW + 2 * k], a0);
+    atomicAdd(&G[OFF_EW + 2 * k + 1], a1);
+    atomicAdd(&G[OFF_EB + k], ab);
+}
+
+__global__ void k_adam(float *__restrict__ P, const float *__restrict__ G, float *__restrict__ m,
+                       float *__restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2,
+                       float clip)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        float g = fminf(fmaxf(G[t], -clip), clip);
+        m[t] = b1 * m[t] + (1.f - b1) * g;
+        v[t] = b2 * v[t] + (1.f - b2) * g * g;
+        P[t] -= lr * (m[t] / c1) / (sqrtf(v[t] / c2) + eps);
+    }
+}
+
+__global__ void k_to_bf16(const float *__restrict__ P, __nv_bfloat16 *__restrict__ wbf)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < LAYERS * H * 2 * H; t += gridDim.x * blockDim.x) {
+        const int l = t / (H * 2 * H), r = t % (H * 2 * H);
+        wbf[t] = __float2bfloat16_rn(P[OFF_L + l * LSZ + r]);
+    }
+}
+
+// ---- host side -------------------------------------------------------------------
+void refresh_bf16(sfc_mpnn *m)
+{
+    k_to_bf16<<<64, 256, 0, m->ctx->stream>>>(m->params.p, m->wbf.p);
+    count_launch(m->ctx);
+}
+
+// bind the network to a system's operator (scaled copy of its FP64 values)
+void bind(sfc_mpnn *m, sfc_system *s)
+{
+    sfc_ctx *ctx = m->ctx;
+    flush_staged(s);
+    build_operator(s);
+    const int64_t N = s->N;
+    if (m->N != N) {
+        m->N = N;
+        m->sdinv.alloc(N);
+        m->x0.alloc(N);
+        m->ax0.alloc(N);
+        m->yhat.alloc(N);
+        m->tgt.alloc(N);
+        m->dvec.alloc(N);
+        m->qvec.alloc(N);
+        for (int l = 0; l <= LAYERS; ++l) {
+            m->H[l].alloc(N * H);
+            m->Y[l].alloc(N * H);
+        }
+        m->dH0.alloc(N * H);
+        m->dH1.alloc(N * H);
+        m->dY.alloc(N * H);
+    }
+    m->ahat.reserve(s->nnz);
+    k_scale_op<<<grid_for(N, 128), 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_op.p, N, m->ahat.p,
+                                                         m->sdinv.p);
+    count_launch(ctx);
+    m->op_sys = s;
+}
+
+unsigned gwarp(sfc_ctx *ctx) { return (unsigned)(ctx->sm_count * 8); }
+
+// forward pass on residual r (device FP64): fills x0, ax0, H[], Y[], yhat
+void forward(sfc_mpnn *m, const double *r)
+{
+    sfc_ctx *ctx = m->ctx;
+    const sfc_system *s = m->op_sys;
+    const int64_t N = m->N;
+    ProfScope ps(ctx, "mpnn_forward", 0.0);
+    SFC_CK(cudaMemsetAsync(m->scal.p, 0, sizeof(double), ctx->stream));
+    k_scaled_norm2<<<grid_for(N, 256, ctx->sm_count * 4), 256, 0, ctx->stream>>>(r, m->sdinv.p, N, m->scal.p);
+    count_launch(ctx);
+    k_x0<<<grid_for(N, 256), 256, 0, ctx->stream>>>(r, m->sdinv.p, m->scal.p, N, m->x0.p);
+    k_spmv32<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->x0.p, m->ax0.p, N);
+    k_encoder<<<grid_for(N * H, 256), 256, 0, ctx->stream>>>(m->x0.p, m->ax0.p, m->params.p, N, m->H[0].p);
+    count_launch(ctx, 3);
+    for (int l = 1; l <= LAYERS; ++l) {
+        k_agg64<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->H[l - 1].p, m->Y[l].p, N, 0);
+        k_dense_fwd<<<gwarp(ctx), 256, 0, ctx->stream>>>(m->H[l - 1].p, m->Y[l].p, m->wbf.p + (l - 1) * H * 2 * H,
+                                                        m->params.p + OFF_L + (l - 1) * LSZ + H * 2 * H, N,
+                                                        m->H[l].p);
+        count_launch(ctx, 2);
+    }
+    k_decoder<<<gwarp(ctx), 256, 0, ctx->stream>>>(m->H[LAYERS].p, m->params.p, m->x0.p, s->mask.p, N, m->yhat.p);
+    count_launch(ctx);
+}
+
+// residual-dependent quantities of a pair: s, x0, target t, d = yhat - t,
+// q = 2 w Ahat d / N (the gradient w.r.t. yhat) and the weighted loss in
+// scal[1]; yhat is the network output, or x0 alone for the Jacobi loss
+void pair_residual(sfc_mpnn *m, const double *e, const float *yhat, double w)
+{
+    sfc_ctx *ctx = m->ctx;
+    const sfc_system *s = m->op_sys;
+    const int64_t N = m->N;
+    SFC_CK(cudaMemsetAsync(m->scal.p + 1, 0, sizeof(double), ctx->stream));
+    k_target<<<grid_for(N, 256), 256, 0, ctx->stream>>>(e, m->sdinv.p, m->scal.p, N, m->tgt.p);
+    k_sub<<<grid_for(N, 256), 256, 0, ctx->stream>>>(yhat, m->tgt.p, N, m->dvec.p);
+    k_spmv32<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->dvec.p, m->qvec.p, N);
+    k_loss<<<grid_for(N, 256, ctx->sm_count * 4), 256, 0, ctx->stream>>>(m->dvec.p, m->qvec.p, N, w, m->scal.p + 1);
+    count_launch(ctx, 4);
+}
+
+// loss of the Jacobi preconditioner (zero network output) for pair (r, e)
+double jacobi_loss(sfc_mpnn *m, const double *r, const double *e)
+{
+    sfc_ctx *ctx = m->ctx;
+    const int64_t N = m->N;
+    SFC_CK(cudaMemsetAsync(m->scal.p, 0, sizeof(double), ctx->stream));
+    k_scaled_norm2<<<grid_for(N, 256, ctx->sm_count * 4), 256, 0, ctx->stream>>>(r, m->sdinv.p, N, m->scal.p);
+    k_x0<<<grid_for(N, 256), 256, 0, ctx->stream>>>(r, m->sdinv.p, m->scal.p, N, m->x0.p);
+    count_launch(ctx, 2);
+    pair_residual(m, e, m->x0.p, 1.0);
+    double hl = 0;
+    download(ctx, &hl, m->scal.p + 1, 1);
+    return hl;
+}
+
+// weighted loss w * L and its parameter gradient for pair (r, e) (device
+// FP64); gradients accumulate into grads; returns w * L
+double loss_grad(sfc_mpnn *m, const double *r, const double *e, double w)
+{
+    sfc_ctx *ctx = m->ctx;
+    const sfc_system *s = m->op_sys;
+    const int64_t N = m->N;
+    forward(m, r);
+    ProfScope ps(ctx, "mpnn_backward", 0.0);
+    pair_residual(m, e, m->yhat.p, w);
+    // qvec = dL/dyhat
+    float *dHa = m->dH0.p, *dHb = m->dH1.p;
+    k_decoder_bwd<<<gwarp(ctx), 256, 0, ctx->stream>>>(m->qvec.p, m->H[LAYERS].p, m->params.p, s->mask.p, N, dHa,
+                                                       m->grads.p);
+    count_launch(ctx);
+    for (int l = LAYERS; l >= 1; --l) {
+        const __nv_bfloat16 *W = m->wbf.p + (l - 1) * H * 2 * H;
+        float *GW = m->grads.p + OFF_L + (l - 1) * LSZ;
+        k_dense_bwd_w<<<(unsigned)(ctx->sm_count * 2), 256, 0, ctx->stream>>>(dHa, m->H[l].p, m->H[l - 1].p, m->Y[l].p,
+                                                                              N, GW, GW + H * 2 * H);
+        k_dense_bwd_x<<<gwarp(ctx), 256, 0, ctx->stream>>>(dHa, m->H[l].p, W, N, dHb, m->dY.p);
+        // dH(l-1) += Ahat^T dY (Ahat is symmetric)
+        k_agg64<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->dY.p, dHb, N, 1);
+        count_launch(ctx, 3);
+        std::swap(dHa, dHb);
+    }
+    k_encoder_bwd<<<grid_for(N * H, 256, ctx->sm_count * 8), 256, 0, ctx->stream>>>(dHa, m->H[0].p, m->x0.p,
+                                                                                     m->ax0.p, N, m->grads.p);
+    count_launch(ctx);
+    double hl = 0;
+    download(ctx, &hl, m->scal.p + 1, 1);
+    return hl;
+}
+
+// z = M(r) (device FP64 vectors)
+void apply(sfc_mpnn *m, const double *r, double *z)
+{
+    forward(m, r);
+    k_unscale<<<grid_for(m->N, 256), 256, 0, m->ctx->stream>>>(m->yhat.p, m->sdinv.p, m->scal.p, m->N, z);
+    count_launch(m->ctx);
+}
+
+void adam_step(sfc_mpnn *m, double lr)
+{
+    ++m->step;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)m->step), c2 = 1.f - std::pow(b2, (float)m->step);
+    k_adam<<<64, 256, 0, m->ctx->stream>>>(m->params.p, m->grads.p, m->adam_m.p, m->adam_v.p, NPARAM, (float)lr, b1, b2,
+                                           1e-8f, c1, c2, 1.0f);
+    count_launch(m->ctx);
+    refresh_bf16(m);
+}
+
+__global__ void k_resid_pair(const double *__restrict__ b, const double *__restrict__ Sx, const double *__restrict__ xs,
+                             const double *__restrict__ x, int64_t N, double *__restrict__ r, double *__restrict__ e)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        r[i] = b[i] - Sx[i];
+        e[i] = xs[i] - x[i];
+    }
+}
+
+// Residual/error pairs from Jacobi-PCG on the system's right-hand side b:
+// x* converged to 1e-12; x_k = k iterations of PCG from 0, for k = 0 and
+// max_pairs - 1 values spaced geometrically up to the iteration at which
+// |r_k| / |b| first drops below `floor` (later iterates carry too few digits
+// of their error).  Each pair's weight is 1 / (its Jacobi loss) when
+// `normalize`, else 1.
+void make_pairs(sfc_mpnn *m, sfc_system *s, int max_pairs, double floor, bool normalize)
+{
+    sfc_ctx *ctx = m->ctx;
+    const int64_t N = s->N;
+    DBuf<double> b, xs, xk, t;
+    b.alloc(N);
+    xs.alloc(N);
+    xk.alloc(N);
+    t.alloc(N);
+    lifted_rhs(s, b.p);
+    const PcgStats ref = pcg64_public(s, b.p, xs.p, 1e-12, 200000, 32);
+    SFC_REQUIRE(ref.converged, "Jacobi-PCG did not converge while generating training pairs");
+    const PcgStats fl = pcg64_public(s, b.p, xk.p, floor, 200000, 1);
+    const int kmax = std::max(1, fl.iters);
+    std::vector<int> ks{0};
+    for (int j = 1; j < max_pairs; ++j) {
+        const int k = (int)std::lround(std::pow((double)kmax, (double)j / (double)std::max(1, max_pairs - 1)));
+        if (k > ks.back()) ks.push_back(k);
+    }
+    const int np = (int)ks.size();
+    m->pr.reserve(N * np);
+    m->pe.reserve(N * np);
+    m->pw.assign(np, 1.0);
+    for (int j = 0; j < np; ++j) {
+        if (ks[j] == 0)
+            SFC_CK(cudaMemsetAsync(xk.p, 0, N * 8, ctx->stream));
+        else
+            pcg64_public(s, b.p, xk.p, 1e-300, ks[j], 1 << 30);
+        spmv_op64(s, xk.p, t.p);
+        k_resid_pair<<<grid_for(N, 256), 256, 0, ctx->stream>>>(b.p, t.p, xs.p, xk.p, N, m->pr.p + j * N,
+                                                               m->pe.p + j * N);
+        count_launch(ctx);
+        if (normalize) {
+            const double lj = jacobi_loss(m, m->pr.p + j * N, m->pe.p + j * N);
+            m->pw[j] = lj > 0 ? 1.0 / lj : 1.0;
+        }
+    }
+    m->npairs = np;
+    SFC_CK(cudaStreamSynchronize(ctx->stream));
+}
+
+__global__ void k_resid(const double *__restrict__ b, const double *__restrict__ Sx, int64_t n, double *__restrict__ r)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        r[i] = b[i] - Sx[i];
+}
+
+__global__ void k_axpy(double *__restrict__ y, const double *__restrict__ x, double a, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += a * x[i];
+}
+
+__global__ void k_xpby(double *__restrict__ p, const double *__restrict__ z, double beta, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+}  // namespace
+
+// Flexible CG (FCG(1), Notay 2000) with z = M(r) from the network; the
+// convergence test is the true FP64 residual ||b - S x|| <= tol ||b||,
+// recomputed whenever the recurrence residual says converged.
+void solve_forward_fcg(sfc_system *s)
+{
+    sfc_ctx *ctx = s->ctx;
+    SFC_REQUIRE(s->mpnn, "no learned preconditioner set (sfc_system_set_mpnn)");
+    sfc_mpnn *m = s->mpnn;
+    bind(m, s);  // the operator's values may have changed since the last use
+    const int64_t N = s->N;
+    const auto &o = s->opt;
+    const int max_iter = o.max_iter > 0 ? o.max_iter : 20000;
+    const double tol = o.tol > 0 ? o.tol : 1e-8;
+    s->X.alloc(N);
+    DBuf<double> b, r, z, p, q, t;
+    b.alloc(N);
+    r.alloc(N);
+    z.alloc(N);
+    p.alloc(N);
+    q.alloc(N);
+    t.alloc(N);
+    cudaEvent_t e0, e1;
+    SFC_CK(cudaEventCreate(&e0));
+    SFC_CK(cudaEventCreate(&e1));
+    SFC_CK(cudaEventRecord(e0, ctx->stream));
+    lifted_rhs(s, b.p);
+    SFC_CK(cudaMemsetAsync(s->X.p, 0, N * 8, ctx->stream));
+    SFC_CK(cudaMemcpyAsync(r.p, b.p, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    const double bb = device_dot(ctx, b.p, b.p, N);
+    const unsigned g = grid_for(N, 256);
+    int it = 0;
+    bool conv = bb == 0.0;
+    double rel = 0.0;
+    if (!conv) {
+        apply(m, r.p, z.p);
+        SFC_CK(cudaMemcpyAsync(p.p, z.p, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        spmv_op64(s, p.p, q.p);
+        double pr = device_dot(ctx, p.p, r.p, N), pq = device_dot(ctx, p.p, q.p, N);
+        while (it < max_iter) {
+            if (!(pq > 0.0)) fail(SFC_ERR_NOT_SPD, "flexible CG breakdown: p^T A p <= 0");
+            ++it;
+            const double alpha = pr / pq;
+            k_axpy<<<g, 256, 0, ctx->stream>>>(s->X.p, p.p, alpha, N);
+            k_axpy<<<g, 256, 0, ctx->stream>>>(r.p, q.p, -alpha, N);
+            count_launch(ctx, 2);
+            const double rr = device_dot(ctx, r.p, r.p, N);
+            if (rr <= tol * tol * bb) {
+                // confirm with the true residual; continue from it if the
+                // recurrence has drifted
+                spmv_op64(s, s->X.p, t.p);
+                k_resid<<<g, 256, 0, ctx->stream>>>(b.p, t.p, N, r.p);
+                count_launch(ctx);
+                rel = std::sqrt(device_dot(ctx, r.p, r.p, N) / bb);
+                if (rel <= tol) {
+                    conv = true;
+                    break;
+                }
+            }
+            apply(m, r.p, z.p);
+            const double beta = -device_dot(ctx, z.p, q.p, N) / pq;  // S-orthogonal to the last direction
+            k_xpby<<<g, 256, 0, ctx->stream>>>(p.p, z.p, beta, N);
+            count_launch(ctx);
+            spmv_op64(s, p.p, q.p);
+            pr = device_dot(ctx, p.p, r.p, N);
+            pq = device_dot(ctx, p.p, q.p, N);
+        }
+        if (!conv) rel = std::sqrt(device_dot(ctx, r.p, r.p, N) / bb);
+    }
+    SFC_CK(cudaEventRecord(e1, ctx->stream));
+    float ms = 0;
+    SFC_CK(cudaEventSynchronize(e1));
+    SFC_CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->stats = {};
+    s->stats.iterations = it;
+    s->stats.num_rhs = 1;
+    s->stats.converged = conv ? 1 : 0;
+    s->stats.max_rel_residual = rel;
+    s->stats.device_ms = ms;
+    if (!conv) fail(SFC_ERR_NOT_CONVERGED, "flexible CG did not converge within max_iter");
+}
+
+}  // namespace sfc
+
+using namespace sfc;
+
+namespace {
+int mguard(sfc_ctx *ctx, const std::function<void()> &fn)
+{
+    try {
+        SFC_CK(cudaSetDevice(ctx->device));
+        fn();
+        return SFC_OK;
+    } catch (const Error &e) {
+        ctx->err = e.msg;
+        if (e.code == SFC_ERR_CUDA) cudaGetLastError();
+        return e.code;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return SFC_ERR_BAD_ARG;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int64_t sfc_mpnn_num_params(void) { return NPARAM; }
+
+int32_t sfc_mpnn_create(sfc_ctx_t *ctx, uint64_t seed, sfc_mpnn_t **out)
+{
+    if (!ctx || !out) return SFC_ERR_BAD_ARG;
+    *out = nullptr;
+    sfc_mpnn *m = new (std::nothrow) sfc_mpnn();
+    if (!m) return SFC_ERR_NO_MEMORY;
+    int rc = mguard(ctx, [&] {
+        m->ctx = ctx;
+        std::vector<float> p(NPARAM, 0.f);
+        std::mt19937_64 gen(seed);
+        std::normal_distribution<float> nd(0.f, 1.f);
+        for (int k = 0; k < 2 * H; ++k) p[OFF_EW + k] = nd(gen) * 0.7f;
+        for (int k = 0; k < H; ++k) p[OFF_EB + k] = 0.05f;
+        for (int l = 0; l < LAYERS; ++l)
+            for (int k = 0; k < H * 2 * H; ++k) p[OFF_L + l * LSZ + k] = nd(gen) * std::sqrt(2.f / (2 * H));
+        // decoder starts at zero: the untrained network is exactly Jacobi
+        m->params.alloc(NPARAM);
+        m->grads.alloc(NPARAM);
+        m->adam_m.alloc(NPARAM);
+        m->adam_v.alloc(NPARAM);
+        m->wbf.alloc(LAYERS * H * 2 * H);
+        m->scal.alloc(4);
+        upload(ctx, m->params, p.data(), NPARAM);
+        SFC_CK(cudaMemsetAsync(m->adam_m.p, 0, NPARAM * 4, ctx->stream));
+        SFC_CK(cudaMemsetAsync(m->adam_v.p, 0, NPARAM * 4, ctx->stream));
+        refresh_bf16(m);
+        SFC_CK(cudaStreamSynchronize(ctx->stream));
+    });
+    if (rc != SFC_OK) {
+        delete m;
+        return rc;
+    }
+    *out = m;
+    return SFC_OK;
+}
+
+int32_t sfc_mpnn_destroy(sfc_mpnn_t *m)
+{
+    if (!m) return SFC_OK;
+    cudaSetDevice(m->ctx->device);
+    cudaStreamSynchronize(m->ctx->stream);
+    delete m;
+    return SFC_OK;
+}
+
+int32_t sfc_mpnn_get_params(const sfc_mpnn_t *m, float *out, int64_t n)
+{
+    if (!m || !out || n != NPARAM) return SFC_ERR_BAD_ARG;
+    return mguard(m->ctx, [&] { download(m->ctx, out, m->params.p, NPARAM); });
+}
+
+int32_t sfc_mpnn_set_params(sfc_mpnn_t *m, const float *in, int64_t n)
+{
+    if (!m || !in || n != NPARAM) return SFC_ERR_BAD_ARG;
+    return mguard(m->ctx, [&] {
+        upload(m->ctx, m->params, in, NPARAM);
+        refresh_bf16(m);
+        SFC_CK(cudaStreamSynchronize(m->ctx->stream));
+    });
+}
+
+int32_t sfc_mpnn_save(const sfc_mpnn_t *m, const char *path)
+{
+    if (!m || !path) return SFC_ERR_BAD_ARG;
+    return mguard(m->ctx, [&] {
+        std::vector<float> buf(3 * (size_t)NPARAM);
+        download(m->ctx, buf.data(), m->params.p, NPARAM);
+        download(m->ctx, buf.data() + NPARAM, m->adam_m.p, NPARAM);
+        download(m->ctx, buf.data() + 2 * NPARAM, m->adam_v.p, NPARAM);
+        FILE *f = std::fopen(path, "wb");
+        SFC_REQUIRE(f, std::string("cannot open ") + path);
+        const int64_t hdr[3] = {0x53464d50, NPARAM, m->step};  // "SFMP"
+        bool ok = std::fwrite(hdr, sizeof hdr, 1, f) == 1 && std::fwrite(buf.data(), 4, buf.size(), f) == buf.size();
+        std::fclose(f);
+        SFC_REQUIRE(ok, "checkpoint write failed");
+    });
+}
+
+int32_t sfc_mpnn_load(sfc_mpnn_t *m, const char *path)
+{
+    if (!m || !path) return SFC_ERR_BAD_ARG;
+    return mguard(m->ctx, [&] {
+        FILE *f = std::fopen(path, "rb");
+        SFC_REQUIRE(f, std::string("cannot open ") + path);
+        int64_t hdr[3] = {};
+        std::vector<float> buf(3 * (size_t)NPARAM);
+        bool ok = std::fread(hdr, sizeof hdr, 1, f) == 1 && hdr[0] == 0x53464d50 && hdr[1] == NPARAM &&
+                  std::fread(buf.data(), 4, buf.size(), f) == buf.size();
+        std::fclose(f);
+        SFC_REQUIRE(ok, "not a checkpoint of this network");
+        upload(m->ctx, m->params, buf.data(), NPARAM);
+        upload(m->ctx, m->adam_m, buf.data() + NPARAM, NPARAM);
+        upload(m->ctx, m->adam_v, buf.data() + 2 * NPARAM, NPARAM);
+        m->step = hdr[2];
+        refresh_bf16(m);
+        SFC_CK(cudaStreamSynchronize(m->ctx->stream));
+    });
+}
+
+int32_t sfc_mpnn_loss_grad(sfc_mpnn_t *m, sfc_system_t *s, const double *r, const double *e, double *loss,
+                           float *grad)
+{
+    if (!m || !s || !r || !e) return SFC_ERR_BAD_ARG;
+    return mguard(m->ctx, [&] {
+        bind(m, s);
+        DBuf<double> dr, de;
+        upload(m->ctx, dr, r, s->N);
+        upload(m->ctx, de, e, s->N);
+        SFC_CK(cudaMemsetAsync(m->grads.p, 0, NPARAM * 4, m->ctx->stream));
+        const double l = loss_grad(m, dr.p, de.p, 1.0);
+        if (loss) *loss = l;
+        if (grad) download(m->ctx, grad, m->grads.p, NPARAM);
+    });
+}
+
+int32_t sfc_mpnn_apply(sfc_mpnn_t *m, sfc_system_t *s, const double *r, double *z)
+{
+    if (!m || !s || !r || !z) return SFC_ERR_BAD_ARG;
+    return mguard(m->ctx, [&] {
+        bind(m, s);
+        DBuf<double> dr, dz;
+        upload(m->ctx, dr, r, s->N);
+        dz.alloc(s->N);
+        apply(m, dr.p, dz.p);
+        download(m->ctx, z, dz.p, s->N);
+    });
+}
+
+int32_t sfc_mpnn_default_train_options(sfc_mpnn_train_options_t *o)
+{
+    if (!o) return SFC_ERR_BAD_ARG;
+    o->steps = 500;
+    o->batch = 4;
+    o->max_pairs = 16;
+    o->normalize = 1;
+    o->lr = 1e-3;
+    o->pair_floor = 1e-6;
+    o->seed = 0;
+    return SFC_OK;
+}
+
+int32_t sfc_mpnn_train(sfc_mpnn_t *m, sfc_system_t *s, const sfc_mpnn_train_options_t *o, double *loss_history)
+{
+    if (!m || !s || !o || o->steps < 0 || o->batch < 1 || o->max_pairs < 1 || o->max_pairs > 64 || !(o->lr > 0) ||
+        !(o->pair_floor > 0 && o->pair_floor < 1)) {
+        if (m) m->ctx->err = "invalid training options";
+        return SFC_ERR_BAD_ARG;
+    }
+    return mguard(m->ctx, [&] {
+        bind(m, s);
+        make_pairs(m, s, o->max_pairs, o->pair_floor, o->normalize != 0);
+        const int64_t N = s->N;
+        std::mt19937_64 gen(o->seed ^ (uint64_t)(m->step * 0x9E3779B97F4A7C15ull));
+        std::uniform_int_distribution<int> pick(0, m->npairs - 1);
+        for (int t = 0; t < o->steps; ++t) {
+            SFC_CK(cudaMemsetAsync(m->grads.p, 0, NPARAM * 4, m->ctx->stream));
+            double acc = 0;
+            for (int j = 0; j < o->batch; ++j) {
+                const int k = pick(gen);
+                acc += loss_grad(m, m->pr.p + k * N, m->pe.p + k * N, m->pw[k] / o->batch);
+            }
+            adam_step(m, o->lr);
+            if (loss_history) loss_history[t] = acc;
+        }
+        SFC_CK(cudaStreamSynchronize(m->ctx->stream));
+    });
+}
+
+int32_t sfc_system_set_mpnn(sfc_system_t *s, sfc_mpnn_t *m)
+{
+    if (!s) return SFC_ERR_BAD_ARG;
+    s->mpnn = m;
+    if (m) m->op_sys = nullptr;  // rebind on next use
+    return SFC_OK;
+}
+
+}  // extern "C"

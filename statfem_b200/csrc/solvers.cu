@@ -1139,6 +1139,23 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
 
 }  // namespace
 
+// y = S x with the FP64 operator (used by the flexible solver in mpnn.cu)
+void spmv_op64(sfc_system *s, const double *x, double *y) { launch_spmv64(s, x, y, nullptr, nullptr); }
+
+// lifted right-hand side b = F - K_fc u_c (see k_lift)
+void lifted_rhs(sfc_system *s, double *b)
+{
+    k_lift<<<grid_for(s->N, 256), 256, 0, s->ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p, s->mask.p,
+                                                           s->F.p, s->N, b);
+    count_launch(s->ctx);
+}
+
+PcgStats pcg64_public(sfc_system *s, const double *b, double *x, double tol, int max_iter, int check)
+{
+    PcgResult r = pcg64(s, b, x, tol, max_iter, check);
+    return {r.iters, r.converged};
+}
+
 double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n)
 {
     struct {
@@ -1156,6 +1173,11 @@ double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n)
 void solve_forward(sfc_system *s)
 {
     sfc_ctx *ctx = s->ctx;
+    if (s->opt.method == SFC_SOLVER_FCG_MPNN) {
+        ProfScope ps(ctx, "phase:forward_solve", 0.0);
+        solve_forward_fcg(s);
+        return;
+    }
     build_operator(s);
     const int64_t N = s->N;
     s->X.alloc(N);
