@@ -320,7 +320,9 @@ int32_t sfc_mpnn_load(sfc_mpnn_t *net, const char *path);
  * be NULL) for one pair of host vectors r, e of length num_dofs. */
 int32_t sfc_mpnn_loss_grad(sfc_mpnn_t *net, sfc_system_t *sys, const double *r, const double *e,
                            double *loss, float *grad);
-/* z = M(r) for host vectors of length num_dofs. */
+/* z = M(r) for host vectors of length num_dofs, by the inference kernels
+ * flexible CG uses (activations stored in BF16, the values the tensor-core
+ * products round them to; training keeps them in FP32). */
 int32_t sfc_mpnn_apply(sfc_mpnn_t *net, sfc_system_t *sys, const double *r, double *z);
 /* Training on the GPU.  Pairs come from Jacobi-PCG on the system's current
  * right-hand side: the initial residual and the iterates after k iterations,

@@ -101,6 +101,31 @@ def apply(params, Ahat, sdinv, mask, r, bf16_ops=True):
     return f["s"] * sdinv * f["yhat"]
 
 
+def apply_inference(params, Ahat, sdinv, mask, r):
+    """M(r) as the inference kernels compute it: rhat = D^-1/2 r in float32
+    scaled by float32(1/s) after the aggregation, activations stored in BF16
+    (H0..H2 rounded after the relu), aggregation of the stored values in
+    float, the last layer's relu output fed to the decoder unrounded."""
+    E, eb, W, b, dw, db = unpack(params)
+    t = np.asarray(r, dtype=np.float64) * sdinv
+    s = np.sqrt(float(t @ t) / len(t))
+    f32 = np.float32
+    rhat = t.astype(f32)
+    inv = f32(1.0 / s if s > 0 else 0.0)
+    x0 = (rhat * inv).astype(np.float64)
+    ax0 = ((Ahat @ rhat.astype(np.float64)).astype(f32) * inv).astype(np.float64)
+    Hc = bf16(np.maximum(np.outer(x0, E[:, 0]) + np.outer(ax0, E[:, 1]) + eb, 0.0))
+    for l in range(LAYERS):
+        Y = Ahat @ Hc
+        Z = np.concatenate([Hc, bf16(Y)], axis=1) @ bf16(W[l]).T + b[l]
+        Hc = np.maximum(Z, 0.0)
+        if l + 1 < LAYERS:
+            Hc = bf16(Hc)
+    free = ~np.asarray(mask, dtype=bool)
+    yhat = x0 + np.where(free, Hc @ dw + db, 0.0)
+    return s * sdinv * yhat
+
+
 def loss_grad(params, Ahat, sdinv, mask, r, e, bf16_ops=True):
     """(loss, gradient) for one residual/error pair."""
     rnd = bf16 if bf16_ops else (lambda a: np.asarray(a, dtype=np.float64))

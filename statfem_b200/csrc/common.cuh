@@ -353,6 +353,8 @@ void solve_block(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, in
 void transpose_fixup(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
 double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n);
 void spmv_op64(sfc_system *s, const double *x, double *y);
+// y = S x and *xy += x . y, skipped entirely when *done != 0 (done may be NULL)
+void spmv_op64_dot(sfc_system *s, const double *x, double *y, double *xy, const int *done);
 void lifted_rhs(sfc_system *s, double *b);
 struct PcgStats {
     int iters;

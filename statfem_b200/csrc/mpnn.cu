@@ -58,6 +58,9 @@ struct sfc_mpnn {
     sfc::DBuf<float> ahat, sdinv;
     // activations and gradients
     sfc::DBuf<float> x0, ax0, yhat, tgt, dvec, qvec, H[LAYERS + 1], Y[LAYERS + 1], dH0, dH1, dY;
+    sfc::DBuf<__nv_bfloat16> hb[2];  // inference activations (BF16, ping-pong)
+    sfc::DBuf<double> fcg_sc;        // flexible-CG scalars, per iteration
+    sfc::DBuf<int> fcg_flags;        // done, breakdown
     sfc::DBuf<double> scal;  // [0]: N s^2 = |D^-1/2 r|^2, [1]: loss
     // training pairs (FP64, N each)
     sfc::DBuf<double> pr, pe;
@@ -165,13 +168,16 @@ __global__ void k_x0(const double *__restrict__ r, const float *__restrict__ sdi
 }
 
 // scal[slot] += sum (D^-1/2 v)^2
-__global__ void k_scaled_norm2(const double *__restrict__ v, const float *__restrict__ sdinv, int64_t N, double *out)
+// (and rhat = FP32(D^-1/2 v) when rhat != NULL)
+__global__ void k_scaled_norm2(const double *__restrict__ v, const float *__restrict__ sdinv, int64_t N, double *out,
+                               float *__restrict__ rhat = nullptr)
 {
     __shared__ double sh[32];
     double s = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
         const double t = v[i] * (double)sdinv[i];
         s += t * t;
+        if (rhat) rhat[i] = (float)t;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -264,15 +270,6 @@ __global__ void k_decoder(const float *__restrict__ H3, const float *__restrict_
         const float s = warp_sumf(fmaf(w0, h.x, w1 * h.y));
         if (lane == 0) yhat[i] = mask[i] ? x0[i] : x0[i] + s + c;
     }
-}
-
-// z = s D^-1/2 yhat  (FP64 output; N s^2 in scal[0])
-__global__ void k_unscale(const float *__restrict__ yhat, const float *__restrict__ sdinv, const double *scal,
-                          int64_t N, double *__restrict__ z)
-{
-    const double s = sqrt(scal[0] / (double)N);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
-        z[i] = s * (double)sdinv[i] * (double)yhat[i];
 }
 
 // target t = D^1/2 e / s
@@ -485,6 +482,179 @@ __global__ void k_to_bf16(const float *__restrict__ P, __nv_bfloat16 *__restrict
     }
 }
 
+// ---- inference: BF16 activations, gather fused with the dense transform --------
+// The stored activations are the BF16 values the tensor-core products round
+// them to anyway; the aggregation reads them (half the gather traffic of
+// FP32) and accumulates in FP32.
+constexpr int kLS = 68;  // shared-memory row stride in 32-bit words (136 BF16): conflict-free fragments
+
+__device__ __forceinline__ float2 bf16x2_to_f2(uint32_t u)
+{
+    __nv_bfloat162 v = *reinterpret_cast<__nv_bfloat162 *>(&u);
+    return __bfloat1622float2(v);
+}
+
+// x0 = rhat / s, H0 = BF16(relu(E [x0, Ahat x0] + e)) with Ahat x0 =
+// (Ahat rhat) / s; 8 lanes per node (8 features each), 4 nodes per warp trip
+__global__ void k_encoder_inf(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                              const float *__restrict__ v, const float *__restrict__ rhat, const double *scal,
+                              const float *__restrict__ P, int64_t N, float *__restrict__ x0, uint4 *__restrict__ H0)
+{
+    const int lane = threadIdx.x & 31, sub = lane >> 3, fl = lane & 7;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const float inv = scal[0] > 0 ? (float)(1.0 / sqrt(scal[0] / (double)N)) : 0.f;
+    float e0[8], e1[8], eb[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        e0[q] = P[OFF_EW + 2 * (fl * 8 + q)];
+        e1[q] = P[OFF_EW + 2 * (fl * 8 + q) + 1];
+        eb[q] = P[OFF_EB + fl * 8 + q];
+    }
+    for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 4; base < N; base += nwarps * 4) {
+        const int64_t i = base + sub;
+        const bool valid = i < N;
+        float acc = 0.f;
+        if (valid)
+            for (int32_t k = rp[i] + fl; k < rp[i + 1]; k += 8) acc = fmaf(v[k], rhat[col[k]], acc);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+        if (!valid) continue;
+        const float xi = rhat[i] * inv, ax = acc * inv;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            w[q] = pack_bf16(fmaxf(fmaf(e0[2 * q], xi, fmaf(e1[2 * q], ax, eb[2 * q])), 0.f),
+                             fmaxf(fmaf(e0[2 * q + 1], xi, fmaf(e1[2 * q + 1], ax, eb[2 * q + 1])), 0.f));
+        H0[i * 8 + fl] = make_uint4(w[0], w[1], w[2], w[3]);
+        if (fl == 0) x0[i] = xi;
+    }
+}
+
+// One message-passing layer, 16 nodes per warp: gather Ahat Hin for the
+// tile's rows into shared memory beside the rows of Hin, then
+// [Hin | Ahat Hin] W^T on BF16 mma fragments (FP32 accumulate), bias, relu.
+// DECODE (last layer): instead of storing H, z = s D^-1/2 (x0 + w . H + c)
+// (x0 alone on constrained dofs).
+template <bool DECODE>
+__global__ void __launch_bounds__(128) k_layer_inf(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                                   const float *__restrict__ v, const uint32_t *__restrict__ Hin,
+                                                   const __nv_bfloat16 *__restrict__ W, const float *__restrict__ bias,
+                                                   int64_t N, uint32_t *__restrict__ Hout,
+                                                   const float *__restrict__ P, const float *__restrict__ x0,
+                                                   const float *__restrict__ sdinv,
+                                                   const unsigned char *__restrict__ mask, const double *scal,
+                                                   double *__restrict__ z)
+{
+    __shared__ __align__(16) uint32_t sW[H * kLS];
+    __shared__ __align__(16) uint32_t sA[4][16 * kLS];
+    const uint32_t *W32 = reinterpret_cast<const uint32_t *>(W);
+    for (int t = threadIdx.x; t < H * H; t += blockDim.x) sW[(t / H) * kLS + (t % H)] = W32[t];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    uint32_t *tileA = sA[warp];
+    const int64_t tiles = (N + 15) / 16;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t tile = blockIdx.x * (int64_t)(blockDim.x >> 5) + warp; tile < tiles; tile += nwarps) {
+        // gather: 8 lanes per row (8 features = 16 bytes each), 4 rows at a
+        // time, 8 neighbours per trip with independent loads
+        const int sub = lane >> 3, fl = lane & 7;
+        const uint4 *Hin4 = reinterpret_cast<const uint4 *>(Hin);
+        for (int pass = 0; pass < 4; ++pass) {
+            const int rr = pass * 4 + sub;
+            const int64_t i = tile * 16 + rr;
+            const bool valid = i < N;
+            const int32_t b = valid ? rp[i] : 0;
+            const int len = valid ? rp[i + 1] - b : 0;
+            int maxlen = len;
+            maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, 8));
+            maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, 16));
+            float acc[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) acc[q] = 0.f;
+            for (int s0 = 0; s0 < maxlen; s0 += 8) {
+                const int sl = s0 + fl;
+                const int32_t cv = sl < len ? col[b + sl] : 0;  // padding: row 0 with weight 0
+                const float av = sl < len ? v[b + sl] : 0.f;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int32_t cj = __shfl_sync(0xffffffffu, cv, j, 8);
+                    const float aj = __shfl_sync(0xffffffffu, av, j, 8);
+                    const uint4 u = Hin4[(int64_t)cj * 8 + fl];
+                    const float2 f0 = bf16x2_to_f2(u.x), f1 = bf16x2_to_f2(u.y), f2 = bf16x2_to_f2(u.z),
+                                 f3 = bf16x2_to_f2(u.w);
+                    acc[0] = fmaf(aj, f0.x, acc[0]);
+                    acc[1] = fmaf(aj, f0.y, acc[1]);
+                    acc[2] = fmaf(aj, f1.x, acc[2]);
+                    acc[3] = fmaf(aj, f1.y, acc[3]);
+                    acc[4] = fmaf(aj, f2.x, acc[4]);
+                    acc[5] = fmaf(aj, f2.y, acc[5]);
+                    acc[6] = fmaf(aj, f3.x, acc[6]);
+                    acc[7] = fmaf(aj, f3.y, acc[7]);
+                }
+            }
+            const uint4 hv = valid ? Hin4[i * 8 + fl] : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4 *>(&tileA[rr * kLS + fl * 4]) = hv;
+            *reinterpret_cast<uint4 *>(&tileA[rr * kLS + 32 + fl * 4]) =
+                make_uint4(pack_bf16(acc[0], acc[1]), pack_bf16(acc[2], acc[3]), pack_bf16(acc[4], acc[5]),
+                           pack_bf16(acc[6], acc[7]));
+        }
+        __syncwarp();
+        float acc[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+            const int kw = ks * 8 + tig;  // 32-bit word of columns (k, k+1), k = ks*16 + 2*tig
+            const uint32_t a[4] = {tileA[gid * kLS + kw], tileA[(gid + 8) * kLS + kw], tileA[gid * kLS + kw + 4],
+                                   tileA[(gid + 8) * kLS + kw + 4]};
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int n = nt * 8 + gid;
+                mma16816(acc[nt], a, sW[n * kLS + kw], sW[n * kLS + kw + 4]);
+            }
+        }
+        __syncwarp();
+        if constexpr (!DECODE) {
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int c = nt * 8 + tig * 2;
+                const float b0 = bias[c], b1 = bias[c + 1];
+                tileA[gid * kLS + c / 2] = pack_bf16(fmaxf(acc[nt][0] + b0, 0.f), fmaxf(acc[nt][1] + b1, 0.f));
+                tileA[(gid + 8) * kLS + c / 2] = pack_bf16(fmaxf(acc[nt][2] + b0, 0.f), fmaxf(acc[nt][3] + b1, 0.f));
+            }
+            __syncwarp();
+            for (int rr = 0; rr < 16; ++rr) {
+                const int64_t i = tile * 16 + rr;
+                if (i < N) Hout[i * (H / 2) + lane] = tileA[rr * kLS + lane];
+            }
+            __syncwarp();
+        } else {
+            float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int c = nt * 8 + tig * 2;
+                const float b0 = bias[c], b1 = bias[c + 1], w0 = P[OFF_DW + c], w1 = P[OFF_DW + c + 1];
+                y0 = fmaf(w0, fmaxf(acc[nt][0] + b0, 0.f), fmaf(w1, fmaxf(acc[nt][1] + b1, 0.f), y0));
+                y1 = fmaf(w0, fmaxf(acc[nt][2] + b0, 0.f), fmaf(w1, fmaxf(acc[nt][3] + b1, 0.f), y1));
+            }
+            y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+            y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+            y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+            if (tig == 0) {
+                const double sc = sqrt(scal[0] / (double)N);
+                const float c0 = P[OFF_DB];
+                const int64_t i0 = tile * 16 + gid, i1 = i0 + 8;
+                if (i0 < N) z[i0] = sc * (double)sdinv[i0] * (double)(mask[i0] ? x0[i0] : x0[i0] + y0 + c0);
+                if (i1 < N) z[i1] = sc * (double)sdinv[i1] * (double)(mask[i1] ? x0[i1] : x0[i1] + y1 + c0);
+            }
+        }
+    }
+}
+
 // ---- host side -------------------------------------------------------------------
 void refresh_bf16(sfc_mpnn *m)
 {
@@ -512,6 +682,8 @@ void bind(sfc_mpnn *m, sfc_system *s)
             m->H[l].alloc(N * H);
             m->Y[l].alloc(N * H);
         }
+        m->hb[0].alloc(N * H);
+        m->hb[1].alloc(N * H);
         m->dH0.alloc(N * H);
         m->dH1.alloc(N * H);
         m->dY.alloc(N * H);
@@ -615,12 +787,34 @@ double loss_grad(sfc_mpnn *m, const double *r, const double *e, double w)
     return hl;
 }
 
-// z = M(r) (device FP64 vectors)
+// z = M(r) (device FP64 vectors): the inference kernels, no host synchronisation
 void apply(sfc_mpnn *m, const double *r, double *z)
 {
-    forward(m, r);
-    k_unscale<<<grid_for(m->N, 256), 256, 0, m->ctx->stream>>>(m->yhat.p, m->sdinv.p, m->scal.p, m->N, z);
-    count_launch(m->ctx);
+    sfc_ctx *ctx = m->ctx;
+    const sfc_system *s = m->op_sys;
+    const int64_t N = m->N;
+    ProfScope ps(ctx, "mpnn_apply", 0.0);
+    SFC_CK(cudaMemsetAsync(m->scal.p, 0, sizeof(double), ctx->stream));
+    k_scaled_norm2<<<grid_for(N, 256, ctx->sm_count * 4), 256, 0, ctx->stream>>>(r, m->sdinv.p, N, m->scal.p,
+                                                                                   m->ax0.p);
+    k_encoder_inf<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->ax0.p, m->scal.p,
+                                                       m->params.p, N, m->x0.p, reinterpret_cast<uint4 *>(m->hb[0].p));
+    count_launch(ctx, 2);
+    const unsigned g = (unsigned)std::min<int64_t>((N + 63) / 64, (int64_t)ctx->sm_count * 12);
+    for (int l = 0; l < LAYERS; ++l) {
+        const uint32_t *hin = reinterpret_cast<const uint32_t *>(m->hb[l & 1].p);
+        uint32_t *hout = reinterpret_cast<uint32_t *>(m->hb[(l + 1) & 1].p);
+        const __nv_bfloat16 *W = m->wbf.p + l * H * 2 * H;
+        const float *b = m->params.p + OFF_L + l * LSZ + H * 2 * H;
+        if (l + 1 < LAYERS)
+            k_layer_inf<false><<<g, 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, hin, W, b, N, hout,
+                                                           m->params.p, m->x0.p, m->sdinv.p, s->mask.p, m->scal.p,
+                                                           nullptr);
+        else
+            k_layer_inf<true><<<g, 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, hin, W, b, N, nullptr,
+                                                          m->params.p, m->x0.p, m->sdinv.p, s->mask.p, m->scal.p, z);
+        count_launch(ctx);
+    }
 }
 
 void adam_step(sfc_mpnn *m, double lr)
@@ -696,23 +890,89 @@ __global__ void k_resid(const double *__restrict__ b, const double *__restrict__
         r[i] = b[i] - Sx[i];
 }
 
-__global__ void k_axpy(double *__restrict__ y, const double *__restrict__ x, double a, int64_t n)
+__device__ double block_sum_d(double v, double *sh)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        y[i] += a * x[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;  // valid in thread 0
 }
 
-__global__ void k_xpby(double *__restrict__ p, const double *__restrict__ z, double beta, int64_t n)
+// *out += a . b unless *done
+__global__ void k_dot_done(const double *__restrict__ a, const double *__restrict__ b, int64_t n, double *out,
+                           const int *done)
 {
+    __shared__ double sh[32];
+    if (done && *done) return;
+    double v = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = z[i] + beta * p[i];
+        v += a[i] * b[i];
+    v = block_sum_d(v, sh);
+    if (threadIdx.x == 0) atomicAdd(out, v);
+}
+
+// alpha = (p.r)/(p.q); x += alpha p; r -= alpha q; rr' += r.r
+__global__ void k_fcg_update(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
+                             const double *__restrict__ q, int64_t n, const double *pq, const double *pr,
+                             double *rr_next, const int *done, int *err)
+{
+    __shared__ double sh[32];
+    if (*done) return;
+    const double den = *pq;
+    if (!(den > 0.0)) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
+    const double alpha = *pr / den;
+    double c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        c += ri * ri;
+    }
+    c = block_sum_d(c, sh);
+    if (threadIdx.x == 0) atomicAdd(rr_next, c);
+}
+
+__global__ void k_fcg_check(const double *rr, double thr, int it, int *done, const int *err)
+{
+    if (!*done && !*err && *rr <= thr) *done = it;
+}
+
+// beta = -(z.q)/(p.q); p = z + beta p; pr' += p.r
+__global__ void k_fcg_pupdate(double *__restrict__ p, const double *__restrict__ z, const double *__restrict__ r,
+                              int64_t n, const double *zq, const double *pq, double *pr_next, const int *done,
+                              const int *err)
+{
+    __shared__ double sh[32];
+    if (*done || *err) return;
+    const double beta = -*zq / *pq;
+    double c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double pi = z[i] + beta * p[i];
+        p[i] = pi;
+        c += pi * r[i];
+    }
+    c = block_sum_d(c, sh);
+    if (threadIdx.x == 0) atomicAdd(pr_next, c);
 }
 
 }  // namespace
 
-// Flexible CG (FCG(1), Notay 2000) with z = M(r) from the network; the
-// convergence test is the true FP64 residual ||b - S x|| <= tol ||b||,
-// recomputed whenever the recurrence residual says converged.
+// Flexible CG (FCG(1), Notay 2000) with z = M(r) from the network:
+// alpha = p.r / p.Sp, p' = z - (z.Sp / p.Sp) p.  The scalars live on the
+// device (one slot per iteration) and the host reads the flags every
+// check_every iterations, so the iteration issues no synchronisation.  When
+// the recurrence residual meets tol, the true FP64 residual ||b - S x|| is
+// computed; if it misses tol, the method restarts from it.
 void solve_forward_fcg(sfc_system *s)
 {
     sfc_ctx *ctx = s->ctx;
@@ -722,61 +982,77 @@ void solve_forward_fcg(sfc_system *s)
     const int64_t N = s->N;
     const auto &o = s->opt;
     const int max_iter = o.max_iter > 0 ? o.max_iter : 20000;
+    const int check = o.check_every > 0 ? o.check_every : 8;
     const double tol = o.tol > 0 ? o.tol : 1e-8;
     s->X.alloc(N);
-    DBuf<double> b, r, z, p, q, t;
-    b.alloc(N);
-    r.alloc(N);
-    z.alloc(N);
-    p.alloc(N);
-    q.alloc(N);
-    t.alloc(N);
+    s->blk64.reserve(6 * N);
+    double *b = s->blk64.p, *r = b + N, *z = r + N, *p = z + N, *q = p + N, *t = q + N;
+    const int64_t slots = (int64_t)max_iter + 2;
+    m->fcg_sc.reserve(4 * slots);
+    double *pq = m->fcg_sc.p, *pr = pq + slots, *rr = pr + slots, *zq = rr + slots;
+    m->fcg_flags.reserve(2);
+    int *done = m->fcg_flags.p, *err = done + 1;
     cudaEvent_t e0, e1;
     SFC_CK(cudaEventCreate(&e0));
     SFC_CK(cudaEventCreate(&e1));
     SFC_CK(cudaEventRecord(e0, ctx->stream));
-    lifted_rhs(s, b.p);
+    SFC_CK(cudaMemsetAsync(m->fcg_sc.p, 0, 4 * slots * sizeof(double), ctx->stream));
+    SFC_CK(cudaMemsetAsync(done, 0, 2 * sizeof(int), ctx->stream));
+    lifted_rhs(s, b);
     SFC_CK(cudaMemsetAsync(s->X.p, 0, N * 8, ctx->stream));
-    SFC_CK(cudaMemcpyAsync(r.p, b.p, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-    const double bb = device_dot(ctx, b.p, b.p, N);
-    const unsigned g = grid_for(N, 256);
-    int it = 0;
+    SFC_CK(cudaMemcpyAsync(r, b, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    const double bb = device_dot(ctx, b, b, N);
+    const double thr = tol * tol * bb;
+    const unsigned g = grid_for(N, 256, ctx->sm_count * 4);
+    auto true_residual = [&]() {  // r = b - S x, returns |r| / |b|
+        spmv_op64(s, s->X.p, t);
+        k_resid<<<grid_for(N, 256), 256, 0, ctx->stream>>>(b, t, N, r);
+        count_launch(ctx);
+        return std::sqrt(device_dot(ctx, r, r, N) / bb);
+    };
+    auto start = [&](int slot) {  // direction from the current residual
+        apply(m, r, z);
+        SFC_CK(cudaMemcpyAsync(p, z, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        spmv_op64_dot(s, p, q, pq + slot, nullptr);
+        k_dot_done<<<g, 256, 0, ctx->stream>>>(p, r, N, pr + slot, nullptr);
+        count_launch(ctx);
+    };
+    int it = 0, iters = 0;
     bool conv = bb == 0.0;
     double rel = 0.0;
     if (!conv) {
-        apply(m, r.p, z.p);
-        SFC_CK(cudaMemcpyAsync(p.p, z.p, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-        spmv_op64(s, p.p, q.p);
-        double pr = device_dot(ctx, p.p, r.p, N), pq = device_dot(ctx, p.p, q.p, N);
-        while (it < max_iter) {
-            if (!(pq > 0.0)) fail(SFC_ERR_NOT_SPD, "flexible CG breakdown: p^T A p <= 0");
-            ++it;
-            const double alpha = pr / pq;
-            k_axpy<<<g, 256, 0, ctx->stream>>>(s->X.p, p.p, alpha, N);
-            k_axpy<<<g, 256, 0, ctx->stream>>>(r.p, q.p, -alpha, N);
+        ProfScope ps(ctx, "fcg_iterations", 0.0);
+        start(0);
+        for (it = 0; it < max_iter; ++it) {
+            k_fcg_update<<<g, 256, 0, ctx->stream>>>(s->X.p, r, p, q, N, pq + it, pr + it, rr + it + 1, done, err);
+            k_fcg_check<<<1, 1, 0, ctx->stream>>>(rr + it + 1, thr, it + 1, done, err);
             count_launch(ctx, 2);
-            const double rr = device_dot(ctx, r.p, r.p, N);
-            if (rr <= tol * tol * bb) {
-                // confirm with the true residual; continue from it if the
-                // recurrence has drifted
-                spmv_op64(s, s->X.p, t.p);
-                k_resid<<<g, 256, 0, ctx->stream>>>(b.p, t.p, N, r.p);
-                count_launch(ctx);
-                rel = std::sqrt(device_dot(ctx, r.p, r.p, N) / bb);
-                if (rel <= tol) {
-                    conv = true;
-                    break;
+            apply(m, r, z);
+            k_dot_done<<<g, 256, 0, ctx->stream>>>(z, q, N, zq + it, done);
+            k_fcg_pupdate<<<g, 256, 0, ctx->stream>>>(p, z, r, N, zq + it, pq + it, pr + it + 1, done, err);
+            count_launch(ctx, 2);
+            spmv_op64_dot(s, p, q, pq + it + 1, done);
+            if ((it + 1) % check == 0 || it + 1 == max_iter) {
+                int hf[2];
+                download(ctx, hf, done, 2);
+                if (hf[1]) fail(SFC_ERR_NOT_SPD, "flexible CG breakdown: p^T A p <= 0");
+                if (hf[0]) {
+                    iters = hf[0];
+                    rel = true_residual();
+                    if (rel <= tol) {
+                        conv = true;
+                        break;
+                    }
+                    // the recurrence drifted: restart from the true residual
+                    SFC_CK(cudaMemsetAsync(done, 0, sizeof(int), ctx->stream));
+                    if (it + 1 < max_iter) start(it + 1);
                 }
             }
-            apply(m, r.p, z.p);
-            const double beta = -device_dot(ctx, z.p, q.p, N) / pq;  // S-orthogonal to the last direction
-            k_xpby<<<g, 256, 0, ctx->stream>>>(p.p, z.p, beta, N);
-            count_launch(ctx);
-            spmv_op64(s, p.p, q.p);
-            pr = device_dot(ctx, p.p, r.p, N);
-            pq = device_dot(ctx, p.p, q.p, N);
         }
-        if (!conv) rel = std::sqrt(device_dot(ctx, r.p, r.p, N) / bb);
+        if (!conv) {
+            iters = max_iter;
+            rel = true_residual();
+        }
     }
     SFC_CK(cudaEventRecord(e1, ctx->stream));
     float ms = 0;
@@ -785,7 +1061,7 @@ void solve_forward_fcg(sfc_system *s)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     s->stats = {};
-    s->stats.iterations = it;
+    s->stats.iterations = iters;
     s->stats.num_rhs = 1;
     s->stats.converged = conv ? 1 : 0;
     s->stats.max_rel_residual = rel;

@@ -1141,6 +1141,10 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
 
 // y = S x with the FP64 operator (used by the flexible solver in mpnn.cu)
 void spmv_op64(sfc_system *s, const double *x, double *y) { launch_spmv64(s, x, y, nullptr, nullptr); }
+void spmv_op64_dot(sfc_system *s, const double *x, double *y, double *xy, const int *done)
+{
+    launch_spmv64(s, x, y, xy, done);
+}
 
 // lifted right-hand side b = F - K_fc u_c (see k_lift)
 void lifted_rhs(sfc_system *s, double *b)

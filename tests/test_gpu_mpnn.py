@@ -59,10 +59,13 @@ def test_loss_and_gradient_match_oracle(ctx, kind, n):
     for a, b in blocks:
         err = np.linalg.norm(g[a:b] - g_ref[a:b])
         assert err <= 1e-2 * np.linalg.norm(g_ref[a:b]) + 1e-6 * np.linalg.norm(g_ref), (a, b, err)
-    # and the application M(r)
+    # the application M(r) by the inference kernels (BF16 activations)
     z = net.apply(s, r)
-    z_ref = R.apply(p, Ahat, sdinv, mask, r)
+    z_ref = R.apply_inference(p, Ahat, sdinv, mask, r)
     assert np.linalg.norm(z - z_ref) <= 1e-3 * np.linalg.norm(z_ref)
+    # and its distance from the FP32-activation forward the training uses
+    z_tr = R.apply(p, Ahat, sdinv, mask, r)
+    assert np.linalg.norm(z - z_tr) <= 3e-2 * np.linalg.norm(z_tr)
     net.close()
 
 
