@@ -348,6 +348,68 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(out))
 
 
+def run_learned(args, ws, rank, local):
+    """Learned-preconditioner workload: 3-D Poisson, 128^3 hex8 elements
+    (2,146,689 dofs), log-conductivity Matérn nu=3/2 (sigma 1, length 0.1).
+    The network is trained on the GPU on --c5-train samples of a
+    --c5-train-n^3 grid (the network is local, so it transfers across grid
+    sizes), then every held-out 128^3 sample is solved to the true relative
+    residual 1e-8 by flexible CG with the network and by plain FP64
+    Jacobi-PCG; value = held-out solves/s of the learned method."""
+    from statfem_b200 import api
+    from statfem_b200 import learned as L
+    ctx = api.Context(local)
+    tr = L.PoissonSamples(ctx, args.c5_train_n, seed0=10_000 + 1000 * rank)
+    net = api.LearnedPreconditioner(ctx, seed=0)
+    info = L.train(net, tr, list(range(args.c5_train)), epochs=1, steps_per_sample=args.c5_steps,
+                   checkpoint=None, lr=1e-3, batch=4)
+    te = L.PoissonSamples(ctx, 128, seed0=900_000 + 1000 * rank)
+    coeffs = [te.coefficients(k) for k in range(args.warmup + args.steps)]
+    net.attach(te.system)
+    rows = []
+    for k, c in enumerate(coeffs):
+        s = te.assemble(k, c)
+        s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=50000, check_every=32)
+        s.solveSystem()
+        sp = s.last_stats()
+        u_pcg = s.giveSolution()
+        s.set_options(method=api.SFC_SOLVER_FCG_MPNN, tol=1e-8, max_iter=50000, check_every=8)
+        s.solveSystem()
+        sf = s.last_stats()
+        u = s.giveSolution()
+        if k >= args.warmup:
+            rows.append((sp, sf, float(np.abs(u - u_pcg).max() / np.abs(u_pcg).max())))
+    pcg_ms = max_over_ranks(ws, sum(r[0]["device_ms"] for r in rows))
+    fcg_ms = max_over_ranks(ws, sum(r[1]["device_ms"] for r in rows))
+    n = len(rows)
+    out = {
+        "metric": "held-out solves/s at rel. residual 1e-8 (FCG + learned preconditioner), 128^3 Poisson",
+        "value": round(ws * n / (fcg_ms / 1e3), 4), "unit": "solves/s", "n_gpus": ws, "steps": n,
+        "warmup": args.warmup, "ms_per_step": round(fcg_ms / n, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (network BF16 x BF16 -> FP32)",
+        "data": "synthetic (seeded Matérn 3/2 log-conductivity, circulant embedding)",
+        "config": {"workload": "3-D Poisson, 128^3 hex8 (2,146,689 dofs), log-conductivity Matérn nu=3/2 "
+                               "sigma 1 length 0.1, u=0 on the boundary, f=1, rel. residual 1e-8",
+                   "train": "%d samples of %d^3, %d Adam steps each (batch 4 pairs), 1 epoch"
+                            % (args.c5_train, args.c5_train_n, args.c5_steps),
+                   "held_out": n, "parallelism": "replicas" if ws > 1 else "single GPU"},
+        "plain_pcg": {"value": round(ws * n / (pcg_ms / 1e3), 4), "unit": "solves/s",
+                      "ms_per_step": round(pcg_ms / n, 2),
+                      "iterations_mean": float(np.mean([r[0]["iterations"] for r in rows]))},
+        "learned": {"iterations_mean": float(np.mean([r[1]["iterations"] for r in rows])),
+                    "max_rel_residual": max(r[1]["max_rel_residual"] for r in rows),
+                    "max_rel_diff_vs_pcg": max(r[2] for r in rows)},
+        "iteration_ratio": round(float(np.mean([r[0]["iterations"] for r in rows])) /
+                                 float(np.mean([r[1]["iterations"] for r in rows])), 3),
+        "time_ratio": round(pcg_ms / fcg_ms, 3),
+        "training": {"seconds": round(info["seconds"], 2), "steps": int(len(info["loss"])),
+                     "loss_first": round(float(info["loss"][:20].mean()), 4),
+                     "loss_last": round(float(info["loss"][-20:].mean()), 4)},
+    }
+    if rank == 0:
+        print(json.dumps(out))
+
+
 def plain_fp64_estimate(g, wl, step_ms, block_stats, fwd_stats, sample):
     """Posterior solves/s of the plain method on the same GPU: FP64 Jacobi-PCG,
     one right-hand side at a time.  The forward solve is measured in full;
@@ -408,9 +470,40 @@ def cpu_baseline(args, wl, g, sample_iters):
                                                                          wl["ns"], its)}
 
 
+def run_reference_c5(args):
+    """CPU arm of the learned-preconditioner workload: the oracle's C
+    assembly and FP64 Jacobi-PCG (1 core) on one held-out 128^3 sample,
+    solved in full to the relative residual 1e-8."""
+    from oracle import oracle as O
+    mesh = mg.unit_cube_hex(128, mg.HEX8_POISSON)
+    rng = np.random.default_rng(900_000)
+    coeff = np.exp(mg.matern32_field_cells(rng, 128, 1.0, 0.1))
+    bc = mg.dirichlet_dofs(mesh, "all")
+    rp, col, val, F = O.fem(mesh, 8, np.array([1.0]), bc, coeff=coeff)
+    mask = np.zeros(mesh.num_dofs, dtype=np.uint8)
+    mask[bc] = 1
+    t0 = time.perf_counter()
+    x, its = O.pcg(rp, col, val, mask, F, tol=1e-8, max_iter=100000)
+    dt = time.perf_counter() - t0
+    value = 1.0 / dt
+    out = {"impl": "reference", "metric": "held-out solves/s at rel. residual 1e-8 (FCG + learned "
+           "preconditioner), 128^3 Poisson", "value": round(value, 6), "unit": "solves/s", "n_gpus": 0,
+           "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic (seeded Matérn 3/2 log-conductivity)",
+           "config": {"workload": "3-D Poisson, 128^3 hex8 (2,146,689 dofs), rel. residual 1e-8",
+                      "method": "CPU FP64 Jacobi-PCG (oracle port)"},
+           "cpu_baseline": {"value": round(value, 6), "unit": "solves/s", "cores": 1, "kind": "port",
+                            "sample": "one held-out sample solved in full: %d iterations, %.1f s" % (its, dt)},
+           "e2e": {"value": round(value, 6), "unit": "solves/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
+    if args.config == "c5":
+        return run_reference_c5(args)
     from oracle import oracle as O
     wl = make_workload(args.config, seed=1234)
     mesh = wl["mesh"]
@@ -448,7 +541,10 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5"])
+    ap.add_argument("--c5-train", type=int, default=48, help="c5: training samples")
+    ap.add_argument("--c5-train-n", type=int, default=32, help="c5: training grid (elements per side)")
+    ap.add_argument("--c5-steps", type=int, default=40, help="c5: Adam steps per training sample")
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cpu-iters", type=int, default=100)
     ap.add_argument("--plain-sample", type=int, default=8)
@@ -462,6 +558,8 @@ def main():
                                                                 int(os.environ.get("RANK", "0")), 0)
     if args.impl == "reference":
         run_reference(args, ws, rank)
+    elif args.config == "c5":
+        run_learned(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
         if ws > 1:
