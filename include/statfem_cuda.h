@@ -348,6 +348,56 @@ int32_t sfc_mpnn_train(sfc_mpnn_t *net, sfc_system_t *sys, const sfc_mpnn_train_
 /* Attach (net != NULL) or detach the network used by SFC_SOLVER_FCG_MPNN. */
 int32_t sfc_system_set_mpnn(sfc_system_t *sys, sfc_mpnn_t *net);
 
+/* ---- batched instances (MCMC proposals) -------------------------------------- */
+/* No single reference counterpart: the reference evaluates one statFEM
+ * instance at a time (ForwardGaussRHS::updateSolution, ForwardGaussRHS.hpp:
+ * 95-139; LikelihoodKOH::giveLogLikelihood and giveProjFEconditionedData,
+ * LikelihoodKOH.ipp:75-120, 311-361), once per MCMC proposal
+ * (hyperParamLearning.hpp:90-249).  Here num_instances 2-D Poisson statFEM
+ * instances are one union mesh (SFC_ELEM_TRI3_POISSON): instance i owns dofs
+ * [dof_offset[i], dof_offset[i+1]), the (grid_side[i]+1)^2 nodes of the unit
+ * square grid, x fastest (checked).  bc_dofs: the homogeneous Dirichlet dofs
+ * of all instances.  Sensors: num_sensors[i] <= 32 per instance, the rows of
+ * P as num_instances x 32 x 3 global dofs (-1 = unused) and weights, and
+ * num_instances x 32 x 2 coordinates (for the mismatch covariance).
+ * forcing_mean: the constant body force f.  cluster_size: CTAs per instance
+ * (0: 8; the largest size the device can co-schedule is used).
+ * One sfc_batch_run assembles all instances (coefficients from
+ * sfc_batch_set_coefficients, one value per element of the union mesh) and
+ * runs one persistent kernel, captured once in a CUDA graph, that solves the
+ * ns adjoint systems of every instance (FP32 block PCG, FP64 residual
+ * refinement to the relative residual tol), forms mean and C_s at the
+ * sensors (C_s with the Kronecker-factored forcing covariance) and evaluates
+ * the log-likelihood and the posterior mean / covariance at the sensors in
+ * FP64.  Per-instance status: SFC_OK, SFC_ERR_NOT_CONVERGED or
+ * SFC_ERR_NOT_SPD (breakdown, NaN, Cholesky failure); a failing instance
+ * does not stop the others. */
+typedef struct sfc_batch sfc_batch_t;
+int32_t sfc_batch_create(sfc_ctx_t *ctx, const sfc_mesh_t *mesh, int32_t num_instances,
+                         const int64_t *dof_offset, const int32_t *grid_side, const uint32_t *bc_dofs,
+                         int64_t num_bc, const int32_t *num_sensors, const int32_t *sensor_dofs,
+                         const double *sensor_weights, const double *sensor_coords, double forcing_mean,
+                         int32_t cluster_size, sfc_batch_t **out);
+int32_t sfc_batch_destroy(sfc_batch_t *batch);
+/* The launch shape in use: CTAs per cluster and CTAs in the grid. */
+int32_t sfc_batch_cluster_size(const sfc_batch_t *batch, int32_t *cluster, int32_t *grid);
+/* tol: true relative residual of every adjoint column (default 1e-8);
+ * inner_tol: FP32 reduction per refinement cycle (1e-4); max_iter: inner
+ * iteration cap per instance. */
+int32_t sfc_batch_set_solver(sfc_batch_t *batch, double tol, double inner_tol, int32_t max_iter);
+int32_t sfc_batch_set_coefficients(sfc_batch_t *batch, const double *elem_coeff);
+/* One sfc_hparams_t per instance (each proposal has its own), reg: the
+ * ForwardGaussRHS regularisation (C_s += (sigma_f reg)^2 P P^T). */
+int32_t sfc_batch_set_hparams(sfc_batch_t *batch, const sfc_hparams_t *hp, double reg);
+/* y: num_instances x 32 x num_readings (rows past num_sensors ignored). */
+int32_t sfc_batch_set_readings(sfc_batch_t *batch, const double *y, int32_t num_readings);
+int32_t sfc_batch_run(sfc_batch_t *batch);
+/* Host copies of the last run's results (any pointer may be NULL):
+ * loglik (n), mean_s (n x 32), cov_s (n x 32 x 32), post_mean (n x 32),
+ * post_cov (n x 32 x 32), status (n), iterations (n, inner iterations). */
+int32_t sfc_batch_results(sfc_batch_t *batch, double *loglik, double *mean_s, double *cov_s,
+                          double *post_mean, double *post_cov, int32_t *status, int32_t *iterations);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,6 +153,16 @@ SIGNATURES = {
     "sfc_mpnn_default_train_options": (_i32, [ctypes.POINTER(MpnnTrainOptions)]),
     "sfc_mpnn_train": (_i32, [_vp, _vp, ctypes.POINTER(MpnnTrainOptions), _dp]),
     "sfc_system_set_mpnn": (_i32, [_vp, _vp]),
+    "sfc_batch_create": (_i32, [_vp, _vp, _i32, _i64p, _i32p, _u32p, _i64, _i32p, _i32p, _dp, _dp, _d, _i32,
+                                ctypes.POINTER(_vp)]),
+    "sfc_batch_destroy": (_i32, [_vp]),
+    "sfc_batch_cluster_size": (_i32, [_vp, _i32p, _i32p]),
+    "sfc_batch_set_solver": (_i32, [_vp, _d, _d, _i32]),
+    "sfc_batch_set_coefficients": (_i32, [_vp, _dp]),
+    "sfc_batch_set_hparams": (_i32, [_vp, ctypes.POINTER(HParams), _d]),
+    "sfc_batch_set_readings": (_i32, [_vp, _dp, _i32]),
+    "sfc_batch_run": (_i32, [_vp]),
+    "sfc_batch_results": (_i32, [_vp, _dp, _dp, _dp, _dp, _dp, _i32p, _i32p]),
 }
 
 _lib = None
@@ -589,6 +599,102 @@ class LearnedPreconditioner:
             self.h = None
 
 
+class BatchStatFEM:
+    """Many independent 2-D Poisson statFEM instances (the blocks of one union
+    mesh, e.g. MCMC proposals) evaluated by one persistent kernel in a CUDA
+    graph: adjoint solves, prior mean / covariance at the sensors,
+    LikelihoodKOH log-likelihood and sensor-space posterior per instance.
+    sensors: per instance (P, coords) with P the (indptr, indices, data)
+    projection rows in the instance's local dofs (<= 3 entries per row, at
+    most 32 rows) and coords ns x 2."""
+
+    MAX_SENSORS = 32
+
+    def __init__(self, ctx, mesh, dof_offset, sides, bc_dofs, sensors, forcing_mean=1.0, cluster_size=0):
+        self.ctx = ctx
+        self.mesh = mesh
+        off = _arr(dof_offset, np.int64)
+        n = len(off) - 1
+        self.n = n
+        K = self.MAX_SENSORS
+        ns = np.zeros(n, dtype=np.int32)
+        sdof = -np.ones((n, K, 3), dtype=np.int32)
+        sw = np.zeros((n, K, 3))
+        sc = np.zeros((n, K, 2))
+        for i, ((ip, ix, dv), xy) in enumerate(sensors):
+            m = len(ip) - 1
+            if m > K:
+                raise ValueError("at most %d sensors per instance" % K)
+            ns[i] = m
+            for c in range(m):
+                cnt = ip[c + 1] - ip[c]
+                if cnt > 3:
+                    raise ValueError("a projection row has more than 3 entries")
+                sdof[i, c, :cnt] = off[i] + np.asarray(ix[ip[c]:ip[c + 1]])
+                sw[i, c, :cnt] = dv[ip[c]:ip[c + 1]]
+            sc[i, :m] = np.asarray(xy)[:, :2]
+        self.ns = ns
+        sides = _arr(sides, np.int32)
+        bc = _arr(bc_dofs, np.uint32)
+        h = _vp()
+        ctx.check(ctx.lib.sfc_batch_create(ctx.h, mesh.h, n, _p(off, _i64p), _p(sides, _i32p), _p(bc, _u32p), len(bc),
+                                           _p(ns, _i32p), _p(sdof, _i32p), _p(sw, _dp), _p(sc, _dp),
+                                           float(forcing_mean), int(cluster_size), ctypes.byref(h)))
+        self.h = h
+
+    def launch_shape(self):
+        c, g = ctypes.c_int32(), ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.sfc_batch_cluster_size(self.h, ctypes.byref(c), ctypes.byref(g)))
+        return c.value, g.value
+
+    def set_solver(self, tol=1e-8, inner_tol=1e-4, max_iter=50000):
+        self.ctx.check(self.ctx.lib.sfc_batch_set_solver(self.h, tol, inner_tol, int(max_iter)))
+
+    def set_coefficients(self, coeff):
+        c = _arr(coeff, np.float64)
+        self.ctx.check(self.ctx.lib.sfc_batch_set_coefficients(self.h, _p(c, _dp)))
+
+    def set_hparams(self, hps, reg=1e-3):
+        """hps: one reference-style hyperparameter map per instance (or one for all)."""
+        if isinstance(hps, dict):
+            hps = [hps] * self.n
+        arr = (HParams * self.n)(*[HParams.from_map(h) for h in hps])
+        self.ctx.check(self.ctx.lib.sfc_batch_set_hparams(self.h, arr, float(reg)))
+
+    def set_readings(self, Y):
+        """Y: n x ns_i x n_o (a list of per-instance arrays, or an n x 32 x n_o array)."""
+        if isinstance(Y, np.ndarray) and Y.ndim == 3 and Y.shape[1] == self.MAX_SENSORS:
+            full = _arr(Y, np.float64)
+        else:
+            n_o = np.asarray(Y[0]).reshape(len(Y[0]), -1).shape[1]
+            full = np.zeros((self.n, self.MAX_SENSORS, n_o))
+            for i, y in enumerate(Y):
+                y = np.asarray(y, dtype=np.float64).reshape(len(y), -1)
+                full[i, : y.shape[0]] = y
+        self.ctx.check(self.ctx.lib.sfc_batch_set_readings(self.h, _p(full, _dp), full.shape[2]))
+
+    def run(self):
+        self.ctx.check(self.ctx.lib.sfc_batch_run(self.h))
+
+    def results(self):
+        n, K = self.n, self.MAX_SENSORS
+        ll = np.zeros(n)
+        ms = np.zeros((n, K))
+        cs = np.zeros((n, K, K))
+        pm = np.zeros((n, K))
+        pc = np.zeros((n, K, K))
+        st = np.zeros(n, dtype=np.int32)
+        it = np.zeros(n, dtype=np.int32)
+        self.ctx.check(self.ctx.lib.sfc_batch_results(self.h, _p(ll, _dp), _p(ms, _dp), _p(cs, _dp), _p(pm, _dp),
+                                                      _p(pc, _dp), _p(st, _i32p), _p(it, _i32p)))
+        return dict(loglik=ll, mean_s=ms, cov_s=cs, post_mean=pm, post_cov=pc, status=st, iterations=it)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_batch_destroy(self.h)
+            self.h = None
+
+
 __all__ = ["Context", "Mesh", "SystemSolveCuda", "CovarianceForcing", "ForwardGaussRHS", "LikelihoodKOH",
-           "LearnedPreconditioner", "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64",
+           "LearnedPreconditioner", "BatchStatFEM", "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64",
            "SFC_SOLVER_PCG_MIXED", "SFC_SOLVER_FCG_MPNN"]

@@ -886,7 +886,7 @@ void apply_constraints_dev(sfc_system *s, const uint32_t *idx_dev, const double 
 
 static void build_bsr(sfc_system *s);
 
-void build_operator(sfc_system *s)
+void build_operator(sfc_system *s, bool require_positive_diag)
 {
     if (s->op_valid) return;
     sfc_ctx *ctx = s->ctx;
@@ -911,7 +911,7 @@ void build_operator(sfc_system *s)
     int h = 0;
     download(ctx, &h, err.p, 1);
     if (h == 4) fail(SFC_ERR_BAD_ARG, "a row has no diagonal entry");
-    if (h == 5) fail(SFC_ERR_NOT_SPD, "non-positive diagonal entry: the operator is not SPD");
+    if (h == 5 && require_positive_diag) fail(SFC_ERR_NOT_SPD, "non-positive diagonal entry: the operator is not SPD");
     build_bsr(s);
     s->op_valid = true;
 }

@@ -344,7 +344,9 @@ void assemble_matrix(sfc_system *s, const sfc_mesh *m);
 void assemble_load(sfc_ctx *ctx, const sfc_mesh *m, const double *f, double *F_dev, bool zero_first);
 void apply_constraints_dev(sfc_system *s, const uint32_t *idx_dev, const double *val_dev, int64_t n,
                            double factor, double scalar);
-void build_operator(sfc_system *s);
+// require_positive_diag: fail on a non-positive (or NaN) diagonal entry; the
+// batch path passes false and lets the affected instance fail alone
+void build_operator(sfc_system *s, bool require_positive_diag = true);
 void flush_staged(sfc_system *s);
 void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);
 // solvers.cu

@@ -232,3 +232,19 @@ def matern32_field_cells(rng, n, sigma, length, dim=3, pad=2):
     f = f[tuple(slice(0, n) for _ in range(dim))]
     # C order is (axis0, axis1, axis2); make x (the last index) fastest
     return np.ascontiguousarray(f).ravel()
+
+
+def disjoint_union(meshes):
+    """One mesh holding the given meshes as disjoint blocks (node ids and dofs
+    offset block by block).  Returns (mesh, dof_offset)."""
+    kind = meshes[0].kind
+    coords, conn, off = [], [], [0]
+    base = 0
+    for m in meshes:
+        if m.kind != kind:
+            raise ValueError("all meshes must have the same element kind")
+        coords.append(m.coords)
+        conn.append(m.conn + base)
+        base += m.num_nodes
+        off.append(off[-1] + m.num_dofs)
+    return Mesh(kind, np.concatenate(coords), np.concatenate(conn).astype(np.uint32)), np.array(off, dtype=np.int64)
