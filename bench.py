@@ -410,6 +410,201 @@ def run_learned(args, ws, rank, local):
         print(json.dumps(out))
 
 
+C3_HP = {"forcing.sigma": 0.1, "forcing.length": 0.2, "rho": 1.0, "mismatch.sigma": 0.0,
+         "mismatch.length": 0.2, "mismatch.sensorEps": 1e-3}
+# algorithmic bytes of one FP32 block-PCG inner iteration per dof, 32 columns:
+# CSR row (7 nnz x 8 B + 4 B), p gather and own row 2 x 128, q write 128,
+# update (x, r, p, q read, x, r write, dinv) 6 x 128 + 4, p update (p, r read,
+# p write, dinv) 3 x 128 + 4
+C3_BYTES_PER_DOF_ITER = 60 + 256 + 128 + 772 + 388
+
+
+def make_batch_workload(seed, n_inst=512, smin=32, smax=256, ns=32):
+    """Config 3: n_inst 2-D Poisson statFEM instances, side s ~ U{smin..smax}
+    cells, P1 triangles, log-conductivity squared-exponential (sigma 0.5,
+    length ~ U[0.05, 0.5]) sampled exactly on the cell-centre grid (both
+    triangles of a cell share the value), ns sensors at seeded interior
+    points, forcing GP sigma_f 0.1 length 0.2, sensor noise 1e-3."""
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(smin, smax + 1, n_inst)
+    meshes, coeffs, bcs, sensors = [], [], [], []
+    for s in sides:
+        s = int(s)
+        mesh = mg.unit_square_tri(s)
+        ax = mg.cell_centre_axes(s)
+        g = mg.se_field_tensor(rng, [ax, ax], 0.5, rng.uniform(0.05, 0.5))
+        coeffs.append(np.repeat(np.exp(g), 2))
+        pts = mg.interior_points(rng, ns, 2, margin=0.02)
+        sensors.append((mg.projection_matrix(mesh, pts), pts))
+        bcs.append(mg.dirichlet_dofs(mesh, "all"))
+        meshes.append(mesh)
+    union, off = mg.disjoint_union(meshes)
+    bc = np.concatenate([b + off[k] for k, b in enumerate(bcs)])
+    return dict(sides=sides, meshes=meshes, coeff=np.concatenate(coeffs), coeffs=coeffs, bcs=bcs,
+                sensors=sensors, union=union, off=off, bc=bc, ns=ns, rng=rng,
+                desc="%d 2-D Poisson statFEM instances, sides U{%d..%d} (P1 triangles, %d dofs in total), "
+                     "%d sensors each, log-likelihood + posterior at the sensors, rel. residual 1e-8"
+                     % (n_inst, smin, smax, int(off[-1]), ns))
+
+
+def run_batch(args, ws, rank, local):
+    """Config 3 on our GPU path: every step assembles all instances and runs
+    the persistent batch kernel (CUDA graph)."""
+    from statfem_b200 import api
+    wl = make_batch_workload(4321 + rank, n_inst=args.c3_instances)
+    n = len(wl["sides"])
+    ctx = api.Context(local)
+    t0 = time.perf_counter()
+    gm = api.Mesh(ctx, mg.TRI3_POISSON, 3, wl["union"].coords, wl["union"].conn)
+    b = api.BatchStatFEM(ctx, gm, wl["off"], wl["sides"], wl["bc"], wl["sensors"], 1.0, args.cluster)
+    b.set_solver(tol=1e-8)
+    b.set_coefficients(wl["coeff"])
+    b.set_hparams(C3_HP, REG)
+    # observations drawn from each instance's prior plus noise
+    b.set_readings(np.zeros((n, 32, 1)))
+    b.run()
+    r = b.results()
+    Y = np.zeros((n, 32, 1))
+    m = wl["ns"]
+    for k in range(n):
+        pts = wl["sensors"][k][1]
+        D = pts[:, None, :] - pts[None, :, :]
+        Ks = C3_HP["mismatch.sigma"] ** 2 * np.exp(-np.sum(D * D, axis=2) / (2 * C3_HP["mismatch.length"] ** 2)) \
+            + C3_HP["mismatch.sensorEps"] ** 2 * np.eye(m)
+        C = Ks + C3_HP["rho"] ** 2 * r["cov_s"][k, :m, :m]
+        Y[k, :m, 0] = C3_HP["rho"] * r["mean_s"][k, :m] + np.linalg.cholesky(C) @ wl["rng"].standard_normal(m)
+    b.set_readings(Y)
+    setup_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        b.run()
+    ctx.synchronize()
+    barrier(ws)
+    cuda_sync(ws)
+    l0 = ctx.kernel_launches()
+    with ClockSampler(local) as clk:
+        ctx.mark(0)
+        for _ in range(args.steps):
+            b.run()
+        ctx.mark(1)
+        ctx.synchronize()
+    cuda_sync(ws)
+    barrier(ws)
+    ms = max_over_ranks(ws, ctx.marker_ms(0, 1))
+    launches = ctx.kernel_launches() - l0
+    res = b.results()
+    # phase split and the persistent kernel's own time (one profiled step)
+    ctx.set_profiling(True)
+    b.run()
+    ctx.synchronize()
+    ctx.set_profiling(False)
+    prof = ctx.profile_report()
+    kern_ms = prof.get("phase:batch_solve_likelihood", (1, float("nan"), 0))[1]
+    asm_ms = prof.get("phase:batch_assembly", (1, float("nan"), 0))[1]
+    dofs = np.diff(wl["off"])
+    alg_bytes = float(np.sum(res["iterations"].astype(np.float64) * dofs) * C3_BYTES_PER_DOF_ITER)
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    # end to end: coefficients and readings from host memory, results back
+    ctx.synchronize()
+    ctx.mark(2)
+    for _ in range(args.steps):
+        b.set_coefficients(wl["coeff"])
+        b.set_readings(Y)
+        b.run()
+        b.results()
+    ctx.mark(3)
+    ctx.synchronize()
+    e2e_ms = max_over_ranks(ws, ctx.marker_ms(2, 3))
+    h2d = wl["coeff"].nbytes + Y.nbytes
+    d2h = 8 * n * (1 + 32 + 32 * 32 + 32 + 32 * 32) + 8 * n
+    value = ws * n * args.steps / (ms / 1e3)
+    cs, grid = b.launch_shape()
+    out = {
+        "metric": "posterior solves/s at rel. residual 1e-8 (batched instances, 1xB200)",
+        "value": round(value, 3), "unit": "posterior solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals, covariance and Cholesky)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": wl["desc"], "cluster_size": cs, "grid_ctas": grid,
+                   "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (solver vectors 17 GB)"},
+        "e2e": {"value": round(ws * n * args.steps / (e2e_ms / 1e3), 3), "unit": "posterior solves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "k_batch (persistent)", "bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_source": peak_kind, "bytes_per_launch": alg_bytes,
+                     "avg_launch_us": round(kern_ms * 1e3, 1),
+                     "algorithmic_bytes": "%d B per dof per inner iteration x sum(iterations x dofs)"
+                                          % C3_BYTES_PER_DOF_ITER},
+        "phases_ms_per_step": {"assembly": round(asm_ms, 2), "solve_likelihood_kernel": round(kern_ms, 2)},
+        "iterations": {"mean": float(res["iterations"].mean()), "max": int(res["iterations"].max())},
+        "status_ok": int((res["status"] == 0).sum()),
+        "setup_s": round(setup_s, 1),
+        "clocks": clk.summary(),
+    }
+    if args.plain_sample > 0:
+        out["plain_fp64"] = batch_plain_estimate(ctx, wl, args.plain_sample)
+        out["speedup_vs_plain_fp64"] = round(out["value"] / ws / out["plain_fp64"]["value"], 2)
+    if rank == 0:
+        print(json.dumps(out))
+    b.close()
+
+
+def batch_plain_estimate(ctx, wl, sample):
+    """Posterior solves/s of the plain method on the same GPU for config 3:
+    each instance through the single-system path (SystemSolveCuda with FP64
+    Jacobi-PCG, one right-hand side at a time; ForwardGaussRHS;
+    LikelihoodKOH), timed on `sample` instances spread over the sizes and
+    interpolated in the side length to all instances."""
+    from statfem_b200 import api
+    sides = wl["sides"]
+    order = np.argsort(sides)
+    pick = order[np.linspace(0, len(order) - 1, sample).astype(int)]
+    times = []
+    for k in pick:
+        mesh = wl["meshes"][k]
+        gm = api.Mesh(ctx, mg.TRI3_POISSON, 3, mesh.coords, mesh.conn)
+        gm.set_coefficients(wl["coeffs"][k])
+        s = api.SystemSolveCuda(ctx, mesh.num_dofs)
+        s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=100000, check_every=32)
+        cf = api.CovarianceForcing(ctx, gm)
+        cf.applyConstraints(wl["bcs"][k])
+        fg = api.ForwardGaussRHS(s, cf, REG)
+        fg.setProjectionMatrix(wl["sensors"][k][0])
+        koh = api.LikelihoodKOH(fg, wl["sensors"][k][1])
+        koh.setSensorValues(np.zeros((wl["ns"], 1)))
+        zero = np.zeros(len(wl["bcs"][k]))
+
+        def one():
+            s.assemble(gm)
+            s.clearRhs()
+            s.assemble_load(gm, np.array([1.0]))
+            s.applyConstraints((wl["bcs"][k], zero))
+            fg.updateSolution(C3_HP)
+            koh.giveLogLikelihood(C3_HP)
+            koh.giveProjFEconditionedData(C3_HP)
+
+        one()
+        ctx.synchronize()
+        ctx.mark(6)
+        one()
+        ctx.mark(7)
+        ctx.synchronize()
+        times.append(ctx.marker_ms(6, 7))
+        for o in (koh, fg, cf, s, gm):
+            o.close()
+    xs = sides[pick].astype(float)
+    est = float(np.sum(np.interp(sides.astype(float), xs, np.array(times))))
+    return {"value": round(len(sides) / (est / 1e3), 4), "unit": "posterior solves/s",
+            "ms_per_step": round(est, 1),
+            "sample": "%d instances (sides %s) through the single-system path with FP64 Jacobi-PCG, one RHS at a "
+                      "time: %s ms; interpolated in the side length over all %d instances"
+                      % (sample, ",".join(str(int(v)) for v in xs), ",".join("%.1f" % t for t in times),
+                         len(sides))}
+
+
 def plain_fp64_estimate(g, wl, step_ms, block_stats, fwd_stats, sample):
     """Posterior solves/s of the plain method on the same GPU: FP64 Jacobi-PCG,
     one right-hand side at a time.  The forward solve is measured in full;
@@ -541,7 +736,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c5"])
+    ap.add_argument("--c3-instances", type=int, default=512, help="c3: number of instances")
+    ap.add_argument("--cluster", type=int, default=0, help="c3: CTAs per instance (0: default)")
     ap.add_argument("--c5-train", type=int, default=48, help="c5: training samples")
     ap.add_argument("--c5-train-n", type=int, default=32, help="c5: training grid (elements per side)")
     ap.add_argument("--c5-steps", type=int, default=40, help="c5: Adam steps per training sample")
@@ -560,6 +757,8 @@ def main():
         run_reference(args, ws, rank)
     elif args.config == "c5":
         run_learned(args, ws, rank, local)
+    elif args.config == "c3":
+        run_batch(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
         if ws > 1:

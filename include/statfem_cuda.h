@@ -392,11 +392,35 @@ int32_t sfc_batch_set_hparams(sfc_batch_t *batch, const sfc_hparams_t *hp, doubl
 /* y: num_instances x 32 x num_readings (rows past num_sensors ignored). */
 int32_t sfc_batch_set_readings(sfc_batch_t *batch, const double *y, int32_t num_readings);
 int32_t sfc_batch_run(sfc_batch_t *batch);
+/* Autotuner: times the batch kernel with 1, 2, 4, 8 and 16 CTAs per
+ * instance on the current inputs and keeps the fastest (cached per device
+ * and shape class, see sfc_autotune_save; remeasure = 0 takes a cached
+ * choice when there is one). */
+int32_t sfc_batch_autotune(sfc_batch_t *batch, int32_t remeasure, int32_t *cluster);
 /* Host copies of the last run's results (any pointer may be NULL):
  * loglik (n), mean_s (n x 32), cov_s (n x 32 x 32), post_mean (n x 32),
  * post_cov (n x 32 x 32), status (n), iterations (n, inner iterations). */
 int32_t sfc_batch_results(sfc_batch_t *batch, double *loglik, double *mean_s, double *cov_s,
                           double *post_mean, double *post_cov, int32_t *status, int32_t *iterations);
+
+/* ---- autotuner ----------------------------------------------------------------- */
+/* No reference counterpart.  Launch shapes chosen by measurement on the
+ * caller's problem and kept in a process-wide table keyed by device and
+ * problem shape class (dof count, dofs per node, row length, right-hand
+ * sides); remeasure = 0 reuses a stored choice for the same class.
+ * sfc_autotune_spmv: lanes per row of the FP64 SpMV (4, 8, 16 or 32), set
+ * on the system.  sfc_autotune_block_solver: block width and preconditioner
+ * of SFC_SOLVER_PCG_MIXED, by the time to solution of the first
+ * min(nrhs, 128) of the given right-hand sides (rhs: nrhs x num_dofs, host,
+ * as sfc_solve_transpose), set on the system's options (tol and max_iter
+ * kept) and returned in best. */
+int32_t sfc_autotune_spmv(sfc_system_t *sys, int32_t remeasure, int32_t *lanes);
+int32_t sfc_autotune_block_solver(sfc_system_t *sys, const double *rhs, int32_t nrhs, int32_t remeasure,
+                                  sfc_solver_options_t *best);
+/* The table as text, one "key value" line per shape class. */
+int32_t sfc_autotune_save(const char *path);
+int32_t sfc_autotune_load(const char *path);
+int32_t sfc_autotune_clear(void);
 
 #ifdef __cplusplus
 }

@@ -163,6 +163,12 @@ SIGNATURES = {
     "sfc_batch_set_readings": (_i32, [_vp, _dp, _i32]),
     "sfc_batch_run": (_i32, [_vp]),
     "sfc_batch_results": (_i32, [_vp, _dp, _dp, _dp, _dp, _dp, _i32p, _i32p]),
+    "sfc_batch_autotune": (_i32, [_vp, _i32, _i32p]),
+    "sfc_autotune_spmv": (_i32, [_vp, _i32, _i32p]),
+    "sfc_autotune_block_solver": (_i32, [_vp, _dp, _i32, _i32, ctypes.POINTER(SolverOptions)]),
+    "sfc_autotune_save": (_i32, [ctypes.c_char_p]),
+    "sfc_autotune_load": (_i32, [ctypes.c_char_p]),
+    "sfc_autotune_clear": (_i32, []),
 }
 
 _lib = None
@@ -289,6 +295,20 @@ class SystemSolveCuda:
                     block_width=0, check_every=16, precond=SFC_PRECOND_JACOBI):
         o = SolverOptions(method, max_iter, tol, inner_tol, block_width, check_every, precond)
         self.ctx.check(self.ctx.lib.sfc_system_set_options(self.h, ctypes.byref(o)))
+
+    def autotune_spmv(self, remeasure=False):
+        v = ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.sfc_autotune_spmv(self.h, int(bool(remeasure)), ctypes.byref(v)))
+        return v.value
+
+    def autotune_block_solver(self, rhs, remeasure=False):
+        """Tune block width and preconditioner of the mixed solver on these
+        right-hand sides (nrhs x num_dofs); returns the chosen options."""
+        R = _arr(rhs, np.float64).reshape(-1, self.N)
+        o = SolverOptions()
+        self.ctx.check(self.ctx.lib.sfc_autotune_block_solver(self.h, _p(R, _dp), R.shape[0], int(bool(remeasure)),
+                                                              ctypes.byref(o)))
+        return {k: getattr(o, k) for k, _ in o._fields_}
 
     def last_stats(self):
         s = SolveStats()
@@ -642,6 +662,11 @@ class BatchStatFEM:
                                            float(forcing_mean), int(cluster_size), ctypes.byref(h)))
         self.h = h
 
+    def autotune(self, remeasure=False):
+        c = ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.sfc_batch_autotune(self.h, int(bool(remeasure)), ctypes.byref(c)))
+        return c.value
+
     def launch_shape(self):
         c, g = ctypes.c_int32(), ctypes.c_int32()
         self.ctx.check(self.ctx.lib.sfc_batch_cluster_size(self.h, ctypes.byref(c), ctypes.byref(g)))
@@ -695,6 +720,22 @@ class BatchStatFEM:
             self.h = None
 
 
+def autotune_save(path):
+    lib = load()
+    if lib.sfc_autotune_save(str(path).encode()):
+        raise SfcError(-2, "cannot write %s" % path)
+
+
+def autotune_load(path):
+    lib = load()
+    if lib.sfc_autotune_load(str(path).encode()):
+        raise SfcError(-2, "cannot read %s" % path)
+
+
+def autotune_clear():
+    load().sfc_autotune_clear()
+
+
 __all__ = ["Context", "Mesh", "SystemSolveCuda", "CovarianceForcing", "ForwardGaussRHS", "LikelihoodKOH",
            "LearnedPreconditioner", "BatchStatFEM", "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64",
-           "SFC_SOLVER_PCG_MIXED", "SFC_SOLVER_FCG_MPNN"]
+           "SFC_SOLVER_PCG_MIXED", "SFC_SOLVER_FCG_MPNN", "autotune_save", "autotune_load", "autotune_clear"]

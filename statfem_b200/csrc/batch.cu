@@ -36,8 +36,9 @@
 // Covariance: k is separable on the grid, K = Ky (x) Kx with Toeplitz
 // factors k1d[|a - a'|], so Z = K W (W = diag(phibar) R^T) costs two passes
 // of O((s+1)^3 ns) and C_s = sigma^2 W^T Z.
-// Workspace per dof: R^T (then Z) and W, T in FP64 [dof][32]; the FP32
-// solver vectors x, r, p, q [dof][32].
+// Workspace per dof: R^T (then Z) and W, T in FP64 [dof][32] (W holds the
+// dense right-hand sides during the solve); the FP32 solver vectors x, r,
+// p, q [dof][32].
 
 #include <cooperative_groups.h>
 
@@ -131,6 +132,43 @@ __device__ void cluster_sum2(cg::cluster_group &cl, const Smem &s, int &slot, do
     __syncthreads();
 }
 
+// The same for the quad layout: lane (g, fl) holds partials of columns
+// 4 fl .. 4 fl + 3 for its rows; the 4 row groups are combined first.
+__device__ void cluster_sum_q(cg::cluster_group &cl, const Smem &s, int &slot, const double (&v0)[4],
+                              const double (&v1)[4])
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, fl = lane & 7;
+    double *red = s.sred + 64 * slot;
+    slot = slot == 2 ? 0 : slot + 1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        double a = v0[q], b = v1[q];
+        a += __shfl_xor_sync(0xffffffffu, a, 8);
+        a += __shfl_xor_sync(0xffffffffu, a, 16);
+        b += __shfl_xor_sync(0xffffffffu, b, 8);
+        b += __shfl_xor_sync(0xffffffffu, b, 16);
+        if (lane < 8) {
+            s.swp[warp * 64 + 4 * fl + q] = a;
+            s.swp[warp * 64 + 32 + 4 * fl + q] = b;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+        double t = 0.0;
+        for (int w = 0; w < BW; ++w) t += s.swp[w * 64 + threadIdx.x];
+        red[threadIdx.x] = t;
+    }
+    __threadfence();
+    cl.sync();
+    if (threadIdx.x < 64) {
+        double t = 0.0;
+        const unsigned cs = cl.num_blocks();
+        for (unsigned r = 0; r < cs; ++r) t += cl.map_shared_rank(red, r)[threadIdx.x];
+        s.sres[threadIdx.x] = t;
+    }
+    __syncthreads();
+}
+
 __device__ __forceinline__ void cluster_barrier(cg::cluster_group &cl)
 {
     __threadfence();
@@ -174,7 +212,7 @@ __device__ void warp_trsm(const double *L, double *X, int n, int m)
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(BT) k_batch(BatchArgs a)
+__global__ void __launch_bounds__(BT, 3) k_batch(BatchArgs a)
 {
     cg::cluster_group cl = cg::this_cluster();
     const unsigned CS = cl.num_blocks(), rank = cl.block_rank();
@@ -204,101 +242,199 @@ __global__ void __launch_bounds__(BT) k_batch(BatchArgs a)
         const int nsens = a.ns[inst];
         const int chunk = (n + (int)CS - 1) / (int)CS;
         const int64_t my0 = r0 + min(n, (int)rank * chunk), my1 = r0 + min(n, ((int)rank + 1) * chunk);
-        // this lane's column: right-hand side = row c of P (up to 3 entries)
-        int sd[3];
-        double swv[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            sd[k] = lane < nsens ? a.sdof[((int64_t)inst * BK + lane) * 3 + k] : -1;
-            swv[k] = lane < nsens ? a.sw[((int64_t)inst * BK + lane) * 3 + k] : 0.0;
-        }
         int status = 0, total_it = 0;
 
         // ---------------- solve: FP64 refinement around FP32 block PCG ----------------
-        for (int64_t i = my0 + warp; i < my1; i += BW) a.x64[i * BK + lane] = 0.0;
-        for (int cycle = 0;; ++cycle) {
-            double prr = 0.0, pbb = 0.0;
-            for (int64_t i = my0 + warp; i < my1; i += BW) {
-                const double bi = (i == sd[0] ? swv[0] : 0.0) + (i == sd[1] ? swv[1] : 0.0) +
-                                  (i == sd[2] ? swv[2] : 0.0);
-                double ri = bi;
-                if (cycle > 0)
-                    for (int32_t k = a.rp[i]; k < a.rp[i + 1]; ++k) ri -= a.a64[k] * a.x64[(int64_t)a.col[k] * BK + lane];
-                a.r32[i * BK + lane] = (float)ri;
-                a.x32[i * BK + lane] = 0.f;
-                prr += ri * ri;
-                pbb += bi * bi;
+        // Quad layout: a warp works on 4 rows at once, 8 lanes per row, each
+        // lane on 4 adjacent columns (16-byte vectors): four rows' loads are
+        // in flight per instruction.  Lane (g, fl): row i0 + g, columns 4 fl .. 4 fl + 3.
+        const int g = lane >> 3, fl = lane & 7;
+        float4 *X4 = reinterpret_cast<float4 *>(a.x32), *R4 = reinterpret_cast<float4 *>(a.r32);
+        float4 *P4 = reinterpret_cast<float4 *>(a.p32), *Q4 = reinterpret_cast<float4 *>(a.q32);
+        // right-hand sides b = P^T, dense in W (W is free until the statistics)
+        for (int64_t i = my0 + warp; i < my1; i += BW) {
+            a.x64[i * BK + lane] = 0.0;
+            a.W[i * BK + lane] = 0.0;
+        }
+        cluster_barrier(cl);
+        if (rank == 0 && warp == 0 && lane < nsens)
+            for (int k = 0; k < 3; ++k) {
+                const int d = a.sdof[((int64_t)inst * BK + lane) * 3 + k];
+                if (d >= r0 && d < r0 + n) a.W[(int64_t)d * BK + lane] += a.sw[((int64_t)inst * BK + lane) * 3 + k];
             }
-            cluster_sum2(cl, s, slot, prr, pbb);
-            const double rr0 = s.sres[lane], bb = s.sres[32 + lane];
-            const bool bad = !(rr0 == rr0) || !(bb == bb);
-            const bool done = bb == 0.0 || rr0 <= a.tol * a.tol * bb;
+        cluster_barrier(cl);
+        for (int cycle = 0;; ++cycle) {
+            double prr[4] = {0, 0, 0, 0}, pbb[4] = {0, 0, 0, 0};
+            for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
+                const int64_t i = i0 + g;
+                if (i >= my1) continue;
+                const double2 *b2 = reinterpret_cast<const double2 *>(a.W + i * BK + 4 * fl);
+                const double2 b01 = b2[0], b23 = b2[1];
+                double r[4] = {b01.x, b01.y, b23.x, b23.y};
+                const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+                if (cycle > 0)
+                    for (int32_t k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+                        const double av = a.a64[k];
+                        const double2 *x2 = reinterpret_cast<const double2 *>(a.x64 + (int64_t)a.col[k] * BK + 4 * fl);
+                        const double2 x01 = x2[0], x23 = x2[1];
+                        r[0] -= av * x01.x;
+                        r[1] -= av * x01.y;
+                        r[2] -= av * x23.x;
+                        r[3] -= av * x23.y;
+                    }
+                R4[i * 8 + fl] = make_float4((float)r[0], (float)r[1], (float)r[2], (float)r[3]);
+                X4[i * 8 + fl] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    prr[q] += r[q] * r[q];
+                    pbb[q] += bv[q] * bv[q];
+                }
+            }
+            cluster_sum_q(cl, s, slot, prr, pbb);
+            double rr0[4], bb[4];
+            bool done[4], bad = false;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                rr0[q] = s.sres[4 * fl + q];
+                bb[q] = s.sres[32 + 4 * fl + q];
+                bad = bad || !(rr0[q] == rr0[q]) || !(bb[q] == bb[q]);
+                done[q] = bb[q] == 0.0 || rr0[q] <= a.tol * a.tol * bb[q];
+            }
             if (__any_sync(0xffffffffu, bad)) {
                 status = SFC_ERR_NOT_SPD;
                 break;
             }
-            if (__all_sync(0xffffffffu, done)) break;
+            if (__all_sync(0xffffffffu, done[0] && done[1] && done[2] && done[3])) break;
             if (cycle >= a.max_cycles || total_it >= a.max_iter) {
                 status = SFC_ERR_NOT_CONVERGED;
                 break;
             }
             // inner FP32 PCG on S d = r for the open columns
-            bool act = !done;
-            const double thr = a.itol * a.itol * rr0;
-            double prz = 0.0;
-            for (int64_t i = my0 + warp; i < my1; i += BW) {
-                const float r = a.r32[i * BK + lane], z = a.dinv32[i] * r;
-                a.p32[i * BK + lane] = z;
-                prz += (double)r * (double)z;
+            bool act[4];
+            double thr[4], rz[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                act[q] = !done[q];
+                thr[q] = a.itol * a.itol * rr0[q];
             }
-            cluster_sum2(cl, s, slot, prz, 0.0);
-            double rz = s.sres[lane];
+            {
+                double prz[4] = {0, 0, 0, 0}, zero[4] = {0, 0, 0, 0};
+                for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
+                    const int64_t i = i0 + g;
+                    if (i >= my1) continue;
+                    const float4 r = R4[i * 8 + fl];
+                    const float d = a.dinv32[i];
+                    const float4 z = make_float4(d * r.x, d * r.y, d * r.z, d * r.w);
+                    P4[i * 8 + fl] = z;
+                    prz[0] += (double)r.x * z.x;
+                    prz[1] += (double)r.y * z.y;
+                    prz[2] += (double)r.z * z.z;
+                    prz[3] += (double)r.w * z.w;
+                }
+                cluster_sum_q(cl, s, slot, prz, zero);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) rz[q] = s.sres[4 * fl + q];
+            }
+            bool inner_bad = false;
             for (; total_it < a.max_iter; ++total_it) {
-                double ppq = 0.0;
-                for (int64_t i = my0 + warp; i < my1; i += BW) {
-                    float acc = 0.f;
-                    for (int32_t k = a.rp[i]; k < a.rp[i + 1]; ++k)
-                        acc = fmaf(a.a32[k], a.p32[(int64_t)a.col[k] * BK + lane], acc);
-                    a.q32[i * BK + lane] = acc;
-                    ppq += (double)a.p32[i * BK + lane] * (double)acc;
+                double ppq[4] = {0, 0, 0, 0}, zero[4] = {0, 0, 0, 0};
+                for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
+                    const int64_t i = i0 + g;
+                    if (i >= my1) continue;
+                    const int32_t kb = a.rp[i], ke = a.rp[i + 1];
+                    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int32_t k = kb; k < ke; k += 4) {
+                        // four independent neighbour loads (padding: weight 0 on the last entry)
+                        const int32_t k1 = min(k + 1, ke - 1), k2 = min(k + 2, ke - 1), k3 = min(k + 3, ke - 1);
+                        const float a0 = a.a32[k], a1 = k + 1 < ke ? a.a32[k1] : 0.f,
+                                    a2 = k + 2 < ke ? a.a32[k2] : 0.f, a3 = k + 3 < ke ? a.a32[k3] : 0.f;
+                        const float4 p0 = P4[(int64_t)a.col[k] * 8 + fl], p1 = P4[(int64_t)a.col[k1] * 8 + fl],
+                                     p2 = P4[(int64_t)a.col[k2] * 8 + fl], p3 = P4[(int64_t)a.col[k3] * 8 + fl];
+                        acc.x = fmaf(a0, p0.x, fmaf(a1, p1.x, fmaf(a2, p2.x, fmaf(a3, p3.x, acc.x))));
+                        acc.y = fmaf(a0, p0.y, fmaf(a1, p1.y, fmaf(a2, p2.y, fmaf(a3, p3.y, acc.y))));
+                        acc.z = fmaf(a0, p0.z, fmaf(a1, p1.z, fmaf(a2, p2.z, fmaf(a3, p3.z, acc.z))));
+                        acc.w = fmaf(a0, p0.w, fmaf(a1, p1.w, fmaf(a2, p2.w, fmaf(a3, p3.w, acc.w))));
+                    }
+                    Q4[i * 8 + fl] = acc;
+                    const float4 pi = P4[i * 8 + fl];
+                    ppq[0] += (double)pi.x * acc.x;
+                    ppq[1] += (double)pi.y * acc.y;
+                    ppq[2] += (double)pi.z * acc.z;
+                    ppq[3] += (double)pi.w * acc.w;
                 }
-                cluster_sum2(cl, s, slot, ppq, 0.0);
-                const double pq = s.sres[lane];
-                if (act && !(pq > 0.0)) {
-                    act = false;
-                    status = SFC_ERR_NOT_SPD;
+                cluster_sum_q(cl, s, slot, ppq, zero);
+                float alpha[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double pq = s.sres[4 * fl + q];
+                    if (act[q] && !(pq > 0.0)) {
+                        act[q] = false;
+                        inner_bad = true;
+                    }
+                    alpha[q] = act[q] ? (float)(rz[q] / pq) : 0.f;
                 }
-                const float alpha = act ? (float)(rz / pq) : 0.f;
-                double prz2 = 0.0, prr2 = 0.0;
-                for (int64_t i = my0 + warp; i < my1; i += BW) {
-                    const int64_t o = i * BK + lane;
-                    a.x32[o] = fmaf(alpha, a.p32[o], a.x32[o]);
-                    const float r = fmaf(-alpha, a.q32[o], a.r32[o]);
-                    a.r32[o] = r;
-                    const float z = a.dinv32[i] * r;
-                    prz2 += (double)r * (double)z;
-                    prr2 += (double)r * (double)r;
+                double prz2[4] = {0, 0, 0, 0}, prr2[4] = {0, 0, 0, 0};
+                for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
+                    const int64_t i = i0 + g;
+                    if (i >= my1) continue;
+                    const int64_t o = i * 8 + fl;
+                    const float4 pv = P4[o], qv = Q4[o];
+                    float4 xv = X4[o], rv = R4[o];
+                    const float d = a.dinv32[i];
+                    xv.x = fmaf(alpha[0], pv.x, xv.x);
+                    xv.y = fmaf(alpha[1], pv.y, xv.y);
+                    xv.z = fmaf(alpha[2], pv.z, xv.z);
+                    xv.w = fmaf(alpha[3], pv.w, xv.w);
+                    rv.x = fmaf(-alpha[0], qv.x, rv.x);
+                    rv.y = fmaf(-alpha[1], qv.y, rv.y);
+                    rv.z = fmaf(-alpha[2], qv.z, rv.z);
+                    rv.w = fmaf(-alpha[3], qv.w, rv.w);
+                    X4[o] = xv;
+                    R4[o] = rv;
+                    prz2[0] += (double)rv.x * (d * rv.x);
+                    prz2[1] += (double)rv.y * (d * rv.y);
+                    prz2[2] += (double)rv.z * (d * rv.z);
+                    prz2[3] += (double)rv.w * (d * rv.w);
+                    prr2[0] += (double)rv.x * rv.x;
+                    prr2[1] += (double)rv.y * rv.y;
+                    prr2[2] += (double)rv.z * rv.z;
+                    prr2[3] += (double)rv.w * rv.w;
                 }
-                cluster_sum2(cl, s, slot, prz2, prr2);
-                const double rzn = s.sres[lane], rrn = s.sres[32 + lane];
-                if (!(rrn == rrn)) {
-                    act = false;
-                    status = SFC_ERR_NOT_SPD;
+                cluster_sum_q(cl, s, slot, prz2, prr2);
+                float beta[4];
+                bool any = false;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double rzn = s.sres[4 * fl + q], rrn = s.sres[32 + 4 * fl + q];
+                    if (!(rrn == rrn)) {
+                        act[q] = false;
+                        inner_bad = true;
+                    }
+                    act[q] = act[q] && rrn > thr[q];
+                    beta[q] = act[q] ? (float)(rzn / rz[q]) : 0.f;
+                    rz[q] = rzn;
+                    any = any || act[q];
                 }
-                act = act && rrn > thr;
-                if (!__any_sync(0xffffffffu, act)) {
+                if (!__any_sync(0xffffffffu, any)) {
                     ++total_it;
                     break;
                 }
-                const float beta = act ? (float)(rzn / rz) : 0.f;
-                rz = rzn;
-                for (int64_t i = my0 + warp; i < my1; i += BW) {
-                    const int64_t o = i * BK + lane;
-                    a.p32[o] = fmaf(beta, a.p32[o], a.dinv32[i] * a.r32[o]);
+                for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
+                    const int64_t i = i0 + g;
+                    if (i >= my1) continue;
+                    const int64_t o = i * 8 + fl;
+                    const float4 rv = R4[o];
+                    float4 pv = P4[o];
+                    const float d = a.dinv32[i];
+                    pv.x = fmaf(beta[0], pv.x, d * rv.x);
+                    pv.y = fmaf(beta[1], pv.y, d * rv.y);
+                    pv.z = fmaf(beta[2], pv.z, d * rv.z);
+                    pv.w = fmaf(beta[3], pv.w, d * rv.w);
+                    P4[o] = pv;
                 }
                 cluster_barrier(cl);
             }
-            status = __any_sync(0xffffffffu, status != 0) ? SFC_ERR_NOT_SPD : 0;
+            status = __any_sync(0xffffffffu, inner_bad) ? SFC_ERR_NOT_SPD : 0;
             for (int64_t i = my0 + warp; i < my1; i += BW) a.x64[i * BK + lane] += (double)a.x32[i * BK + lane];
             cluster_barrier(cl);
             if (status) break;
@@ -877,6 +1013,57 @@ int32_t sfc_batch_run(sfc_batch_t *b)
 {
     if (!b) return SFC_ERR_BAD_ARG;
     return bguard(b->ctx, [&] { batch_run(b); });
+}
+
+int32_t sfc_batch_autotune(sfc_batch_t *b, int32_t remeasure, int32_t *cluster)
+{
+    if (!b) return SFC_ERR_BAD_ARG;
+    return bguard(b->ctx, [&] {
+        SFC_REQUIRE(b->have_y && b->have_hp, "set readings and hyperparameters before tuning the batch");
+        int smax_log = 0;
+        for (int v = b->smax; v > 1; v >>= 1) ++smax_log;
+        int nlog = 0;
+        for (int v = b->n; v > 1; v >>= 1) ++nlog;
+        const std::string key = "batch:" + tune_device_key(b->ctx) + ":i" + std::to_string(nlog) + ":s" +
+                                std::to_string(smax_log);
+        std::string v;
+        if (!remeasure && tune_lookup(key, v)) {
+            batch_release_graph(b);
+            batch_configure(b, std::atoi(v.c_str()));
+        } else {
+            sfc_ctx *ctx = b->ctx;
+            batch_assemble(b);
+            double best_ms = 1e300;
+            int best = b->cluster;
+            for (int cs : {1, 2, 4, 8, 16}) {
+                batch_release_graph(b);
+                batch_configure(b, cs);
+                if (b->cluster != cs) continue;  // not co-schedulable on this device
+                batch_capture(b);
+                SFC_CK(cudaGraphLaunch(b->gexec, ctx->stream));  // warm
+                cudaEvent_t e0, e1;
+                SFC_CK(cudaEventCreate(&e0));
+                SFC_CK(cudaEventCreate(&e1));
+                SFC_CK(cudaEventRecord(e0, ctx->stream));
+                SFC_CK(cudaGraphLaunch(b->gexec, ctx->stream));
+                SFC_CK(cudaEventRecord(e1, ctx->stream));
+                SFC_CK(cudaEventSynchronize(e1));
+                float ms = 0;
+                SFC_CK(cudaEventElapsedTime(&ms, e0, e1));
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                count_launch(ctx, 2);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = cs;
+                }
+            }
+            batch_release_graph(b);
+            batch_configure(b, best);
+            tune_store(key, std::to_string(best));
+        }
+        if (cluster) *cluster = b->cluster;
+    });
 }
 
 int32_t sfc_batch_results(sfc_batch_t *b, double *loglik, double *mean_s, double *cov_s, double *post_mean,

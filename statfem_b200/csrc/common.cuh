@@ -288,6 +288,7 @@ struct sfc_system {
     sfc::DBuf<uint32_t> cidx;  // constraint upload buffers
     sfc::DBuf<double> cval;
     struct sfc_mpnn *mpnn = nullptr;  // learned preconditioner for SFC_SOLVER_FCG_MPNN
+    int spmv_lanes = 0;               // lanes per row of the FP64 SpMV (0: by row length; set by the tuner)
 };
 
 // ---------------------------------------------------------------------------
@@ -365,6 +366,12 @@ struct PcgStats {
 PcgStats pcg64_public(sfc_system *s, const double *b, double *x, double tol, int max_iter, int check);
 // mpnn.cu
 void solve_forward_fcg(sfc_system *s);
+// solvers.cu: FP64 SpMV with a given number of lanes per row (4, 8, 16, 32)
+void spmv_op64_lanes(sfc_system *s, int lanes, const double *x, double *y);
 // stats.cu
 void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp);
+// autotune.cu: the process-wide table of tuned launch shapes
+std::string tune_device_key(sfc_ctx *ctx);
+bool tune_lookup(const std::string &key, std::string &val);
+void tune_store(const std::string &key, const std::string &val);
 }  // namespace sfc

@@ -828,13 +828,14 @@ void launch_spmv64(sfc_system *s, const double *x, double *y, double *dot, const
     sfc_ctx *ctx = s->ctx;
     ProfScope ps(ctx, "spmv64", (double)s->nnz * 12 + 4.0 * (s->N + 1) + 16.0 * s->N);
     const unsigned grid = (unsigned)(ctx->sm_count * 8);
-    if (avg > 24)
+    const int lanes = s->spmv_lanes;  // tuned, else chosen by the mean row length
+    if (lanes == 32 || (lanes == 0 && avg > 24))
         k_spmv64<32><<<grid_for(s->N * 32, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
                                                                                               s->a_op.p, x, y, s->N, dot, done);
-    else if (avg > 12)
+    else if (lanes == 16 || (lanes == 0 && avg > 12))
         k_spmv64<16><<<grid_for(s->N * 16, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
                                                                                               s->a_op.p, x, y, s->N, dot, done);
-    else if (avg > 6)
+    else if (lanes == 8 || (lanes == 0 && avg > 6))
         k_spmv64<8><<<grid_for(s->N * 8, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
                                                                                             s->a_op.p, x, y, s->N, dot, done);
     else
@@ -1141,6 +1142,13 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
 
 // y = S x with the FP64 operator (used by the flexible solver in mpnn.cu)
 void spmv_op64(sfc_system *s, const double *x, double *y) { launch_spmv64(s, x, y, nullptr, nullptr); }
+void spmv_op64_lanes(sfc_system *s, int lanes, const double *x, double *y)
+{
+    const int keep = s->spmv_lanes;
+    s->spmv_lanes = lanes;
+    launch_spmv64(s, x, y, nullptr, nullptr);
+    s->spmv_lanes = keep;
+}
 void spmv_op64_dot(sfc_system *s, const double *x, double *y, double *xy, const int *done)
 {
     launch_spmv64(s, x, y, xy, done);

@@ -118,12 +118,19 @@ __global__ void __launch_bounds__(256) k_kw_dense(const double *__restrict__ coo
 
 // one axis of the Kronecker product: for every node, column a:
 // out[node(m)] = sum_k Kd[m][k] in[node(k)]  along axis d (stride sd, length nd)
+// STAGE: the nd x nd factor is staged in shared memory (it fits); else it
+// is read through the cache
+template <bool STAGE>
 __global__ void k_kron_axis(const double *__restrict__ Kd, int nd, int64_t sd, int64_t nodes, int dof, int c,
                             int64_t ns, const double *__restrict__ in, double *__restrict__ out)
 {
-    extern __shared__ double sK[];
-    for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) sK[t] = Kd[t];
-    __syncthreads();
+    extern __shared__ double sKd[];
+    const double *sK = Kd;
+    if (STAGE) {
+        for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) sKd[t] = Kd[t];
+        __syncthreads();
+        sK = sKd;
+    }
     const int64_t total = nodes * ns;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t node = t / ns;
@@ -510,8 +517,19 @@ static void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, doub
                 const int nd = m->gn[a];
                 double *dst = bufs[cur];
                 ProfScope ps(ctx, "kron_axis", 2.0 * nodes * ns * 8);
-                k_kron_axis<<<grid_for(nodes * ns, 256), 256, (size_t)nd * nd * 8, ctx->stream>>>(
-                    dK[a].p, nd, sd, nodes, dof, c, ns, src, dst);
+                const size_t kb = (size_t)nd * nd * 8;
+                if (kb <= 48 * 1024) {
+                    k_kron_axis<true><<<grid_for(nodes * ns, 256), 256, kb, ctx->stream>>>(dK[a].p, nd, sd, nodes, dof,
+                                                                                         c, ns, src, dst);
+                } else if (kb <= 200 * 1024) {
+                    SFC_CK(cudaFuncSetAttribute(k_kron_axis<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)kb));
+                    k_kron_axis<true><<<grid_for(nodes * ns, 256), 256, kb, ctx->stream>>>(dK[a].p, nd, sd, nodes, dof,
+                                                                                         c, ns, src, dst);
+                } else {
+                    k_kron_axis<false><<<grid_for(nodes * ns, 256), 256, 0, ctx->stream>>>(dK[a].p, nd, sd, nodes,
+                                                                                         dof, c, ns, src, dst);
+                }
                 count_launch(ctx);
                 src = dst;
                 cur ^= 1;

@@ -53,7 +53,10 @@ HP = {"forcing.sigma": 0.1, "forcing.length": 0.2, "rho": 1.0, "mismatch.sigma":
 
 
 @pytest.mark.parametrize("kind,n,ns,amount", [(mg.TRI3_POISSON, 16, 16, 0.0), (mg.TRI3_POISSON, 12, 9, 0.3),
-                                              (mg.HEX8_POISSON, 5, 12, 0.0), (mg.HEX8_ELASTIC, 4, 12, 0.0)])
+                                              (mg.HEX8_POISSON, 5, 12, 0.0), (mg.HEX8_ELASTIC, 4, 12, 0.0),
+                                              # grid axes of 121 and 301 nodes: the Kronecker factor is
+                                              # staged in opted-in shared memory / read through the cache
+                                              (mg.LINE2_POISSON, 120, 8, 0.0), (mg.LINE2_POISSON, 300, 8, 0.0)])
 @pytest.mark.parametrize("method", [api.SFC_SOLVER_PCG_FP64, api.SFC_SOLVER_PCG_MIXED])
 def test_prior_posterior_loglik(ctx, kind, n, ns, amount, method):
     faces = "x0" if kind == mg.HEX8_ELASTIC else "all"
