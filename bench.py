@@ -451,13 +451,13 @@ def run_batch(args, ws, rank, local):
     """Config 3 on our GPU path: every step assembles all instances and runs
     the persistent batch kernel (CUDA graph)."""
     from statfem_b200 import api
-    wl = make_batch_workload(4321 + rank, n_inst=args.c3_instances)
+    wl = make_batch_workload(4321 + rank, n_inst=args.c3_instances, smin=args.c3_sides[0], smax=args.c3_sides[1])
     n = len(wl["sides"])
     ctx = api.Context(local)
     t0 = time.perf_counter()
     gm = api.Mesh(ctx, mg.TRI3_POISSON, 3, wl["union"].coords, wl["union"].conn)
     b = api.BatchStatFEM(ctx, gm, wl["off"], wl["sides"], wl["bc"], wl["sensors"], 1.0, args.cluster)
-    b.set_solver(tol=1e-8)
+    b.set_solver(tol=1e-8, inner_tol=args.inner_tol)
     b.set_coefficients(wl["coeff"])
     b.set_hparams(C3_HP, REG)
     # observations drawn from each instance's prior plus noise
@@ -738,6 +738,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c5"])
     ap.add_argument("--c3-instances", type=int, default=512, help="c3: number of instances")
+    ap.add_argument("--c3-sides", type=int, nargs=2, default=[32, 256], help="c3: range of the grid sides")
+    ap.add_argument("--inner-tol", type=float, default=1e-2, help="c3: FP32 reduction between FP64 residuals")
     ap.add_argument("--cluster", type=int, default=0, help="c3: CTAs per instance (0: default)")
     ap.add_argument("--c5-train", type=int, default=48, help="c5: training samples")
     ap.add_argument("--c5-train-n", type=int, default=32, help="c5: training grid (elements per side)")

@@ -382,8 +382,9 @@ int32_t sfc_batch_destroy(sfc_batch_t *batch);
 /* The launch shape in use: CTAs per cluster and CTAs in the grid. */
 int32_t sfc_batch_cluster_size(const sfc_batch_t *batch, int32_t *cluster, int32_t *grid);
 /* tol: true relative residual of every adjoint column (default 1e-8);
- * inner_tol: FP32 reduction per refinement cycle (1e-4); max_iter: inner
- * iteration cap per instance. */
+ * inner_tol: reduction of a column's FP32 recurrence residual between two
+ * FP64 residual replacements (default 1e-2; the search direction is kept
+ * across them); max_iter: inner iteration cap per instance. */
 int32_t sfc_batch_set_solver(sfc_batch_t *batch, double tol, double inner_tol, int32_t max_iter);
 int32_t sfc_batch_set_coefficients(sfc_batch_t *batch, const double *elem_coeff);
 /* One sfc_hparams_t per instance (each proposal has its own), reg: the

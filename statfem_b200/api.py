@@ -672,7 +672,7 @@ class BatchStatFEM:
         self.ctx.check(self.ctx.lib.sfc_batch_cluster_size(self.h, ctypes.byref(c), ctypes.byref(g)))
         return c.value, g.value
 
-    def set_solver(self, tol=1e-8, inner_tol=1e-4, max_iter=50000):
+    def set_solver(self, tol=1e-8, inner_tol=1e-2, max_iter=50000):
         self.ctx.check(self.ctx.lib.sfc_batch_set_solver(self.h, tol, inner_tol, int(max_iter)))
 
     def set_coefficients(self, coeff):

@@ -25,8 +25,9 @@
 // reductions go through distributed shared memory and cluster barriers, the
 // only waits in the kernel (hardware barriers among co-scheduled CTAs).
 //
-// Solve: FP32 block Jacobi-PCG inner iterations, FP64 residual b - S x64
-// recomputed at the start of each refinement cycle (defect correction);
+// Solve: FP32 block Jacobi-PCG inner iterations; at the start of each cycle
+// the FP64 residual b - S x64 replaces the recurrence residual (reliable
+// update: the search direction is kept unless the recurrence drifted);
 // converged columns are frozen; the instance stops when every column meets
 // the true relative residual tol.  With homogeneous constraints the
 // constrained rows of S are diagonal and phibar and F vanish there, so the
@@ -212,7 +213,7 @@ __device__ void warp_trsm(const double *L, double *X, int n, int m)
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(BT, 3) k_batch(BatchArgs a)
+__global__ void __launch_bounds__(BT, 4) k_batch(BatchArgs a)
 {
     cg::cluster_group cl = cg::this_cluster();
     const unsigned CS = cl.num_blocks(), rank = cl.block_rank();
@@ -263,6 +264,9 @@ __global__ void __launch_bounds__(BT, 3) k_batch(BatchArgs a)
                 if (d >= r0 && d < r0 + n) a.W[(int64_t)d * BK + lane] += a.sw[((int64_t)inst * BK + lane) * 3 + k];
             }
         cluster_barrier(cl);
+        // per column, across cycles: r.z the current direction was built
+        // from, and the recurrence residual norm^2 when the column stopped
+        double rzd[4] = {0, 0, 0, 0}, rrl[4] = {0, 0, 0, 0};
         for (int cycle = 0;; ++cycle) {
             double prr[4] = {0, 0, 0, 0}, pbb[4] = {0, 0, 0, 0};
             for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
@@ -318,22 +322,47 @@ __global__ void __launch_bounds__(BT, 3) k_batch(BatchArgs a)
                 thr[q] = a.itol * a.itol * rr0[q];
             }
             {
+                // reliable update: the FP64 residual replaces the recurrence
+                // one and the search direction is kept, p = z + (r.z / rzd) p,
+                // unless the recurrence had drifted from the true residual by
+                // more than a factor 1.5 (then, and in the first cycle, p = z)
                 double prz[4] = {0, 0, 0, 0}, zero[4] = {0, 0, 0, 0};
                 for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
                     const int64_t i = i0 + g;
                     if (i >= my1) continue;
                     const float4 r = R4[i * 8 + fl];
                     const float d = a.dinv32[i];
-                    const float4 z = make_float4(d * r.x, d * r.y, d * r.z, d * r.w);
-                    P4[i * 8 + fl] = z;
-                    prz[0] += (double)r.x * z.x;
-                    prz[1] += (double)r.y * z.y;
-                    prz[2] += (double)r.z * z.z;
-                    prz[3] += (double)r.w * z.w;
+                    prz[0] += (double)r.x * (d * r.x);
+                    prz[1] += (double)r.y * (d * r.y);
+                    prz[2] += (double)r.z * (d * r.z);
+                    prz[3] += (double)r.w * (d * r.w);
                 }
                 cluster_sum_q(cl, s, slot, prz, zero);
+                bool cont[4];
+                float b0[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) rz[q] = s.sres[4 * fl + q];
+                for (int q = 0; q < 4; ++q) {
+                    rz[q] = s.sres[4 * fl + q];
+                    cont[q] = cycle > 0 && act[q] && rzd[q] > 0.0 && rr0[q] <= 2.25 * rrl[q] &&
+                              rr0[q] * 2.25 >= rrl[q];
+                    b0[q] = cont[q] ? (float)(rz[q] / rzd[q]) : 0.f;
+                }
+                for (int64_t i0 = my0 + 4 * warp; i0 < my1; i0 += 4 * BW) {
+                    const int64_t i = i0 + g;
+                    if (i >= my1) continue;
+                    const float4 r = R4[i * 8 + fl];
+                    const float d = a.dinv32[i];
+                    float4 pv = make_float4(d * r.x, d * r.y, d * r.z, d * r.w);
+                    if (cont[0] || cont[1] || cont[2] || cont[3]) {  // P holds a previous direction
+                        const float4 po = P4[i * 8 + fl];
+                        if (cont[0]) pv.x = fmaf(b0[0], po.x, pv.x);
+                        if (cont[1]) pv.y = fmaf(b0[1], po.y, pv.y);
+                        if (cont[2]) pv.z = fmaf(b0[2], po.z, pv.z);
+                        if (cont[3]) pv.w = fmaf(b0[3], po.w, pv.w);
+                    }
+                    P4[i * 8 + fl] = pv;
+                }
+                cluster_barrier(cl);
             }
             bool inner_bad = false;
             for (; total_it < a.max_iter; ++total_it) {
@@ -410,9 +439,14 @@ __global__ void __launch_bounds__(BT, 3) k_batch(BatchArgs a)
                         act[q] = false;
                         inner_bad = true;
                     }
+                    const bool was = act[q];
                     act[q] = act[q] && rrn > thr[q];
+                    if (was && !act[q]) {  // stops here: keep its direction for the next cycle
+                        rzd[q] = rz[q];
+                        rrl[q] = rrn;
+                    }
                     beta[q] = act[q] ? (float)(rzn / rz[q]) : 0.f;
-                    rz[q] = rzn;
+                    if (act[q]) rz[q] = rzn;
                     any = any || act[q];
                 }
                 if (!__any_sync(0xffffffffu, any)) {
@@ -426,10 +460,11 @@ __global__ void __launch_bounds__(BT, 3) k_batch(BatchArgs a)
                     const float4 rv = R4[o];
                     float4 pv = P4[o];
                     const float d = a.dinv32[i];
-                    pv.x = fmaf(beta[0], pv.x, d * rv.x);
-                    pv.y = fmaf(beta[1], pv.y, d * rv.y);
-                    pv.z = fmaf(beta[2], pv.z, d * rv.z);
-                    pv.w = fmaf(beta[3], pv.w, d * rv.w);
+                    // stopped columns keep their direction
+                    if (act[0]) pv.x = fmaf(beta[0], pv.x, d * rv.x);
+                    if (act[1]) pv.y = fmaf(beta[1], pv.y, d * rv.y);
+                    if (act[2]) pv.z = fmaf(beta[2], pv.z, d * rv.z);
+                    if (act[3]) pv.w = fmaf(beta[3], pv.w, d * rv.w);
                     P4[o] = pv;
                 }
                 cluster_barrier(cl);
@@ -635,8 +670,8 @@ struct sfc_batch {
     sfc::BatchArgs args{};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
-    double tol = 1e-8, itol = 1e-4;
-    int max_iter = 50000, max_cycles = 30;
+    double tol = 1e-8, itol = 1e-2;
+    int max_iter = 50000, max_cycles = 200;
     ~sfc_batch()
     {
         if (gexec) cudaGraphExecDestroy(gexec);
