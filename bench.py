@@ -605,6 +605,127 @@ def batch_plain_estimate(ctx, wl, sample):
                          len(sides))}
 
 
+def pivoted_cholesky(K, rel=1e-12):
+    """Greedy (largest remaining diagonal) pivoted Cholesky K ~ L L^T, stopped
+    when the largest remaining diagonal drops below rel * max(diag K)."""
+    n = K.shape[0]
+    d = np.diag(K).astype(np.float64).copy()
+    L = np.zeros((n, 0))
+    stop = rel * d.max()
+    while L.shape[1] < n and d.max() > stop:
+        j = int(np.argmax(d))
+        col = (K[:, j] - L @ L[j]) / np.sqrt(d[j])
+        L = np.column_stack([L, col])
+        d = np.maximum(d - col * col, 0.0)
+        d[j] = 0.0
+    return L
+
+
+def multi_rhs_columns(wl, nrhs, sigma, length):
+    """The nrhs leading columns of the forcing covariance's factor on the c2
+    grid: diag(phibar) (Lz (x) Ly (x) Lx) with L_a the pivoted Cholesky factor
+    of exp(-d^2/(2 l^2)) on axis a (numerical rank to 1e-12), the Kronecker
+    columns ordered by decreasing norm, one displacement component per column
+    (cycling x, y, z), scaled by sigma.  Returns nrhs x num_dofs."""
+    mesh = wl["mesh"]
+    n = mesh.grid[0] + 1
+    x = np.arange(n) / (n - 1)
+    L = pivoted_cholesky(np.exp(-(x[:, None] - x[None, :]) ** 2 / (2 * length * length)))
+    nrm = np.linalg.norm(L, axis=0)
+    r = L.shape[1]
+    w = np.einsum("i,j,k->ijk", nrm, nrm, nrm).ravel()
+    order = np.argsort(-w, kind="stable")
+    phibar = wl["phibar"]
+    out = np.zeros((nrhs, mesh.num_dofs))
+    for c in range(nrhs):
+        t = order[c // 3] if c // 3 < len(order) else order[-1]
+        kz, ky, kx = t // (r * r), (t // r) % r, t % r
+        v = sigma * np.einsum("i,j,k->ijk", L[:, kz], L[:, ky], L[:, kx]).ravel()  # z slowest, x fastest
+        out[c, c % 3::3] = v
+    return out * phibar[None, :]
+
+
+def run_multi(args, ws, rank, local):
+    """Config 4: 1024 right-hand sides (forcing-covariance factor columns) on
+    the c2 elasticity mesh, mixed block PCG to the true relative residual
+    1e-10, inputs resident on the device."""
+    import torch
+    from statfem_b200 import api
+    wl = make_workload("c2", seed=1234 + rank)
+    nrhs = args.c4_rhs
+    g = GpuStatFEM(wl, local, api.SFC_SOLVER_PCG_MIXED, args.block_width,
+                   api.SFC_PRECOND_BLOCK_JACOBI if args.precond == "block-jacobi" else api.SFC_PRECOND_JACOBI)
+    ctx, s = g.ctx, g.s
+    wl["phibar"] = g.cf.phibar()
+    B = multi_rhs_columns(wl, nrhs, HP["forcing.sigma"], HP["forcing.length"])
+    N = B.shape[1]
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, max_iter=30000, inner_tol=1e-4,
+                  block_width=args.block_width, check_every=32, precond=g.precond)
+    dev = torch.device("cuda", local)
+    Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)  # interleaved [N][nrhs]
+    Ud = torch.empty_like(Bd)
+    torch.cuda.synchronize(dev)
+    for _ in range(args.warmup):
+        s.solve_multi_device(Bd.data_ptr(), Ud.data_ptr(), nrhs)
+    ctx.synchronize()
+    barrier(ws)
+    l0 = ctx.kernel_launches()
+    with ClockSampler(local) as clk:
+        ctx.mark(0)
+        for _ in range(args.steps):
+            s.solve_multi_device(Bd.data_ptr(), Ud.data_ptr(), nrhs)
+        ctx.mark(1)
+        ctx.synchronize()
+    barrier(ws)
+    ms = max_over_ranks(ws, ctx.marker_ms(0, 1))
+    launches = ctx.kernel_launches() - l0
+    st = s.last_stats()
+    U = Ud.cpu().numpy().T
+    # per-column error against FP64 Jacobi-PCG to 1e-13 on a sample of columns
+    pick = np.linspace(0, nrhs - 1, args.c4_check).astype(int)
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-13, max_iter=200000, check_every=32)
+    Uref = s.solveSystemMulti(B[pick])
+    errs = [float(np.linalg.norm(U[k] - Uref[t]) / np.linalg.norm(Uref[t])) for t, k in enumerate(pick)]
+    # plain FP64 PCG at 1e-10, one column at a time, on the sample
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-10, max_iter=200000, check_every=32)
+    s.solveSystemMulti(B[pick])
+    plain = s.last_stats()
+    # end to end through the host API
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, max_iter=30000, inner_tol=1e-4,
+                  block_width=args.block_width, check_every=32, precond=g.precond)
+    ctx.synchronize()
+    ctx.mark(2)
+    s.solveSystemMulti(B)
+    ctx.mark(3)
+    ctx.synchronize()
+    e2e_ms = ctx.marker_ms(2, 3)
+    value = ws * nrhs * args.steps / (ms / 1e3)
+    out = {
+        "metric": "right-hand-side solves/s at rel. residual 1e-10 (multi-RHS prior covariance, 1xB200)",
+        "value": round(value, 2), "unit": "RHS solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals)", "data": "synthetic (seeded)",
+        "config": {"workload": "c2 mesh (48^3 hex8 elasticity, 352,947 dofs), %d right-hand sides = leading "
+                               "columns of the forcing covariance's pivoted Cholesky factor, rel. residual 1e-10"
+                               % nrhs,
+                   "block_width": args.block_width, "precond": args.precond,
+                   "parallelism": "replicas" if ws > 1 else "single GPU"},
+        "e2e": {"value": round(nrhs / (e2e_ms / 1e3), 2), "unit": "RHS solves/s",
+                "h2d_bytes_per_step": int(B.nbytes), "d2h_bytes_per_step": int(B.nbytes)},
+        "gpu_launches": int(launches),
+        "solver": st,
+        "column_error_vs_fp64_pcg_1e-13": {"max": max(errs), "median": float(np.median(errs)),
+                                           "columns": len(errs)},
+        "plain_fp64": {"value": round(len(pick) / (plain["device_ms"] / 1e3), 3), "unit": "RHS solves/s",
+                       "sample": "%d columns, FP64 Jacobi-PCG one at a time to 1e-10, max %d iterations"
+                                 % (len(pick), plain["iterations"])},
+        "clocks": clk.summary(),
+    }
+    out["speedup_vs_plain_fp64"] = round(out["value"] / ws / out["plain_fp64"]["value"], 2)
+    if rank == 0:
+        print(json.dumps(out))
+
+
 def plain_fp64_estimate(g, wl, step_ms, block_stats, fwd_stats, sample):
     """Posterior solves/s of the plain method on the same GPU: FP64 Jacobi-PCG,
     one right-hand side at a time.  The forward solve is measured in full;
@@ -736,7 +857,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c4", "c5"])
+    ap.add_argument("--c4-rhs", type=int, default=1024, help="c4: right-hand sides")
+    ap.add_argument("--c4-check", type=int, default=8, help="c4: columns checked against FP64 PCG at 1e-13")
     ap.add_argument("--c3-instances", type=int, default=512, help="c3: number of instances")
     ap.add_argument("--c3-sides", type=int, nargs=2, default=[32, 256], help="c3: range of the grid sides")
     ap.add_argument("--inner-tol", type=float, default=1e-2, help="c3: FP32 reduction between FP64 residuals")
@@ -761,6 +884,8 @@ def main():
         run_learned(args, ws, rank, local)
     elif args.config == "c3":
         run_batch(args, ws, rank, local)
+    elif args.config == "c4":
+        run_multi(args, ws, rank, local)
     else:
         run_ours(args, ws, rank, local)
         if ws > 1:

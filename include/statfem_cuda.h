@@ -84,6 +84,9 @@ typedef struct sfc_solve_stats {
     int32_t converged;        /* 1 when every RHS met tol                      */
     double max_rel_residual;  /* max over RHS of the true FP64 ||b-Ax||/||b||  */
     double device_ms;         /* device time of the last solve call            */
+    int32_t fallback_columns; /* mixed solver: columns finished by FP64
+                                 Jacobi-PCG after repeated FP32 breakdowns    */
+    int32_t reserved;
 } sfc_solve_stats_t;
 
 /* Hyperparameters; the reference keeps them in std::map<std::string,double>
@@ -197,6 +200,18 @@ int32_t sfc_solve(sfc_system_t *sys, int32_t reuse);
  * for num_rhs right-hand sides (rhs, u: num_rhs x num_dofs, row-major, host). */
 int32_t sfc_solve_transpose(sfc_system_t *sys, const double *rhs, double *u, int32_t num_rhs,
                             int32_t reuse);
+/* Many right-hand sides at once for A u = b, with A the reference's
+ * row-zeroed system (solveSystem applied to each column; no single reference
+ * counterpart, the reference solves one vector per call,
+ * SystemSolveEigenSparse.hpp:273-310).  rhs, u: nrhs x num_dofs, host.
+ * With SFC_SOLVER_PCG_MIXED the columns go through the FP32 block solver with
+ * FP64 residual replacement, else FP64 Jacobi-PCG one column at a time. */
+int32_t sfc_solve_multi(sfc_system_t *sys, const double *rhs, double *u, int32_t nrhs);
+/* The same on device memory of the context's device, interleaved:
+ * column a of row i at [i * ld + a] (ld >= nrhs); issued on the context
+ * stream. */
+int32_t sfc_solve_multi_device(sfc_system_t *sys, const double *rhs_dev, double *u_dev, int32_t nrhs,
+                               int32_t ld);
 /* giveSolution / giveForce, SystemSolveEigenSparse.hpp:408-428 */
 int32_t sfc_give_solution(const sfc_system_t *sys, const uint32_t *dofs, int64_t n,
                           double *out);

@@ -50,7 +50,8 @@ class SolverOptions(ctypes.Structure):
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("refinements", ctypes.c_int32),
                 ("num_rhs", ctypes.c_int32), ("converged", ctypes.c_int32),
-                ("max_rel_residual", ctypes.c_double), ("device_ms", ctypes.c_double)]
+                ("max_rel_residual", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("fallback_columns", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -115,6 +116,8 @@ SIGNATURES = {
     "sfc_fix_dof": (_i32, [_vp, ctypes.c_uint32, _d]),
     "sfc_solve": (_i32, [_vp, _i32]),
     "sfc_solve_transpose": (_i32, [_vp, _dp, _dp, _i32, _i32]),
+    "sfc_solve_multi": (_i32, [_vp, _dp, _dp, _i32]),
+    "sfc_solve_multi_device": (_i32, [_vp, _vp, _vp, _i32, _i32]),
     "sfc_give_solution": (_i32, [_vp, _u32p, _i64, _dp]),
     "sfc_give_force": (_i32, [_vp, _u32p, _i64, _dp]),
     "sfc_clear_matrix": (_i32, [_vp]),
@@ -371,6 +374,19 @@ class SystemSolveCuda:
         self.ctx.check(self.ctx.lib.sfc_solve_transpose(self.h, _p(R, _dp), _p(U, _dp), R.shape[0],
                                                         int(bool(reuse))))
         return U[0] if single else U
+
+    def solveSystemMulti(self, rhs):
+        """A U = B for the rows of rhs (nrhs x num_dofs)."""
+        R = _arr(rhs, np.float64).reshape(-1, self.N)
+        U = np.zeros_like(R)
+        self.ctx.check(self.ctx.lib.sfc_solve_multi(self.h, _p(R, _dp), _p(U, _dp), R.shape[0]))
+        return U
+
+    def solve_multi_device(self, rhs_ptr, u_ptr, nrhs, ld=None):
+        """Device-memory variant: interleaved [num_dofs][ld] arrays given as
+        device addresses (integers)."""
+        self.ctx.check(self.ctx.lib.sfc_solve_multi_device(self.h, rhs_ptr, u_ptr, int(nrhs),
+                                                           int(nrhs if ld is None else ld)))
 
     def giveSolution(self, dofs=None):
         d = _arr(np.arange(self.N) if dofs is None else dofs, np.uint32)

@@ -425,6 +425,34 @@ int32_t sfc_solve_transpose(sfc_system_t *s, const double *rhs, double *u, int32
     });
 }
 
+int32_t sfc_solve_multi(sfc_system_t *s, const double *rhs, double *u, int32_t nrhs)
+{
+    if (!s || !rhs || !u || nrhs <= 0) return SFC_ERR_BAD_ARG;
+    return guard(s->ctx, [&] {
+        flush_staged(s);
+        const int64_t N = s->N;
+        std::vector<double> Bt((size_t)N * nrhs);
+        for (int a = 0; a < nrhs; ++a)
+            for (int64_t i = 0; i < N; ++i) Bt[(size_t)i * nrhs + a] = rhs[(size_t)a * N + i];
+        DBuf<double> B, X;
+        upload(s->ctx, B, Bt.data(), Bt.size());
+        X.alloc((size_t)N * nrhs);
+        solve_multi(s, B.p, X.p, nrhs, nrhs);
+        download(s->ctx, Bt.data(), X.p, Bt.size());
+        for (int a = 0; a < nrhs; ++a)
+            for (int64_t i = 0; i < N; ++i) u[(size_t)a * N + i] = Bt[(size_t)i * nrhs + a];
+    });
+}
+
+int32_t sfc_solve_multi_device(sfc_system_t *s, const double *rhs_dev, double *u_dev, int32_t nrhs, int32_t ld)
+{
+    if (!s || !rhs_dev || !u_dev || nrhs <= 0 || ld < nrhs) return SFC_ERR_BAD_ARG;
+    return guard(s->ctx, [&] {
+        flush_staged(s);
+        solve_multi(s, rhs_dev, u_dev, nrhs, ld);
+    });
+}
+
 static int give_vec(const sfc_system *s, const double *src, const uint32_t *dofs, int64_t n, double *out)
 {
     if (!s || !out || (n > 0 && !dofs)) return SFC_ERR_BAD_ARG;

@@ -354,6 +354,7 @@ void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);
 void solve_forward(sfc_system *s);
 void solve_block(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
 void transpose_fixup(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
+void solve_multi(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
 double device_dot(sfc_ctx *ctx, const double *a, const double *b, int64_t n);
 void spmv_op64(sfc_system *s, const double *x, double *y);
 // y = S x and *xy += x . y, skipped entirely when *done != 0 (done may be NULL)

@@ -187,6 +187,25 @@ __global__ void k_lift(const int32_t *__restrict__ rp, const int32_t *__restrict
     }
 }
 
+// the same lifting for nrhs interleaved columns ([N][ld] in and out)
+__global__ void k_lift_block(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                             const int32_t *__restrict__ diag, const double *__restrict__ a_ref,
+                             const unsigned char *__restrict__ mask, const double *__restrict__ B, int ld, int nrhs,
+                             int64_t N, double *__restrict__ out)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N * nrhs; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / nrhs;
+        const int c = (int)(t - i * nrhs);
+        double v = B[i * ld + c];
+        if (!mask[i])
+            for (int32_t s = rp[i]; s < rp[i + 1]; ++s) {
+                const int32_t j = col[s];
+                if (mask[j]) v -= a_ref[s] * (B[(int64_t)j * ld + c] / a_ref[diag[j]]);
+            }
+        out[i * ld + c] = v;
+    }
+}
+
 __global__ void k_axpby(double *__restrict__ y, const double *__restrict__ x, double a, double b, int64_t n)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -774,6 +793,13 @@ __global__ void k_gather_cols(const double *__restrict__ B, int ld, int c0, int 
     }
 }
 
+// X[i][c] += d[i] (column c of an [N][K] block)
+__global__ void k_add_col(double *__restrict__ X, int K, int c, const double *__restrict__ d, int64_t N)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        X[i * K + c] += d[i];
+}
+
 __global__ void k_scatter_cols(const double *__restrict__ in, int ld, int c0, int kb, int K, int64_t N,
                                double *__restrict__ X)
 {
@@ -941,7 +967,8 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     // (p^T A p <= 0) in column c
     s->flags.reserve(1 + K);
     int *stop = s->flags.p, *err = s->flags.p + 1;
-    std::vector<int> hflags(1 + K), nbreak(K);
+    std::vector<int> hflags(1 + K), nbreak(K), fallback(K), nstall(K);
+    int n_fallback = 0;
     const bool debug = std::getenv("SFC_DEBUG_SOLVER") != nullptr;
     const unsigned gw = (unsigned)(ctx->sm_count * 8);  // warp-per-row kernels: 8 warps/block
     const bool bsr = s->has_bsr;
@@ -1001,6 +1028,9 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         SFC_CK(cudaMemsetAsync(s->scal.p, 0, nsc * 8, ctx->stream));
         SFC_CK(cudaMemsetAsync(s->flags.p, 0, (1 + K) * sizeof(int), ctx->stream));
         std::fill(nbreak.begin(), nbreak.end(), 0);
+        std::fill(fallback.begin(), fallback.end(), 0);
+        std::fill(nstall.begin(), nstall.end(), 0);
+        int it_update = 0, last_interval = 0;
         count_launch(ctx);
         resid(x64.p, b64.p, r64.p, bn2);  // r64 = b, ||b_c||^2
         download(ctx, hb.data(), bn2, K);
@@ -1058,8 +1088,10 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             for (int c = 0; c < K; ++c)
                 if (active[c] && hflags[1 + c]) {
                     // a breakdown restarts the column at the next update; a
-                    // column that keeps breaking down is not SPD in FP32
-                    if (++nbreak[c] > 4) fail(SFC_ERR_NOT_SPD, "block PCG breakdown: p^T A p <= 0");
+                    // column that keeps breaking down (p^T S p lost in FP32
+                    // rounding near the end of a tight solve) leaves the FP32
+                    // iteration and is finished by FP64 Jacobi-PCG below
+                    if (++nbreak[c] > 4) fallback[c] = 1;
                     update = true;
                 }
             if (!update) {
@@ -1067,7 +1099,14 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                 for (int c = 0; c < K; ++c)
                     if (active[c] && rr_now[c] > ht[c] && rr_now[c] > 1e-2 * rr_last[c]) update = false;
             }
+            // a column whose FP32 recurrence stagnates (p^T S p dominated by
+            // rounding on ill-conditioned smooth modes) would hold the whole
+            // block back: force the update after three times the previous
+            // interval (at least 512 iterations)
+            if (!update && it - it_update >= std::max(512, 3 * last_interval)) update = true;
             if (!update) continue;
+            last_interval = it - it_update;
+            it_update = it;
             // reliable update: x64 += ||b|| x32, true FP64 residual
             k_bacc64<V><<<grid_for(N * K, 256), 256, 0, ctx->stream>>>(x64.p, xr, norm, N);
             count_launch(ctx);
@@ -1097,6 +1136,18 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                     ht[c] = INFINITY;
                     continue;
                 }
+                // no progress of the true residual over three updates in a
+                // row: FP32 cannot resolve this column any further
+                if ((r / bn) * (r / bn) >= 0.25 * rr_last[c]) {
+                    if (++nstall[c] >= 3) fallback[c] = 1;
+                } else {
+                    nstall[c] = 0;
+                }
+                if (fallback[c]) {
+                    active[c] = false;
+                    ht[c] = INFINITY;
+                    continue;
+                }
                 ++nactive;
                 if (rr_now[c] <= ht[c]) {  // recurrence converged, true residual not
                     ht[c] = std::max(ht[c] * 1e-2, 1e-30);
@@ -1120,11 +1171,42 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             // r32 <- scaled true residual, x32 <- 0, p kept (restarted columns: p = z)
             init32(rz + o1, rrs + o1);
         }
+        // FP64 fallback: S d = r_c (the column's true residual) by Jacobi-PCG
+        // to tol ||b_c|| / ||r_c||, then x_c += d
+        bool any_fb = false;
+        for (int c = 0; c < kb; ++c) {
+            if (!fallback[c]) continue;
+            any_fb = true;
+            ++n_fallback;
+            s->tmpN.reserve(N);
+            s->tmpN2.reserve(N);
+            k_gather_cols<<<grid_for(N, 256), 256, 0, ctx->stream>>>(r64.p, K, c, 1, 1, N, s->tmpN.p);
+            count_launch(ctx);
+            const double bn = std::sqrt(hb[c]), r = std::sqrt(rn[c]);
+            if (r > tol * bn) {
+                PcgResult pr = pcg64(s, s->tmpN.p, s->tmpN2.p, tol * bn / r, max_iter, check);
+                if (!pr.converged) all_conv = false;
+                if (debug)
+                    std::fprintf(stderr, "[sfc block %d] column %d: FP64 fallback from rel %.3e, %d iterations%s\n", c0,
+                                 c, r / bn, pr.iters, pr.converged ? "" : " (not converged)");
+                k_add_col<<<grid_for(N, 256), 256, 0, ctx->stream>>>(x64.p, K, c, s->tmpN2.p, N);
+                count_launch(ctx);
+            }
+        }
+        if (any_fb) {
+            SFC_CK(cudaMemsetAsync(rn2, 0, K * 8, ctx->stream));
+            resid(x64.p, b64.p, r64.p, rn2);
+            download(ctx, rn.data(), rn2, K);
+        }
         for (int c = 0; c < kb; ++c) {
             const double bn = std::sqrt(hb[c]);
             if (bn > 0) worst = std::max(worst, std::sqrt(rn[c]) / bn);
         }
-        if (nactive > 0) all_conv = false;
+        if (nactive > 0) {
+            all_conv = false;
+            if (debug)
+                std::fprintf(stderr, "[sfc block %d] %d columns still open after %d iterations\n", c0, nactive, it);
+        }
         k_scatter_cols<<<grid_for(N * kb, 256), 256, 0, ctx->stream>>>(x64.p, ld, c0, kb, K, N, X);
         count_launch(ctx);
         max_inner = std::max(max_inner, it);
@@ -1136,6 +1218,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     st.num_rhs = nrhs;
     st.max_rel_residual = worst;
     st.converged = all_conv ? 1 : 0;
+    st.fallback_columns = n_fallback;
 }
 
 }  // namespace
@@ -1279,6 +1362,25 @@ void solve_block(sfc_system *s, const double *B, double *X, int nrhs, int ld)
     st.device_ms = ms;
     s->stats = st;
     if (!st.converged) fail(SFC_ERR_NOT_CONVERGED, "block PCG did not converge within max_iter");
+}
+
+// A X = B for nrhs interleaved columns with the reference's row-zeroed A:
+// constrained rows give x_c = b_c / a_cc, the free rows solve
+// S x_f = b_f - K_fc x_c (one block solve of the lifted right-hand sides)
+void solve_multi(sfc_system *s, const double *B, double *X, int nrhs, int ld)
+{
+    sfc_ctx *ctx = s->ctx;
+    build_operator(s);
+    if (!s->any_constraint) {
+        solve_block(s, B, X, nrhs, ld);
+        return;
+    }
+    const int64_t N = s->N;
+    s->fix.reserve(N * (int64_t)ld);
+    k_lift_block<<<grid_for(N * nrhs, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p,
+                                                                   s->mask.p, B, ld, nrhs, N, s->fix.p);
+    count_launch(ctx);
+    solve_block(s, s->fix.p, X, nrhs, ld);
 }
 
 void transpose_fixup(sfc_system *s, const double *B, double *X, int nrhs, int ld)

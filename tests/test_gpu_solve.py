@@ -105,3 +105,18 @@ def test_zero_rhs_gives_zero(ctx):
     s.clearRhs()
     s.solveSystem()
     assert np.all(s.giveSolution() == 0.0)
+
+
+@pytest.mark.parametrize("kind,n,faces", CASES)
+@pytest.mark.parametrize("method", [api.SFC_SOLVER_PCG_FP64, api.SFC_SOLVER_PCG_MIXED])
+def test_multi_rhs_forward(ctx, kind, n, faces, method):
+    """A U = B for many right-hand sides (constrained rows included) against
+    the LU solve of the row-zeroed A, for both solvers."""
+    mesh, s, ds, F, bc = setup(ctx, kind, n, 7 + kind, faces=faces,
+                               bc_vals=lambda rng, k: rng.standard_normal(k))
+    rng = np.random.default_rng(4)
+    R = rng.standard_normal((41, mesh.num_dofs))
+    s.set_options(method=method, tol=1e-11, inner_tol=1e-3)
+    U = s.solveSystemMulti(R)
+    U_ref = np.stack([ds.solve(r) for r in R])
+    assert np.abs(U - U_ref).max() <= 1e-8 * np.abs(U_ref).max()
