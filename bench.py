@@ -360,7 +360,9 @@ def run_learned(args, ws, rank, local):
     from statfem_b200 import api
     from statfem_b200 import learned as L
     ctx = api.Context(local)
-    tr = L.PoissonSamples(ctx, args.c5_train_n, seed0=10_000 + 1000 * rank)
+    # the network is local: train on smaller grids whose fields have the same
+    # correlation length in cells as the 128^3 target (length 0.1 x 128 / n)
+    tr = L.PoissonSamples(ctx, args.c5_train_n, length=0.1 * 128 / args.c5_train_n, seed0=10_000 + 1000 * rank)
     net = api.LearnedPreconditioner(ctx, seed=0)
     info = L.train(net, tr, list(range(args.c5_train)), epochs=1, steps_per_sample=args.c5_steps,
                    checkpoint=None, lr=1e-3, batch=4)
@@ -391,8 +393,9 @@ def run_learned(args, ws, rank, local):
         "data": "synthetic (seeded Matérn 3/2 log-conductivity, circulant embedding)",
         "config": {"workload": "3-D Poisson, 128^3 hex8 (2,146,689 dofs), log-conductivity Matérn nu=3/2 "
                                "sigma 1 length 0.1, u=0 on the boundary, f=1, rel. residual 1e-8",
-                   "train": "%d samples of %d^3, %d Adam steps each (batch 4 pairs), 1 epoch"
-                            % (args.c5_train, args.c5_train_n, args.c5_steps),
+                   "train": "%d samples of %d^3 (Matern length %.2f: the same length in cells), %d Adam steps "
+                            "each (batch 4 pairs), 1 epoch"
+                            % (args.c5_train, args.c5_train_n, 0.1 * 128 / args.c5_train_n, args.c5_steps),
                    "held_out": n, "parallelism": "replicas" if ws > 1 else "single GPU"},
         "plain_pcg": {"value": round(ws * n / (pcg_ms / 1e3), 4), "unit": "solves/s",
                       "ms_per_step": round(pcg_ms / n, 2),

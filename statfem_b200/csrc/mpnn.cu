@@ -918,6 +918,12 @@ __global__ void k_dot_done(const double *__restrict__ a, const double *__restric
     if (threadIdx.x == 0) atomicAdd(out, v);
 }
 
+__global__ void k_axpy(double *__restrict__ y, const double *__restrict__ x, double a, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] += a * x[i];
+}
+
 // alpha = (p.r)/(p.q); x += alpha p; r -= alpha q; rr' += r.r
 __global__ void k_fcg_update(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
                              const double *__restrict__ q, int64_t n, const double *pq, const double *pr,
@@ -967,7 +973,8 @@ __global__ void k_fcg_pupdate(double *__restrict__ p, const double *__restrict__
 
 }  // namespace
 
-// Flexible CG (FCG(1), Notay 2000) with z = M(r) from the network:
+// Flexible CG (FCG(1), Notay 2000) with z = M(r) from the network, with
+// plain Jacobi-PCG as the fallback when the network stalls or breaks down:
 // alpha = p.r / p.Sp, p' = z - (z.Sp / p.Sp) p.  The scalars live on the
 // device (one slot per iteration) and the host reads the flags every
 // check_every iterations, so the iteration issues no synchronisation.  When
@@ -1017,7 +1024,9 @@ void solve_forward_fcg(sfc_system *s)
         k_dot_done<<<g, 256, 0, ctx->stream>>>(p, r, N, pr + slot, nullptr);
         count_launch(ctx);
     };
-    int it = 0, iters = 0;
+    int it = 0, iters = 0, fallback = 0, mark_it = 0;
+    constexpr int kStall = 400;
+    double mark_rr = bb;
     bool conv = bb == 0.0;
     double rel = 0.0;
     if (!conv) {
@@ -1035,8 +1044,8 @@ void solve_forward_fcg(sfc_system *s)
             if ((it + 1) % check == 0 || it + 1 == max_iter) {
                 int hf[2];
                 download(ctx, hf, done, 2);
-                if (hf[1]) fail(SFC_ERR_NOT_SPD, "flexible CG breakdown: p^T A p <= 0");
-                if (hf[0]) {
+                bool give_up = hf[1] != 0;  // breakdown (p^T S p <= 0)
+                if (!give_up && hf[0]) {
                     iters = hf[0];
                     rel = true_residual();
                     if (rel <= tol) {
@@ -1046,12 +1055,37 @@ void solve_forward_fcg(sfc_system *s)
                     // the recurrence drifted: restart from the true residual
                     SFC_CK(cudaMemsetAsync(done, 0, sizeof(int), ctx->stream));
                     if (it + 1 < max_iter) start(it + 1);
+                    mark_it = it + 1;
+                } else if (!give_up) {
+                    // stagnation: no 100-fold reduction of the recurrence
+                    // residual^2 (10-fold of the residual) within kStall iterations
+                    double rr_now = 0;
+                    download(ctx, &rr_now, rr + it + 1, 1);
+                    if (rr_now < 0.01 * mark_rr) {
+                        mark_rr = rr_now;
+                        mark_it = it + 1;
+                    } else if (it + 1 - mark_it > kStall) {
+                        give_up = true;
+                    }
                 }
+                if (give_up) break;
             }
         }
         if (!conv) {
-            iters = max_iter;
+            // the network failed this system (stagnation, breakdown or the
+            // iteration cap): plain FP64 Jacobi-PCG finishes from the current
+            // x on the true residual, S d = b - S x, x += d
+            iters = std::max(iters, std::min(it + 1, max_iter));
             rel = true_residual();
+            if (rel > tol) {
+                fallback = 1;
+                const PcgStats pr = pcg64_public(s, r, z, tol / rel, max_iter, 32);
+                k_axpy<<<g, 256, 0, ctx->stream>>>(s->X.p, z, 1.0, N);
+                count_launch(ctx);
+                iters += pr.iters;
+                rel = true_residual();
+            }
+            conv = rel <= tol * (1.0 + 1e-9);
         }
     }
     SFC_CK(cudaEventRecord(e1, ctx->stream));
@@ -1066,7 +1100,8 @@ void solve_forward_fcg(sfc_system *s)
     s->stats.converged = conv ? 1 : 0;
     s->stats.max_rel_residual = rel;
     s->stats.device_ms = ms;
-    if (!conv) fail(SFC_ERR_NOT_CONVERGED, "flexible CG did not converge within max_iter");
+    s->stats.fallback_columns = fallback;
+    if (!conv) fail(SFC_ERR_NOT_CONVERGED, "flexible CG (and the Jacobi-PCG fallback) did not converge within max_iter");
 }
 
 }  // namespace sfc

@@ -153,3 +153,21 @@ def test_training_gain(ctx):
     assert st["iterations"] <= 0.6 * it_pcg
     net.close()
     base.close()
+
+
+def test_fcg_falls_back_to_jacobi_pcg(ctx):
+    """A useless network (huge random decoder) stalls or breaks flexible CG;
+    plain FP64 Jacobi-PCG then finishes the solve from the current iterate,
+    and the answer still matches the direct oracle."""
+    mesh, s, S, F, ds, _ = setup(ctx, mg.HEX8_POISSON, 10, 5)
+    net = api.LearnedPreconditioner(ctx, seed=1)
+    net.set_params(R.init_params(9, decoder_scale=300.0))
+    net.attach(s)
+    s.set_options(method=api.SFC_SOLVER_FCG_MPNN, tol=1e-10)
+    s.solveSystem()
+    st = s.last_stats()
+    assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
+    assert st["fallback_columns"] == 1
+    u_ref = ds.solve(F)
+    assert np.abs(s.giveSolution() - u_ref).max() <= 1e-8 * np.abs(u_ref).max()
+    net.close()
