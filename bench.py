@@ -366,7 +366,7 @@ def run_learned(args, ws, rank, local):
     net = api.LearnedPreconditioner(ctx, seed=0)
     info = L.train(net, tr, list(range(args.c5_train)), epochs=1, steps_per_sample=args.c5_steps,
                    checkpoint=None, lr=1e-3, batch=4)
-    te = L.PoissonSamples(ctx, 128, seed0=900_000 + 1000 * rank)
+    te = L.PoissonSamples(ctx, args.c5_n, seed0=900_000 + 1000 * rank)
     coeffs = [te.coefficients(k) for k in range(args.warmup + args.steps)]
     net.attach(te.system)
     rows = []
@@ -391,7 +391,8 @@ def run_learned(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": round(fcg_ms / n, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (network BF16 x BF16 -> FP32)",
         "data": "synthetic (seeded Matérn 3/2 log-conductivity, circulant embedding)",
-        "config": {"workload": "3-D Poisson, 128^3 hex8 (2,146,689 dofs), log-conductivity Matérn nu=3/2 "
+        "config": {"workload": "3-D Poisson, %d^3 hex8 (%d dofs), log-conductivity Matérn nu=3/2 "
+                               % (args.c5_n, (args.c5_n + 1) ** 3) + 
                                "sigma 1 length 0.1, u=0 on the boundary, f=1, rel. residual 1e-8",
                    "train": "%d samples of %d^3 (Matern length %.2f: the same length in cells), %d Adam steps "
                             "each (batch 4 pairs), 1 epoch"
@@ -407,8 +408,8 @@ def run_learned(args, ws, rank, local):
                                  float(np.mean([r[1]["iterations"] for r in rows])), 3),
         "time_ratio": round(pcg_ms / fcg_ms, 3),
         "training": {"seconds": round(info["seconds"], 2), "steps": int(len(info["loss"])),
-                     "loss_first": round(float(info["loss"][:20].mean()), 4),
-                     "loss_last": round(float(info["loss"][-20:].mean()), 4)},
+                     "loss_first": round(float(info["loss"][:20].mean()), 4) if len(info["loss"]) else None,
+                     "loss_last": round(float(info["loss"][-20:].mean()), 4) if len(info["loss"]) else None},
     }
     if rank == 0:
         print(json.dumps(out))
@@ -871,6 +872,7 @@ def main():
     ap.add_argument("--c5-train", type=int, default=48, help="c5: training samples")
     ap.add_argument("--c5-train-n", type=int, default=32, help="c5: training grid (elements per side)")
     ap.add_argument("--c5-steps", type=int, default=40, help="c5: Adam steps per training sample")
+    ap.add_argument("--c5-n", type=int, default=128, help="c5: held-out grid (elements per side)")
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cpu-iters", type=int, default=100)
     ap.add_argument("--plain-sample", type=int, default=8)
