@@ -281,6 +281,14 @@ int32_t sfc_koh_proj_conditioned(sfc_koh_t *koh, const sfc_hparams_t *hp, double
  * posterior mean (num_dofs) and covariance (num_dofs^2; may be NULL).  Needs
  * num_dofs adjoint solves, so it is limited to num_dofs <= 8192. */
 int32_t sfc_koh_woodbury(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean, double *cov);
+/* The posterior mean field of giveFEconditionedDataWoodbury
+ * (LikelihoodKOH.ipp:442-508) for any mesh size: the same quantity as
+ * sfc_koh_woodbury's mean, from the adjoint solution of the last
+ * sfc_forward_gauss_update plus num_sensors + 1 forward solves (G = C_u P^T
+ * = A^-1 C_f R^T + (sigma_f reg)^2 P^T, ubar = A^-1 F) and sensor-space FP64
+ * Cholesky solves, instead of the num_dofs solves of the unprojected prior.
+ * mean: num_dofs, host. */
+int32_t sfc_koh_woodbury_mean(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean);
 
 /* ---- allocation-free log-likelihood ----------------------------------------- */
 /* No counterpart in the reference.  The same quantity as

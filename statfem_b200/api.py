@@ -142,6 +142,7 @@ SIGNATURES = {
     "sfc_koh_log_likelihood": (_i32, [_vp, ctypes.POINTER(HParams), _dp]),
     "sfc_koh_proj_conditioned": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
     "sfc_koh_woodbury": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
+    "sfc_koh_woodbury_mean": (_i32, [_vp, ctypes.POINTER(HParams), _dp]),
     "sfc_koh_log_likelihood_noalloc": (_i32, [_vp, _vp, _vp, _i32, _vp, _i32, _i32, ctypes.POINTER(HParams), _vp,
                                               _vp, _vp]),
     "sfc_mpnn_num_params": (_i64, []),
@@ -554,6 +555,14 @@ class LikelihoodKOH:
         c = np.zeros((self.ns, self.ns))
         self.ctx.check(self.ctx.lib.sfc_koh_proj_conditioned(self.h, ctypes.byref(h), _p(m, _dp), _p(c, _dp)))
         return m, c
+
+    def giveFEconditionedMeanWoodbury(self, hp):
+        """The posterior mean field of giveFEconditionedDataWoodbury at
+        sensor-space cost (any mesh size)."""
+        h = HParams.from_map(hp)
+        m = np.zeros(self.fg.solver.N)
+        self.ctx.check(self.ctx.lib.sfc_koh_woodbury_mean(self.h, ctypes.byref(h), _p(m, _dp)))
+        return m
 
     def giveFEconditionedDataWoodbury(self, hp, with_cov=True):
         h = HParams.from_map(hp)

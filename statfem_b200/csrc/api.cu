@@ -16,6 +16,7 @@ void covar_projected_host(sfc_covar_forcing *cf, const sfc_hparams_t *hp, const 
 void koh_loglik(sfc_koh *k, const sfc_hparams_t *hp, double *out);
 void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov);
 void koh_woodbury(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov);
+void koh_woodbury_mean(sfc_koh *k, const sfc_hparams_t *hp, double *mean);
 
 void *pinned(sfc_ctx *ctx, size_t bytes)
 {
@@ -760,6 +761,12 @@ int32_t sfc_koh_woodbury(sfc_koh_t *k, const sfc_hparams_t *hp, double *mean, do
 {
     if (!k || !hp) return SFC_ERR_BAD_ARG;
     return guard(k->ctx, [&] { koh_woodbury(k, hp, mean, cov); });
+}
+
+int32_t sfc_koh_woodbury_mean(sfc_koh_t *k, const sfc_hparams_t *hp, double *mean)
+{
+    if (!k || !hp || !mean) return SFC_ERR_BAD_ARG;
+    return guard(k->ctx, [&] { koh_woodbury_mean(k, hp, mean); });
 }
 
 }  // extern "C"

@@ -677,6 +677,115 @@ void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
     if (cov) download(ctx, cov, pc, (size_t)ns * ns);
 }
 
+// lower Cholesky in place (n x n, row-major); false when not positive definite
+static bool host_chol(std::vector<double> &A, int n)
+{
+    for (int j = 0; j < n; ++j) {
+        double d = A[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) d -= A[(size_t)j * n + k] * A[(size_t)j * n + k];
+        if (!(d > 0.0)) return false;
+        d = std::sqrt(d);
+        A[(size_t)j * n + j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double v = A[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) v -= A[(size_t)i * n + k] * A[(size_t)j * n + k];
+            A[(size_t)i * n + j] = v / d;
+        }
+    }
+    return true;
+}
+
+// x := (L L^T)^-1 x
+static void host_chol_solve(const std::vector<double> &L, int n, std::vector<double> &x)
+{
+    for (int i = 0; i < n; ++i) {
+        double v = x[i];
+        for (int k = 0; k < i; ++k) v -= L[(size_t)i * n + k] * x[k];
+        x[i] = v / L[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double v = x[i];
+        for (int k = i + 1; k < n; ++k) v -= L[(size_t)k * n + i] * x[k];
+        x[i] = v / L[(size_t)i * n + i];
+    }
+}
+
+// The posterior mean field of giveFEconditionedDataWoodbury
+// (LikelihoodKOH.ipp:442-508) at sensor-space cost.  With G = C_u P^T,
+// S = K_s/(rho^2 n_o) + C_s and P G = C_s, P ubar = mean_s:
+//   D (rho G K_s^-1 ysum + ubar) = ubar + G w,
+//   w = rho K_s^-1 ysum - S^-1 (rho C_s K_s^-1 ysum + mean_s),
+// and G = A^-1 (C_f R^T) + (sigma_f reg)^2 P^T from the adjoint solution
+// R^T = A^-T P^T already at hand: ns forward solves and one forward solve for
+// ubar = A^-1 F instead of the N solves of the unprojected prior.
+void koh_woodbury_mean(sfc_koh *k, const sfc_hparams_t *hp, double *mean)
+{
+    sfc_ctx *ctx = k->ctx;
+    sfc_forward_gauss *fg = k->fg;
+    sfc_system *s = fg->sys;
+    SFC_REQUIRE(fg->valid, "forward model not updated");
+    SFC_REQUIRE(k->n_o > 0, "sensor values not set");
+    const int64_t N = s->N, ns = fg->ns;
+    const int n = (int)ns, n_o = k->n_o;
+    const double rho = hp->rho;
+    // sensor space on the host (FP64 Cholesky, ns x ns)
+    std::vector<double> Cs((size_t)ns * ns), ms(ns), Y((size_t)ns * n_o), xy((size_t)ns * 3);
+    download(ctx, Cs.data(), fg->cov.p, Cs.size());
+    download(ctx, ms.data(), fg->mean.p, ms.size());
+    download(ctx, Y.data(), k->Y.p, Y.size());
+    download(ctx, xy.data(), k->sensor_coords.p, xy.size());
+    std::vector<double> Ks((size_t)ns * ns);
+    for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b) {
+            double d2 = 0.0;
+            for (int c = 0; c < k->dim; ++c) {
+                const double t = xy[(size_t)a * 3 + c] - xy[(size_t)b * 3 + c];
+                d2 += t * t;
+            }
+            Ks[(size_t)a * n + b] = hp->mismatch_sigma * hp->mismatch_sigma *
+                                        std::exp(-d2 / (2.0 * hp->mismatch_length * hp->mismatch_length)) +
+                                    (a == b ? hp->mismatch_sensor_eps * hp->mismatch_sensor_eps : 0.0);
+        }
+    std::vector<double> S(Ks);
+    for (size_t t = 0; t < S.size(); ++t) S[t] = Ks[t] / (rho * rho * n_o) + Cs[t];
+    std::vector<double> Lk(Ks), Ls(S);
+    if (!host_chol(Lk, n) || !host_chol(Ls, n)) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not positive definite");
+    std::vector<double> kys(ns, 0.0);  // K_s^-1 ysum
+    for (int a = 0; a < n; ++a)
+        for (int j = 0; j < n_o; ++j) kys[a] += Y[(size_t)a * n_o + j];
+    host_chol_solve(Lk, n, kys);
+    std::vector<double> t(ns), w(ns);
+    for (int a = 0; a < n; ++a) {
+        double v = ms[a];
+        for (int b = 0; b < n; ++b) v += rho * Cs[(size_t)a * n + b] * kys[b];
+        t[a] = v;
+    }
+    host_chol_solve(Ls, n, t);
+    for (int a = 0; a < n; ++a) w[a] = rho * kys[a] - t[a];
+    // ubar = A^-1 F (forward solve, the system's own method)
+    solve_forward(s);
+    // G = A^-1 (C_f R^T) + (sigma_f reg)^2 P^T
+    DBuf<double> W, T, G, wd, out;
+    W.alloc(N * ns);
+    T.alloc(3 * N * ns);
+    G.alloc(N * ns);
+    k_scale_rows<<<grid_for(N * ns, 256), 256, 0, ctx->stream>>>(fg->R.p, fg->cf->phibar.p, N, ns, W.p);
+    count_launch(ctx);
+    kernel_times(ctx, fg->cf, hp->forcing_sigma, hp->forcing_length, W.p, T.p, ns, T.p + N * ns);
+    k_scale_rows<<<grid_for(N * ns, 256), 256, 0, ctx->stream>>>(T.p, fg->cf->phibar.p, N, ns, W.p);
+    count_launch(ctx);
+    solve_multi(s, W.p, G.p, (int)ns, (int)ns);
+    const double add = hp->forcing_sigma * fg->reg;
+    k_add_scaled<<<grid_for(N * ns, 256), 256, 0, ctx->stream>>>(G.p, fg->B.p, add * add, N * ns);
+    count_launch(ctx);
+    // mean = ubar + G w
+    upload(ctx, wd, w.data(), ns);
+    out.alloc(N);
+    SFC_CK(cudaMemcpyAsync(out.p, s->X.p, N * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    gemm(ctx, 0, 0, N, 1, ns, 1.0, G.p, ns, wd.p, 1, 1.0, out.p, 1);
+    download(ctx, mean, out.p, N);
+}
+
 // giveFEconditionedDataWoodbury (LikelihoodKOH.ipp:442-508)
 void koh_woodbury(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
 {

@@ -137,3 +137,37 @@ def test_kat1_woodbury_posterior_on_gpu(ctx):
     mean, cov = koh.giveFEconditionedDataWoodbury(hp)
     assert np.abs(mean - k["expected_mean"]).max() < 1e-6
     assert np.all(np.isfinite(cov)) and np.allclose(cov, cov.T, atol=1e-12)
+    # the sensor-space-cost form of the same mean
+    m2 = koh.giveFEconditionedMeanWoodbury(hp)
+    assert np.abs(m2 - k["expected_mean"]).max() < 1e-6
+    assert np.abs(m2 - mean).max() <= 1e-9 * np.abs(mean).max()
+
+
+@pytest.mark.parametrize("kind,n,ns,amount", [(mg.TRI3_POISSON, 12, 9, 0.3), (mg.HEX8_POISSON, 5, 12, 0.0),
+                                              (mg.HEX8_ELASTIC, 3, 10, 0.0)])
+@pytest.mark.parametrize("method", [api.SFC_SOLVER_PCG_FP64, api.SFC_SOLVER_PCG_MIXED])
+def test_woodbury_mean_at_sensor_cost(ctx, kind, n, ns, amount, method):
+    """Full-field posterior mean from ns + 1 forward solves against the
+    N-solve Woodbury form on the GPU and against the oracle's Woodbury."""
+    faces = "x0" if kind == mg.HEX8_ELASTIC else "all"
+    prob = statfem_problem(kind, n, ns, seed=kind * 11 + n, amount=amount, faces=faces)
+    f = np.array([0.0, 0.0, -1.0]) if kind == mg.HEX8_ELASTIC else 1.0
+    reg = 0.001
+    g = gpu_prior(ctx, prob, HP, reg, f, method, tol=1e-12)
+    rng = np.random.default_rng(3)
+    Y = g["mean"][:, None] + 1e-3 * rng.standard_normal((ns, 2))
+    koh = api.LikelihoodKOH(g["fg"], prob["pts"])
+    koh.setSensorValues(Y)
+    m_full, _ = koh.giveFEconditionedDataWoodbury(HP, with_cov=False)
+    m = koh.giveFEconditionedMeanWoodbury(HP)
+    assert np.abs(m - m_full).max() <= 1e-8 * np.abs(m_full).max()
+    o = oracle_prior(prob, HP, reg, f)
+    mesh = prob["mesh"]
+    Pd = o["Pd"]
+    N = mesh.num_dofs
+    I = np.eye(N)
+    u_mean, C_u, _ = O.forward_gauss_rhs(o["solver"], o["F"], I, mesh.coords, o["phibar"], mesh.dim, mesh.dof,
+                                         HP["forcing.sigma"], HP["forcing.length"], reg)
+    Ks = O.mismatch_covariance(prob["pts"], HP["mismatch.sigma"], HP["mismatch.length"], HP["mismatch.sensorEps"])
+    m_ref, _ = O.koh_woodbury(o["C_s"], Ks, Y, HP["rho"], Pd, C_u, u_mean)
+    assert np.abs(m - m_ref).max() <= 1e-7 * np.abs(m_ref).max()
