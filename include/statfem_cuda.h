@@ -290,6 +290,29 @@ int32_t sfc_koh_woodbury(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean, 
  * mean: num_dofs, host. */
 int32_t sfc_koh_woodbury_mean(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean);
 
+/* ---- first-order material uncertainty ------------------------------------------ */
+/* Replaces statX::infer::ForwardPerturbation (ForwardPerturbation.hpp:109-195)
+ * with CovarianceMaterial (CovarianceMaterial.hpp) and the stiffness
+ * derivative of ElementPotential (ElementPotential.ipp:225-237), Poisson
+ * element kinds.  Built on a ForwardGaussRHS object (its system, forcing
+ * covariance and projection).  sfc_perturbation_update runs the forward
+ * model (adjoint and forward solves) and forms
+ *   C_s = R C_f R^T + sum_{e,d} C_m(e,d) R A'_e (A^-1 C_f A^-T + u u^T) A'_d^T R^T
+ *         + (reg material_sigma)^2 P P^T,     mean = P u,
+ * C_m the squared-exponential covariance ("material.sigma",
+ * "material.length") of the element centroids, through a pivoted Cholesky
+ * factor of C_m (stopped when the largest remaining diagonal is below
+ * factor_tol * material_sigma^2, or at max_rank columns; rank returns the
+ * columns used).  reg: the reference's regFactor (default 1e-4). */
+typedef struct sfc_perturbation sfc_perturbation_t;
+int32_t sfc_perturbation_create(sfc_forward_gauss_t *fg, double reg, sfc_perturbation_t **out);
+int32_t sfc_perturbation_destroy(sfc_perturbation_t *pt);
+int32_t sfc_perturbation_update(sfc_perturbation_t *pt, const sfc_hparams_t *hp, double material_sigma,
+                                double material_length, double factor_tol, int32_t max_rank, int32_t *rank);
+/* giveProjectedMeanU / giveProjectedCovarU: num_sensors, num_sensors^2. */
+int32_t sfc_perturbation_mean(const sfc_perturbation_t *pt, double *mean);
+int32_t sfc_perturbation_covar(const sfc_perturbation_t *pt, double *cov);
+
 /* ---- allocation-free log-likelihood ----------------------------------------- */
 /* No counterpart in the reference.  The same quantity as
  * sfc_koh_log_likelihood (LikelihoodKOH::giveLogLikelihood), for callers that

@@ -210,6 +210,46 @@ def forward_gauss_rhs(solver, F, P, coords, phibar, dim, dof, sigma_f, length_f,
     return mean, C, R
 
 
+def forward_perturbation(mesh, qps, F, rp, col, val, bc_dofs, P, phibar, sigma_f, length_f, sigma_m, length_m,
+                         reg):
+    """ForwardPerturbation::updateSolution (statX/infer/ForwardPerturbation.hpp:
+    109-195), dense: R = P A^-1, u = A^-1 F, M = A^-1 C_f A^-T + u u^T, the
+    material covariance C_m over element centroids (CovarianceMaterial.hpp,
+    SE kernel under "material."), dA/dkappa_e = the unit-conductivity element
+    matrix (ElementPotential.ipp:225-237) scattered with the constrained rows
+    zeroed; C = R C_f R^T + sum_e sum_d C_m[e,d] R dA_e M dA_d^T R^T
+    + (reg sigma_m)^2 P P^T, mean = P u.  The whole A^-1 is used (the
+    reference fills the rows of its A^-1 only up to the number of sensors)."""
+    N = mesh.num_dofs
+    A = sp.csr_matrix((val, col, rp), shape=(N, N)).toarray()
+    Ainv = np.linalg.inv(A)
+    u = Ainv @ F
+    R = P @ Ainv
+    Cf = forcing_covariance_dense(mesh.dim, mesh.dof, mesh.coords, phibar, sigma_f, length_f)
+    M = Ainv @ Cf @ Ainv.T + np.outer(u, u)
+    cent = mesh.coords[mesh.conn].mean(axis=1)[:, :mesh.dim]
+    Cm = se_matrix(cent, cent, sigma_m, length_m)
+    free = np.ones(N)
+    free[np.asarray(bc_dofs, dtype=np.int64)] = 0.0
+    E = mesh.num_elems
+    Q = []
+    for e in range(E):
+        X = mesh.coords[mesh.conn[e]]
+        ke = element_matrix(mesh.kind, qps, X, coeff=1.0)
+        dofs = mesh.conn[e].astype(np.int64)
+        D = np.zeros((N, N))
+        D[np.ix_(dofs, dofs)] = ke
+        D *= free[:, None]
+        Q.append(R @ D)
+    Q = np.stack(Q)                      # E x ns x N
+    QM = np.einsum("eai,ij->eaj", Q, M)  # R dA_e M
+    QS = np.einsum("ed,dbj->ebj", Cm, Q)  # sum_d C_m[e,d] R dA_d
+    Cmat = np.einsum("eaj,ebj->ab", QM, QS)
+    add = reg * sigma_m
+    C = R @ Cf @ R.T + Cmat + add * add * (P @ P.T)
+    return P @ u, C
+
+
 def mismatch_covariance(sensor_coords, sigma_d, length_d, eps):
     """MismatchCovariance::giveCovariance (statX/infer/MismatchCovariance.hpp:76-99)."""
     K = se_matrix(sensor_coords, sensor_coords, sigma_d, length_d)

@@ -143,6 +143,11 @@ SIGNATURES = {
     "sfc_koh_proj_conditioned": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
     "sfc_koh_woodbury": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
     "sfc_koh_woodbury_mean": (_i32, [_vp, ctypes.POINTER(HParams), _dp]),
+    "sfc_perturbation_create": (_i32, [_vp, _d, ctypes.POINTER(_vp)]),
+    "sfc_perturbation_destroy": (_i32, [_vp]),
+    "sfc_perturbation_update": (_i32, [_vp, ctypes.POINTER(HParams), _d, _d, _d, _i32, _i32p]),
+    "sfc_perturbation_mean": (_i32, [_vp, _dp]),
+    "sfc_perturbation_covar": (_i32, [_vp, _dp]),
     "sfc_koh_log_likelihood_noalloc": (_i32, [_vp, _vp, _vp, _i32, _vp, _i32, _i32, ctypes.POINTER(HParams), _vp,
                                               _vp, _vp]),
     "sfc_mpnn_num_params": (_i64, []),
@@ -578,6 +583,43 @@ class LikelihoodKOH:
             self.h = None
 
 
+class ForwardPerturbation:
+    """statX::infer::ForwardPerturbation: prior mean and covariance at the
+    sensors with first-order material (conductivity) uncertainty; hp is the
+    reference's map including "material.sigma" and "material.length"."""
+
+    def __init__(self, forward_gauss, reg=1e-4):
+        self.fg = forward_gauss
+        self.ctx = forward_gauss.ctx
+        h = _vp()
+        self.ctx.check(self.ctx.lib.sfc_perturbation_create(forward_gauss.h, float(reg), ctypes.byref(h)))
+        self.h = h
+        self.rank = 0
+
+    def updateSolution(self, hp, factor_tol=1e-12, max_rank=4096):
+        h = HParams.from_map(hp)
+        r = ctypes.c_int32()
+        self.ctx.check(self.ctx.lib.sfc_perturbation_update(self.h, ctypes.byref(h), float(hp["material.sigma"]),
+                                                            float(hp["material.length"]), float(factor_tol),
+                                                            int(max_rank), ctypes.byref(r)))
+        self.rank = r.value
+
+    def giveProjectedMeanU(self):
+        m = np.zeros(self.fg.ns)
+        self.ctx.check(self.ctx.lib.sfc_perturbation_mean(self.h, _p(m, _dp)))
+        return m
+
+    def giveProjectedCovarU(self):
+        c = np.zeros((self.fg.ns, self.fg.ns))
+        self.ctx.check(self.ctx.lib.sfc_perturbation_covar(self.h, _p(c, _dp)))
+        return c
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.sfc_perturbation_destroy(self.h)
+            self.h = None
+
+
 class LearnedPreconditioner:
     """Message-passing network M(r) ~ S^-1 r used by flexible CG
     (SFC_SOLVER_FCG_MPNN); no counterpart in the reference, which factorises
@@ -762,5 +804,5 @@ def autotune_clear():
 
 
 __all__ = ["Context", "Mesh", "SystemSolveCuda", "CovarianceForcing", "ForwardGaussRHS", "LikelihoodKOH",
-           "LearnedPreconditioner", "BatchStatFEM", "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64",
+           "LearnedPreconditioner", "BatchStatFEM", "ForwardPerturbation", "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64",
            "SFC_SOLVER_PCG_MIXED", "SFC_SOLVER_FCG_MPNN", "autotune_save", "autotune_load", "autotune_clear"]

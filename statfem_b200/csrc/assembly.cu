@@ -835,6 +835,66 @@ void assemble_matrix(sfc_system *s, const sfc_mesh *mc)
     s->inhomogeneous = false;
 }
 
+// Element matrices of the Poisson kinds with conductivity 1: the stiffness
+// derivative d K_e / d kappa_e (ElementPotential::stiffnessDerivIntegrand,
+// del2/fem/ElementPotential.ipp:225-237, 1.0 * detG * w * dphiDx^T dphiDx)
+void element_matrices_unit(const sfc_mesh *m, double *ke0)
+{
+    sfc_ctx *ctx = m->ctx;
+    const int64_t E = m->num_elems;
+    DBuf<double> ones;
+    std::vector<double> h(E, 1.0);
+    upload(ctx, ones, h.data(), E);
+    DevInt err = status_word(ctx);
+    SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
+    switch (m->kind) {
+    case SFC_ELEM_LINE2_POISSON:
+        k_elem_poisson<1, 2><<<grid_for(E, 128), 128, 0, ctx->stream>>>(m->coords.p, m->conn.p, ones.p, m->quad, E,
+                                                                         ke0, err.p);
+        break;
+    case SFC_ELEM_TRI3_POISSON:
+        k_elem_poisson<2, 3><<<grid_for(E, 128), 128, 0, ctx->stream>>>(m->coords.p, m->conn.p, ones.p, m->quad, E,
+                                                                         ke0, err.p);
+        break;
+    case SFC_ELEM_HEX8_POISSON:
+        k_elem_poisson<3, 8><<<grid_for(E, 128), 128, 0, ctx->stream>>>(m->coords.p, m->conn.p, ones.p, m->quad, E,
+                                                                         ke0, err.p);
+        break;
+    default:
+        fail(SFC_ERR_BAD_ARG, "stiffness derivatives are defined for the Poisson element kinds");
+    }
+    count_launch(ctx);
+    int h_err = 0;
+    download(ctx, &h_err, err.p, 1);
+    if (h_err) fail(SFC_ERR_NEG_JACOBIAN, "Negative Jacobian in an element");
+}
+
+// CSR values of sum_e w_e K_e for kc weight vectors at once:
+// out[k * nnz + s] = sum over the slot's element entries of w[k * E + e] ke[entry]
+__global__ void k_gather_weighted(const int32_t *__restrict__ slot_ptr, const int32_t *__restrict__ contrib,
+                                  const double *__restrict__ ke, int LL, const double *__restrict__ w, int64_t E,
+                                  int kc, int64_t nnz, double *__restrict__ out)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nnz * kc; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = t / nnz, sl = t - k * nnz;
+        double v = 0.0;
+        for (int32_t q = slot_ptr[sl]; q < slot_ptr[sl + 1]; ++q) {
+            const int32_t id = contrib[q];
+            v += w[k * E + id / LL] * ke[id];
+        }
+        out[t] = v;
+    }
+}
+
+void gather_weighted(const sfc_mesh *m, const double *ke0, const double *w_dev, int kc, double *out)
+{
+    sfc_ctx *ctx = m->ctx;
+    k_gather_weighted<<<grid_for(m->nnz * kc, 256), 256, 0, ctx->stream>>>(m->slot_ptr.p, m->contrib.p, ke0,
+                                                                          m->L * m->L, w_dev, m->num_elems, kc,
+                                                                          m->nnz, out);
+    count_launch(ctx);
+}
+
 void assemble_load(sfc_ctx *ctx, const sfc_mesh *m, const double *f, double *F_dev, bool zero_first)
 {
     if (zero_first) SFC_CK(cudaMemsetAsync(F_dev, 0, m->num_dofs * 8, ctx->stream));

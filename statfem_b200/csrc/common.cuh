@@ -350,6 +350,8 @@ void apply_constraints_dev(sfc_system *s, const uint32_t *idx_dev, const double 
 void build_operator(sfc_system *s, bool require_positive_diag = true);
 void flush_staged(sfc_system *s);
 void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);
+void element_matrices_unit(const sfc_mesh *m, double *ke0);
+void gather_weighted(const sfc_mesh *m, const double *ke0, const double *w_dev, int kc, double *out);
 // solvers.cu
 void solve_forward(sfc_system *s);
 void solve_block(sfc_system *s, const double *B_dev, double *X_dev, int nrhs, int ld);
@@ -371,6 +373,11 @@ void solve_forward_fcg(sfc_system *s);
 void spmv_op64_lanes(sfc_system *s, int lanes, const double *x, double *y);
 // stats.cu
 void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp);
+void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *X, int64_t ns,
+                     double *C, DBuf<double> &work);
+void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *W, double *T,
+                  int64_t ns, double *tmp);
+void atb_accumulate(sfc_ctx *ctx, const double *A, const double *B, int64_t K, int64_t M, int64_t Nn, double *C);
 // autotune.cu: the process-wide table of tuned launch shapes
 std::string tune_device_key(sfc_ctx *ctx);
 bool tune_lookup(const std::string &key, std::string &val);

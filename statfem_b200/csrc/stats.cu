@@ -491,7 +491,7 @@ std::vector<double> se_axis(const std::vector<double> &x, double length)
 }  // namespace
 
 // T = K W (per component); W, T, tmp: num_dofs x ns device arrays
-static void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *W,
+void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *W,
                          double *T, int64_t ns, double *tmp)
 {
     const sfc_mesh *m = cf->mesh;
@@ -554,7 +554,7 @@ static void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, doub
 }
 
 // C (ns x ns) = W^T (K W) with W = diag(phibar) X, X: num_dofs x ns (device)
-static void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *X,
+void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *X,
                             int64_t ns, double *C, DBuf<double> &work)
 {
     const int64_t N = cf->num_dofs;
@@ -572,6 +572,19 @@ static void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, d
     dim3 g((unsigned)splits, (unsigned)((ns + 63) / 64), (unsigned)((ns + 63) / 64));
     ProfScope ps(ctx, "covar_atb", 2.0 * N * ns * 8);
     k_atb<<<g, 256, 0, ctx->stream>>>(W, T, N, ns, ns, rows, 1.0, C);
+    count_launch(ctx);
+}
+
+// C (M x Nn) += A^T B for A: K x M, B: K x Nn (row-major), split-K
+void atb_accumulate(sfc_ctx *ctx, const double *A, const double *B, int64_t K, int64_t M, int64_t Nn, double *C)
+{
+    const int64_t tiles = ((M + 63) / 64) * ((Nn + 63) / 64);
+    int64_t splits = std::max<int64_t>(1, (ctx->sm_count * 4) / tiles);
+    int64_t rows = (K + splits - 1) / splits;
+    rows = ((rows + 15) / 16) * 16;
+    splits = (K + rows - 1) / rows;
+    dim3 g((unsigned)splits, (unsigned)((M + 63) / 64), (unsigned)((Nn + 63) / 64));
+    k_atb<<<g, 256, 0, ctx->stream>>>(A, B, K, M, Nn, rows, 1.0, C);
     count_launch(ctx);
 }
 

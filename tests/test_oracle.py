@@ -122,3 +122,24 @@ def test_se_field_tensor_matches_kernel_covariance():
     X = np.stack(np.meshgrid(ax[0], ax[1], indexing="xy"), axis=-1).reshape(-1, 2)
     K = O.se_matrix(X, X, 0.7, 0.3)
     assert np.abs(np.cov(S.T) - K).max() < 0.03
+
+
+def test_perturbation_oracle_reduces_to_forcing_only():
+    """With zero material variance the perturbation covariance is the
+    ForwardGaussRHS covariance without its regularisation term; it is
+    symmetric positive semidefinite otherwise."""
+    from tests.problems import statfem_problem
+    pr = statfem_problem(mg.TRI3_POISSON, 5, 4, seed=2)
+    mesh = pr["mesh"]
+    rp, col, val, F = O.fem(mesh, 3, 1.0, pr["bc"], coeff=pr["coeff"])
+    phibar = O.unit_load(mesh, 3, pr["bc"])
+    Pd = mg.projection_dense(mesh, *pr["P"])
+    solver = O.DirectSolver(rp, col, val)
+    mean0, C0, _ = O.forward_gauss_rhs(solver, F, Pd, mesh.coords, phibar, 2, 1, 0.1, 0.2, 0.0)
+    m, C = O.forward_perturbation(mesh, 3, F, rp, col, val, pr["bc"], Pd, phibar, 0.1, 0.2, 0.0, 0.3, 1e-4)
+    np.testing.assert_allclose(m, mean0, rtol=1e-10)
+    np.testing.assert_allclose(C, C0, rtol=1e-9, atol=1e-14)
+    m, C = O.forward_perturbation(mesh, 3, F, rp, col, val, pr["bc"], Pd, phibar, 0.1, 0.2, 0.5, 0.3, 1e-4)
+    assert np.allclose(C, C.T, rtol=1e-10, atol=1e-16)
+    assert np.linalg.eigvalsh(C).min() > -1e-12 * np.abs(C).max()
+    assert (np.diag(C) > np.diag(C0)).all()
