@@ -280,6 +280,14 @@ int32_t sfc_koh_proj_conditioned(sfc_koh_t *koh, const sfc_hparams_t *hp, double
 /* giveFEconditionedDataWoodbury, LikelihoodKOH.ipp:442-508: full-field
  * posterior mean (num_dofs) and covariance (num_dofs^2; may be NULL).  Needs
  * num_dofs adjoint solves, so it is limited to num_dofs <= 8192. */
+/* giveLogLikelihood (LikelihoodKOH.ipp:75-120) for n hyperparameter sets at
+ * once against the forward model of the last sfc_forward_gauss_update: the
+ * sets differ in rho and the mismatch parameters (their forcing parameters
+ * are not used), one CTA each, one launch per chunk -- the inner loop of
+ * hyperparameter MCMC (hyperParamLearning.hpp:90-249) over many proposals or
+ * chains.  A set whose total covariance is not positive definite, or whose
+ * quadratic term is not negative, gets NaN. */
+int32_t sfc_koh_log_likelihood_batch(sfc_koh_t *koh, const sfc_hparams_t *hps, int32_t n, double *loglik);
 int32_t sfc_koh_woodbury(sfc_koh_t *koh, const sfc_hparams_t *hp, double *mean, double *cov);
 /* The posterior mean field of giveFEconditionedDataWoodbury
  * (LikelihoodKOH.ipp:442-508) for any mesh size: the same quantity as

@@ -143,6 +143,7 @@ SIGNATURES = {
     "sfc_koh_proj_conditioned": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
     "sfc_koh_woodbury": (_i32, [_vp, ctypes.POINTER(HParams), _dp, _dp]),
     "sfc_koh_woodbury_mean": (_i32, [_vp, ctypes.POINTER(HParams), _dp]),
+    "sfc_koh_log_likelihood_batch": (_i32, [_vp, ctypes.POINTER(HParams), _i32, _dp]),
     "sfc_perturbation_create": (_i32, [_vp, _d, ctypes.POINTER(_vp)]),
     "sfc_perturbation_destroy": (_i32, [_vp]),
     "sfc_perturbation_update": (_i32, [_vp, ctypes.POINTER(HParams), _d, _d, _d, _i32, _i32p]),
@@ -560,6 +561,13 @@ class LikelihoodKOH:
         c = np.zeros((self.ns, self.ns))
         self.ctx.check(self.ctx.lib.sfc_koh_proj_conditioned(self.h, ctypes.byref(h), _p(m, _dp), _p(c, _dp)))
         return m, c
+
+    def giveLogLikelihoodBatch(self, hps):
+        """giveLogLikelihood for a list of hyperparameter maps in one launch."""
+        arr = (HParams * len(hps))(*[HParams.from_map(h) for h in hps])
+        out = np.zeros(len(hps))
+        self.ctx.check(self.ctx.lib.sfc_koh_log_likelihood_batch(self.h, arr, len(hps), _p(out, _dp)))
+        return out
 
     def giveFEconditionedMeanWoodbury(self, hp):
         """The posterior mean field of giveFEconditionedDataWoodbury at

@@ -17,6 +17,7 @@ void koh_loglik(sfc_koh *k, const sfc_hparams_t *hp, double *out);
 void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov);
 void koh_woodbury(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov);
 void koh_woodbury_mean(sfc_koh *k, const sfc_hparams_t *hp, double *mean);
+void koh_loglik_batch(sfc_koh *k, const sfc_hparams_t *hps, int n, double *out);
 
 void *pinned(sfc_ctx *ctx, size_t bytes)
 {
@@ -761,6 +762,12 @@ int32_t sfc_koh_woodbury(sfc_koh_t *k, const sfc_hparams_t *hp, double *mean, do
 {
     if (!k || !hp) return SFC_ERR_BAD_ARG;
     return guard(k->ctx, [&] { koh_woodbury(k, hp, mean, cov); });
+}
+
+int32_t sfc_koh_log_likelihood_batch(sfc_koh_t *k, const sfc_hparams_t *hps, int32_t n, double *loglik)
+{
+    if (!k || !hps || n <= 0 || !loglik) return SFC_ERR_BAD_ARG;
+    return guard(k->ctx, [&] { koh_loglik_batch(k, hps, n, loglik); });
 }
 
 int32_t sfc_koh_woodbury_mean(sfc_koh_t *k, const sfc_hparams_t *hp, double *mean)

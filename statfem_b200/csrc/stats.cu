@@ -327,10 +327,34 @@ __device__ void mismatch_cov(int ns, const double *xs, int dim, double sd, doubl
 
 // LikelihoodKOH::giveLogLikelihood (statX/infer/LikelihoodKOH.ipp:75-120)
 // work: 2*ns*ns + ns*n_o doubles per batch item
+__device__ void koh_loglik_dev(int ns, int n_o, const double *__restrict__ mean, const double *__restrict__ Cs,
+                               const double *__restrict__ xs, int dim, const double *__restrict__ Y,
+                               const sfc_hparams_t &hp, double *__restrict__ work, double *out, int *info);
+
 __global__ void __launch_bounds__(1024) k_koh_loglik(int ns, int n_o, const double *__restrict__ mean,
                                                      const double *__restrict__ Cs, const double *__restrict__ xs,
                                                      int dim, const double *__restrict__ Y, sfc_hparams_t hp,
                                                      double *__restrict__ work, double *out, int *info)
+{
+    koh_loglik_dev(ns, n_o, mean, Cs, xs, dim, Y, hp, work, out, info);
+}
+
+// many hyperparameter sets against the same forward model, one CTA each
+__global__ void __launch_bounds__(1024) k_koh_loglik_batch(int ns, int n_o, const double *__restrict__ mean,
+                                                           const double *__restrict__ Cs,
+                                                           const double *__restrict__ xs, int dim,
+                                                           const double *__restrict__ Y,
+                                                           const sfc_hparams_t *__restrict__ hps, int64_t wsz,
+                                                           double *__restrict__ work, double *out, int *info)
+{
+    const int b = blockIdx.x;
+    const sfc_hparams_t hp = hps[b];
+    koh_loglik_dev(ns, n_o, mean, Cs, xs, dim, Y, hp, work + (int64_t)b * wsz, out + b, info + b);
+}
+
+__device__ void koh_loglik_dev(int ns, int n_o, const double *__restrict__ mean, const double *__restrict__ Cs,
+                               const double *__restrict__ xs, int dim, const double *__restrict__ Y,
+                               const sfc_hparams_t &hp, double *__restrict__ work, double *out, int *info)
 {
     double *C = work;
     double *D = work + (int64_t)ns * ns;
@@ -663,6 +687,40 @@ void koh_loglik(sfc_koh *k, const sfc_hparams_t *hp, double *out)
     if (hi > 0) fail(SFC_ERR_NOT_SPD, "total covariance is not positive definite (LLT failed)");
     if (hi < 0) fail(SFC_ERR_BAD_ARG, "non-negative quadratic term in the log-likelihood");
     download(ctx, out, d.p, 1);
+}
+
+// LikelihoodKOH::giveLogLikelihood for n hyperparameter sets (rho and the
+// mismatch parameters; the forcing parameters of the last forward update
+// apply) in one launch; an item whose total covariance is not positive
+// definite, or whose quadratic term is not negative, gives NaN
+void koh_loglik_batch(sfc_koh *k, const sfc_hparams_t *hps, int n, double *out)
+{
+    sfc_ctx *ctx = k->ctx;
+    sfc_forward_gauss *fg = k->fg;
+    SFC_REQUIRE(fg->valid, "forward model not updated");
+    SFC_REQUIRE(k->n_o > 0, "sensor values not set");
+    const int ns = (int)k->ns;
+    const int64_t wsz = 2 * (int64_t)ns * ns + (int64_t)ns * k->n_o;
+    const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(n, (int64_t)(256e6 / 8) / std::max<int64_t>(wsz, 1)));
+    DBuf<double> work, res;
+    DBuf<int> info;
+    DBuf<sfc_hparams_t> h;
+    work.alloc((size_t)chunk * wsz);
+    res.alloc(chunk);
+    info.alloc(chunk);
+    std::vector<int> hinfo(chunk);
+    for (int c0 = 0; c0 < n; c0 += chunk) {
+        const int m = std::min(chunk, n - c0);
+        upload(ctx, h, hps + c0, m);
+        SFC_CK(cudaMemsetAsync(info.p, 0, m * sizeof(int), ctx->stream));
+        k_koh_loglik_batch<<<m, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim,
+                                                        k->Y.p, h.p, wsz, work.p, res.p, info.p);
+        count_launch(ctx);
+        download(ctx, out + c0, res.p, m);
+        download(ctx, hinfo.data(), info.p, m);
+        for (int t = 0; t < m; ++t)
+            if (hinfo[t]) out[c0 + t] = NAN;
+    }
 }
 
 void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
