@@ -190,8 +190,13 @@ def cuda_sync(ws):
 # ---------------------------------------------------------------------------
 # our GPU arm
 # ---------------------------------------------------------------------------
+def precond_code(api, name):
+    return {"jacobi": api.SFC_PRECOND_JACOBI, "block-jacobi": api.SFC_PRECOND_BLOCK_JACOBI,
+            "two-level": api.SFC_PRECOND_TWO_LEVEL}[name]
+
+
 class GpuStatFEM:
-    def __init__(self, wl, device, method, block_width=128, precond=0):
+    def __init__(self, wl, device, method, block_width=128, precond=0, coarse_size=0):
         from statfem_b200 import api
         self.api = api
         self.wl = wl
@@ -202,8 +207,9 @@ class GpuStatFEM:
         self.s = api.SystemSolveCuda(self.ctx, m.num_dofs)
         self.block_width = block_width
         self.precond = precond
+        self.coarse_size = coarse_size
         self.s.set_options(method=method, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=block_width,
-                           check_every=32, precond=precond)
+                           check_every=32, precond=precond, coarse_size=coarse_size)
         self.cf = api.CovarianceForcing(self.ctx, self.gm)
         self.cf.applyConstraints(wl["bc"])
         self.fg = api.ForwardGaussRHS(self.s, self.cf, REG)
@@ -246,8 +252,7 @@ def run_ours(args, ws, rank, local):
     from statfem_b200 import api
     method = api.SFC_SOLVER_PCG_MIXED if args.method == "mixed" else api.SFC_SOLVER_PCG_FP64
     wl = make_workload(args.config, seed=1234 + rank)
-    precond = api.SFC_PRECOND_BLOCK_JACOBI if args.precond == "block-jacobi" else api.SFC_PRECOND_JACOBI
-    g = GpuStatFEM(wl, local, method, args.block_width, precond)
+    g = GpuStatFEM(wl, local, method, args.block_width, precond_code(api, args.precond), args.coarse_size)
     ctx = g.ctx
     for _ in range(args.warmup):
         g.step()
@@ -325,7 +330,7 @@ def run_ours(args, ws, rank, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals)",
         "data": "synthetic (seeded)",
         "config": {"workload": wl["desc"], "block_width": args.block_width, "precond": args.precond,
-                   "method": "mixed block Jacobi-PCG" if args.method == "mixed"
+                   "method": "mixed block PCG (%s preconditioner)" % args.precond if args.method == "mixed"
                    else "plain FP64 Jacobi-PCG", "parallelism": "replicas" if ws > 1 else "single GPU",
                    "l2": "inputs larger than L2 (matrix 220+ MB)"},
         "e2e": ({"value": round(ws * e2e_steps / (e2e_ms / 1e3), 4), "unit": "posterior solves/s",
@@ -659,13 +664,13 @@ def run_multi(args, ws, rank, local):
     wl = make_workload("c2", seed=1234 + rank)
     nrhs = args.c4_rhs
     g = GpuStatFEM(wl, local, api.SFC_SOLVER_PCG_MIXED, args.block_width,
-                   api.SFC_PRECOND_BLOCK_JACOBI if args.precond == "block-jacobi" else api.SFC_PRECOND_JACOBI)
+                   precond_code(api, args.precond), args.coarse_size)
     ctx, s = g.ctx, g.s
     wl["phibar"] = g.cf.phibar()
     B = multi_rhs_columns(wl, nrhs, HP["forcing.sigma"], HP["forcing.length"])
     N = B.shape[1]
     s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, max_iter=30000, inner_tol=1e-4,
-                  block_width=args.block_width, check_every=32, precond=g.precond)
+                  block_width=args.block_width, check_every=32, precond=g.precond, coarse_size=g.coarse_size)
     dev = torch.device("cuda", local)
     Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)  # interleaved [N][nrhs]
     Ud = torch.empty_like(Bd)
@@ -697,7 +702,7 @@ def run_multi(args, ws, rank, local):
     plain = s.last_stats()
     # end to end through the host API
     s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, max_iter=30000, inner_tol=1e-4,
-                  block_width=args.block_width, check_every=32, precond=g.precond)
+                  block_width=args.block_width, check_every=32, precond=g.precond, coarse_size=g.coarse_size)
     ctx.synchronize()
     ctx.mark(2)
     s.solveSystemMulti(B)
@@ -745,16 +750,18 @@ def plain_fp64_estimate(g, wl, step_ms, block_stats, fwd_stats, sample):
     for k, a in enumerate(pick):
         rows[k, ix[ip[a]:ip[a + 1]]] = dv[ip[a]:ip[a + 1]]
     g.s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=30000, check_every=32)
+    g.s.solveSystem()
+    plain_fwd = g.s.last_stats()
     g.s.solveSystemTranspose(rows)
     st = g.s.last_stats()
     g.s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=g.block_width,
-                    check_every=32, precond=g.precond)
+                    check_every=32, precond=g.precond, coarse_size=g.coarse_size)
     other_ms = max(0.0, step_ms - block_stats["device_ms"] - fwd_stats["device_ms"])
-    plain_ms = fwd_stats["device_ms"] + st["device_ms"] * ns / sample + other_ms
+    plain_ms = plain_fwd["device_ms"] + st["device_ms"] * ns / sample + other_ms
     return {"value": round(1e3 / plain_ms, 5), "unit": "posterior solves/s", "ms_per_step": round(plain_ms, 1),
             "sample": "FP64 Jacobi-PCG one RHS at a time: forward solve measured (%d it), %d of %d adjoint "
                       "solves measured (%.1f ms, max %d it) and scaled; non-solve work from the timed step"
-                      % (fwd_stats["iterations"], sample, ns, st["device_ms"], st["iterations"])}
+                      % (plain_fwd["iterations"], sample, ns, st["device_ms"], st["iterations"])}
 
 
 # ---------------------------------------------------------------------------
@@ -779,9 +786,16 @@ def cpu_baseline(args, wl, g, sample_iters):
     F = g.s.giveForce()
     mask = np.zeros(len(rp) - 1, dtype=np.uint8)
     mask[wl["bc"]] = 1
-    # iterations to 1e-8 of the same FP64 Jacobi-PCG, taken from the GPU
-    # forward solve on the identical matrix (avoids a minutes-long CPU solve)
-    its = int(g.fwd_iters)
+    # iterations to 1e-8 of the same FP64 Jacobi-PCG, taken from a GPU FP64
+    # Jacobi-PCG forward solve of the identical matrix (avoids a minutes-long
+    # CPU solve)
+    from statfem_b200 import api
+    keep = g.s.get_options()
+    g.s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=30000, check_every=32,
+                    precond=api.SFC_PRECOND_JACOBI)
+    g.s.solveSystem()
+    its = int(g.s.last_stats()["iterations"])
+    g.s.set_options(**keep)
     rate, per_iter = cpu_solve_rate(wl, rp, col, val, mask, F, its, sample_iters)
     threads = 1  # the C port is single-threaded, like the reference path
     return {"value": round(rate, 6), "unit": "posterior solves/s", "cores": threads, "kind": "port",
@@ -859,7 +873,7 @@ def run_reference(args, ws, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c4", "c5"])
@@ -879,7 +893,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--prof-steps", type=int, default=1)
     ap.add_argument("--block-width", type=int, default=128, choices=[32, 64, 128])
-    ap.add_argument("--precond", default="block-jacobi", choices=["jacobi", "block-jacobi"])
+    ap.add_argument("--precond", default="two-level", choices=["jacobi", "block-jacobi", "two-level"])
+    ap.add_argument("--coarse-size", type=int, default=0,
+                    help="two-level: nodes per aggregate along each axis (0: library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     ws, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),

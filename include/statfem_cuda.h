@@ -69,13 +69,22 @@ typedef struct sfc_solver_options {
     double inner_tol;      /* FP32 inner reduction per refinement cycle        */
     int32_t block_width;   /* RHS per block for SFC_SOLVER_PCG_MIXED (0: auto) */
     int32_t check_every;   /* iterations between convergence checks (0: auto)  */
-    int32_t precond;       /* SFC_PRECOND_* for SFC_SOLVER_PCG_MIXED          */
+    int32_t precond;       /* SFC_PRECOND_*                                    */
+    int32_t coarse_size;   /* SFC_PRECOND_TWO_LEVEL: nodes per aggregate along
+                              each axis (0: 8)                                */
 } sfc_solver_options_t;
 
-/* preconditioners of the mixed solver (the FP64 solver is always Jacobi) */
+/* preconditioners.  JACOBI and BLOCK_JACOBI select the FP32 iteration's
+ * preconditioner of SFC_SOLVER_PCG_MIXED (its FP64 solves use point Jacobi);
+ * TWO_LEVEL applies to every PCG of the system, FP64 and mixed. */
 #define SFC_PRECOND_JACOBI        0 /* point Jacobi                            */
 #define SFC_PRECOND_BLOCK_JACOBI  1 /* nodal 3x3 block Jacobi on 3-dof meshes,
                                        point Jacobi otherwise                  */
+#define SFC_PRECOND_TWO_LEVEL     2 /* nodal 3x3 block Jacobi plus an additive
+                                       coarse correction on the six rigid-body
+                                       modes of box aggregates of the mesh's
+                                       nodes (3-dof meshes assembled from a
+                                       mesh; block Jacobi otherwise)          */
 
 typedef struct sfc_solve_stats {
     int32_t iterations;       /* max over right-hand sides, inner iterations   */
@@ -86,7 +95,8 @@ typedef struct sfc_solve_stats {
     double device_ms;         /* device time of the last solve call            */
     int32_t fallback_columns; /* mixed solver: columns finished by FP64
                                  Jacobi-PCG after repeated FP32 breakdowns    */
-    int32_t reserved;
+    int32_t coarse_dofs;      /* size of the coarse space used (TWO_LEVEL),
+                                 0 when the solve had none                    */
 } sfc_solve_stats_t;
 
 /* Hyperparameters; the reference keeps them in std::map<std::string,double>

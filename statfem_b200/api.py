@@ -30,6 +30,7 @@ SFC_SOLVER_PCG_MIXED = 1
 SFC_SOLVER_FCG_MPNN = 2
 SFC_PRECOND_JACOBI = 0
 SFC_PRECOND_BLOCK_JACOBI = 1
+SFC_PRECOND_TWO_LEVEL = 2
 
 _ERR = {-1: "CUDA error", -2: "bad argument", -3: "not SPD", -4: "not converged", -5: "timeout",
         -6: "out of memory", -7: "negative Jacobian", -8: "too large for the fixed scratch"}
@@ -44,14 +45,15 @@ class SfcError(RuntimeError):
 class SolverOptions(ctypes.Structure):
     _fields_ = [("method", ctypes.c_int32), ("max_iter", ctypes.c_int32), ("tol", ctypes.c_double),
                 ("inner_tol", ctypes.c_double), ("block_width", ctypes.c_int32),
-                ("check_every", ctypes.c_int32), ("precond", ctypes.c_int32)]
+                ("check_every", ctypes.c_int32), ("precond", ctypes.c_int32),
+                ("coarse_size", ctypes.c_int32)]
 
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("refinements", ctypes.c_int32),
                 ("num_rhs", ctypes.c_int32), ("converged", ctypes.c_int32),
                 ("max_rel_residual", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("fallback_columns", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("fallback_columns", ctypes.c_int32), ("coarse_dofs", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -302,9 +304,14 @@ class SystemSolveCuda:
 
     # -- options / stats (no reference counterpart) --
     def set_options(self, method=SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=20000, inner_tol=1e-4,
-                    block_width=0, check_every=16, precond=SFC_PRECOND_JACOBI):
-        o = SolverOptions(method, max_iter, tol, inner_tol, block_width, check_every, precond)
+                    block_width=0, check_every=16, precond=SFC_PRECOND_JACOBI, coarse_size=0):
+        o = SolverOptions(method, max_iter, tol, inner_tol, block_width, check_every, precond, coarse_size)
         self.ctx.check(self.ctx.lib.sfc_system_set_options(self.h, ctypes.byref(o)))
+
+    def get_options(self):
+        o = SolverOptions()
+        self.ctx.check(self.ctx.lib.sfc_system_get_options(self.h, ctypes.byref(o)))
+        return {k: getattr(o, k) for k, _ in o._fields_}
 
     def autotune_spmv(self, remeasure=False):
         v = ctypes.c_int32()

@@ -291,8 +291,13 @@ int32_t sfc_system_destroy(sfc_system_t *s)
 int32_t sfc_system_set_options(sfc_system_t *s, const sfc_solver_options_t *o)
 {
     if (!s || !o) return SFC_ERR_BAD_ARG;
-    if (o->precond != SFC_PRECOND_JACOBI && o->precond != SFC_PRECOND_BLOCK_JACOBI) {
+    if (o->precond != SFC_PRECOND_JACOBI && o->precond != SFC_PRECOND_BLOCK_JACOBI &&
+        o->precond != SFC_PRECOND_TWO_LEVEL) {
         s->ctx->err = "unknown preconditioner";
+        return SFC_ERR_BAD_ARG;
+    }
+    if (o->coarse_size < 0) {
+        s->ctx->err = "coarse_size must be >= 0";
         return SFC_ERR_BAD_ARG;
     }
     if (o->method != SFC_SOLVER_PCG_FP64 && o->method != SFC_SOLVER_PCG_MIXED && o->method != SFC_SOLVER_FCG_MPNN) {

@@ -780,6 +780,7 @@ void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m)
     SFC_CK(cudaMemsetAsync(s->a_ref.p, 0, s->nnz * 8, ctx->stream));
     s->has_pattern = true;
     s->pattern_mesh = m;
+    s->coarse.built = false;  // aggregates belong to the installed mesh
     s->op_valid = false;
 }
 
@@ -974,6 +975,7 @@ void build_operator(sfc_system *s, bool require_positive_diag)
     if (h == 5 && require_positive_diag) fail(SFC_ERR_NOT_SPD, "non-positive diagonal entry: the operator is not SPD");
     build_bsr(s);
     s->op_valid = true;
+    ++s->op_serial;
 }
 
 // ---------------------------------------------------------------------------

@@ -175,10 +175,11 @@ int32_t sfc_autotune_block_solver(sfc_system_t *s, const double *rhs, int32_t nr
         o.method = SFC_SOLVER_PCG_MIXED;
         std::string v;
         if (!remeasure && tune_lookup(key, v)) {
-            int bw = 0, pc = 0;
-            if (std::sscanf(v.c_str(), "%d %d", &bw, &pc) == 2) {
+            int bw = 0, pc = 0, cs = 0;
+            if (std::sscanf(v.c_str(), "%d %d %d", &bw, &pc, &cs) >= 2) {
                 o.block_width = bw;
                 o.precond = pc;
+                o.coarse_size = cs;
                 s->opt = o;
                 if (best) *best = o;
                 return;
@@ -195,14 +196,22 @@ int32_t sfc_autotune_block_solver(sfc_system_t *s, const double *rhs, int32_t nr
         X.alloc((size_t)N * k);
         const sfc_solver_options_t keep = s->opt;
         double best_ms = 1e300;
-        int best_bw = 32, best_pc = SFC_PRECOND_JACOBI;
+        int best_bw = 32, best_pc = SFC_PRECOND_JACOBI, best_cs = 0;
+        // (preconditioner, coarse size) candidates; the two-level ones only
+        // where the system has a coarse space
+        std::vector<std::pair<int, int>> pcs{{SFC_PRECOND_JACOBI, 0}};
+        if (dof == 3) {
+            pcs.push_back({SFC_PRECOND_BLOCK_JACOBI, 0});
+            if (s->pattern_mesh)
+                for (int cs : {6, 8, 12}) pcs.push_back({SFC_PRECOND_TWO_LEVEL, cs});
+        }
         for (int bw : {32, 64, 128}) {
             if (bw > 32 && bw / 2 >= k) continue;  // wider blocks would be mostly padding
-            for (int pc : {SFC_PRECOND_JACOBI, SFC_PRECOND_BLOCK_JACOBI}) {
-                if (pc == SFC_PRECOND_BLOCK_JACOBI && dof != 3) continue;
+            for (auto [pc, csz] : pcs) {
                 sfc_solver_options_t c = o;
                 c.block_width = bw;
                 c.precond = pc;
+                c.coarse_size = csz;
                 s->opt = c;
                 double ms = 0;
                 try {
@@ -215,10 +224,12 @@ int32_t sfc_autotune_block_solver(sfc_system_t *s, const double *rhs, int32_t nr
                     }
                     continue;  // this candidate does not reach tol within max_iter
                 }
+                if (pc == SFC_PRECOND_TWO_LEVEL && s->stats.coarse_dofs == 0) continue;  // no coarse space
                 if (ms < best_ms) {
                     best_ms = ms;
                     best_bw = bw;
                     best_pc = pc;
+                    best_cs = csz;
                 }
             }
         }
@@ -226,8 +237,9 @@ int32_t sfc_autotune_block_solver(sfc_system_t *s, const double *rhs, int32_t nr
         SFC_REQUIRE(best_ms < 1e300, "no block-solver candidate converged on the sample");
         o.block_width = best_bw;
         o.precond = best_pc;
+        o.coarse_size = best_cs;
         s->opt = o;
-        tune_store(key, std::to_string(best_bw) + " " + std::to_string(best_pc));
+        tune_store(key, std::to_string(best_bw) + " " + std::to_string(best_pc) + " " + std::to_string(best_cs));
         if (best) *best = o;
     });
 }

@@ -1,0 +1,692 @@
+// Two-level preconditioner for the 3-dof (elasticity) solves: the nodal 3x3
+// block-Jacobi smoother plus an additive coarse correction on the rigid-body
+// modes of geometric aggregates,
+//
+//     M^-1 r = D^-1 r + P A_c^+ P^T r,     A_c = P^T S P,
+//
+// where P holds, for every aggregate (a box of nodes), its six rigid-body
+// modes (three translations and three rotations about the aggregate's
+// centroid), zero on constrained dofs, and A_c^+ is the inverse of the
+// Galerkin matrix on the span of the modes that are not numerically dependent.
+// Both terms are symmetric positive (semi)definite and the first is definite,
+// so M is SPD and plain PCG applies.  The reference solves with a direct
+// factorisation (corlib/SystemSolveEigenSparse.hpp:273-404); this is the
+// iterative replacement's stronger preconditioner: block Jacobi alone needs a
+// number of iterations that grows with the mesh size, the coarse space removes
+// the smooth, nearly rigid error components that it cannot reach.
+//
+// Layout and cost per iteration (K right-hand sides, nc = 6 x aggregates):
+//  * k_coarse_restrict32: c = P^T r, one CTA per aggregate, reads r once;
+//  * k_coarse_apply32:    e = A_c^+ c (FP32, dense nc x nc, L2-resident) and
+//                         the coarse share c.e of each column's r.z;
+//  * the p update (solvers.cu) adds z += P e on the fly from each node's
+//    aggregate id and centroid offset.
+// Setup per operator: the Galerkin product on the GPU (one CTA per
+// aggregate, FP64), then the inverse by block Gauss-Jordan elimination
+// (FP64, 32-wide panels) with dependent pivots dropped.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "common.cuh"
+
+namespace sfc {
+
+namespace {
+
+constexpr int kSlots = 27;   // 3 x 3 x 3 colour classes of the box grid
+constexpr int kGJ = 32;      // panel width of the Gauss-Jordan inverse
+constexpr int kMaxAggs = 512;
+
+// R(d): column k is e_k x d (the displacement of rotation mode k at offset d)
+__device__ __forceinline__ void rot_matrix(const float4 m, double (&R)[9])
+{
+    const double dx = m.x, dy = m.y, dz = m.z;
+    // rows: components; columns: rotation axes
+    R[0] = 0.0;  R[1] = dz;   R[2] = -dy;
+    R[3] = -dz;  R[4] = 0.0;  R[5] = dx;
+    R[6] = dy;   R[7] = -dx;  R[8] = 0.0;
+}
+
+__device__ __forceinline__ int mask_bits(const float4 m) { return (int)m.w; }
+
+// per node: offset from its aggregate's centroid in units of the box edge
+// (x, y, z) and the constrained components as bits in w
+__global__ void k_coarse_modes(const float4 *__restrict__ offset, const unsigned char *__restrict__ mask,
+                               int64_t nodes, float4 *__restrict__ mode)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        float4 m = offset[i];
+        const int bits = (mask[3 * i] ? 1 : 0) | (mask[3 * i + 1] ? 2 : 0) | (mask[3 * i + 2] ? 4 : 0);
+        m.w = (float)bits;
+        mode[i] = m;
+    }
+}
+
+// A_c = P^T S P.  One CTA per aggregate a: for every node i of a and every
+// block (i, j) of S, the 6 x 6 product M_i^T S_ij M_j is added to the slot of
+// j's aggregate (its colour class, unique among a's neighbours), then the
+// row block of a is written out.  M = diag(free) [I | R(d)].
+__global__ void __launch_bounds__(256) k_coarse_galerkin(const int32_t *__restrict__ agg_ptr,
+                                                         const int32_t *__restrict__ agg_nodes,
+                                                         const int32_t *__restrict__ node_agg,
+                                                         const int32_t *__restrict__ agg_slot,
+                                                         const int32_t *__restrict__ nbr, const float4 *__restrict__ mode,
+                                                         const int32_t *__restrict__ bptr,
+                                                         const int32_t *__restrict__ bcol,
+                                                         const double *__restrict__ bval, int64_t nc,
+                                                         double *__restrict__ A)
+{
+    __shared__ double acc[kSlots * 36];
+    const int a = blockIdx.x;
+    for (int t = threadIdx.x; t < kSlots * 36; t += blockDim.x) acc[t] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int32_t t = agg_ptr[a] + w; t < agg_ptr[a + 1]; t += nw) {
+        const int32_t i = agg_nodes[t];
+        const float4 mi = mode[i];
+        double Ri[9];
+        rot_matrix(mi, Ri);
+        const int bi = mask_bits(mi);
+        for (int32_t b = bptr[i] + lane; b < bptr[i + 1]; b += 32) {
+            const int32_t j = bcol[b];
+            const float4 mj = mode[j];
+            double Rj[9];
+            rot_matrix(mj, Rj);
+            const int bj = mask_bits(mj);
+            const int slot = agg_slot[node_agg[j]];
+            // S' = diag(free_i) S_ij diag(free_j)
+            double Sp[9];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    Sp[3 * r + c] = ((bi >> r) & 1) || ((bj >> c) & 1) ? 0.0 : bval[9 * (int64_t)b + 3 * r + c];
+            // U = S' R_j, V = R_i^T S', W = R_i^T U
+            double U[9], Vm[9], W[9];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    U[3 * r + k] = Sp[3 * r] * Rj[k] + Sp[3 * r + 1] * Rj[3 + k] + Sp[3 * r + 2] * Rj[6 + k];
+                    Vm[3 * r + k] = Ri[r] * Sp[k] + Ri[3 + r] * Sp[3 + k] + Ri[6 + r] * Sp[6 + k];
+                }
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    W[3 * r + k] = Ri[r] * U[k] + Ri[3 + r] * U[3 + k] + Ri[6 + r] * U[6 + k];
+            double *o = acc + slot * 36;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (Sp[3 * r + k] != 0.0) atomicAdd(o + r * 6 + k, Sp[3 * r + k]);
+                    if (U[3 * r + k] != 0.0) atomicAdd(o + r * 6 + 3 + k, U[3 * r + k]);
+                    if (Vm[3 * r + k] != 0.0) atomicAdd(o + (3 + r) * 6 + k, Vm[3 * r + k]);
+                    if (W[3 * r + k] != 0.0) atomicAdd(o + (3 + r) * 6 + 3 + k, W[3 * r + k]);
+                }
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < kSlots * 36; t += blockDim.x) {
+        const int slot = t / 36, mk = t - slot * 36;
+        const int32_t b = nbr[kSlots * a + slot];
+        if (b >= 0) A[(int64_t)(6 * a + mk / 6) * nc + 6 * b + mk % 6] = acc[t];
+    }
+}
+
+__global__ void k_diag_of(const double *__restrict__ A, int64_t n, double *__restrict__ d)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = A[i * n + i];
+}
+
+// Gauss-Jordan step, part 1: invert the kb x kb diagonal block D of panel k0
+// (in shared memory, every CTA redundantly; a pivot that is not above
+// 1e-10 x the dof's original diagonal is dropped: its row and column are
+// zeroed), save the old column panel colp[i][m] = A[i][k0+m] and form the new
+// row panel rowp[m][j] = (D^-1 A[k0.., j])[m] (= D^-1 itself inside the block).
+__global__ void __launch_bounds__(256) k_gj_panel(const double *__restrict__ A, int64_t n, int64_t k0, int kb,
+                                                  const double *__restrict__ adiag, double *__restrict__ rowp,
+                                                  double *__restrict__ colp, int *dropped)
+{
+    __shared__ double D[kGJ][kGJ + 1];
+    __shared__ double rowv[kGJ], colv[kGJ];
+    __shared__ int drop;
+    for (int t = threadIdx.x; t < kGJ * kGJ; t += blockDim.x) {
+        const int r = t / kGJ, c = t % kGJ;
+        D[r][c] = (r < kb && c < kb) ? A[(k0 + r) * n + k0 + c] : 0.0;
+    }
+    __syncthreads();
+    for (int p = 0; p < kb; ++p) {
+        if (threadIdx.x == 0) {
+            const double piv = D[p][p];
+            drop = !(piv > 1e-10 * adiag[k0 + p]);
+        }
+        if (threadIdx.x < kGJ) {
+            rowv[threadIdx.x] = D[p][threadIdx.x];
+            colv[threadIdx.x] = D[threadIdx.x][p];
+        }
+        __syncthreads();
+        const double piv = rowv[p];
+        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+            const int r = t / kb, c = t % kb;
+            double v;
+            if (drop)
+                v = (r == p || c == p) ? 0.0 : D[r][c];
+            else if (r == p && c == p)
+                v = 1.0 / piv;
+            else if (r == p)
+                v = rowv[c] / piv;
+            else if (c == p)
+                v = -colv[r] / piv;
+            else
+                v = D[r][c] - colv[r] * rowv[c] / piv;
+            D[r][c] = v;
+        }
+        if (drop && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(dropped, 1);
+        __syncthreads();
+    }
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        for (int m = 0; m < kb; ++m) colp[j * kGJ + m] = A[j * n + k0 + m];
+        if (j >= k0 && j < k0 + kb) {
+            for (int m = 0; m < kb; ++m) rowp[m * n + j] = D[m][j - k0];
+        } else {
+            double aj[kGJ];
+#pragma unroll
+            for (int l = 0; l < kGJ; ++l) aj[l] = l < kb ? A[(k0 + l) * n + j] : 0.0;
+            for (int m = 0; m < kb; ++m) {
+                double s = 0.0;
+#pragma unroll
+                for (int l = 0; l < kGJ; ++l) s += D[m][l] * aj[l];
+                rowp[m * n + j] = s;
+            }
+        }
+    }
+}
+
+// Gauss-Jordan step, part 2 (64 x 64 tile per CTA):
+//   rows of the panel:     A[i][j] = rowp[i-k0][j]
+//   columns of the panel:  A[i][j] = -colp[i] . rowp[:, j]   (= -A[i,k] D^-1)
+//   elsewhere:             A[i][j] -= colp[i] . rowp[:, j]
+__global__ void __launch_bounds__(256) k_gj_update(double *__restrict__ A, int64_t n, int64_t k0, int kb,
+                                                   const double *__restrict__ rowp, const double *__restrict__ colp)
+{
+    __shared__ double cp[64][kGJ + 1];
+    __shared__ double rp[kGJ][64 + 1];
+    const int64_t i0 = (int64_t)blockIdx.y * 64, j0 = (int64_t)blockIdx.x * 64;
+    for (int t = threadIdx.x; t < 64 * kGJ; t += blockDim.x) {
+        const int r = t / kGJ, m = t % kGJ;
+        cp[r][m] = (i0 + r < n && m < kb) ? colp[(i0 + r) * kGJ + m] : 0.0;
+        const int mm = t / 64, c = t % 64;
+        rp[mm][c] = (j0 + c < n && mm < kb) ? rowp[mm * n + j0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+    for (int u = 0; u < 4; ++u) {
+        const int64_t i = i0 + ty + 16 * u;
+        if (i >= n) continue;
+        for (int v = 0; v < 4; ++v) {
+            const int64_t j = j0 + tx + 16 * v;
+            if (j >= n) continue;
+            if (i >= k0 && i < k0 + kb) {
+                A[i * n + j] = rp[i - k0][tx + 16 * v];
+                continue;
+            }
+            double s = 0.0;
+#pragma unroll
+            for (int m = 0; m < kGJ; ++m) s += cp[ty + 16 * u][m] * rp[m][tx + 16 * v];
+            A[i * n + j] = (j >= k0 && j < k0 + kb) ? -s : A[i * n + j] - s;
+        }
+    }
+}
+
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// c[6a + m][col] = (P^T r)[6a + m][col] for K = 32 V interleaved columns
+template <int V>
+__global__ void __launch_bounds__(256) k_coarse_restrict32(const float *__restrict__ r,
+                                                           const int32_t *__restrict__ agg_ptr,
+                                                           const int32_t *__restrict__ agg_nodes,
+                                                           const float4 *__restrict__ mode, float *__restrict__ c,
+                                                           const int *stop)
+{
+    constexpr int K = 32 * V;
+    __shared__ float red[8][6][K];
+    if (stop && *stop) return;
+    const int a = blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float acc[6][V];
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[m][v] = 0.f;
+    for (int32_t t = agg_ptr[a] + w; t < agg_ptr[a + 1]; t += 8) {
+        const int32_t i = agg_nodes[t];
+        const float4 m = mode[i];
+        const int bits = (int)m.w;
+        float rv[3][V];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const float *src = r + (3 * (int64_t)i + q) * K + lane * V;
+            if constexpr (V == 4) {
+                const float4 t4 = *reinterpret_cast<const float4 *>(src);
+                rv[q][0] = t4.x; rv[q][1] = t4.y; rv[q][2] = t4.z; rv[q][3] = t4.w;
+            } else if constexpr (V == 2) {
+                const float2 t2 = *reinterpret_cast<const float2 *>(src);
+                rv[q][0] = t2.x; rv[q][1] = t2.y;
+            } else {
+                rv[q][0] = *src;
+            }
+            if ((bits >> q) & 1)
+#pragma unroll
+                for (int v = 0; v < V; ++v) rv[q][v] = 0.f;
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            acc[0][v] += rv[0][v];
+            acc[1][v] += rv[1][v];
+            acc[2][v] += rv[2][v];
+            acc[3][v] += m.y * rv[2][v] - m.z * rv[1][v];
+            acc[4][v] += m.z * rv[0][v] - m.x * rv[2][v];
+            acc[5][v] += m.x * rv[1][v] - m.y * rv[0][v];
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+#pragma unroll
+        for (int v = 0; v < V; ++v) red[w][m][lane * V + v] = acc[m][v];
+    __syncthreads();
+    for (int t = threadIdx.x; t < 6 * K; t += blockDim.x) {
+        const int m = t / K, col = t % K;
+        float s = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s += red[q][m][col];
+        c[(int64_t)(6 * a + m) * K + col] = s;
+    }
+}
+
+// e = A c (A: nc x nc FP32, c and e: [nc][K]); rz[col] += sum_rows c e
+template <int V>
+__global__ void __launch_bounds__(256) k_coarse_apply32(const float *__restrict__ A, const float *__restrict__ c,
+                                                        float *__restrict__ e, int64_t nc, double *rz,
+                                                        const int *stop)
+{
+    constexpr int K = 32 * V;
+    constexpr int CG = K / 4;         // float4 column groups
+    constexpr int RS = 256 / CG;      // row sets
+    constexpr int R = 2;              // rows per thread
+    constexpr int ROWS = RS * R;
+    __shared__ float sa[ROWS][33];
+    __shared__ float4 sc[32][CG];
+    __shared__ double sred[RS][K];
+    if (stop && *stop) return;
+    const int g = threadIdx.x % CG, rs = threadIdx.x / CG;
+    const int64_t row0 = (int64_t)blockIdx.x * ROWS;
+    float acc[R][4];
+#pragma unroll
+    for (int u = 0; u < R; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[u][q] = 0.f;
+    for (int64_t k0 = 0; k0 < nc; k0 += 32) {
+        for (int t = threadIdx.x; t < ROWS * 32; t += 256) {
+            const int rr = t / 32, kk = t % 32;
+            const int64_t row = row0 + rr, k = k0 + kk;
+            sa[rr][kk] = (row < nc && k < nc) ? A[row * nc + k] : 0.f;
+        }
+        for (int t = threadIdx.x; t < 32 * CG; t += 256) {
+            const int kk = t / CG, gg = t % CG;
+            sc[kk][gg] = (k0 + kk < nc) ? *reinterpret_cast<const float4 *>(c + (k0 + kk) * K + 4 * gg)
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 32; ++kk) {
+            const float4 cv = sc[kk][g];
+#pragma unroll
+            for (int u = 0; u < R; ++u) {
+                const float av = sa[rs * R + u][kk];
+                acc[u][0] = fmaf(av, cv.x, acc[u][0]);
+                acc[u][1] = fmaf(av, cv.y, acc[u][1]);
+                acc[u][2] = fmaf(av, cv.z, acc[u][2]);
+                acc[u][3] = fmaf(av, cv.w, acc[u][3]);
+            }
+        }
+        __syncthreads();
+    }
+    double d[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+        const int64_t row = row0 + rs * R + u;
+        if (row >= nc) continue;
+        *reinterpret_cast<float4 *>(e + row * K + 4 * g) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+        const float4 cv = *reinterpret_cast<const float4 *>(c + row * K + 4 * g);
+        d[0] += (double)cv.x * acc[u][0];
+        d[1] += (double)cv.y * acc[u][1];
+        d[2] += (double)cv.z * acc[u][2];
+        d[3] += (double)cv.w * acc[u][3];
+    }
+    if (!rz) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sred[rs][4 * g + q] = d[q];
+    __syncthreads();
+    for (int col = threadIdx.x; col < K; col += 256) {
+        double s = 0.0;
+        for (int q = 0; q < RS; ++q) s += sred[q][col];
+        atomicAdd(rz + col, s);
+    }
+}
+
+// single FP64 vector: c[6a + m] = (P^T r)[6a + m]
+__global__ void __launch_bounds__(256) k_coarse_restrict64(const double *__restrict__ r,
+                                                           const int32_t *__restrict__ agg_ptr,
+                                                           const int32_t *__restrict__ agg_nodes,
+                                                           const float4 *__restrict__ mode, double *__restrict__ c,
+                                                           const int *done)
+{
+    __shared__ double red[6][8];
+    if (done && *done) return;
+    const int a = blockIdx.x;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int32_t t = agg_ptr[a] + threadIdx.x; t < agg_ptr[a + 1]; t += blockDim.x) {
+        const int32_t i = agg_nodes[t];
+        const float4 m = mode[i];
+        const int bits = (int)m.w;
+        const double r0 = (bits & 1) ? 0.0 : r[3 * (int64_t)i], r1 = (bits & 2) ? 0.0 : r[3 * (int64_t)i + 1],
+                     r2 = (bits & 4) ? 0.0 : r[3 * (int64_t)i + 2];
+        acc[0] += r0;
+        acc[1] += r1;
+        acc[2] += r2;
+        acc[3] += (double)m.y * r2 - (double)m.z * r1;
+        acc[4] += (double)m.z * r0 - (double)m.x * r2;
+        acc[5] += (double)m.x * r1 - (double)m.y * r0;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        double v = acc[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[m][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double s = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += red[threadIdx.x][q];
+        c[6 * a + threadIdx.x] = s;
+    }
+}
+
+// e = A c (FP64, warp per row); rz += c.e
+__global__ void __launch_bounds__(256) k_coarse_apply64(const double *__restrict__ A, const double *__restrict__ c,
+                                                        double *__restrict__ e, int64_t nc, double *rz, const int *done)
+{
+    __shared__ double sh[8];
+    if (done && *done) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t row = (int64_t)blockIdx.x * 8 + w;
+    double part = 0.0;
+    if (row < nc) {
+        double s = 0.0;
+        for (int64_t k = lane; k < nc; k += 32) s += A[row * nc + k] * c[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            e[row] = s;
+            part = s * c[row];
+        }
+    }
+    if (lane == 0) sh[w] = part;
+    __syncthreads();
+    if (threadIdx.x == 0 && rz) {
+        double t = 0.0;
+        for (int q = 0; q < 8; ++q) t += sh[q];
+        atomicAdd(rz, t);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+// Aggregates = the non-empty boxes of a grid laid over the mesh's bounding
+// box, about `size` nodes along each axis (at most kMaxAggs boxes).  The
+// colour classes (box index mod 3 per axis) make the Galerkin product a
+// single pass; they need every element's nodes to lie in boxes at most one
+// apart per axis, which is checked over the connectivity (the grid is
+// coarsened until it holds).
+static bool coarse_aggregate(sfc_system *s, int size)
+{
+    sfc_ctx *ctx = s->ctx;
+    const sfc_mesh *m = s->pattern_mesh;
+    CoarseSpace &cs = s->coarse;
+    cs.built = false;
+    if (!m || m->dof != 3 || !s->has_bsr || m->num_nodes != s->nodes) return false;
+    const int64_t nodes = m->num_nodes;
+    const double *X = m->h_coords.data();
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = INFINITY;
+        hi[d] = -INFINITY;
+    }
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], X[3 * i + d]);
+            hi[d] = std::max(hi[d], X[3 * i + d]);
+        }
+    double ext[3], emax = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        ext[d] = hi[d] - lo[d];
+        emax = std::max(emax, ext[d]);
+    }
+    if (!(emax > 0.0)) return false;
+    int dim = 0;
+    double vol = 1.0;
+    for (int d = 0; d < 3; ++d)
+        if (ext[d] > 1e-12 * emax) {
+            ++dim;
+            vol *= ext[d];
+        }
+    const double per = std::pow((double)std::max(size, 2), dim);
+    const double target = std::min<double>(kMaxAggs, std::max(1.0, (double)nodes / per));
+    const double hb = std::pow(vol / target, 1.0 / dim);
+    int nb[3];
+    for (int d = 0; d < 3; ++d) nb[d] = ext[d] > 1e-12 * emax ? std::max(1, (int)std::lround(ext[d] / hb)) : 1;
+    std::vector<uint32_t> conn((size_t)m->num_elems * m->nn);
+    download(ctx, conn.data(), m->conn.p, conn.size());
+    std::vector<int32_t> box(nodes * 3);
+    bool ok = false;
+    for (int attempt = 0; attempt < 8 && !ok; ++attempt) {
+        for (int64_t i = 0; i < nodes; ++i)
+            for (int d = 0; d < 3; ++d) {
+                int b = ext[d] > 1e-12 * emax ? (int)std::floor((X[3 * i + d] - lo[d]) / ext[d] * nb[d]) : 0;
+                box[3 * i + d] = std::min(std::max(b, 0), nb[d] - 1);
+            }
+        ok = true;
+        for (int64_t e = 0; e < m->num_elems && ok; ++e)
+            for (int d = 0; d < 3 && ok; ++d) {
+                int bmin = INT32_MAX, bmax = INT32_MIN;
+                for (int k = 0; k < m->nn; ++k) {
+                    const int b = box[3 * (int64_t)conn[(size_t)e * m->nn + k] + d];
+                    bmin = std::min(bmin, b);
+                    bmax = std::max(bmax, b);
+                }
+                if (bmax - bmin > 1) ok = false;
+            }
+        if (!ok) {
+            if (nb[0] == 1 && nb[1] == 1 && nb[2] == 1) break;
+            for (int d = 0; d < 3; ++d) nb[d] = std::max(1, nb[d] / 2);
+        }
+    }
+    if (!ok) return false;
+    const int64_t nboxes = (int64_t)nb[0] * nb[1] * nb[2];
+    std::vector<int32_t> box_agg(nboxes, -1), count;
+    std::vector<int32_t> node_agg(nodes);
+    int32_t nagg = 0;
+    for (int64_t i = 0; i < nodes; ++i) {
+        const int64_t id = box[3 * i] + (int64_t)nb[0] * (box[3 * i + 1] + (int64_t)nb[1] * box[3 * i + 2]);
+        if (box_agg[id] < 0) box_agg[id] = nagg++;
+        node_agg[i] = box_agg[id];
+    }
+    // aggregates in box order (deterministic numbering)
+    {
+        int32_t next = 0;
+        std::vector<int32_t> remap(nagg, -1);
+        for (int64_t id = 0; id < nboxes; ++id)
+            if (box_agg[id] >= 0) {
+                remap[box_agg[id]] = next;
+                box_agg[id] = next++;
+            }
+        for (auto &a : node_agg) a = remap[a];
+    }
+    std::vector<int32_t> agg_ptr(nagg + 1, 0), agg_nodes(nodes);
+    for (int64_t i = 0; i < nodes; ++i) ++agg_ptr[node_agg[i] + 1];
+    for (int32_t a = 0; a < nagg; ++a) agg_ptr[a + 1] += agg_ptr[a];
+    {
+        std::vector<int32_t> fill(agg_ptr.begin(), agg_ptr.end() - 1);
+        for (int64_t i = 0; i < nodes; ++i) agg_nodes[fill[node_agg[i]]++] = (int32_t)i;
+    }
+    std::vector<double> cen(3 * (size_t)nagg, 0.0);
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int d = 0; d < 3; ++d) cen[3 * node_agg[i] + d] += X[3 * i + d];
+    for (int32_t a = 0; a < nagg; ++a)
+        for (int d = 0; d < 3; ++d) cen[3 * a + d] /= (double)(agg_ptr[a + 1] - agg_ptr[a]);
+    double hsum = 0.0;
+    int hn = 0;
+    for (int d = 0; d < 3; ++d)
+        if (ext[d] > 1e-12 * emax) {
+            hsum += ext[d] / nb[d];
+            ++hn;
+        }
+    const double h = hsum / hn;
+    std::vector<float4> off(nodes);
+    for (int64_t i = 0; i < nodes; ++i) {
+        const int32_t a = node_agg[i];
+        off[i] = make_float4((float)((X[3 * i] - cen[3 * a]) / h), (float)((X[3 * i + 1] - cen[3 * a + 1]) / h),
+                             (float)((X[3 * i + 2] - cen[3 * a + 2]) / h), 0.f);
+    }
+    std::vector<int32_t> slot(nagg), nbr((size_t)nagg * kSlots, -1);
+    for (int64_t id = 0; id < nboxes; ++id) {
+        const int32_t a = box_agg[id];
+        if (a < 0) continue;
+        const int bx = (int)(id % nb[0]), by = (int)((id / nb[0]) % nb[1]), bz = (int)(id / ((int64_t)nb[0] * nb[1]));
+        slot[a] = bx % 3 + 3 * (by % 3) + 9 * (bz % 3);
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int x = bx + dx, y = by + dy, z = bz + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= nb[0] || y >= nb[1] || z >= nb[2]) continue;
+                    const int32_t b = box_agg[x + (int64_t)nb[0] * (y + (int64_t)nb[1] * z)];
+                    if (b < 0) continue;
+                    nbr[(size_t)a * kSlots + (x % 3) + 3 * (y % 3) + 9 * (z % 3)] = b;
+                }
+    }
+    cs.nagg = nagg;
+    cs.nc = 6 * (int64_t)nagg;
+    for (int d = 0; d < 3; ++d) cs.nb[d] = nb[d];
+    upload(ctx, cs.node_agg, node_agg.data(), nodes);
+    upload(ctx, cs.agg_ptr, agg_ptr.data(), agg_ptr.size());
+    upload(ctx, cs.agg_nodes, agg_nodes.data(), nodes);
+    upload(ctx, cs.agg_slot, slot.data(), nagg);
+    upload(ctx, cs.nbr, nbr.data(), nbr.size());
+    upload(ctx, cs.offset, off.data(), nodes);
+    cs.mode.alloc(nodes);
+    cs.mesh = m;
+    cs.size = size;
+    cs.built = true;
+    cs.op_serial = 0;
+    return true;
+}
+
+// (Re)builds the coarse space for the current operator; false when the
+// system has none (not a 3-dof mesh, or no valid box grid).
+bool coarse_prepare(sfc_system *s)
+{
+    CoarseSpace &cs = s->coarse;
+    const int size = s->opt.coarse_size > 0 ? s->opt.coarse_size : 8;
+    if (!cs.built || cs.mesh != s->pattern_mesh || cs.size != size) {
+        if (!coarse_aggregate(s, size)) return false;
+    }
+    if (cs.op_serial == s->op_serial) return true;
+    sfc_ctx *ctx = s->ctx;
+    ProfScope ps(ctx, "phase:coarse_setup", 0.0);
+    const int64_t nodes = s->nodes, nc = cs.nc;
+    k_coarse_modes<<<grid_for(nodes, 256), 256, 0, ctx->stream>>>(cs.offset.p, s->mask.p, nodes, cs.mode.p);
+    cs.a64.alloc(nc * nc);
+    cs.a32.alloc(nc * nc);
+    SFC_CK(cudaMemsetAsync(cs.a64.p, 0, nc * nc * sizeof(double), ctx->stream));
+    k_coarse_galerkin<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(cs.agg_ptr.p, cs.agg_nodes.p, cs.node_agg.p,
+                                                                 cs.agg_slot.p, cs.nbr.p, cs.mode.p, s->bptr.p,
+                                                                 s->bcol.p, s->bval64.p, nc, cs.a64.p);
+    count_launch(ctx, 2);
+    cs.diag.alloc(nc);
+    cs.rowp.alloc(kGJ * nc);
+    cs.colp.alloc(kGJ * nc);
+    k_diag_of<<<grid_for(nc, 256), 256, 0, ctx->stream>>>(cs.a64.p, nc, cs.diag.p);
+    DevInt dropped = status_word(ctx, 2);
+    SFC_CK(cudaMemsetAsync(dropped.p, 0, sizeof(int), ctx->stream));
+    count_launch(ctx);
+    const unsigned gp = grid_for(nc, 256), gt = (unsigned)((nc + 63) / 64);
+    for (int64_t k0 = 0; k0 < nc; k0 += kGJ) {
+        const int kb = (int)std::min<int64_t>(kGJ, nc - k0);
+        k_gj_panel<<<gp, 256, 0, ctx->stream>>>(cs.a64.p, nc, k0, kb, cs.diag.p, cs.rowp.p, cs.colp.p, dropped.p);
+        k_gj_update<<<dim3(gt, gt), 256, 0, ctx->stream>>>(cs.a64.p, nc, k0, kb, cs.rowp.p, cs.colp.p);
+        count_launch(ctx, 2);
+    }
+    k_to_f32<<<grid_for(nc * nc, 256), 256, 0, ctx->stream>>>(cs.a64.p, cs.a32.p, nc * nc);
+    count_launch(ctx);
+    int h = 0;
+    download(ctx, &h, dropped.p, 1);
+    cs.dropped = h;
+    cs.op_serial = s->op_serial;
+    return true;
+}
+
+template <int V>
+void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *stop)
+{
+    constexpr int K = 32 * V;
+    CoarseSpace &cs = s->coarse;
+    sfc_ctx *ctx = s->ctx;
+    cs.c32.reserve(cs.nc * K);
+    cs.e32.reserve(cs.nc * K);
+    {
+        ProfScope ps(ctx, "coarse_restrict32", 3.0 * s->nodes * K * 4 + 20.0 * s->nodes + 4.0 * cs.nc * K);
+        k_coarse_restrict32<V><<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p,
+                                                                           cs.c32.p, stop);
+    }
+    {
+        constexpr int ROWS = (256 / (K / 4)) * 2;
+        ProfScope ps(ctx, "coarse_apply32", 4.0 * cs.nc * cs.nc + 8.0 * cs.nc * K);
+        k_coarse_apply32<V><<<(unsigned)((cs.nc + ROWS - 1) / ROWS), 256, 0, ctx->stream>>>(cs.a32.p, cs.c32.p,
+                                                                                             cs.e32.p, cs.nc, rz, stop);
+    }
+    count_launch(ctx, 2);
+}
+template void coarse_block_apply<1>(sfc_system *, const float *, double *, const int *);
+template void coarse_block_apply<2>(sfc_system *, const float *, double *, const int *);
+template void coarse_block_apply<4>(sfc_system *, const float *, double *, const int *);
+
+void coarse_vec_apply(sfc_system *s, const double *r, double *rz, const int *done)
+{
+    CoarseSpace &cs = s->coarse;
+    sfc_ctx *ctx = s->ctx;
+    cs.c64.reserve(cs.nc);
+    cs.e64.reserve(cs.nc);
+    k_coarse_restrict64<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p,
+                                                                    cs.c64.p, done);
+    k_coarse_apply64<<<(unsigned)((cs.nc + 7) / 8), 256, 0, ctx->stream>>>(cs.a64.p, cs.c64.p, cs.e64.p, cs.nc, rz,
+                                                                            done);
+    count_launch(ctx, 2);
+}
+
+}  // namespace sfc

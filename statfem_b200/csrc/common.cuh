@@ -200,6 +200,34 @@ void make_quadrature(int kind, int qps, QuadTable &t);
 }  // namespace sfc
 
 // ---------------------------------------------------------------------------
+// coarse space of the two-level preconditioner (coarse.cu): rigid-body modes
+// of box aggregates on 3-dof meshes
+// ---------------------------------------------------------------------------
+struct sfc_mesh;
+namespace sfc {
+struct CoarseSpace {
+    bool built = false;                 // aggregates for (mesh, size)
+    const sfc_mesh *mesh = nullptr;
+    int size = 0;                       // nodes per aggregate along each axis (target)
+    uint64_t op_serial = 0;             // operator the inverse below belongs to
+    int64_t nagg = 0, nc = 0;           // aggregates, coarse dofs (6 per aggregate)
+    int nb[3] = {1, 1, 1};              // boxes per axis
+    int dropped = 0;                    // dependent coarse dofs left out of the inverse
+    DBuf<int32_t> node_agg;             // nodes
+    DBuf<int32_t> agg_ptr, agg_nodes;   // aggregate -> its nodes
+    DBuf<int32_t> agg_slot;             // colour class (box index mod 3 per axis)
+    DBuf<int32_t> nbr;                  // [nagg][27]: neighbour aggregate per colour class
+    DBuf<float4> offset;                // node offset from the centroid / box edge
+    DBuf<float4> mode;                  // offset + constrained components (bits in w)
+    DBuf<double> a64;                   // nc x nc: Galerkin matrix, inverted in place
+    DBuf<float> a32;                    // FP32 copy of the inverse
+    DBuf<double> diag, rowp, colp;      // Gauss-Jordan scratch
+    DBuf<float> c32, e32;               // [nc][K] restriction and correction (block)
+    DBuf<double> c64, e64;              // single FP64 vector
+};
+}  // namespace sfc
+
+// ---------------------------------------------------------------------------
 // mesh + its symbolic (pattern) data
 // ---------------------------------------------------------------------------
 struct sfc_mesh {
@@ -289,6 +317,8 @@ struct sfc_system {
     sfc::DBuf<double> cval;
     struct sfc_mpnn *mpnn = nullptr;  // learned preconditioner for SFC_SOLVER_FCG_MPNN
     int spmv_lanes = 0;               // lanes per row of the FP64 SpMV (0: by row length; set by the tuner)
+    uint64_t op_serial = 0;           // bumped by every operator (re)build
+    sfc::CoarseSpace coarse;          // SFC_PRECOND_TWO_LEVEL
 };
 
 // ---------------------------------------------------------------------------
@@ -371,6 +401,11 @@ PcgStats pcg64_public(sfc_system *s, const double *b, double *x, double tol, int
 void solve_forward_fcg(sfc_system *s);
 // solvers.cu: FP64 SpMV with a given number of lanes per row (4, 8, 16, 32)
 void spmv_op64_lanes(sfc_system *s, int lanes, const double *x, double *y);
+// two-level preconditioner (coarse.cu)
+bool coarse_prepare(sfc_system *s);
+template <int V>
+void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *stop);
+void coarse_vec_apply(sfc_system *s, const double *r, double *rz, const int *done);
 // stats.cu
 void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp);
 void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *X, int64_t ns,

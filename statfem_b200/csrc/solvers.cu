@@ -624,7 +624,7 @@ __device__ __forceinline__ void bj_apply(const float *__restrict__ D, const floa
         for (int v = 0; v < V; ++v) z[i][v] = fmaf(d[3 * i + 2], r[2][v], fmaf(d[3 * i + 1], r[1][v], d[3 * i] * r[0][v]));
 }
 
-template <int V>
+template <int V, bool SETP = true>
 __global__ void __launch_bounds__(256) k_ninit32(const double *__restrict__ R64, const double *__restrict__ scale,
                                                  const float *__restrict__ bdinv, const int *__restrict__ restart,
                                                  float *__restrict__ r, float *__restrict__ x, float *__restrict__ p,
@@ -652,14 +652,18 @@ __global__ void __launch_bounds__(256) k_ninit32(const double *__restrict__ R64,
             for (int v = 0; v < V; ++v) zero[v] = 0.f;
             stv<V>(r + o, rv[i]);
             stv<V>(x + o, zero);
-            ldv<V>(p + o, pv);
+            if constexpr (SETP) {
+                ldv<V>(p + o, pv);
+#pragma unroll
+                for (int v = 0; v < V; ++v)
+                    if (restart[lane * V + v]) pv[v] = zv[i][v];
+                stv<V>(p + o, pv);
+            }
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                if (restart[lane * V + v]) pv[v] = zv[i][v];
                 a1[v] += (double)rv[i][v] * zv[i][v];
                 a2[v] += (double)rv[i][v] * rv[i][v];
             }
-            stv<V>(p + o, pv);
         }
     }
     block_cols_add<V>(a1, sh, rz0);
@@ -755,6 +759,184 @@ __global__ void __launch_bounds__(256) k_npupdate32(float *__restrict__ p, const
             for (int v = 0; v < V; ++v)
                 if (act[v]) pv[v] = fmaf(beta[v], pv[v], zv[i][v]);
             stv<V>(p + o, pv);
+        }
+    }
+}
+
+// two-level variant of the p update: z = Dinv_n r_n + M_n e_a (the coarse
+// correction e of the node's aggregate a, M_n = diag(free) [I | R(d_n)]:
+// translation t plus rotation w x d), then p = z + beta p for the active
+// columns.  INIT: p = z for the restarted columns, others keep p.
+template <int V, bool INIT>
+__global__ void __launch_bounds__(256) k_ncpupdate32(float *__restrict__ p, const float *__restrict__ r,
+                                                     const float *__restrict__ bdinv,
+                                                     const int32_t *__restrict__ node_agg,
+                                                     const float4 *__restrict__ mode, const float *__restrict__ e,
+                                                     int64_t nodes, const double *rz, const double *rz_next,
+                                                     const double *rr_next, const double *thr, const int *stop,
+                                                     const int *brk, const int *restart)
+{
+    constexpr int K = 32 * V;
+    if (!INIT && *stop) return;
+    const int lane = threadIdx.x & 31;
+    float beta[V];
+    bool act[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int c = lane * V + v;
+        if constexpr (INIT) {
+            act[v] = restart[c] != 0;
+            beta[v] = 0.f;
+        } else {
+            act[v] = rr_next[c] > thr[c] && !brk[c];
+            beta[v] = act[v] ? (float)(rz_next[c] / rz[c]) : 0.f;
+        }
+    }
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t n = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; n < nodes; n += warps) {
+        float rv[3][V], zv[3][V];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) ldv<V>(r + (3 * n + i) * K + lane * V, rv[i]);
+        bj_apply<V>(bdinv + 9 * n, rv, zv);
+        const int32_t a = node_agg[n];
+        const float4 m = mode[n];
+        const int bits = (int)m.w;
+        float ev[6][V];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ldv<V>(e + (6 * (int64_t)a + k) * K + lane * V, ev[k]);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const float c0 = ev[0][v] + ev[4][v] * m.z - ev[5][v] * m.y;
+            const float c1 = ev[1][v] + ev[5][v] * m.x - ev[3][v] * m.z;
+            const float c2 = ev[2][v] + ev[3][v] * m.y - ev[4][v] * m.x;
+            if (!(bits & 1)) zv[0][v] += c0;
+            if (!(bits & 2)) zv[1][v] += c1;
+            if (!(bits & 4)) zv[2][v] += c2;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t o = (3 * n + i) * K + lane * V;
+            float pv[V];
+            ldv<V>(p + o, pv);
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                if (act[v]) pv[v] = fmaf(beta[v], pv[v], zv[i][v]);
+            stv<V>(p + o, pv);
+        }
+    }
+}
+
+// ---- FP64 two-level PCG (one vector, 3-dof nodes, thread per node) ---------
+__device__ __forceinline__ void bj_apply64(const float *__restrict__ D, const double (&r)[3], double (&z)[3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        z[i] = (double)D[3 * i] * r[0] + (double)D[3 * i + 1] * r[1] + (double)D[3 * i + 2] * r[2];
+}
+
+// r = b, x = 0; rz0 += r . Dinv r (block-Jacobi share), bb += r . r
+__global__ void __launch_bounds__(kRedThreads) k_pcg2_init(const double *__restrict__ b, const float *__restrict__ bdinv,
+                                                            double *__restrict__ x, double *__restrict__ r,
+                                                            int64_t nodes, double *rz0, double *bb)
+{
+    __shared__ double sh[32];
+    double a = 0, c = 0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        double rv[3], zv[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            rv[i] = b[3 * n + i];
+            r[3 * n + i] = rv[i];
+            x[3 * n + i] = 0.0;
+        }
+        bj_apply64(bdinv + 9 * n, rv, zv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            a += rv[i] * zv[i];
+            c += rv[i] * rv[i];
+        }
+    }
+    a = block_sum(a, sh);
+    c = block_sum(c, sh);
+    if (threadIdx.x == 0) {
+        atomicAdd(rz0, a);
+        atomicAdd(bb, c);
+    }
+}
+
+// alpha = rz/pq; x += alpha p; r -= alpha q; rz' += r . Dinv r; rr' += r . r
+__global__ void __launch_bounds__(kRedThreads) k_pcg2_update(double *__restrict__ x, double *__restrict__ r,
+                                                              const double *__restrict__ p, const double *__restrict__ q,
+                                                              const float *__restrict__ bdinv, int64_t nodes,
+                                                              const double *pq, const double *rz, double *rz_next,
+                                                              double *rr_next, const int *done, int *err)
+{
+    __shared__ double sh[32];
+    if (*done) return;
+    const double den = *pq;
+    if (!(den > 0.0)) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
+    const double alpha = *rz / den;
+    double a = 0, c = 0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        double rv[3], zv[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int64_t k = 3 * n + i;
+            x[k] += alpha * p[k];
+            rv[i] = r[k] - alpha * q[k];
+            r[k] = rv[i];
+        }
+        bj_apply64(bdinv + 9 * n, rv, zv);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            a += rv[i] * zv[i];
+            c += rv[i] * rv[i];
+        }
+    }
+    a = block_sum(a, sh);
+    c = block_sum(c, sh);
+    if (threadIdx.x == 0) {
+        atomicAdd(rz_next, a);
+        atomicAdd(rr_next, c);
+    }
+}
+
+// convergence test on rr'; else p = Dinv r + M e + beta p (INIT: p = z)
+template <bool INIT>
+__global__ void k_pcg2_pupdate(double *__restrict__ p, const double *__restrict__ r, const float *__restrict__ bdinv,
+                               const int32_t *__restrict__ node_agg, const float4 *__restrict__ mode,
+                               const double *__restrict__ e, int64_t nodes, const double *rz,
+                               const double *rz_next, const double *rr_next, double thr, int it_next, int *done,
+                               const int *err)
+{
+    double beta = 0.0;
+    if constexpr (!INIT) {
+        if (*done || *err) return;
+        if (*rr_next <= thr) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *done = it_next;
+            return;
+        }
+        beta = *rz_next / *rz;
+    }
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nodes; n += (int64_t)gridDim.x * blockDim.x) {
+        double rv[3], zv[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) rv[i] = r[3 * n + i];
+        bj_apply64(bdinv + 9 * n, rv, zv);
+        const int64_t a = node_agg[n];
+        const float4 m = mode[n];
+        const int bits = (int)m.w;
+        const double *ea = e + 6 * a;
+        const double dx = m.x, dy = m.y, dz = m.z;
+        const double c[3] = {ea[0] + ea[4] * dz - ea[5] * dy, ea[1] + ea[5] * dx - ea[3] * dz,
+                             ea[2] + ea[3] * dy - ea[4] * dx};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double z = zv[i] + (((bits >> i) & 1) ? 0.0 : c[i]);
+            p[3 * n + i] = INIT ? z : z + beta * p[3 * n + i];
         }
     }
 }
@@ -870,8 +1052,18 @@ void launch_spmv64(sfc_system *s, const double *x, double *y, double *dot, const
     count_launch(ctx);
 }
 
-// FP64 Jacobi-PCG on S x = b (device vectors, length N)
-PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_iter, int check)
+// the two-level preconditioner is used when it is selected and the system
+// has a coarse space (a 3-dof mesh with a valid box grid); builds it for the
+// current operator
+bool use_two_level(sfc_system *s)
+{
+    return s->opt.precond == SFC_PRECOND_TWO_LEVEL && s->has_bsr && s->bdinv32.p && coarse_prepare(s);
+}
+
+// FP64 PCG on S x = b (device vectors, length N): point Jacobi, or with
+// `two` the two-level preconditioner (nodal block Jacobi + coarse correction;
+// the caller has run coarse_prepare)
+PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_iter, int check, bool two)
 {
     sfc_ctx *ctx = s->ctx;
     const int64_t N = s->N;
@@ -885,7 +1077,19 @@ PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_i
     SFC_CK(cudaMemsetAsync(s->scal.p, 0, nsc * sizeof(double), ctx->stream));
     SFC_CK(cudaMemsetAsync(s->flags.p, 0, 2 * sizeof(int), ctx->stream));
     const unsigned g = grid_for(N, kRedThreads, ctx->sm_count * 4);
-    k_pcg_init<<<g, kRedThreads, 0, ctx->stream>>>(b, s->dinv.p, x, r, p, N, rz, bb);
+    const int64_t nodes = s->nodes;
+    const unsigned gn = grid_for(nodes, kRedThreads, ctx->sm_count * 4);
+    const CoarseSpace &cs = s->coarse;
+    if (two) {
+        k_pcg2_init<<<gn, kRedThreads, 0, ctx->stream>>>(b, s->bdinv32.p, x, r, nodes, rz, bb);
+        count_launch(ctx);
+        coarse_vec_apply(s, r, rz, nullptr);
+        k_pcg2_pupdate<true><<<gn, kRedThreads, 0, ctx->stream>>>(p, r, s->bdinv32.p, cs.node_agg.p, cs.mode.p,
+                                                                  cs.e64.p, nodes, nullptr, nullptr, nullptr, 0.0, 0,
+                                                                  done, err);
+    } else {
+        k_pcg_init<<<g, kRedThreads, 0, ctx->stream>>>(b, s->dinv.p, x, r, p, N, rz, bb);
+    }
     count_launch(ctx);
     double hbb = 0;
     download(ctx, &hbb, bb, 1);
@@ -895,17 +1099,34 @@ PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_i
     PcgResult res{max_iter, false};
     for (it = 0; it < max_iter; ++it) {
         launch_spmv64(s, p, q, pq + it, done);
-        {
-            ProfScope ps(ctx, "pcg_update", 56.0 * N);
-            k_pcg_update<<<g, kRedThreads, 0, ctx->stream>>>(x, r, p, q, s->dinv.p, N, pq + it, rz + it, rz + it + 1,
-                                                             rr + it + 1, done, err);
+        if (two) {
+            {
+                ProfScope ps(ctx, "pcg_update", 56.0 * N + 36.0 * nodes);
+                k_pcg2_update<<<gn, kRedThreads, 0, ctx->stream>>>(x, r, p, q, s->bdinv32.p, nodes, pq + it, rz + it,
+                                                                   rz + it + 1, rr + it + 1, done, err);
+            }
+            count_launch(ctx);
+            coarse_vec_apply(s, r, rz + it + 1, done);
+            {
+                ProfScope ps(ctx, "pcg_pupdate", 32.0 * N + 56.0 * nodes);
+                k_pcg2_pupdate<false><<<gn, kRedThreads, 0, ctx->stream>>>(
+                    p, r, s->bdinv32.p, cs.node_agg.p, cs.mode.p, cs.e64.p, nodes, rz + it, rz + it + 1, rr + it + 1,
+                    thr, it + 1, done, err);
+            }
+            count_launch(ctx);
+        } else {
+            {
+                ProfScope ps(ctx, "pcg_update", 56.0 * N);
+                k_pcg_update<<<g, kRedThreads, 0, ctx->stream>>>(x, r, p, q, s->dinv.p, N, pq + it, rz + it,
+                                                                 rz + it + 1, rr + it + 1, done, err);
+            }
+            {
+                ProfScope ps(ctx, "pcg_pupdate", 32.0 * N);
+                k_pcg_pupdate<<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, N, rz + it, rz + it + 1,
+                                                                  rr + it + 1, thr, it + 1, done, err);
+            }
+            count_launch(ctx, 2);
         }
-        {
-            ProfScope ps(ctx, "pcg_pupdate", 32.0 * N);
-            k_pcg_pupdate<<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, N, rz + it, rz + it + 1, rr + it + 1,
-                                                              thr, it + 1, done, err);
-        }
-        count_launch(ctx, 2);
         if ((it + 1) % check == 0 || it + 1 == max_iter) {
             int hf[2];
             download(ctx, hf, s->flags.p, 2);
@@ -972,7 +1193,9 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     const bool debug = std::getenv("SFC_DEBUG_SOLVER") != nullptr;
     const unsigned gw = (unsigned)(ctx->sm_count * 8);  // warp-per-row kernels: 8 warps/block
     const bool bsr = s->has_bsr;
-    const bool bj = bsr && o.precond == SFC_PRECOND_BLOCK_JACOBI && s->bdinv32.p;
+    const bool two = use_two_level(s);
+    const bool bj = bsr && (o.precond == SFC_PRECOND_BLOCK_JACOBI || two) && s->bdinv32.p;
+    const CoarseSpace &crs = s->coarse;
     // R = B - S X (FP64) and Q = S P (FP32), node-block kernels for 3-dof meshes
     auto resid = [&](const double *X, const double *Bm, double *R, double *out) {
         ProfScope ps(ctx, "resid64",
@@ -998,7 +1221,16 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     DBuf<int> &restart = s->restart;
     // r32 = scaled r64, x32 = 0, p = z for restarted columns; rz, rr into the slots
     auto init32 = [&](double *rz_slot, double *rr_slot) {
-        if (bj)
+        if (two) {
+            // p = z needs the coarse correction of the new residual first
+            k_ninit32<V, false><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->bdinv32.p, restart.p, rr32, xr, pp,
+                                                             s->nodes, rz_slot, rr_slot);
+            count_launch(ctx);
+            coarse_block_apply<V>(s, rr32, rz_slot, nullptr);
+            k_ncpupdate32<V, true><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, crs.node_agg.p, crs.mode.p,
+                                                                crs.e32.p, s->nodes, nullptr, nullptr, nullptr,
+                                                                nullptr, nullptr, nullptr, restart.p);
+        } else if (bj)
             k_ninit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->bdinv32.p, restart.p, rr32, xr, pp, s->nodes,
                                                       rz_slot, rr_slot);
         else
@@ -1067,9 +1299,14 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                     k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
                                                                 rrs + o0, thr, rz + o1, rrs + o1, stop, err);
             }
+            if (two) coarse_block_apply<V>(s, rr32, rz + o1, stop);
             {
-                ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + (bj ? 12.0 : 4.0) * N);
-                if (bj)
+                ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
+                if (two)
+                    k_ncpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, crs.node_agg.p,
+                                                                         crs.mode.p, crs.e32.p, s->nodes, rz + o0,
+                                                                         rz + o1, rrs + o1, thr, stop, err, nullptr);
+                else if (bj)
                     k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz + o0, rz + o1,
                                                                  rrs + o1, thr, stop, err);
                 else
@@ -1184,7 +1421,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             count_launch(ctx);
             const double bn = std::sqrt(hb[c]), r = std::sqrt(rn[c]);
             if (r > tol * bn) {
-                PcgResult pr = pcg64(s, s->tmpN.p, s->tmpN2.p, tol * bn / r, max_iter, check);
+                PcgResult pr = pcg64(s, s->tmpN.p, s->tmpN2.p, tol * bn / r, max_iter, check, two);
                 if (!pr.converged) all_conv = false;
                 if (debug)
                     std::fprintf(stderr, "[sfc block %d] column %d: FP64 fallback from rel %.3e, %d iterations%s\n", c0,
@@ -1219,6 +1456,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     st.max_rel_residual = worst;
     st.converged = all_conv ? 1 : 0;
     st.fallback_columns = n_fallback;
+    st.coarse_dofs = two ? (int32_t)(crs.nc - crs.dropped) : 0;
 }
 
 }  // namespace
@@ -1247,7 +1485,7 @@ void lifted_rhs(sfc_system *s, double *b)
 
 PcgStats pcg64_public(sfc_system *s, const double *b, double *x, double tol, int max_iter, int check)
 {
-    PcgResult r = pcg64(s, b, x, tol, max_iter, check);
+    PcgResult r = pcg64(s, b, x, tol, max_iter, check, false);
     return {r.iters, r.converged};
 }
 
@@ -1290,9 +1528,11 @@ void solve_forward(sfc_system *s)
     SFC_CK(cudaEventCreate(&e1));
     SFC_CK(cudaEventRecord(e0, ctx->stream));
     PcgResult r;
+    bool two = false;
     {
         ProfScope ps(ctx, "phase:forward_solve", 0.0);
-        r = pcg64(s, b.p, s->X.p, tol, max_iter, check);
+        two = use_two_level(s);
+        r = pcg64(s, b.p, s->X.p, tol, max_iter, check, two);
     }
     SFC_CK(cudaEventRecord(e1, ctx->stream));
     const double rel = true_rel_residual(s, b.p, s->X.p);
@@ -1307,6 +1547,7 @@ void solve_forward(sfc_system *s)
     s->stats.converged = r.converged ? 1 : 0;
     s->stats.max_rel_residual = rel;
     s->stats.device_ms = ms;
+    s->stats.coarse_dofs = two ? (int32_t)(s->coarse.nc - s->coarse.dropped) : 0;
     if (!r.converged) fail(SFC_ERR_NOT_CONVERGED, "PCG did not converge within max_iter");
 }
 
@@ -1339,11 +1580,13 @@ void solve_block(sfc_system *s, const double *B, double *X, int nrhs, int ld)
         s->tmpN.reserve(N);
         s->blk64.reserve(N);
         DBuf<double> &b = s->tmpN, &x = s->blk64;
+        const bool two = use_two_level(s);
         st.converged = 1;
+        st.coarse_dofs = two ? (int32_t)(s->coarse.nc - s->coarse.dropped) : 0;
         for (int a = 0; a < nrhs; ++a) {
             k_gather_cols<<<grid_for(N, 256), 256, 0, ctx->stream>>>(B, ld, a, 1, 1, N, b.p);
             count_launch(ctx);
-            PcgResult r = pcg64(s, b.p, x.p, tol, max_iter, check);
+            PcgResult r = pcg64(s, b.p, x.p, tol, max_iter, check, two);
             st.iterations = std::max(st.iterations, r.iters);
             if (!r.converged) st.converged = 0;
             k_scatter_cols<<<grid_for(N, 256), 256, 0, ctx->stream>>>(x.p, ld, a, 1, 1, N, X);

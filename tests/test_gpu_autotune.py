@@ -32,7 +32,9 @@ def test_block_solver_choice(ctx):
     s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10)
     best = s.autotune_block_solver(R, remeasure=True)
     assert best["block_width"] in (32, 64, 128)
-    assert best["precond"] in (api.SFC_PRECOND_JACOBI, api.SFC_PRECOND_BLOCK_JACOBI)
+    assert best["precond"] in (api.SFC_PRECOND_JACOBI, api.SFC_PRECOND_BLOCK_JACOBI, api.SFC_PRECOND_TWO_LEVEL)
+    if best["precond"] == api.SFC_PRECOND_TWO_LEVEL:
+        assert best["coarse_size"] in (6, 8, 12)
     assert best["method"] == api.SFC_SOLVER_PCG_MIXED and best["tol"] == 1e-10
     U = s.solveSystemTranspose(R)
     U_ref = np.stack([ds.solve_transpose(r) for r in R])

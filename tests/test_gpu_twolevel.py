@@ -1,0 +1,189 @@
+"""Two-level preconditioner (nodal block Jacobi + rigid-body-mode coarse
+correction on box aggregates): the solutions are those of the oracle's direct
+solve of the reference's row-zeroed system, only the iteration counts change."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from statfem_b200 import api
+from statfem_b200 import meshgen as mg
+from tests.problems import QPS, coefficients, small_mesh, statfem_problem
+
+pytestmark = pytest.mark.gpu
+
+EL = mg.HEX8_ELASTIC
+
+
+def elastic_system(ctx, n, seed, amount=0.0, bc=None, bc_vals=None, coeff=None):
+    rng = np.random.default_rng(seed)
+    mesh = small_mesh(EL, n, rng, amount)
+    if coeff is None:
+        coeff = coefficients(mesh, rng, EL)
+    gm = api.Mesh(ctx, EL, QPS[EL], mesh.coords, mesh.conn)
+    gm.set_coefficients(coeff)
+    s = api.SystemSolveCuda(ctx, mesh.num_dofs)
+    s.assemble(gm)
+    f = np.array([0.3, -0.5, 1.0])
+    s.assemble_load(gm, f)
+    if bc is None:
+        bc = mg.dirichlet_dofs(mesh, "x0")
+    vals = np.zeros(len(bc)) if bc_vals is None else bc_vals
+    s.applyConstraints((bc, vals))
+    rp, col, val, F = O.fem(mesh, QPS[EL], f, bc, coeff=coeff, bc_values=vals)
+    return mesh, gm, s, O.DirectSolver(rp, col, val), F, f
+
+
+@pytest.mark.parametrize("amount", [0.0, 0.3])
+def test_forward_fp64_two_level(ctx, amount):
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 12, 3, amount)
+    u_ref = ds.solve(F)
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-12, precond=api.SFC_PRECOND_JACOBI)
+    s.solveSystem()
+    it_jacobi = s.last_stats()["iterations"]
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-12, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=4)
+    s.solveSystem()
+    st = s.last_stats()
+    u = s.giveSolution()
+    assert st["converged"] == 1 and st["max_rel_residual"] < 1e-11
+    assert st["coarse_dofs"] > 0 and st["coarse_dofs"] % 6 == 0
+    assert np.abs(u - u_ref).max() <= 1e-9 * np.abs(u_ref).max()
+    assert st["iterations"] < 0.6 * it_jacobi, (st["iterations"], it_jacobi)
+
+
+@pytest.mark.parametrize("bw", [32, 128])
+def test_transpose_mixed_two_level(ctx, bw):
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 12, 5)
+    rng = np.random.default_rng(4)
+    Rhs = rng.standard_normal((45, mesh.num_dofs))
+    refs = np.stack([ds.solve_transpose(r) for r in Rhs])
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, block_width=bw, precond=api.SFC_PRECOND_BLOCK_JACOBI)
+    s.solveSystemTranspose(Rhs)
+    it_bj = s.last_stats()["iterations"]
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, block_width=bw, precond=api.SFC_PRECOND_TWO_LEVEL,
+                  coarse_size=4)
+    U = s.solveSystemTranspose(Rhs)
+    st = s.last_stats()
+    assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
+    assert st["coarse_dofs"] > 0
+    assert np.abs(U - refs).max() <= 1e-7 * np.abs(refs).max()
+    assert st["iterations"] < it_bj, (st["iterations"], it_bj)
+
+
+def test_multi_rhs_inhomogeneous_two_level(ctx):
+    rng = np.random.default_rng(8)
+    mesh = small_mesh(EL, 10)
+    bc = mg.dirichlet_dofs(mesh, "x0")
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 10, 8, 0.2, bc=bc, bc_vals=rng.standard_normal(len(bc)))
+    R = rng.standard_normal((40, mesh.num_dofs))
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-11, inner_tol=1e-3, precond=api.SFC_PRECOND_TWO_LEVEL,
+                  coarse_size=3)
+    U = s.solveSystemMulti(R)
+    U_ref = np.stack([ds.solve(r) for r in R])
+    assert np.abs(U - U_ref).max() <= 1e-8 * np.abs(U_ref).max()
+    s.solveSystem()
+    u_ref = ds.solve(F)
+    assert np.abs(s.giveSolution() - u_ref).max() <= 1e-7 * np.abs(u_ref).max()
+
+
+def test_fully_constrained_aggregates_are_dropped(ctx):
+    """A slab of fully constrained nodes leaves aggregates whose modes vanish:
+    their coarse dofs are dropped from the inverse and the solve is unchanged."""
+    mesh = small_mesh(EL, 12)
+    s0 = elastic_system(ctx, 12, 11)[2]
+    s0.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-11, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=4)
+    s0.solveSystem()
+    full = s0.last_stats()["coarse_dofs"]
+    slab = np.nonzero(mesh.coords[:, 0] < 0.34)[0]
+    bc = np.sort(np.concatenate([3 * slab, 3 * slab + 1, 3 * slab + 2]))
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 12, 11, bc=bc)
+    for method in (api.SFC_SOLVER_PCG_FP64, api.SFC_SOLVER_PCG_MIXED):
+        s.set_options(method=method, tol=1e-11, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=4)
+        s.solveSystem()
+        st = s.last_stats()
+        assert 0 < st["coarse_dofs"] < full
+        u_ref = ds.solve(F)
+        assert np.abs(s.giveSolution() - u_ref).max() <= 1e-8 * np.abs(u_ref).max()
+
+
+@pytest.mark.parametrize("size", [2, 5, 100])
+def test_coarse_sizes(ctx, size):
+    """From many small aggregates to a single one (six global modes)."""
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 8, 12)
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-12, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=size)
+    s.solveSystem()
+    st = s.last_stats()
+    u_ref = ds.solve(F)
+    assert st["converged"] == 1 and np.abs(s.giveSolution() - u_ref).max() <= 1e-9 * np.abs(u_ref).max()
+    if size == 100:
+        assert st["coarse_dofs"] == 6
+
+
+def test_rebuilt_after_coefficient_change(ctx):
+    """The coarse inverse follows the operator: new coefficients, new answer."""
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 10, 13)
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=4)
+    s.solveSystem()
+    rng = np.random.default_rng(14)
+    coeff2 = np.exp(0.8 * rng.standard_normal(mesh.num_elems))
+    gm.set_coefficients(coeff2)
+    s.assemble(gm)
+    s.clearRhs()
+    s.assemble_load(gm, f)
+    bc = mg.dirichlet_dofs(mesh, "x0")
+    s.applyConstraints((bc, np.zeros(len(bc))))
+    s.solveSystem()
+    rp, col, val, F2 = O.fem(mesh, QPS[EL], f, bc, coeff=coeff2)
+    u_ref = O.DirectSolver(rp, col, val).solve(F2)
+    assert np.abs(s.giveSolution() - u_ref).max() <= 1e-8 * np.abs(u_ref).max()
+
+
+def test_scalar_mesh_falls_back(ctx):
+    """Poisson (one dof per node) has no rigid-body coarse space: the solver
+    runs with its one-level preconditioner and reports no coarse dofs."""
+    rng = np.random.default_rng(2)
+    mesh = small_mesh(mg.HEX8_POISSON, 6)
+    coeff = coefficients(mesh, rng, mg.HEX8_POISSON)
+    gm = api.Mesh(ctx, mg.HEX8_POISSON, 8, mesh.coords, mesh.conn)
+    gm.set_coefficients(coeff)
+    s = api.SystemSolveCuda(ctx, mesh.num_dofs)
+    s.assemble(gm)
+    s.assemble_load(gm, np.array([1.0]))
+    bc = mg.dirichlet_dofs(mesh, "all")
+    s.applyConstraints((bc, np.zeros(len(bc))))
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, precond=api.SFC_PRECOND_TWO_LEVEL)
+    s.solveSystem()
+    st = s.last_stats()
+    rp, col, val, F = O.fem(mesh, 8, np.array([1.0]), bc, coeff=coeff)
+    u_ref = O.DirectSolver(rp, col, val).solve(F)
+    assert st["coarse_dofs"] == 0
+    assert np.abs(s.giveSolution() - u_ref).max() <= 1e-8 * np.abs(u_ref).max()
+
+
+def test_statfem_posterior_two_level(ctx):
+    """ForwardGaussRHS / LikelihoodKOH on elasticity: the sensor-space prior and
+    posterior do not depend on the preconditioner."""
+    pb = statfem_problem(EL, 8, 24, seed=21, faces="x0")
+    mesh = pb["mesh"]
+    hp = {"forcing.sigma": 0.05, "forcing.length": 0.3, "rho": 1.0, "mismatch.sigma": 0.01,
+          "mismatch.length": 0.25, "mismatch.sensorEps": 1e-4}
+    out = []
+    for precond in (api.SFC_PRECOND_BLOCK_JACOBI, api.SFC_PRECOND_TWO_LEVEL):
+        gm = api.Mesh(ctx, EL, 8, mesh.coords, mesh.conn)
+        gm.set_coefficients(pb["coeff"])
+        s = api.SystemSolveCuda(ctx, mesh.num_dofs)
+        s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, precond=precond, coarse_size=3)
+        s.assemble(gm)
+        s.assemble_load(gm, np.array([0.0, 0.0, -1.0]))
+        s.applyConstraints((pb["bc"], np.zeros(len(pb["bc"]))))
+        s.solveSystem()
+        cf = api.CovarianceForcing(ctx, gm)
+        cf.applyConstraints(pb["bc"])
+        fg = api.ForwardGaussRHS(s, cf, 1e-3)
+        fg.setProjectionMatrix(pb["P"])
+        fg.updateSolution(hp)
+        if precond == api.SFC_PRECOND_TWO_LEVEL:
+            assert s.last_stats()["coarse_dofs"] > 0
+        out.append((fg.giveProjectedMeanU(), fg.giveProjectedCovarU()))
+    (m0, c0), (m1, c1) = out
+    assert np.abs(m1 - m0).max() <= 1e-8 * np.abs(m0).max()
+    assert np.abs(c1 - c0).max() <= 1e-7 * np.abs(c0).max()
