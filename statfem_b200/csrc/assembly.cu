@@ -1068,9 +1068,9 @@ static void build_bsr(sfc_system *s)
     int h = 0;
     download(ctx, &h, err.p, 1);
     s->has_bsr = (h == 0);
-    s->bdinv32.release();
+    if (!s->has_bsr) s->bdinv32.release();
     if (s->has_bsr) {
-        s->bdinv32.alloc(nodes * 9);
+        s->bdinv32.alloc(nodes * 9);  // kept across rebuilds: a free + malloc here synchronises the device
         k_bsr_dinv<<<grid_for(nodes, 128), 128, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval64.p, nodes,
                                                                   s->bdinv32.p, err.p);
         count_launch(ctx);

@@ -16,9 +16,11 @@
 // the smooth, nearly rigid error components that it cannot reach.
 //
 // Layout and cost per iteration (K right-hand sides, nc = 6 x aggregates):
-//  * k_coarse_restrict32: c = P^T r, one CTA per aggregate, reads r once;
-//  * k_coarse_apply32:    e = A_c^+ c (FP32, dense nc x nc, L2-resident) and
-//                         the coarse share c.e of each column's r.z;
+//  * k_coarse_restrict32: c = P^T r, a cluster of CTAs per aggregate (a
+//    version fused into the x/r update ran slower: its register count halved
+//    the resident warps);
+//  * k_coarse_apply32: e = A_c^+ c (FP32, dense nc x nc, L2-resident) and the
+//    coarse share c.e of each column's r.z, split over k across a cluster;
 //  * the p update (solvers.cu) adds z += P e on the fly from each node's
 //    aggregate id and centroid offset.
 // Setup per operator: the Galerkin product on the GPU (one CTA per
@@ -30,14 +32,17 @@
 #include <cstdio>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace sfc {
 
 namespace {
 
+namespace cg = cooperative_groups;
+
 constexpr int kSlots = 27;   // 3 x 3 x 3 colour classes of the box grid
-constexpr int kGJ = 32;      // panel width of the Gauss-Jordan inverse
 constexpr int kMaxAggs = 512;
 
 // R(d): column k is e_k x d (the displacement of rotation mode k at offset d)
@@ -138,137 +143,37 @@ __global__ void __launch_bounds__(256) k_coarse_galerkin(const int32_t *__restri
     }
 }
 
-__global__ void k_diag_of(const double *__restrict__ A, int64_t n, double *__restrict__ d)
-{
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        d[i] = A[i * n + i];
-}
-
-// Gauss-Jordan step, part 1: invert the kb x kb diagonal block D of panel k0
-// (in shared memory, every CTA redundantly; a pivot that is not above
-// 1e-10 x the dof's original diagonal is dropped: its row and column are
-// zeroed), save the old column panel colp[i][m] = A[i][k0+m] and form the new
-// row panel rowp[m][j] = (D^-1 A[k0.., j])[m] (= D^-1 itself inside the block).
-__global__ void __launch_bounds__(256) k_gj_panel(const double *__restrict__ A, int64_t n, int64_t k0, int kb,
-                                                  const double *__restrict__ adiag, double *__restrict__ rowp,
-                                                  double *__restrict__ colp, int *dropped)
-{
-    __shared__ double D[kGJ][kGJ + 1];
-    __shared__ double rowv[kGJ], colv[kGJ];
-    __shared__ int drop;
-    for (int t = threadIdx.x; t < kGJ * kGJ; t += blockDim.x) {
-        const int r = t / kGJ, c = t % kGJ;
-        D[r][c] = (r < kb && c < kb) ? A[(k0 + r) * n + k0 + c] : 0.0;
-    }
-    __syncthreads();
-    for (int p = 0; p < kb; ++p) {
-        if (threadIdx.x == 0) {
-            const double piv = D[p][p];
-            drop = !(piv > 1e-10 * adiag[k0 + p]);
-        }
-        if (threadIdx.x < kGJ) {
-            rowv[threadIdx.x] = D[p][threadIdx.x];
-            colv[threadIdx.x] = D[threadIdx.x][p];
-        }
-        __syncthreads();
-        const double piv = rowv[p];
-        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-            const int r = t / kb, c = t % kb;
-            double v;
-            if (drop)
-                v = (r == p || c == p) ? 0.0 : D[r][c];
-            else if (r == p && c == p)
-                v = 1.0 / piv;
-            else if (r == p)
-                v = rowv[c] / piv;
-            else if (c == p)
-                v = -colv[r] / piv;
-            else
-                v = D[r][c] - colv[r] * rowv[c] / piv;
-            D[r][c] = v;
-        }
-        if (drop && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(dropped, 1);
-        __syncthreads();
-    }
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
-        for (int m = 0; m < kb; ++m) colp[j * kGJ + m] = A[j * n + k0 + m];
-        if (j >= k0 && j < k0 + kb) {
-            for (int m = 0; m < kb; ++m) rowp[m * n + j] = D[m][j - k0];
-        } else {
-            double aj[kGJ];
-#pragma unroll
-            for (int l = 0; l < kGJ; ++l) aj[l] = l < kb ? A[(k0 + l) * n + j] : 0.0;
-            for (int m = 0; m < kb; ++m) {
-                double s = 0.0;
-#pragma unroll
-                for (int l = 0; l < kGJ; ++l) s += D[m][l] * aj[l];
-                rowp[m * n + j] = s;
-            }
-        }
-    }
-}
-
-// Gauss-Jordan step, part 2 (64 x 64 tile per CTA):
-//   rows of the panel:     A[i][j] = rowp[i-k0][j]
-//   columns of the panel:  A[i][j] = -colp[i] . rowp[:, j]   (= -A[i,k] D^-1)
-//   elsewhere:             A[i][j] -= colp[i] . rowp[:, j]
-__global__ void __launch_bounds__(256) k_gj_update(double *__restrict__ A, int64_t n, int64_t k0, int kb,
-                                                   const double *__restrict__ rowp, const double *__restrict__ colp)
-{
-    __shared__ double cp[64][kGJ + 1];
-    __shared__ double rp[kGJ][64 + 1];
-    const int64_t i0 = (int64_t)blockIdx.y * 64, j0 = (int64_t)blockIdx.x * 64;
-    for (int t = threadIdx.x; t < 64 * kGJ; t += blockDim.x) {
-        const int r = t / kGJ, m = t % kGJ;
-        cp[r][m] = (i0 + r < n && m < kb) ? colp[(i0 + r) * kGJ + m] : 0.0;
-        const int mm = t / 64, c = t % 64;
-        rp[mm][c] = (j0 + c < n && mm < kb) ? rowp[mm * n + j0 + c] : 0.0;
-    }
-    __syncthreads();
-    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
-    for (int u = 0; u < 4; ++u) {
-        const int64_t i = i0 + ty + 16 * u;
-        if (i >= n) continue;
-        for (int v = 0; v < 4; ++v) {
-            const int64_t j = j0 + tx + 16 * v;
-            if (j >= n) continue;
-            if (i >= k0 && i < k0 + kb) {
-                A[i * n + j] = rp[i - k0][tx + 16 * v];
-                continue;
-            }
-            double s = 0.0;
-#pragma unroll
-            for (int m = 0; m < kGJ; ++m) s += cp[ty + 16 * u][m] * rp[m][tx + 16 * v];
-            A[i * n + j] = (j >= k0 && j < k0 + kb) ? -s : A[i * n + j] - s;
-        }
-    }
-}
-
 __global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         b[i] = (float)a[i];
 }
 
-// c[6a + m][col] = (P^T r)[6a + m][col] for K = 32 V interleaved columns
+// c[6a + m][col] = (P^T r)[6a + m][col] for K = 32 V interleaved columns: a
+// cluster of kRestrictSplit CTAs per aggregate (warp per node), partial sums
+// added in rank order through distributed shared memory
+constexpr int kRestrictSplit = 4;
+
 template <int V>
-__global__ void __launch_bounds__(256) k_coarse_restrict32(const float *__restrict__ r,
-                                                           const int32_t *__restrict__ agg_ptr,
-                                                           const int32_t *__restrict__ agg_nodes,
-                                                           const float4 *__restrict__ mode, float *__restrict__ c,
-                                                           const int *stop)
+__global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
+    k_coarse_restrict32(const float *__restrict__ r, const int32_t *__restrict__ agg_ptr,
+                        const int32_t *__restrict__ agg_nodes, const float4 *__restrict__ mode, float *__restrict__ c,
+                        const int *stop)
 {
     constexpr int K = 32 * V;
     __shared__ float red[8][6][K];
-    if (stop && *stop) return;
-    const int a = blockIdx.x;
+    if (stop && *stop) return;  // uniform: stop changes only between launches
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    const int a = blockIdx.x / kRestrictSplit;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     float acc[6][V];
 #pragma unroll
     for (int m = 0; m < 6; ++m)
 #pragma unroll
         for (int v = 0; v < V; ++v) acc[m][v] = 0.f;
-    for (int32_t t = agg_ptr[a] + w; t < agg_ptr[a + 1]; t += 8) {
+#pragma unroll 2
+    for (int32_t t = agg_ptr[a] + (int32_t)rank * 8 + w; t < agg_ptr[a + 1]; t += 8 * kRestrictSplit) {
         const int32_t i = agg_nodes[t];
         const float4 m = mode[i];
         const int bits = (int)m.w;
@@ -306,47 +211,87 @@ __global__ void __launch_bounds__(256) k_coarse_restrict32(const float *__restri
     __syncthreads();
     for (int t = threadIdx.x; t < 6 * K; t += blockDim.x) {
         const int m = t / K, col = t % K;
-        float s = 0.f;
+        float sum = 0.f;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) s += red[q][m][col];
-        c[(int64_t)(6 * a + m) * K + col] = s;
+        for (int q = 0; q < 8; ++q) sum += red[q][m][col];
+        red[0][m][col] = sum;  // entry (m, col) is read and written by this thread only
     }
+    cl.sync();
+    for (int t = (int)rank * blockDim.x + threadIdx.x; t < 6 * K; t += kRestrictSplit * blockDim.x) {
+        float sum = 0.f;
+        for (unsigned j = 0; j < kRestrictSplit; ++j) sum += cl.map_shared_rank(&red[0][0][0], j)[t];
+        c[(6 * (int64_t)a + t / K) * K + t % K] = sum;
+    }
+    cl.sync();  // the other CTAs' shared memory stays alive until every read is done
 }
 
-// e = A c (A: nc x nc FP32, c and e: [nc][K]); rz[col] += sum_rows c e
+// e = A c (A: nc x nc FP32, c and e: [nc][K]); rz[col] += sum_rows c e.
+// Split over k: a cluster of kSplitK CTAs shares one block of ROWS output
+// rows, each CTA takes a quarter of the k range (register-prefetched 32-wide
+// chunks of A's rows and of c), and the partial tiles are added in rank
+// order through distributed shared memory, each CTA finishing ROWS/kSplitK
+// of the rows.
+constexpr int kSplitK = 4;
+
 template <int V>
-__global__ void __launch_bounds__(256) k_coarse_apply32(const float *__restrict__ A, const float *__restrict__ c,
-                                                        float *__restrict__ e, int64_t nc, double *rz,
-                                                        const int *stop)
+__global__ void __cluster_dims__(1, kSplitK, 1) __launch_bounds__(256)
+    k_coarse_apply32(const float *__restrict__ A, const float *__restrict__ c, float *__restrict__ e, int64_t nc,
+                     double *rz, const int *stop)
 {
     constexpr int K = 32 * V;
     constexpr int CG = K / 4;         // float4 column groups
     constexpr int RS = 256 / CG;      // row sets
     constexpr int R = 2;              // rows per thread
-    constexpr int ROWS = RS * R;
+    constexpr int ROWS = RS * R;      // 16, 32, 64 for V = 4, 2, 1
+    constexpr int NA = ROWS * 32 / 256;  // A values per thread and chunk
+    constexpr int NC = 32 * CG / 256;    // c float4 per thread and chunk
     __shared__ float sa[ROWS][33];
-    __shared__ float4 sc[32][CG];
+    __shared__ __align__(16) float4 sc[32][CG];
+    __shared__ __align__(16) float part[ROWS][K];
     __shared__ double sred[RS][K];
     if (stop && *stop) return;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
     const int g = threadIdx.x % CG, rs = threadIdx.x / CG;
     const int64_t row0 = (int64_t)blockIdx.x * ROWS;
+    const int64_t nchunks = (nc + 31) / 32, per = (nchunks + kSplitK - 1) / kSplitK;
+    const int64_t kc0 = (int64_t)rank * per, kc1 = kc0 + per < nchunks ? kc0 + per : nchunks;
     float acc[R][4];
 #pragma unroll
     for (int u = 0; u < R; ++u)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[u][q] = 0.f;
-    for (int64_t k0 = 0; k0 < nc; k0 += 32) {
-        for (int t = threadIdx.x; t < ROWS * 32; t += 256) {
-            const int rr = t / 32, kk = t % 32;
+    float pa[NA];
+    float4 pc[NC];
+    auto fetch = [&](int64_t kc) {
+        const int64_t k0 = kc * 32;
+#pragma unroll
+        for (int j = 0; j < NA; ++j) {
+            const int t = threadIdx.x + 256 * j, rr = t / 32, kk = t % 32;
             const int64_t row = row0 + rr, k = k0 + kk;
-            sa[rr][kk] = (row < nc && k < nc) ? A[row * nc + k] : 0.f;
+            pa[j] = (row < nc && k < nc) ? A[row * nc + k] : 0.f;
         }
-        for (int t = threadIdx.x; t < 32 * CG; t += 256) {
-            const int kk = t / CG, gg = t % CG;
-            sc[kk][gg] = (k0 + kk < nc) ? *reinterpret_cast<const float4 *>(c + (k0 + kk) * K + 4 * gg)
-                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < NC; ++j) {
+            const int t = threadIdx.x + 256 * j, kk = t / CG, gg = t % CG;
+            pc[j] = (k0 + kk < nc) ? *reinterpret_cast<const float4 *>(c + (k0 + kk) * K + 4 * gg)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    if (kc0 < kc1) fetch(kc0);
+    for (int64_t kc = kc0; kc < kc1; ++kc) {
+#pragma unroll
+        for (int j = 0; j < NA; ++j) {
+            const int t = threadIdx.x + 256 * j;
+            sa[t / 32][t % 32] = pa[j];
+        }
+#pragma unroll
+        for (int j = 0; j < NC; ++j) {
+            const int t = threadIdx.x + 256 * j;
+            sc[t / CG][t % CG] = pc[j];
         }
         __syncthreads();
+        if (kc + 1 < kc1) fetch(kc + 1);  // in flight during the products below
 #pragma unroll 8
         for (int kk = 0; kk < 32; ++kk) {
             const float4 cv = sc[kk][g];
@@ -361,26 +306,40 @@ __global__ void __launch_bounds__(256) k_coarse_apply32(const float *__restrict_
         }
         __syncthreads();
     }
-    double d[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-    for (int u = 0; u < R; ++u) {
-        const int64_t row = row0 + rs * R + u;
-        if (row >= nc) continue;
-        *reinterpret_cast<float4 *>(e + row * K + 4 * g) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
-        const float4 cv = *reinterpret_cast<const float4 *>(c + row * K + 4 * g);
-        d[0] += (double)cv.x * acc[u][0];
-        d[1] += (double)cv.y * acc[u][1];
-        d[2] += (double)cv.z * acc[u][2];
-        d[3] += (double)cv.w * acc[u][3];
+    for (int u = 0; u < R; ++u)
+        *reinterpret_cast<float4 *>(&part[rs * R + u][4 * g]) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+    cl.sync();
+    // this CTA finishes rows [rank ROWS/kSplitK, (rank + 1) ROWS/kSplitK) of the block
+    constexpr int MY = ROWS / kSplitK;
+    double d[(MY * K + 255) / 256];
+#pragma unroll
+    for (int j = 0; j < (MY * K + 255) / 256; ++j) {
+        d[j] = 0.0;
+        const int t = threadIdx.x + 256 * j;
+        if (t >= MY * K) continue;
+        const int lr = (int)rank * MY + t / K, col = t % K;
+        const int64_t row = row0 + lr;
+        float sum = 0.f;
+        for (unsigned q = 0; q < kSplitK; ++q) sum += cl.map_shared_rank(&part[0][0], q)[lr * K + col];
+        if (row < nc) {
+            e[row * K + col] = sum;
+            d[j] = (double)c[row * K + col] * sum;
+        }
     }
+    cl.sync();  // partial tiles stay alive until every CTA has read them
     if (!rz) return;
+    // column sums of c.e over this CTA's rows: threads t and t + 256 j share column t % K
 #pragma unroll
-    for (int q = 0; q < 4; ++q) sred[rs][4 * g + q] = d[q];
+    for (int j = 1; j < (MY * K + 255) / 256; ++j) d[0] += d[j];
+    // (MY K is a multiple of 256 for V = 1, 2, 4: every thread holds one column's partial)
+    double *sd = &sred[0][0];
+    sd[threadIdx.x] = d[0];
     __syncthreads();
     for (int col = threadIdx.x; col < K; col += 256) {
-        double s = 0.0;
-        for (int q = 0; q < RS; ++q) s += sred[q][col];
-        atomicAdd(rz + col, s);
+        double sum = 0.0;
+        for (int t = col; t < 256; t += K) sum += sd[t];
+        atomicAdd(rz + col, sum);
     }
 }
 
@@ -434,8 +393,18 @@ __global__ void __launch_bounds__(256) k_coarse_apply64(const double *__restrict
     const int64_t row = (int64_t)blockIdx.x * 8 + w;
     double part = 0.0;
     if (row < nc) {
-        double s = 0.0;
-        for (int64_t k = lane; k < nc; k += 32) s += A[row * nc + k] * c[k];
+        // four independent partial sums keep four loads of the row in flight
+        const double *Ar = A + row * nc;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int64_t k = lane;
+        for (; k + 96 < nc; k += 128) {
+            s0 += Ar[k] * c[k];
+            s1 += Ar[k + 32] * c[k + 32];
+            s2 += Ar[k + 64] * c[k + 64];
+            s3 += Ar[k + 96] * c[k + 96];
+        }
+        for (; k < nc; k += 32) s0 += Ar[k] * c[k];
+        double s = (s0 + s1) + (s2 + s3);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) {
@@ -628,25 +597,12 @@ bool coarse_prepare(sfc_system *s)
                                                                  cs.agg_slot.p, cs.nbr.p, cs.mode.p, s->bptr.p,
                                                                  s->bcol.p, s->bval64.p, nc, cs.a64.p);
     count_launch(ctx, 2);
-    cs.diag.alloc(nc);
-    cs.rowp.alloc(kGJ * nc);
-    cs.colp.alloc(kGJ * nc);
-    k_diag_of<<<grid_for(nc, 256), 256, 0, ctx->stream>>>(cs.a64.p, nc, cs.diag.p);
-    DevInt dropped = status_word(ctx, 2);
-    SFC_CK(cudaMemsetAsync(dropped.p, 0, sizeof(int), ctx->stream));
-    count_launch(ctx);
-    const unsigned gp = grid_for(nc, 256), gt = (unsigned)((nc + 63) / 64);
-    for (int64_t k0 = 0; k0 < nc; k0 += kGJ) {
-        const int kb = (int)std::min<int64_t>(kGJ, nc - k0);
-        k_gj_panel<<<gp, 256, 0, ctx->stream>>>(cs.a64.p, nc, k0, kb, cs.diag.p, cs.rowp.p, cs.colp.p, dropped.p);
-        k_gj_update<<<dim3(gt, gt), 256, 0, ctx->stream>>>(cs.a64.p, nc, k0, kb, cs.rowp.p, cs.colp.p);
-        count_launch(ctx, 2);
-    }
+    cs.gj.reserve(nc);
+    int dropped = 0;
+    spd_inverse_gj(ctx, cs.a64.p, nc, 1e-10, cs.gj, nullptr, &dropped);
     k_to_f32<<<grid_for(nc * nc, 256), 256, 0, ctx->stream>>>(cs.a64.p, cs.a32.p, nc * nc);
     count_launch(ctx);
-    int h = 0;
-    download(ctx, &h, dropped.p, 1);
-    cs.dropped = h;
+    cs.dropped = dropped;
     cs.op_serial = s->op_serial;
     return true;
 }
@@ -661,16 +617,17 @@ void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *st
     cs.e32.reserve(cs.nc * K);
     {
         ProfScope ps(ctx, "coarse_restrict32", 3.0 * s->nodes * K * 4 + 20.0 * s->nodes + 4.0 * cs.nc * K);
-        k_coarse_restrict32<V><<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p,
-                                                                           cs.c32.p, stop);
+        k_coarse_restrict32<V><<<(unsigned)(cs.nagg * kRestrictSplit), 256, 0, ctx->stream>>>(
+            r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p, cs.c32.p, stop);
+        count_launch(ctx);
     }
     {
         constexpr int ROWS = (256 / (K / 4)) * 2;
         ProfScope ps(ctx, "coarse_apply32", 4.0 * cs.nc * cs.nc + 8.0 * cs.nc * K);
-        k_coarse_apply32<V><<<(unsigned)((cs.nc + ROWS - 1) / ROWS), 256, 0, ctx->stream>>>(cs.a32.p, cs.c32.p,
-                                                                                             cs.e32.p, cs.nc, rz, stop);
+        const dim3 grid((unsigned)((cs.nc + ROWS - 1) / ROWS), kSplitK);
+        k_coarse_apply32<V><<<grid, 256, 0, ctx->stream>>>(cs.a32.p, cs.c32.p, cs.e32.p, cs.nc, rz, stop);
+        count_launch(ctx);
     }
-    count_launch(ctx, 2);
 }
 template void coarse_block_apply<1>(sfc_system *, const float *, double *, const int *);
 template void coarse_block_apply<2>(sfc_system *, const float *, double *, const int *);
@@ -682,10 +639,16 @@ void coarse_vec_apply(sfc_system *s, const double *r, double *rz, const int *don
     sfc_ctx *ctx = s->ctx;
     cs.c64.reserve(cs.nc);
     cs.e64.reserve(cs.nc);
-    k_coarse_restrict64<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p,
-                                                                    cs.c64.p, done);
-    k_coarse_apply64<<<(unsigned)((cs.nc + 7) / 8), 256, 0, ctx->stream>>>(cs.a64.p, cs.c64.p, cs.e64.p, cs.nc, rz,
-                                                                            done);
+    {
+        ProfScope ps(ctx, "coarse_restrict64", 3.0 * s->nodes * 8 + 20.0 * s->nodes + 8.0 * cs.nc);
+        k_coarse_restrict64<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p,
+                                                                        cs.c64.p, done);
+    }
+    {
+        ProfScope ps(ctx, "coarse_apply64", 8.0 * cs.nc * cs.nc + 16.0 * cs.nc);
+        k_coarse_apply64<<<(unsigned)((cs.nc + 7) / 8), 256, 0, ctx->stream>>>(cs.a64.p, cs.c64.p, cs.e64.p, cs.nc,
+                                                                                rz, done);
+    }
     count_launch(ctx, 2);
 }
 

@@ -205,6 +205,13 @@ void make_quadrature(int kind, int qps, QuadTable &t);
 // ---------------------------------------------------------------------------
 struct sfc_mesh;
 namespace sfc {
+// scratch of spd_inverse_gj (dense.cu)
+struct GjScratch {
+    DBuf<double> diag, rowp, colp;
+    DBuf<int> word;
+    void reserve(int64_t n);
+};
+
 struct CoarseSpace {
     bool built = false;                 // aggregates for (mesh, size)
     const sfc_mesh *mesh = nullptr;
@@ -221,7 +228,7 @@ struct CoarseSpace {
     DBuf<float4> mode;                  // offset + constrained components (bits in w)
     DBuf<double> a64;                   // nc x nc: Galerkin matrix, inverted in place
     DBuf<float> a32;                    // FP32 copy of the inverse
-    DBuf<double> diag, rowp, colp;      // Gauss-Jordan scratch
+    GjScratch gj;                       // inverse scratch
     DBuf<float> c32, e32;               // [nc][K] restriction and correction (block)
     DBuf<double> c64, e64;              // single FP64 vector
 };
@@ -366,6 +373,11 @@ struct sfc_koh {
     sfc::DBuf<double> work;
     sfc::DBuf<double> outv;           // posterior mean / covariance / log-likelihood
     sfc::DBuf<int> info;
+    sfc::GjScratch gj;                // sensor-space inverses
+    // batched log-likelihood scratch
+    sfc::DBuf<double> bwork, bres;
+    sfc::DBuf<int> binfo;
+    sfc::DBuf<sfc_hparams_t> bhp;
 };
 
 namespace sfc {
@@ -401,6 +413,12 @@ PcgStats pcg64_public(sfc_system *s, const double *b, double *x, double tol, int
 void solve_forward_fcg(sfc_system *s);
 // solvers.cu: FP64 SpMV with a given number of lanes per row (4, 8, 16, 32)
 void spmv_op64_lanes(sfc_system *s, int lanes, const double *x, double *y);
+// In-place inverse of the n x n symmetric positive (semi)definite device
+// matrix A by block Gauss-Jordan elimination (dense.cu).  A pivot not above
+// rel x its original diagonal is dropped (row and column zeroed);
+// *dropped = their number (rel = 0: the non-positive pivots, i.e. A is not
+// positive definite).  pivots (device, n, nullable): the Schur pivots.
+void spd_inverse_gj(sfc_ctx *ctx, double *A, int64_t n, double rel, GjScratch &w, double *pivots, int *dropped);
 // two-level preconditioner (coarse.cu)
 bool coarse_prepare(sfc_system *s);
 template <int V>

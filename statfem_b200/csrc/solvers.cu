@@ -8,9 +8,10 @@
 // A^T r = p  <=>  S r = p on the free dofs with r_c = (p_c - K_cf r_f)/scalar.
 //
 // Two methods:
-//  * plain FP64 Jacobi-PCG, one right-hand side at a time (the baseline and
-//    the judge): CSR SpMV with sub-warp row groups, fused p.q reduction,
-//    fused x/r/z update with the r.r and r.z reductions;
+//  * plain FP64 PCG, one right-hand side at a time (point Jacobi, the
+//    baseline method; or the two-level preconditioner of coarse.cu): CSR SpMV
+//    with sub-warp row groups, fused p.q reduction, fused x/r/z update with
+//    the r.r and r.z reductions;
 //  * mixed block PCG: up to 128 right-hand sides share each pass over the
 //    FP32 copy of the matrix (one warp per row, each lane owns 1-4 columns of
 //    an RHS-interleaved [N][K] block), iterations in FP32, and an outer FP64
@@ -28,11 +29,15 @@
 #include <cstdlib>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace sfc {
 
 namespace {
+
+namespace cg = cooperative_groups;
 
 constexpr int kRedThreads = 256;
 

@@ -143,6 +143,57 @@ __global__ void k_kron_axis(const double *__restrict__ Kd, int nd, int64_t sd, i
     }
 }
 
+// The same axis product as a batch of small dense products, for nd <= 64
+// points per line: one CTA per (line, 128 columns) stages the line's input
+// rows and the factor in shared memory; warp w computes the output points
+// m = w, w + 8, ... and lane l the columns l, l + 32, l + 64, l + 96, so each
+// staged value feeds up to 8 multiply-adds from registers.
+constexpr int kLineCols = 128;
+
+__global__ void __launch_bounds__(256) k_kron_line(const double *__restrict__ Kd, int nd, int64_t sd, int dof, int c,
+                                                   int64_t ns, const double *__restrict__ in, double *__restrict__ out)
+{
+    extern __shared__ double sm[];
+    double *sK = sm, *sIn = sm + nd * nd;
+    const int64_t L = blockIdx.x;  // line: nodes base + k sd, k < nd
+    const int64_t base = (L / sd) * sd * nd + L % sd;
+    const int64_t col0 = (int64_t)blockIdx.y * kLineCols;
+    const int ncols = (int)(ns - col0 < kLineCols ? ns - col0 : kLineCols);
+    for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) sK[t] = Kd[t];
+    for (int t = threadIdx.x; t < nd * kLineCols; t += blockDim.x) {
+        const int k = t / kLineCols, j = t % kLineCols;
+        sIn[t] = j < ncols ? in[((base + k * sd) * dof + c) * ns + col0 + j] : 0.0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double acc[8][4];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[u][q] = 0.0;
+    for (int k = 0; k < nd; ++k) {
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = sIn[k * kLineCols + lane + 32 * q];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int m = w + 8 * u;
+            const double kv = m < nd ? sK[m * nd + k] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[u][q] = fma(kv, v[q], acc[u][q]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const int m = w + 8 * u;
+        if (m >= nd) continue;
+        double *o = out + ((base + m * sd) * dof + c) * ns + col0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (lane + 32 * q < ncols) o[lane + 32 * q] = acc[u][q];
+    }
+}
+
 // C[a][b] += sum_i A[i][a] B[i][b] over a slice of rows (split-K, atomics);
 // 64 x 64 output tile per block, 4 x 4 per thread
 __global__ void __launch_bounds__(256) k_atb(const double *__restrict__ A, const double *__restrict__ B, int64_t K,
@@ -299,20 +350,6 @@ __device__ void trsm_lower_t(int n, const double *L, int ldl, int m, double *B, 
     }
 }
 
-// Ainv = A^-1 for SPD A (n x n); L is scratch n x n; info as chol_lower
-__device__ void spd_inverse(int n, const double *A, double *L, double *Ainv, int *info)
-{
-    for (int64_t t = threadIdx.x; t < (int64_t)n * n; t += blockDim.x) {
-        L[t] = A[t];
-        Ainv[t] = (t / n == t % n) ? 1.0 : 0.0;
-    }
-    __syncthreads();
-    chol_lower(n, L, n, info);
-    if (*info) return;
-    trsm_lower(n, L, n, n, Ainv, n);
-    trsm_lower_t(n, L, n, n, Ainv, n);
-}
-
 // MismatchCovariance::giveCovariance (statX/infer/MismatchCovariance.hpp:76-99)
 __device__ void mismatch_cov(int ns, const double *xs, int dim, double sd, double ld, double eps, double *K)
 {
@@ -330,14 +367,6 @@ __device__ void mismatch_cov(int ns, const double *xs, int dim, double sd, doubl
 __device__ void koh_loglik_dev(int ns, int n_o, const double *__restrict__ mean, const double *__restrict__ Cs,
                                const double *__restrict__ xs, int dim, const double *__restrict__ Y,
                                const sfc_hparams_t &hp, double *__restrict__ work, double *out, int *info);
-
-__global__ void __launch_bounds__(1024) k_koh_loglik(int ns, int n_o, const double *__restrict__ mean,
-                                                     const double *__restrict__ Cs, const double *__restrict__ xs,
-                                                     int dim, const double *__restrict__ Y, sfc_hparams_t hp,
-                                                     double *__restrict__ work, double *out, int *info)
-{
-    koh_loglik_dev(ns, n_o, mean, Cs, xs, dim, Y, hp, work, out, info);
-}
 
 // many hyperparameter sets against the same forward model, one CTA each
 __global__ void __launch_bounds__(1024) k_koh_loglik_batch(int ns, int n_o, const double *__restrict__ mean,
@@ -405,60 +434,6 @@ __device__ void koh_loglik_dev(int ns, int n_o, const double *__restrict__ mean,
     }
 }
 
-// LikelihoodKOH::giveProjFEconditionedData (LikelihoodKOH.ipp:311-361):
-// Sigma = (rho^2 n_o Ks^-1 + Cs^-1)^-1, m = Sigma (rho Ks^-1 sum_k y_k + Cs^-1 mean)
-// work: 5*ns*ns + 3*ns doubles
-__global__ void __launch_bounds__(1024) k_koh_proj(int ns, int n_o, const double *__restrict__ mean,
-                                                   const double *__restrict__ Cs, const double *__restrict__ xs, int dim,
-                                                   const double *__restrict__ Y, sfc_hparams_t hp,
-                                                   double *__restrict__ work, double *post_mean, double *post_cov,
-                                                   int *info)
-{
-    const int64_t nn = (int64_t)ns * ns;
-    double *Ks = work, *L = work + nn, *Ksi = work + 2 * nn, *Cui = work + 3 * nn, *Msum = work + 4 * nn;
-    double *ysum = work + 5 * nn, *v = ysum + ns;
-    mismatch_cov(ns, xs, dim, hp.mismatch_sigma, hp.mismatch_length, hp.mismatch_sensor_eps, Ks);
-    spd_inverse(ns, Ks, L, Ksi, info);
-    if (*info) return;
-    __syncthreads();
-    spd_inverse(ns, Cs, L, Cui, info);
-    if (*info) {
-        if (threadIdx.x == 0) *info += 100000;
-        return;
-    }
-    const double rho = hp.rho;
-    for (int64_t t = threadIdx.x; t < nn; t += blockDim.x) Msum[t] = rho * rho * n_o * Ksi[t] + Cui[t];
-    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-        double s = 0;
-        for (int r = 0; r < n_o; ++r) s += Y[(int64_t)k * n_o + r];
-        ysum[k] = s;
-    }
-    __syncthreads();
-    spd_inverse(ns, Msum, L, post_cov, info);
-    if (*info) {
-        if (threadIdx.x == 0) *info += 200000;
-        return;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-        double s = 0;
-        for (int j = 0; j < ns; ++j) s += rho * Ksi[(int64_t)k * ns + j] * ysum[j] + Cui[(int64_t)k * ns + j] * mean[j];
-        v[k] = s;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-        double s = 0;
-        for (int j = 0; j < ns; ++j) s += post_cov[(int64_t)k * ns + j] * v[j];
-        post_mean[k] = s;
-    }
-}
-
-// SPD inverse of one n x n matrix (used by the Woodbury form)
-__global__ void __launch_bounds__(1024) k_spd_inverse(int n, const double *A, double *L, double *Ainv, int *info)
-{
-    spd_inverse(n, A, L, Ainv, info);
-}
-
 __global__ void k_mismatch(int ns, const double *xs, int dim, sfc_hparams_t hp, double *K)
 {
     mismatch_cov(ns, xs, dim, hp.mismatch_sigma, hp.mismatch_length, hp.mismatch_sensor_eps, K);
@@ -468,6 +443,61 @@ __global__ void k_add_scaled(double *__restrict__ y, const double *__restrict__ 
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
         y[t] += a * x[t];
+}
+
+// C = K_s + rho^2 C_s (ns x ns) and D = Y - rho mean (ns x n_o)
+__global__ void k_koh_system(int ns, int n_o, const double *__restrict__ mean, const double *__restrict__ Cs,
+                             const double *__restrict__ xs, int dim, const double *__restrict__ Y, sfc_hparams_t hp,
+                             double *__restrict__ C, double *__restrict__ D)
+{
+    const int64_t nn = (int64_t)ns * ns;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn; t += (int64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t / ns), l = (int)(t % ns);
+        double v = se_value(xs + 3 * k, xs + 3 * l, dim, hp.mismatch_sigma, hp.mismatch_length);
+        if (k == l) v += hp.mismatch_sensor_eps * hp.mismatch_sensor_eps;
+        C[t] = v + hp.rho * hp.rho * Cs[t];
+        if (t < (int64_t)ns * n_o) D[t] = Y[t] - hp.rho * mean[t / n_o];
+    }
+}
+
+// log-likelihood from C^-1, the Schur pivots of C (log det C = sum log piv)
+// and D: n_o (-ns/2 log 2 pi - 1/2 log det C) - 1/2 sum_r d_r^T C^-1 d_r;
+// info = -1 when a quadratic term is not negative (LikelihoodKOH.ipp:100-120)
+__global__ void __launch_bounds__(1024) k_koh_loglik_terms(int ns, int n_o, const double *__restrict__ Ci,
+                                                           const double *__restrict__ D, const double *__restrict__ piv,
+                                                           double *out, int *info)
+{
+    __shared__ double red[1024];
+    auto block_total = [&](double v) {
+        red[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        const double r = red[0];
+        __syncthreads();
+        return r;
+    };
+    double ld = 0.0;
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) ld += log(piv[k]);
+    const double logdet = block_total(ld);
+    double t3 = 0.0;
+    bool ok = true;
+    for (int r = 0; r < n_o; ++r) {
+        double q = 0.0;
+        for (int64_t t = threadIdx.x; t < (int64_t)ns * ns; t += blockDim.x) {
+            const int i = (int)(t / ns), j = (int)(t % ns);
+            q += D[(int64_t)i * n_o + r] * Ci[t] * D[(int64_t)j * n_o + r];
+        }
+        const double comp = -0.5 * block_total(q);
+        if (!(comp < 0.0)) ok = false;
+        t3 += comp;
+    }
+    if (threadIdx.x == 0) {
+        *out = n_o * (-0.5 * ns * log(2. * M_PI) - 0.5 * logdet) + t3;
+        if (!ok) *info = -1;
+    }
 }
 
 __global__ void k_lincomb(double *__restrict__ y, double a, const double *__restrict__ x, double b, int64_t n)
@@ -542,7 +572,12 @@ void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double leng
                 double *dst = bufs[cur];
                 ProfScope ps(ctx, "kron_axis", 2.0 * nodes * ns * 8);
                 const size_t kb = (size_t)nd * nd * 8;
-                if (kb <= 48 * 1024) {
+                if (nd <= 64) {
+                    const size_t smem = (size_t)(nd * nd + nd * kLineCols) * 8;
+                    SFC_CK(cudaFuncSetAttribute(k_kron_line, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    const dim3 g((unsigned)(nodes / nd), (unsigned)((ns + kLineCols - 1) / kLineCols));
+                    k_kron_line<<<g, 256, smem, ctx->stream>>>(dK[a].p, nd, sd, dof, c, ns, src, dst);
+                } else if (kb <= 48 * 1024) {
                     k_kron_axis<true><<<grid_for(nodes * ns, 256), 256, kb, ctx->stream>>>(dK[a].p, nd, sd, nodes, dof,
                                                                                          c, ns, src, dst);
                 } else if (kb <= 200 * 1024) {
@@ -670,23 +705,29 @@ void koh_loglik(sfc_koh *k, const sfc_hparams_t *hp, double *out)
     sfc_forward_gauss *fg = k->fg;
     SFC_REQUIRE(fg->valid, "forward model not updated");
     SFC_REQUIRE(k->n_o > 0, "sensor values not set");
-    const int ns = (int)k->ns;
-    k->work.reserve((size_t)2 * ns * ns + (size_t)ns * k->n_o + 16);
+    const int ns = (int)k->ns, n_o = k->n_o;
+    const int64_t nn = (int64_t)ns * ns;
+    k->work.reserve((size_t)nn + (size_t)ns * n_o + ns + 16);
     k->outv.reserve(1);
     k->info.reserve(1);
-    DBuf<double> &d = k->outv;
-    DBuf<int> &info = k->info;
+    double *C = k->work.p, *D = C + nn, *piv = D + (int64_t)ns * n_o;
+    int dropped = 0;
     {
         ProfScope ps(ctx, "phase:koh_loglik", 0.0);
-        k_koh_loglik<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim,
-                                                  k->Y.p, *hp, k->work.p, d.p, info.p);
+        // C = K_s + rho^2 C_s, D = Y - rho mean (LikelihoodKOH.ipp:75-100)
+        k_koh_system<<<grid_for(nn, 256), 256, 0, ctx->stream>>>(ns, n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p,
+                                                                  k->dim, k->Y.p, *hp, C, D);
+        count_launch(ctx);
+        spd_inverse_gj(ctx, C, ns, 0.0, k->gj, piv, &dropped);
+        if (dropped) fail(SFC_ERR_NOT_SPD, "total covariance is not positive definite (LLT failed)");
+        SFC_CK(cudaMemsetAsync(k->info.p, 0, sizeof(int), ctx->stream));
+        k_koh_loglik_terms<<<1, 1024, 0, ctx->stream>>>(ns, n_o, C, D, piv, k->outv.p, k->info.p);
+        count_launch(ctx);
     }
-    count_launch(ctx);
     int hi = 0;
-    download(ctx, &hi, info.p, 1);
-    if (hi > 0) fail(SFC_ERR_NOT_SPD, "total covariance is not positive definite (LLT failed)");
+    download(ctx, &hi, k->info.p, 1);
     if (hi < 0) fail(SFC_ERR_BAD_ARG, "non-negative quadratic term in the log-likelihood");
-    download(ctx, out, d.p, 1);
+    download(ctx, out, k->outv.p, 1);
 }
 
 // LikelihoodKOH::giveLogLikelihood for n hyperparameter sets (rho and the
@@ -702,12 +743,14 @@ void koh_loglik_batch(sfc_koh *k, const sfc_hparams_t *hps, int n, double *out)
     const int ns = (int)k->ns;
     const int64_t wsz = 2 * (int64_t)ns * ns + (int64_t)ns * k->n_o;
     const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(n, (int64_t)(256e6 / 8) / std::max<int64_t>(wsz, 1)));
-    DBuf<double> work, res;
-    DBuf<int> info;
-    DBuf<sfc_hparams_t> h;
-    work.alloc((size_t)chunk * wsz);
-    res.alloc(chunk);
-    info.alloc(chunk);
+    // persistent on the likelihood object (grown, never shrunk): an MCMC loop
+    // calls this every step
+    DBuf<double> &work = k->bwork, &res = k->bres;
+    DBuf<int> &info = k->binfo;
+    DBuf<sfc_hparams_t> &h = k->bhp;
+    work.reserve((size_t)chunk * wsz);
+    res.reserve(chunk);
+    info.reserve(chunk);
     std::vector<int> hinfo(chunk);
     for (int c0 = 0; c0 < n; c0 += chunk) {
         const int m = std::min(chunk, n - c0);
@@ -729,23 +772,37 @@ void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
     sfc_forward_gauss *fg = k->fg;
     SFC_REQUIRE(fg->valid, "forward model not updated");
     SFC_REQUIRE(k->n_o > 0, "sensor values not set");
-    const int ns = (int)k->ns;
-    k->work.reserve((size_t)5 * ns * ns + 3 * (size_t)ns + 16);
-    k->outv.reserve((size_t)ns + (size_t)ns * ns);
-    k->info.reserve(1);
+    const int ns = (int)k->ns, n_o = k->n_o;
+    const int64_t nn = (int64_t)ns * ns;
+    k->work.reserve((size_t)2 * nn + 2 * (size_t)ns + 16);
+    k->outv.reserve((size_t)ns + (size_t)nn);
+    double *Ksi = k->work.p, *Cui = Ksi + nn, *ysum = Cui + nn, *v = ysum + ns;
     double *pm = k->outv.p, *pc = k->outv.p + ns;
-    DBuf<int> &info = k->info;
+    const double rho = hp->rho;
     {
         ProfScope ps(ctx, "phase:koh_posterior", 0.0);
-        k_koh_proj<<<1, 1024, 0, ctx->stream>>>(ns, k->n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim, k->Y.p,
-                                                *hp, k->work.p, pm, pc, info.p);
+        // Sigma = (rho^2 n_o K_s^-1 + C_s^-1)^-1, m = Sigma (rho K_s^-1 sum_k y_k + C_s^-1 mean)
+        int d1 = 0, d2 = 0, d3 = 0;
+        k_mismatch<<<1, 1024, 0, ctx->stream>>>(ns, k->sensor_coords.p, k->dim, *hp, Ksi);
+        SFC_CK(cudaMemcpyAsync(Cui, fg->cov.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        count_launch(ctx);
+        spd_inverse_gj(ctx, Ksi, ns, 0.0, k->gj, nullptr, &d1);
+        if (d1) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible (mismatch covariance)");
+        spd_inverse_gj(ctx, Cui, ns, 0.0, k->gj, nullptr, &d2);
+        if (d2) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible (projected prior covariance)");
+        SFC_CK(cudaMemcpyAsync(pc, Cui, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        k_add_scaled<<<grid_for(nn, 256), 256, 0, ctx->stream>>>(pc, Ksi, rho * rho * n_o, nn);
+        k_rowsum<<<1, 256, 0, ctx->stream>>>(k->Y.p, ns, n_o, ysum);
+        count_launch(ctx, 2);
+        spd_inverse_gj(ctx, pc, ns, 0.0, k->gj, nullptr, &d3);
+        if (d3) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible (posterior precision)");
+        gemm(ctx, 0, 0, ns, 1, ns, rho, Ksi, ns, ysum, 1, 0.0, v, 1);
+        gemm(ctx, 0, 0, ns, 1, ns, 1.0, Cui, ns, fg->mean.p, 1, 1.0, v, 1);
+        gemm(ctx, 0, 0, ns, 1, ns, 1.0, pc, ns, v, 1, 0.0, pm, 1);
     }
-    count_launch(ctx);
-    int hi = 0;
-    download(ctx, &hi, info.p, 1);
-    if (hi) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible (code " + std::to_string(hi) + ")");
     if (mean) download(ctx, mean, pm, ns);
-    if (cov) download(ctx, cov, pc, (size_t)ns * ns);
+    if (cov) download(ctx, cov, pc, (size_t)nn);
+    SFC_CK(cudaStreamSynchronize(ctx->stream));
 }
 
 // lower Cholesky in place (n x n, row-major); false when not positive definite
@@ -870,26 +927,21 @@ void koh_woodbury(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov
     const double rho = hp->rho;
     const int n_o = k->n_o;
     // K_s, K_s^-1, S = K_s/(rho^2 n_o) + C_s, S^-1
-    DBuf<double> Ks, Ksi, L, Sm, Si, ysum, P;
-    DBuf<int> info;
+    DBuf<double> Ks, Ksi, Si, ysum, P;
     Ks.alloc(ns * ns);
     Ksi.alloc(ns * ns);
-    L.alloc(std::max<int64_t>(ns * ns, 1));
-    Sm.alloc(ns * ns);
     Si.alloc(ns * ns);
     ysum.alloc(ns);
-    info.alloc(1);
-    SFC_CK(cudaMemsetAsync(info.p, 0, sizeof(int), ctx->stream));
     k_mismatch<<<1, 1024, 0, ctx->stream>>>((int)ns, k->sensor_coords.p, k->dim, *hp, Ks.p);
-    k_spd_inverse<<<1, 1024, 0, ctx->stream>>>((int)ns, Ks.p, L.p, Ksi.p, info.p);
-    SFC_CK(cudaMemcpyAsync(Sm.p, fg->cov.p, ns * ns * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-    k_add_scaled<<<grid_for(ns * ns, 256), 256, 0, ctx->stream>>>(Sm.p, Ks.p, 1.0 / (rho * rho * n_o), ns * ns);
-    k_spd_inverse<<<1, 1024, 0, ctx->stream>>>((int)ns, Sm.p, L.p, Si.p, info.p);
+    SFC_CK(cudaMemcpyAsync(Ksi.p, Ks.p, ns * ns * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    SFC_CK(cudaMemcpyAsync(Si.p, fg->cov.p, ns * ns * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    k_add_scaled<<<grid_for(ns * ns, 256), 256, 0, ctx->stream>>>(Si.p, Ks.p, 1.0 / (rho * rho * n_o), ns * ns);
     k_rowsum<<<1, 256, 0, ctx->stream>>>(k->Y.p, ns, n_o, ysum.p);
-    count_launch(ctx, 5);
-    int hi = 0;
-    download(ctx, &hi, info.p, 1);
-    if (hi) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible");
+    count_launch(ctx, 3);
+    int d1 = 0, d2 = 0;
+    spd_inverse_gj(ctx, Ksi.p, ns, 0.0, k->gj, nullptr, &d1);
+    spd_inverse_gj(ctx, Si.p, ns, 0.0, k->gj, nullptr, &d2);
+    if (d1 || d2) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not invertible");
     // dense P (ns x N)
     std::vector<double> hP((size_t)ns * N, 0.0);
     for (int64_t a = 0; a < ns; ++a)
