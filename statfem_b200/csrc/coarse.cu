@@ -70,77 +70,117 @@ __global__ void k_coarse_modes(const float4 *__restrict__ offset, const unsigned
     }
 }
 
-// A_c = P^T S P.  One CTA per aggregate a: for every node i of a and every
-// block (i, j) of S, the 6 x 6 product M_i^T S_ij M_j is added to the slot of
-// j's aggregate (its colour class, unique among a's neighbours), then the
-// row block of a is written out.  M = diag(free) [I | R(d)].
-__global__ void __launch_bounds__(256) k_coarse_galerkin(const int32_t *__restrict__ agg_ptr,
-                                                         const int32_t *__restrict__ agg_nodes,
-                                                         const int32_t *__restrict__ node_agg,
-                                                         const int32_t *__restrict__ agg_slot,
-                                                         const int32_t *__restrict__ nbr, const float4 *__restrict__ mode,
-                                                         const int32_t *__restrict__ bptr,
-                                                         const int32_t *__restrict__ bcol,
-                                                         const double *__restrict__ bval, int64_t nc,
-                                                         double *__restrict__ A)
+// A_c = P^T S P.  A cluster of kGalSplit CTAs of kGalWarps warps per
+// aggregate a: a warp takes a node i of a, its lanes the blocks (i, j) of S, and each lane forms the 6 x 6
+// product M_i^T S_ij M_j (M = diag(free) [I | R(d)]) for the colour class of
+// j's aggregate (unique among a's neighbours).  Lanes with the same class
+// are summed by warp shuffles (the 27 blocks of a node reach at most 8
+// classes) into the warp's own accumulators; the cluster's warp accumulators
+// are added in a fixed order at the end (through distributed shared memory),
+// so the result is deterministic.
+constexpr int kGalWarps = 4;
+constexpr int kGalSplit = 4;
+
+__device__ __forceinline__ double warp_sum_masked(double v)
 {
-    __shared__ double acc[kSlots * 36];
-    const int a = blockIdx.x;
-    for (int t = threadIdx.x; t < kSlots * 36; t += blockDim.x) acc[t] = 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __cluster_dims__(kGalSplit, 1, 1) __launch_bounds__(32 * kGalWarps) k_coarse_galerkin(const int32_t *__restrict__ agg_ptr,
+                                                                    const int32_t *__restrict__ agg_nodes,
+                                                                    const int32_t *__restrict__ node_agg,
+                                                                    const int32_t *__restrict__ agg_slot,
+                                                                    const int32_t *__restrict__ nbr,
+                                                                    const float4 *__restrict__ mode,
+                                                                    const int32_t *__restrict__ bptr,
+                                                                    const int32_t *__restrict__ bcol,
+                                                                    const double *__restrict__ bval, int64_t nc,
+                                                                    double *__restrict__ A)
+{
+    __shared__ double acc[kGalWarps][kSlots * 36];
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    const int a = blockIdx.x / kGalSplit;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int t = threadIdx.x; t < kGalWarps * kSlots * 36; t += blockDim.x) (&acc[0][0])[t] = 0.0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int32_t t = agg_ptr[a] + w; t < agg_ptr[a + 1]; t += nw) {
+    for (int32_t t = agg_ptr[a] + (int32_t)rank * kGalWarps + w; t < agg_ptr[a + 1]; t += kGalWarps * kGalSplit) {
         const int32_t i = agg_nodes[t];
         const float4 mi = mode[i];
         double Ri[9];
         rot_matrix(mi, Ri);
         const int bi = mask_bits(mi);
-        for (int32_t b = bptr[i] + lane; b < bptr[i + 1]; b += 32) {
-            const int32_t j = bcol[b];
-            const float4 mj = mode[j];
-            double Rj[9];
-            rot_matrix(mj, Rj);
-            const int bj = mask_bits(mj);
-            const int slot = agg_slot[node_agg[j]];
-            // S' = diag(free_i) S_ij diag(free_j)
-            double Sp[9];
+        for (int32_t b0 = bptr[i]; b0 < bptr[i + 1]; b0 += 32) {
+            const int32_t b = b0 + lane;
+            const bool has = b < bptr[i + 1];
+            double G[36];
+            int slot = -1;
+            if (has) {
+                const int32_t j = bcol[b];
+                const float4 mj = mode[j];
+                double Rj[9];
+                rot_matrix(mj, Rj);
+                const int bj = mask_bits(mj);
+                slot = agg_slot[node_agg[j]];
+                double Sp[9];
 #pragma unroll
-            for (int r = 0; r < 3; ++r)
+                for (int r = 0; r < 3; ++r)
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    Sp[3 * r + c] = ((bi >> r) & 1) || ((bj >> c) & 1) ? 0.0 : bval[9 * (int64_t)b + 3 * r + c];
-            // U = S' R_j, V = R_i^T S', W = R_i^T U
-            double U[9], Vm[9], W[9];
+                    for (int c = 0; c < 3; ++c)
+                        Sp[3 * r + c] = ((bi >> r) & 1) || ((bj >> c) & 1) ? 0.0 : bval[9 * (int64_t)b + 3 * r + c];
+                // G = [[S', S' R_j], [R_i^T S', R_i^T S' R_j]]
 #pragma unroll
-            for (int r = 0; r < 3; ++r)
+                for (int r = 0; r < 3; ++r)
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    U[3 * r + k] = Sp[3 * r] * Rj[k] + Sp[3 * r + 1] * Rj[3 + k] + Sp[3 * r + 2] * Rj[6 + k];
-                    Vm[3 * r + k] = Ri[r] * Sp[k] + Ri[3 + r] * Sp[3 + k] + Ri[6 + r] * Sp[6 + k];
+                    for (int k = 0; k < 3; ++k) {
+                        const double u = Sp[3 * r] * Rj[k] + Sp[3 * r + 1] * Rj[3 + k] + Sp[3 * r + 2] * Rj[6 + k];
+                        G[r * 6 + k] = Sp[3 * r + k];
+                        G[r * 6 + 3 + k] = u;
+                        G[(3 + r) * 6 + k] = Ri[r] * Sp[k] + Ri[3 + r] * Sp[3 + k] + Ri[6 + r] * Sp[6 + k];
+                    }
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        G[(3 + r) * 6 + 3 + k] = Ri[r] * G[3 + k] + Ri[3 + r] * G[6 + 3 + k] + Ri[6 + r] * G[12 + 3 + k];
+            } else {
+#pragma unroll
+                for (int m = 0; m < 36; ++m) G[m] = 0.0;
+            }
+            // segmented sum over the lanes of each colour class present
+            unsigned left = __ballot_sync(0xffffffffu, has);
+            while (left) {
+                const int leader = __ffs(left) - 1;
+                const int cls = __shfl_sync(0xffffffffu, slot, leader);
+                const bool mine = has && slot == cls;
+                left &= ~__ballot_sync(0xffffffffu, mine);
+                double keep = 0.0;
+#pragma unroll
+                for (int m = 0; m < 36; ++m) {
+                    const double v = warp_sum_masked(mine ? G[m] : 0.0);
+                    if (lane == (m & 31)) keep = (m < 32) ? v : keep;
+                    if (m >= 32 && lane == m - 32) acc[w][cls * 36 + m] += v;
                 }
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    W[3 * r + k] = Ri[r] * U[k] + Ri[3 + r] * U[3 + k] + Ri[6 + r] * U[6 + k];
-            double *o = acc + slot * 36;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    if (Sp[3 * r + k] != 0.0) atomicAdd(o + r * 6 + k, Sp[3 * r + k]);
-                    if (U[3 * r + k] != 0.0) atomicAdd(o + r * 6 + 3 + k, U[3 * r + k]);
-                    if (Vm[3 * r + k] != 0.0) atomicAdd(o + (3 + r) * 6 + k, Vm[3 * r + k]);
-                    if (W[3 * r + k] != 0.0) atomicAdd(o + (3 + r) * 6 + 3 + k, W[3 * r + k]);
-                }
+                acc[w][cls * 36 + lane] += keep;
+            }
         }
     }
-    __syncthreads();
-    for (int t = threadIdx.x; t < kSlots * 36; t += blockDim.x) {
+    cl.sync();
+    for (int t = (int)rank * blockDim.x + threadIdx.x; t < kSlots * 36; t += kGalSplit * blockDim.x) {
         const int slot = t / 36, mk = t - slot * 36;
         const int32_t b = nbr[kSlots * a + slot];
-        if (b >= 0) A[(int64_t)(6 * a + mk / 6) * nc + 6 * b + mk % 6] = acc[t];
+        if (b < 0) continue;
+        double sum = 0.0;
+        for (unsigned r = 0; r < kGalSplit; ++r) {
+            const double *ra = cl.map_shared_rank(&acc[0][0], r);
+#pragma unroll
+            for (int q = 0; q < kGalWarps; ++q) sum += ra[q * kSlots * 36 + t];
+        }
+        A[(int64_t)(6 * a + mk / 6) * nc + 6 * b + mk % 6] = sum;
     }
+    cl.sync();  // the other CTAs' accumulators stay alive until every read is done
 }
 
 __global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n)
@@ -593,13 +633,19 @@ bool coarse_prepare(sfc_system *s)
     cs.a64.alloc(nc * nc);
     cs.a32.alloc(nc * nc);
     SFC_CK(cudaMemsetAsync(cs.a64.p, 0, nc * nc * sizeof(double), ctx->stream));
-    k_coarse_galerkin<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(cs.agg_ptr.p, cs.agg_nodes.p, cs.node_agg.p,
-                                                                 cs.agg_slot.p, cs.nbr.p, cs.mode.p, s->bptr.p,
-                                                                 s->bcol.p, s->bval64.p, nc, cs.a64.p);
+    {
+        ProfScope pg(ctx, "coarse_galerkin", 0.0);
+        k_coarse_galerkin<<<(unsigned)(cs.nagg * kGalSplit), 32 * kGalWarps, 0, ctx->stream>>>(cs.agg_ptr.p, cs.agg_nodes.p, cs.node_agg.p,
+                                                                     cs.agg_slot.p, cs.nbr.p, cs.mode.p, s->bptr.p,
+                                                                     s->bcol.p, s->bval64.p, nc, cs.a64.p);
+    }
     count_launch(ctx, 2);
     cs.gj.reserve(nc);
     int dropped = 0;
-    spd_inverse_gj(ctx, cs.a64.p, nc, 1e-10, cs.gj, nullptr, &dropped);
+    {
+        ProfScope pg(ctx, "coarse_inverse", 0.0);
+        spd_inverse_gj(ctx, cs.a64.p, nc, 1e-10, cs.gj, nullptr, &dropped);
+    }
     k_to_f32<<<grid_for(nc * nc, 256), 256, 0, ctx->stream>>>(cs.a64.p, cs.a32.p, nc * nc);
     count_launch(ctx);
     cs.dropped = dropped;

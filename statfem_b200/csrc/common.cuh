@@ -209,7 +209,20 @@ namespace sfc {
 struct GjScratch {
     DBuf<double> diag, rowp, colp;
     DBuf<int> word;
+    struct Graph {  // captured launch sequence of one (matrix, size)
+        const double *A;
+        int64_t n;
+        double rel;
+        const double *pivots;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    GjScratch() = default;
+    GjScratch(const GjScratch &) = delete;
+    GjScratch &operator=(const GjScratch &) = delete;
+    ~GjScratch();
     void reserve(int64_t n);
+    void drop_graphs();
 };
 
 struct CoarseSpace {

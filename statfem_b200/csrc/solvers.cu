@@ -255,6 +255,22 @@ __device__ __forceinline__ void stv(float *p, const float (&v)[V])
     if constexpr (V == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
+// V consecutive doubles (16-byte loads where V >= 2; the rows are 16-byte aligned)
+template <int V>
+__device__ __forceinline__ void ldv64(const double *p, double (&v)[V])
+{
+    if constexpr (V == 1) {
+        v[0] = *p;
+    } else {
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            const double2 t = *reinterpret_cast<const double2 *>(p + k);
+            v[k] = t.x;
+            v[k + 1] = t.y;
+        }
+    }
+}
+
 // reduce per-lane column partials acc[V] (column lane*V+v) over the block's
 // warps and add them to out[K]
 template <int V>
@@ -435,13 +451,14 @@ __global__ void __launch_bounds__(256) k_bresid64(const int32_t *__restrict__ bp
             for (int t = 0; t < nbk; ++t) {
                 const double *xj = X + (int64_t)(3 * sc[w][t]) * K + lane * V;
                 const double *bv = &sv[w][t * 9];
+                double xv[3][V];
 #pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const double x0 = xj[v], x1 = xj[K + v], x2 = xj[2 * K + v];
+                for (int q = 0; q < 3; ++q) ldv64<V>(xj + q * K, xv[q]);
+#pragma unroll
+                for (int v = 0; v < V; ++v)
 #pragma unroll
                     for (int r = 0; r < 3; ++r)
-                        acc[r][v] = fma(bv[3 * r + 2], x2, fma(bv[3 * r + 1], x1, fma(bv[3 * r], x0, acc[r][v])));
-                }
+                        acc[r][v] = fma(bv[3 * r + 2], xv[2][v], fma(bv[3 * r + 1], xv[1][v], fma(bv[3 * r], xv[0][v], acc[r][v])));
             }
         }
 #pragma unroll
@@ -458,6 +475,29 @@ __global__ void __launch_bounds__(256) k_bresid64(const int32_t *__restrict__ bp
 }
 
 // R = B - S X in FP64 (warp per row); rr[c] += R[i][c]^2
+// R = B and rr[c] += sum_i B[i][c]^2: the residual of x = 0 (no product)
+template <int V>
+__global__ void __launch_bounds__(256) k_bcopy_norm64(const double *__restrict__ B, double *__restrict__ R, int64_t N,
+                                                      double *rr)
+{
+    constexpr int K = 32 * V;
+    __shared__ double sh[8 * K];
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double dacc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps)
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int64_t o = i * K + lane * V + v;
+            const double b = B[o];
+            R[o] = b;
+            dacc[v] += b * b;
+        }
+    block_cols_add<V>(dacc, sh, rr);
+}
+
 template <int V>
 __global__ void __launch_bounds__(256) k_resid64(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
                                                  const double *__restrict__ a, const double *__restrict__ X,
@@ -1269,7 +1309,11 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         std::fill(nstall.begin(), nstall.end(), 0);
         int it_update = 0, last_interval = 0;
         count_launch(ctx);
-        resid(x64.p, b64.p, r64.p, bn2);  // r64 = b, ||b_c||^2
+        {  // x = 0: r64 = b, ||b_c||^2
+            ProfScope ps(ctx, "resid64", 16.0 * N * K);
+            k_bcopy_norm64<V><<<gw, 256, 0, ctx->stream>>>(b64.p, r64.p, N, bn2);
+            count_launch(ctx);
+        }
         download(ctx, hb.data(), bn2, K);
         std::vector<bool> active(K);
         int nactive = 0;
