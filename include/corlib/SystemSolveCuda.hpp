@@ -205,6 +205,12 @@ public:
     {
         sfc_detail::check(sfc_system_set_options(sys_, &opt), ctx_, "setOptions");
     }
+    sfc_solver_options_t options() const
+    {
+        sfc_solver_options_t opt;
+        sfc_detail::check(sfc_system_get_options(sys_, &opt), ctx_, "options");
+        return opt;
+    }
     sfc_solve_stats_t lastStats() const
     {
         sfc_solve_stats_t st;
