@@ -42,10 +42,10 @@ HP = {"forcing.sigma": 0.05, "forcing.length": 0.3, "rho": 1.0, "mismatch.sigma"
 REG = 0.001
 
 
-def make_workload(config, seed):
+def make_workload(config, seed, c2_n=48):
     rng = np.random.default_rng(seed)
     if config == "c2":
-        n, ns = 48, 256
+        n, ns = c2_n, 256
         mesh = mg.unit_cube_hex(n, mg.HEX8_ELASTIC)
         ax = mg.cell_centre_axes(n)
         g = mg.se_field_tensor(rng, [ax, ax, ax], 0.3, 0.25)
@@ -56,7 +56,7 @@ def make_workload(config, seed):
         P = mg.projection_matrix(mesh, pts, comps)
         f = np.array([0.0, 0.0, -1.0])
         hp = dict(HP)
-        desc = "3-D elasticity statFEM, 48^3 hex8 (352,947 dofs), 256 sensors, rel. residual 1e-8"
+        desc = "3-D elasticity statFEM, %d^3 hex8 (%d dofs), 256 sensors, rel. residual 1e-8" % (n, mesh.num_dofs)
         qps = 8
     elif config == "c1":
         n, ns = 64, 16
@@ -251,7 +251,7 @@ class GpuStatFEM:
 def run_ours(args, ws, rank, local):
     from statfem_b200 import api
     method = api.SFC_SOLVER_PCG_MIXED if args.method == "mixed" else api.SFC_SOLVER_PCG_FP64
-    wl = make_workload(args.config, seed=1234 + rank)
+    wl = make_workload(args.config, seed=1234 + rank, c2_n=args.c2_n)
     g = GpuStatFEM(wl, local, method, args.block_width, precond_code(api, args.precond), args.coarse_size)
     ctx = g.ctx
     for _ in range(args.warmup):
@@ -873,6 +873,8 @@ def run_reference(args, ws, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--c2-n", type=int, default=48,
+                    help="c2: elements per side (48 is the benchmark; smaller for profiler captures)")
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])

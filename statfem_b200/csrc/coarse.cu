@@ -212,12 +212,11 @@ __global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
     for (int m = 0; m < 6; ++m)
 #pragma unroll
         for (int v = 0; v < V; ++v) acc[m][v] = 0.f;
-#pragma unroll 2
-    for (int32_t t = agg_ptr[a] + (int32_t)rank * 8 + w; t < agg_ptr[a + 1]; t += 8 * kRestrictSplit) {
+    // two nodes per trip: six row loads in flight per warp
+    auto load_node = [&](int32_t t, float4 &m, float (&rv)[3][V]) {
         const int32_t i = agg_nodes[t];
-        const float4 m = mode[i];
+        m = mode[i];
         const int bits = (int)m.w;
-        float rv[3][V];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             const float *src = r + (3 * (int64_t)i + q) * K + lane * V;
@@ -234,6 +233,8 @@ __global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
 #pragma unroll
                 for (int v = 0; v < V; ++v) rv[q][v] = 0.f;
         }
+    };
+    auto add_node = [&](const float4 &m, const float (&rv)[3][V]) {
 #pragma unroll
         for (int v = 0; v < V; ++v) {
             acc[0][v] += rv[0][v];
@@ -243,6 +244,22 @@ __global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
             acc[4][v] += m.z * rv[0][v] - m.x * rv[2][v];
             acc[5][v] += m.x * rv[1][v] - m.y * rv[0][v];
         }
+    };
+    const int32_t step = 8 * kRestrictSplit, end = agg_ptr[a + 1];
+    int32_t t = agg_ptr[a] + (int32_t)rank * 8 + w;
+    for (; t + step < end; t += 2 * step) {
+        float4 m0, m1;
+        float r0[3][V], r1[3][V];
+        load_node(t, m0, r0);
+        load_node(t + step, m1, r1);
+        add_node(m0, r0);
+        add_node(m1, r1);
+    }
+    if (t < end) {
+        float4 m0;
+        float r0[3][V];
+        load_node(t, m0, r0);
+        add_node(m0, r0);
     }
 #pragma unroll
     for (int m = 0; m < 6; ++m)

@@ -351,6 +351,7 @@ struct sfc_covar_forcing {
     int64_t num_nodes = 0, num_dofs = 0;
     sfc::DBuf<double> phibar;  // num_dofs
     sfc::DBuf<double> kron[3]; // 1-D SE factors along the grid axes
+    sfc::DBuf<double> atb_part; // split-K partial tiles of the projected covariance
 };
 
 struct sfc_forward_gauss {
@@ -444,6 +445,9 @@ void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double l
 void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *W, double *T,
                   int64_t ns, double *tmp);
 void atb_accumulate(sfc_ctx *ctx, const double *A, const double *B, int64_t K, int64_t M, int64_t Nn, double *C);
+// C = A^T B (M x M) for A, B: K x M when A^T B is symmetric (stats.cu)
+void atb_symmetric(sfc_ctx *ctx, const double *A, const double *B, int64_t K, int64_t M, double *C,
+                   sfc::DBuf<double> &part);
 // autotune.cu: the process-wide table of tuned launch shapes
 std::string tune_device_key(sfc_ctx *ctx);
 bool tune_lookup(const std::string &key, std::string &val);

@@ -716,7 +716,9 @@ __global__ void __launch_bounds__(256) k_ninit32(const double *__restrict__ R64,
     block_cols_add<V>(a2, sh, rr0);
 }
 
-template <int V>
+// XUPD = false: x is left to the p update (k_npupdate32 / k_ncpupdate32 with
+// x given), so this pass reads r and q only
+template <int V, bool XUPD = true>
 __global__ void __launch_bounds__(256) k_nupdate32(float *__restrict__ x, float *__restrict__ r,
                                                    const float *__restrict__ p, const float *__restrict__ q,
                                                    const float *__restrict__ bdinv, int64_t nodes, const double *pq,
@@ -745,17 +747,19 @@ __global__ void __launch_bounds__(256) k_nupdate32(float *__restrict__ x, float 
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
             const int64_t o = (3 * n + i) * K + lane * V;
-            float xv[V], pv[V], qv[V];
-            ldv<V>(x + o, xv);
+            float qv[V];
             ldv<V>(r + o, rv[i]);
-            ldv<V>(p + o, pv);
             ldv<V>(q + o, qv);
+            if constexpr (XUPD) {
+                float xv[V], pv[V];
+                ldv<V>(x + o, xv);
+                ldv<V>(p + o, pv);
 #pragma unroll
-            for (int v = 0; v < V; ++v) {
-                xv[v] = fmaf(alpha[v], pv[v], xv[v]);
-                rv[i][v] = fmaf(-alpha[v], qv[v], rv[i][v]);
+                for (int v = 0; v < V; ++v) xv[v] = fmaf(alpha[v], pv[v], xv[v]);
+                stv<V>(x + o, xv);
             }
-            stv<V>(x + o, xv);
+#pragma unroll
+            for (int v = 0; v < V; ++v) rv[i][v] = fmaf(-alpha[v], qv[v], rv[i][v]);
             stv<V>(r + o, rv[i]);
         }
         bj_apply<V>(bdinv + 9 * n, rv, zv);
@@ -772,22 +776,34 @@ __global__ void __launch_bounds__(256) k_nupdate32(float *__restrict__ x, float 
     block_cols_add<V>(a2, sh, rr_next);
 }
 
+// x (nullable): x += alpha p with this iteration's alpha (computed as in
+// k_nupdate32) before p is overwritten
+__device__ __forceinline__ float iter_alpha(int c, const double *pq, const double *rz, const double *rr,
+                                            const double *thr, const int *brk)
+{
+    const bool frozen = rr[c] <= thr[c] || brk[c];
+    const double den = pq[c];
+    return (frozen || !(den > 0.0)) ? 0.f : (float)(rz[c] / den);
+}
+
 template <int V>
 __global__ void __launch_bounds__(256) k_npupdate32(float *__restrict__ p, const float *__restrict__ r,
                                                     const float *__restrict__ bdinv, int64_t nodes, const double *rz,
                                                     const double *rz_next, const double *rr_next, const double *thr,
-                                                    const int *stop, const int *brk)
+                                                    const int *stop, const int *brk, float *__restrict__ x,
+                                                    const double *pq, const double *rr)
 {
     constexpr int K = 32 * V;
     if (*stop) return;
     const int lane = threadIdx.x & 31;
-    float beta[V];
+    float beta[V], alpha[V];
     bool act[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
         const int c = lane * V + v;
         act[v] = rr_next[c] > thr[c] && !brk[c];
         beta[v] = act[v] ? (float)(rz_next[c] / rz[c]) : 0.f;
+        alpha[v] = x ? iter_alpha(c, pq, rz, rr, thr, brk) : 0.f;
     }
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t n = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; n < nodes; n += warps) {
@@ -800,6 +816,13 @@ __global__ void __launch_bounds__(256) k_npupdate32(float *__restrict__ p, const
             const int64_t o = (3 * n + i) * K + lane * V;
             float pv[V];
             ldv<V>(p + o, pv);
+            if (x) {
+                float xv[V];
+                ldv<V>(x + o, xv);
+#pragma unroll
+                for (int v = 0; v < V; ++v) xv[v] = fmaf(alpha[v], pv[v], xv[v]);
+                stv<V>(x + o, xv);
+            }
 #pragma unroll
             for (int v = 0; v < V; ++v)
                 if (act[v]) pv[v] = fmaf(beta[v], pv[v], zv[i][v]);
@@ -819,12 +842,13 @@ __global__ void __launch_bounds__(256) k_ncpupdate32(float *__restrict__ p, cons
                                                      const float4 *__restrict__ mode, const float *__restrict__ e,
                                                      int64_t nodes, const double *rz, const double *rz_next,
                                                      const double *rr_next, const double *thr, const int *stop,
-                                                     const int *brk, const int *restart)
+                                                     const int *brk, const int *restart, float *__restrict__ x,
+                                                     const double *pq, const double *rr)
 {
     constexpr int K = 32 * V;
     if (!INIT && *stop) return;
     const int lane = threadIdx.x & 31;
-    float beta[V];
+    float beta[V], alpha[V];
     bool act[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
@@ -832,9 +856,11 @@ __global__ void __launch_bounds__(256) k_ncpupdate32(float *__restrict__ p, cons
         if constexpr (INIT) {
             act[v] = restart[c] != 0;
             beta[v] = 0.f;
+            alpha[v] = 0.f;
         } else {
             act[v] = rr_next[c] > thr[c] && !brk[c];
             beta[v] = act[v] ? (float)(rz_next[c] / rz[c]) : 0.f;
+            alpha[v] = x ? iter_alpha(c, pq, rz, rr, thr, brk) : 0.f;
         }
     }
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -863,6 +889,13 @@ __global__ void __launch_bounds__(256) k_ncpupdate32(float *__restrict__ p, cons
             const int64_t o = (3 * n + i) * K + lane * V;
             float pv[V];
             ldv<V>(p + o, pv);
+            if (!INIT && x) {
+                float xv[V];
+                ldv<V>(x + o, xv);
+#pragma unroll
+                for (int v = 0; v < V; ++v) xv[v] = fmaf(alpha[v], pv[v], xv[v]);
+                stv<V>(x + o, xv);
+            }
 #pragma unroll
             for (int v = 0; v < V; ++v)
                 if (act[v]) pv[v] = fmaf(beta[v], pv[v], zv[i][v]);
@@ -1274,7 +1307,8 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             coarse_block_apply<V>(s, rr32, rz_slot, nullptr);
             k_ncpupdate32<V, true><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, crs.node_agg.p, crs.mode.p,
                                                                 crs.e32.p, s->nodes, nullptr, nullptr, nullptr,
-                                                                nullptr, nullptr, nullptr, restart.p);
+                                                                nullptr, nullptr, nullptr, restart.p, nullptr, nullptr,
+                                                                nullptr);
         } else if (bj)
             k_ninit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->bdinv32.p, restart.p, rr32, xr, pp, s->nodes,
                                                       rz_slot, rr_slot);
@@ -1340,9 +1374,9 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             const int64_t o0 = (int64_t)it * K, o1 = (int64_t)(it + 1) * K;
             spmm(pp, qq, pq + o0);
             {
-                ProfScope ps(ctx, "bupdate32", 6.0 * N * K * 4 + (bj ? 12.0 : 4.0) * N);
+                ProfScope ps(ctx, "bupdate32", (bj ? 3.0 : 6.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N);
                 if (bj)
-                    k_nupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pq + o0,
+                    k_nupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pq + o0,
                                                                 rz + o0, rrs + o0, thr, rz + o1, rrs + o1, stop, err);
                 else
                     k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
@@ -1350,14 +1384,14 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             }
             if (two) coarse_block_apply<V>(s, rr32, rz + o1, stop);
             {
-                ProfScope ps(ctx, "bpupdate32", 3.0 * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
+                ProfScope ps(ctx, "bpupdate32", (bj ? 5.0 : 3.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
                 if (two)
                     k_ncpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, crs.node_agg.p,
                                                                          crs.mode.p, crs.e32.p, s->nodes, rz + o0,
-                                                                         rz + o1, rrs + o1, thr, stop, err, nullptr);
+                                                                         rz + o1, rrs + o1, thr, stop, err, nullptr, xr, pq + o0, rrs + o0);
                 else if (bj)
                     k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz + o0, rz + o1,
-                                                                 rrs + o1, thr, stop, err);
+                                                                 rrs + o1, thr, stop, err, xr, pq + o0, rrs + o0);
                 else
                     k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
                                                                  thr, stop, err);

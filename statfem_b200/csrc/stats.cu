@@ -612,6 +612,102 @@ void kernel_times(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double leng
     }
 }
 
+// C = A^T B for a symmetric product (A^T B = B^T A, as W^T K W): only the
+// 128 x 128 tiles on and above the diagonal are formed, over a slice of the
+// K rows per CTA (8 x 8 outputs per thread, 8-row chunks double-buffered in
+// shared memory); partial tiles go to part[split][tile] and k_atb_sym_reduce
+// adds them in split order and mirrors the upper tiles (deterministic, exactly
+// symmetric).
+constexpr int kSymT = 128;
+constexpr int kSymK = 8;
+
+__global__ void __launch_bounds__(256) k_atb_sym(const double *__restrict__ A, const double *__restrict__ B, int64_t K,
+                                                 int64_t M, int64_t rows_per_split, const int2 *__restrict__ tiles,
+                                                 int ntiles, double *__restrict__ part)
+{
+    __shared__ __align__(16) double sa[2][kSymK][kSymT];
+    __shared__ __align__(16) double sb[2][kSymK][kSymT];
+    const int2 tile = tiles[blockIdx.y];
+    const int64_t a0 = (int64_t)tile.x * kSymT, b0 = (int64_t)tile.y * kSymT;
+    const int64_t k0 = (int64_t)blockIdx.x * rows_per_split;
+    const int64_t k1 = k0 + rows_per_split < K ? k0 + rows_per_split : K;
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    // each thread stages 4 values of each operand per chunk: row t / 128, column t % 128
+    double ra[4], rb[4];
+    auto fetch = [&](int64_t kk) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int t = threadIdx.x + 256 * q, r = t / kSymT, c = t % kSymT;
+            const int64_t k = kk + r;
+            ra[q] = (k < k1 && a0 + c < M) ? A[k * M + a0 + c] : 0.0;
+            rb[q] = (k < k1 && b0 + c < M) ? B[k * M + b0 + c] : 0.0;
+        }
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int t = threadIdx.x + 256 * q, r = t / kSymT, c = t % kSymT;
+            sa[buf][r][c] = ra[q];
+            sb[buf][r][c] = rb[q];
+        }
+    };
+    int buf = 0;
+    if (k0 < k1) {
+        fetch(k0);
+        stash(0);
+    }
+    __syncthreads();
+    for (int64_t kk = k0; kk < k1; kk += kSymK) {
+        const bool more = kk + kSymK < k1;
+        if (more) fetch(kk + kSymK);  // in flight during the products
+#pragma unroll
+        for (int r = 0; r < kSymK; ++r) {
+            double av[8], bv[8];
+#pragma unroll
+            for (int i = 0; i < 8; i += 2) {
+                const double2 x = *reinterpret_cast<const double2 *>(&sa[buf][r][ty * 8 + i]);
+                const double2 y = *reinterpret_cast<const double2 *>(&sb[buf][r][tx * 8 + i]);
+                av[i] = x.x; av[i + 1] = x.y;
+                bv[i] = y.x; bv[i + 1] = y.y;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
+        if (more) stash(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+    }
+    double *o = part + ((int64_t)blockIdx.x * ntiles + blockIdx.y) * kSymT * kSymT;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) o[(ty * 8 + i) * kSymT + tx * 8 + j] = acc[i][j];
+}
+
+__global__ void k_atb_sym_reduce(const double *__restrict__ part, int splits, const int2 *__restrict__ tiles,
+                                 int ntiles, int64_t M, double alpha, double *__restrict__ C)
+{
+    const int64_t total = (int64_t)ntiles * kSymT * kSymT;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int ti = (int)(t / (kSymT * kSymT));
+        const int e = (int)(t % (kSymT * kSymT)), i = e / kSymT, j = e % kSymT;
+        const int64_t a = (int64_t)tiles[ti].x * kSymT + i, b = (int64_t)tiles[ti].y * kSymT + j;
+        if (a >= M || b >= M) continue;
+        double sum = 0.0;
+        for (int sp = 0; sp < splits; ++sp) sum += part[((int64_t)sp * ntiles + ti) * kSymT * kSymT + e];
+        sum *= alpha;
+        C[a * M + b] = sum;
+        if (tiles[ti].x != tiles[ti].y) C[b * M + a] = sum;
+    }
+}
+
 // C (ns x ns) = W^T (K W) with W = diag(phibar) X, X: num_dofs x ns (device)
 void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double length, const double *X,
                             int64_t ns, double *C, DBuf<double> &work)
@@ -622,16 +718,32 @@ void projected_covar(sfc_ctx *ctx, sfc_covar_forcing *cf, double sigma, double l
     k_scale_rows<<<grid_for(N * ns, 256), 256, 0, ctx->stream>>>(X, cf->phibar.p, N, ns, W);
     count_launch(ctx);
     kernel_times(ctx, cf, sigma, length, W, T, ns, tmpp);
-    SFC_CK(cudaMemsetAsync(C, 0, ns * ns * 8, ctx->stream));
-    const int64_t tiles = ((ns + 63) / 64) * ((ns + 63) / 64);
-    int64_t splits = std::max<int64_t>(1, (ctx->sm_count * 4) / tiles);
-    int64_t rows = (N + splits - 1) / splits;
-    rows = ((rows + 15) / 16) * 16;
-    splits = (N + rows - 1) / rows;
-    dim3 g((unsigned)splits, (unsigned)((ns + 63) / 64), (unsigned)((ns + 63) / 64));
     ProfScope ps(ctx, "covar_atb", 2.0 * N * ns * 8);
-    k_atb<<<g, 256, 0, ctx->stream>>>(W, T, N, ns, ns, rows, 1.0, C);
-    count_launch(ctx);
+    atb_symmetric(ctx, W, T, N, ns, C, cf->atb_part);
+}
+
+// C (M x M) = A^T B for A, B: K x M (row-major) with A^T B symmetric
+void atb_symmetric(sfc_ctx *ctx, const double *A, const double *B, int64_t K, int64_t M, double *C,
+                   DBuf<double> &part)
+{
+    const int nt = (int)((M + kSymT - 1) / kSymT);
+    std::vector<int2> ht;
+    for (int i = 0; i < nt; ++i)
+        for (int j = i; j < nt; ++j) ht.push_back(make_int2(i, j));
+    const int ntiles = (int)ht.size();
+    int64_t splits = std::max<int64_t>(1, (ctx->sm_count * 2) / ntiles);
+    int64_t rows = (K + splits - 1) / splits;
+    rows = ((rows + kSymK - 1) / kSymK) * kSymK;
+    splits = (K + rows - 1) / rows;
+    static_assert(sizeof(int2) == 8, "tile list packing");
+    part.reserve((size_t)splits * ntiles * kSymT * kSymT + (size_t)ntiles);
+    int2 *dtiles = reinterpret_cast<int2 *>(part.p + (size_t)splits * ntiles * kSymT * kSymT);
+    SFC_CK(cudaMemcpyAsync(dtiles, ht.data(), ntiles * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+    k_atb_sym<<<dim3((unsigned)splits, (unsigned)ntiles), 256, 0, ctx->stream>>>(A, B, K, M, rows, dtiles, ntiles,
+                                                                                  part.p);
+    k_atb_sym_reduce<<<grid_for((int64_t)ntiles * kSymT * kSymT, 256), 256, 0, ctx->stream>>>(part.p, (int)splits,
+                                                                                               dtiles, ntiles, M, 1.0, C);
+    count_launch(ctx, 2);
 }
 
 // C (M x Nn) += A^T B for A: K x M, B: K x Nn (row-major), split-K
