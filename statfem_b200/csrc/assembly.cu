@@ -525,15 +525,19 @@ __global__ void k_build_op(const int32_t *__restrict__ row_ptr, const int32_t *_
                            float *__restrict__ a_op32, double *__restrict__ dinv, float *__restrict__ dinv32,
                            int *err)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    // warp per row, lanes over the row's entries (coalesced)
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
         const bool mi = mask[i];
-        for (int32_t s = row_ptr[i]; s < row_ptr[i + 1]; ++s) {
+        for (int32_t s = row_ptr[i] + lane; s < row_ptr[i + 1]; s += 32) {
             const int32_t j = col[s];
             double v = a_ref[s];
             if ((mi || mask[j]) && j != i) v = 0.0;
             a_op[s] = v;
             a_op32[s] = (float)v;
         }
+        if (lane) continue;
         const int32_t d = diag[i];
         if (d < 0) {
             atomicExch(err, 4);
@@ -965,7 +969,7 @@ void build_operator(sfc_system *s, bool require_positive_diag)
     s->dinv32.alloc(s->N);
     DevInt err = status_word(ctx);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
-    k_build_op<<<grid_for(s->N, 128), 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p,
+    k_build_op<<<grid_for(s->N * 32, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p,
                                                              s->mask.p, s->N, s->a_op.p, s->a_op32.p, s->dinv.p,
                                                              s->dinv32.p, err.p);
     count_launch(ctx);
@@ -1003,20 +1007,21 @@ __global__ void k_bsr_fill(const int32_t *__restrict__ row_ptr, const int32_t *_
                            const double *__restrict__ a_op, const int32_t *__restrict__ bptr, int64_t nodes,
                            int32_t *__restrict__ bcol, float *__restrict__ b32, double *__restrict__ b64, int *err)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+    // warp per node, lanes over the node's 9 nb block values (coalesced writes)
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nodes; i += warps) {
         const int32_t r0 = row_ptr[3 * i];
         const int32_t nb = bptr[i + 1] - bptr[i];
-        for (int32_t t = 0; t < nb; ++t) {
+        for (int32_t e = lane; e < 9 * nb; e += 32) {
+            const int32_t t = e / 9, r = (e % 9) / 3, c = e % 3;
             const int64_t b = bptr[i] + t;
             const int32_t j = col[r0 + 3 * t] / 3;
-            bcol[b] = j;
-            for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c) {
-                    const int32_t s = r0 + r * 3 * nb + 3 * t + c;
-                    if (col[s] != 3 * j + c) atomicExch(err, 1);
-                    b64[b * 9 + r * 3 + c] = a_op[s];
-                    b32[b * 9 + r * 3 + c] = (float)a_op[s];
-                }
+            if (r == 0 && c == 0) bcol[b] = j;
+            const int32_t s = r0 + r * 3 * nb + 3 * t + c;
+            if (col[s] != 3 * j + c) atomicExch(err, 1);
+            b64[b * 9 + r * 3 + c] = a_op[s];
+            b32[b * 9 + r * 3 + c] = (float)a_op[s];
         }
     }
 }
@@ -1062,7 +1067,7 @@ static void build_bsr(sfc_system *s)
     DevInt err = status_word(ctx);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
     k_bsr_ptr<<<grid_for(nodes + 1, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, nodes, s->bptr.p, err.p);
-    k_bsr_fill<<<grid_for(nodes, 128), 128, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, s->bptr.p, nodes,
+    k_bsr_fill<<<grid_for(nodes * 32, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_op.p, s->bptr.p, nodes,
                                                               s->bcol.p, s->bval32.p, s->bval64.p, err.p);
     count_launch(ctx, 2);
     int h = 0;

@@ -128,11 +128,22 @@ __global__ void __launch_bounds__(256) k_gj_update(double *__restrict__ A, int64
     __shared__ double cp[64][kGJ + 1];
     __shared__ double rp[kGJ][64 + 1];
     const int64_t i0 = (int64_t)blockIdx.y * 64, j0 = (int64_t)blockIdx.x * 64;
-    for (int t = threadIdx.x; t < 64 * kGJ; t += blockDim.x) {
-        const int r = t / kGJ, m = t % kGJ;
-        cp[r][m] = (i0 + r < n && m < kb) ? colp[(i0 + r) * kGJ + m] : 0.0;
-        const int mm = t / 64, c = t % 64;
-        rp[mm][c] = (j0 + c < n && mm < kb) ? rowp[mm * n + j0 + c] : 0.0;
+    {  // all 16 loads of a thread in flight before the stores (launched with 256 threads)
+        double vc[64 * kGJ / 256], vr[64 * kGJ / 256];
+#pragma unroll
+        for (int u = 0; u < 64 * kGJ / 256; ++u) {
+            const int t = threadIdx.x + 256 * u;
+            const int r = t / kGJ, m = t % kGJ;
+            vc[u] = (i0 + r < n && m < kb) ? colp[(i0 + r) * kGJ + m] : 0.0;
+            const int mm = t / 64, c = t % 64;
+            vr[u] = (j0 + c < n && mm < kb) ? rowp[mm * n + j0 + c] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 64 * kGJ / 256; ++u) {
+            const int t = threadIdx.x + 256 * u;
+            cp[t / kGJ][t % kGJ] = vc[u];
+            rp[t / 64][t % 64] = vr[u];
+        }
     }
     __syncthreads();
     const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;

@@ -1088,6 +1088,72 @@ __global__ void k_fix_accum(const int32_t *__restrict__ rp, const int32_t *__res
     }
 }
 
+// The same fix-up as a gather, for structurally symmetric patterns (every
+// system assembled from a mesh): one warp per constrained dof c reads the
+// couplings a_ref[f, c] of its free neighbours f (found in row f by binary
+// search, the columns being sorted) and forms
+//   X[c][a] = (B[c][a] - sum_f a_ref[f, c] X[f][a]) / a_ref[c, c]
+// in a fixed order, with no atomics and no N x nrhs scratch.
+__global__ void __launch_bounds__(256) k_fix_gather(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                                    const int32_t *__restrict__ diag, const double *__restrict__ a_ref,
+                                                    const unsigned char *__restrict__ mask,
+                                                    const double *__restrict__ B, int ld, int nrhs, int64_t N,
+                                                    double *__restrict__ X)
+{
+    constexpr int NA = 8;  // columns per lane and pass
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < N; c += warps) {
+        if (!mask[c]) continue;  // warp-uniform
+        const double dcc = a_ref[diag[c]];
+        const int32_t e0 = rp[c], e1 = rp[c + 1];
+        for (int a0 = 0; a0 < nrhs; a0 += 32 * NA) {
+            double acc[NA];
+#pragma unroll
+            for (int q = 0; q < NA; ++q) acc[q] = 0.0;
+            for (int32_t s0 = e0; s0 < e1; s0 += 32) {
+                const int32_t sl = s0 + lane;
+                int32_t f = 0;
+                double w = 0.0;
+                if (sl < e1) {
+                    f = col[sl];
+                    if (f != c && !mask[f]) {
+                        int32_t lo = rp[f], hi = rp[f + 1] - 1;
+                        while (lo <= hi) {  // column c in the sorted row f
+                            const int32_t mid = (lo + hi) >> 1;
+                            const int32_t cm = col[mid];
+                            if (cm == c) {
+                                w = a_ref[mid];
+                                break;
+                            }
+                            if (cm < c)
+                                lo = mid + 1;
+                            else
+                                hi = mid - 1;
+                        }
+                    }
+                }
+                const int n = min(32, e1 - s0);
+                for (int t = 0; t < n; ++t) {
+                    const double wt = __shfl_sync(0xffffffffu, w, t);
+                    const int32_t ft = __shfl_sync(0xffffffffu, f, t);
+                    if (wt == 0.0) continue;  // warp-uniform
+#pragma unroll
+                    for (int q = 0; q < NA; ++q) {
+                        const int a = a0 + lane + 32 * q;
+                        if (a < nrhs) acc[q] += wt * X[(int64_t)ft * ld + a];
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NA; ++q) {
+                const int a = a0 + lane + 32 * q;
+                if (a < nrhs) X[c * ld + a] = (B[c * ld + a] - acc[q]) / dcc;
+            }
+        }
+    }
+}
+
 __global__ void k_fix_apply(const int32_t *__restrict__ diag, const double *__restrict__ a_ref,
                             const unsigned char *__restrict__ mask, const double *__restrict__ B,
                             const double *__restrict__ Y, int ld, int nrhs, int64_t N, double *__restrict__ X)
@@ -1714,6 +1780,12 @@ void transpose_fixup(sfc_system *s, const double *B, double *X, int nrhs, int ld
     if (!s->any_constraint) return;
     sfc_ctx *ctx = s->ctx;
     const int64_t N = s->N;
+    if (s->pattern_mesh) {  // element couplings: the pattern is symmetric
+        k_fix_gather<<<grid_for(N * 32, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p,
+                                                                      s->mask.p, B, ld, nrhs, N, X);
+        count_launch(ctx);
+        return;
+    }
     s->fix.reserve(N * (int64_t)nrhs);
     SFC_CK(cudaMemsetAsync(s->fix.p, 0, N * (int64_t)nrhs * 8, ctx->stream));
     k_fix_accum<<<grid_for(N * nrhs, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->a_ref.p, s->mask.p, X,

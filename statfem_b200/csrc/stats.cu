@@ -160,9 +160,20 @@ __global__ void __launch_bounds__(256) k_kron_line(const double *__restrict__ Kd
     const int64_t col0 = (int64_t)blockIdx.y * kLineCols;
     const int ncols = (int)(ns - col0 < kLineCols ? ns - col0 : kLineCols);
     for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) sK[t] = Kd[t];
-    for (int t = threadIdx.x; t < nd * kLineCols; t += blockDim.x) {
-        const int k = t / kLineCols, j = t % kLineCols;
-        sIn[t] = j < ncols ? in[((base + k * sd) * dof + c) * ns + col0 + j] : 0.0;
+    // eight loads in flight per thread before they are stored
+    const int total = nd * kLineCols;
+    for (int t0 = threadIdx.x; t0 < total; t0 += 8 * blockDim.x) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int t = t0 + u * blockDim.x, k = t / kLineCols, j = t % kLineCols;
+            v[u] = (t < total && j < ncols) ? in[((base + k * sd) * dof + c) * ns + col0 + j] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int t = t0 + u * blockDim.x;
+            if (t < total) sIn[t] = v[u];
+        }
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
