@@ -36,67 +36,73 @@ __global__ void __launch_bounds__(256) k_gj_panel(const double *__restrict__ A, 
                                                   const double *__restrict__ adiag, double rel, double *__restrict__ rowp,
                                                   double *__restrict__ colp, int *dropped, double *pivots)
 {
-    __shared__ double D[kGJ][kGJ + 1];
-    // warp 0 inverts the diagonal block in registers: lane c holds column c
-    if (threadIdx.x < 32) {
-        const int c = threadIdx.x;
-        double col[kGJ];
+    // launched with 256 threads
+    __shared__ double D[2][kGJ][kGJ + 1];
+    __shared__ double T[kGJ][kPanelCols + 1];
+    __shared__ double sad[kGJ];
+    const int64_t j0 = (int64_t)blockIdx.x * kPanelCols;
+    if (threadIdx.x < kGJ) sad[threadIdx.x] = threadIdx.x < kb ? adiag[k0 + threadIdx.x] : 0.0;
+    // stage the diagonal block, this CTA's 64 columns of the row panel and its
+    // 64 rows of the column panel, every load of a thread in flight together
+    {
+        double vd[kGJ * kGJ / 256], vt[kPanelCols * kGJ / 256], vc[kPanelCols * kGJ / 256];
 #pragma unroll
-        for (int r = 0; r < kGJ; ++r) col[r] = (r < kb && c < kb) ? A[(k0 + r) * n + k0 + c] : 0.0;
-        int ndrop = 0;
-        const double ad = c < kb ? adiag[k0 + c] : 0.0;  // lane p's is broadcast at pivot p
-        for (int p = 0; p < kb; ++p) {
-            // pivot = D[p][p] (lane p), column p of D (lane p's registers)
-            double piv = 0.0, colv[kGJ];
-#pragma unroll
-            for (int r = 0; r < kGJ; ++r) {
-                colv[r] = __shfl_sync(0xffffffffu, col[r], p);
-                if (r == p) piv = colv[r];
-            }
-            const bool drop = !(piv > rel * __shfl_sync(0xffffffffu, ad, p));
-            if (pivots && blockIdx.x == 0 && c == 0) pivots[k0 + p] = piv;
-            double rowp_c = 0.0;  // D[p][c]
-#pragma unroll
-            for (int r = 0; r < kGJ; ++r)
-                if (r == p) rowp_c = col[r];
-            if (drop) {
-                ++ndrop;
-#pragma unroll
-                for (int r = 0; r < kGJ; ++r)
-                    if (r == p || c == p) col[r] = 0.0;
-            } else {
-                const double ip = 1.0 / piv;
-#pragma unroll
-                for (int r = 0; r < kGJ; ++r) {
-                    double v;
-                    if (r == p && c == p)
-                        v = ip;
-                    else if (r == p)
-                        v = rowp_c * ip;
-                    else if (c == p)
-                        v = -colv[r] * ip;
-                    else
-                        v = col[r] - colv[r] * (rowp_c * ip);
-                    col[r] = v;
-                }
-            }
+        for (int u = 0; u < kGJ * kGJ / 256; ++u) {
+            const int t = threadIdx.x + 256 * u, r = t / kGJ, c = t % kGJ;
+            vd[u] = (r < kb && c < kb) ? A[(k0 + r) * n + k0 + c] : 0.0;
         }
 #pragma unroll
-        for (int r = 0; r < kGJ; ++r) D[r][c] = col[r];
-        if (blockIdx.x == 0 && c == 0 && ndrop) atomicAdd(dropped, ndrop);
+        for (int u = 0; u < kPanelCols * kGJ / 256; ++u) {
+            const int t = threadIdx.x + 256 * u;
+            const int l = t / kPanelCols, c = t % kPanelCols;
+            vt[u] = (l < kb && j0 + c < n) ? A[(k0 + l) * n + j0 + c] : 0.0;
+            const int jj = t / kGJ, m = t % kGJ;  // m fastest: row j0 + jj of A read contiguously
+            vc[u] = (j0 + jj < n && m < kb) ? A[(j0 + jj) * n + k0 + m] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < kGJ * kGJ / 256; ++u) {
+            const int t = threadIdx.x + 256 * u;
+            D[0][t / kGJ][t % kGJ] = vd[u];
+        }
+#pragma unroll
+        for (int u = 0; u < kPanelCols * kGJ / 256; ++u) {
+            const int t = threadIdx.x + 256 * u;
+            T[t / kPanelCols][t % kPanelCols] = vt[u];
+            const int jj = t / kGJ, m = t % kGJ;
+            if (j0 + jj < n && m < kb) colp[(j0 + jj) * kGJ + m] = vc[u];
+        }
     }
     __syncthreads();
-    // this CTA's 64 columns j0.. (and rows, for the column panel)
-    __shared__ double T[kGJ][kPanelCols + 1];
-    const int64_t j0 = (int64_t)blockIdx.x * kPanelCols;
-    for (int t = threadIdx.x; t < kPanelCols * kGJ; t += blockDim.x) {
-        const int jj = t / kGJ, m = t % kGJ;  // m fastest: row j0 + jj of A read contiguously
-        const int64_t j = j0 + jj;
-        if (j < n && m < kb) colp[j * kGJ + m] = A[j * n + k0 + m];
-        const int l = t / kPanelCols, c = t % kPanelCols;
-        T[l][c] = (l < kb && j0 + c < n) ? A[(k0 + l) * n + j0 + c] : 0.0;
+    // Gauss-Jordan on the diagonal block: every thread owns 4 entries, reads
+    // buffer cur and writes the other, one barrier per pivot; the drop test
+    // is evaluated identically by every thread
+    int cur = 0, ndrop = 0;
+    for (int p = 0; p < kb; ++p) {
+        const double piv = D[cur][p][p];
+        const bool drop = !(piv > rel * sad[p]);
+        if (pivots && blockIdx.x == 0 && threadIdx.x == 0) pivots[k0 + p] = piv;
+        ndrop += drop;
+        const double ip = drop ? 0.0 : 1.0 / piv;
+#pragma unroll
+        for (int u = 0; u < kGJ * kGJ / 256; ++u) {
+            const int t = threadIdx.x + 256 * u, r = t / kGJ, c = t % kGJ;
+            double v;
+            if (drop)
+                v = (r == p || c == p) ? 0.0 : D[cur][r][c];
+            else if (r == p && c == p)
+                v = ip;
+            else if (r == p)
+                v = D[cur][p][c] * ip;
+            else if (c == p)
+                v = -D[cur][r][p] * ip;
+            else
+                v = D[cur][r][c] - D[cur][r][p] * (D[cur][p][c] * ip);
+            D[cur ^ 1][r][c] = v;
+        }
+        cur ^= 1;
+        __syncthreads();
     }
-    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ndrop) atomicAdd(dropped, ndrop);
     const int c = threadIdx.x % kPanelCols, mg = threadIdx.x / kPanelCols;  // 4 groups of 8 rows of D^-1
     const int64_t j = j0 + c;
     if (j < n) {
@@ -107,11 +113,11 @@ __global__ void __launch_bounds__(256) k_gj_panel(const double *__restrict__ A, 
             if (m >= kb) continue;
             double v;
             if (inside) {
-                v = D[m][j - k0];
+                v = D[cur][m][j - k0];
             } else {
                 v = 0.0;
 #pragma unroll 8
-                for (int l = 0; l < kGJ; ++l) v += D[m][l] * T[l][c];
+                for (int l = 0; l < kGJ; ++l) v += D[cur][m][l] * T[l][c];
             }
             rowp[m * n + j] = v;
         }
