@@ -187,3 +187,15 @@ def test_statfem_posterior_two_level(ctx):
     (m0, c0), (m1, c1) = out
     assert np.abs(m1 - m0).max() <= 1e-8 * np.abs(m0).max()
     assert np.abs(c1 - c0).max() <= 1e-7 * np.abs(c0).max()
+
+
+@pytest.mark.parametrize("size", [3, 4, 6])
+def test_coarse_space_size_matches_oracle_boxes(ctx, size):
+    """The library's box grid is the oracle's (oracle/coarse_ref.py): six
+    coarse dofs per non-empty box when no box is fully constrained."""
+    from oracle import coarse_ref as C
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 12, 15)
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-10, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=size)
+    s.solveSystem()
+    agg, _ = C.box_aggregates(mesh.coords, size)
+    assert s.last_stats()["coarse_dofs"] == 6 * (int(agg.max()) + 1)
