@@ -105,6 +105,49 @@ __global__ void __launch_bounds__(kRedThreads) k_spmv64(const int32_t *__restric
     }
 }
 
+// y = S x through the node-block (3 x 3) view on 3-dof meshes: one warp per
+// node, lanes over its blocks (one index and nine values per block instead of
+// nine indices); dot += x.y
+__global__ void __launch_bounds__(kRedThreads) k_bspmv64(const int32_t *__restrict__ bptr,
+                                                          const int32_t *__restrict__ bcol,
+                                                          const double *__restrict__ bval,
+                                                          const double *__restrict__ x, double *__restrict__ y,
+                                                          int64_t nodes, double *dot, const int *done)
+{
+    __shared__ double sh[32];
+    if (done && *done) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    double d = 0.0;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nodes; i += warps) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int32_t b = bptr[i] + lane; b < bptr[i + 1]; b += 32) {
+            const int64_t j = bcol[b];
+            const double *v = bval + 9 * (int64_t)b;
+            const double x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
+            a0 += v[0] * x0 + v[1] * x1 + v[2] * x2;
+            a1 += v[3] * x0 + v[4] * x1 + v[5] * x2;
+            a2 += v[6] * x0 + v[7] * x1 + v[8] * x2;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (lane == 0) {
+            y[3 * i] = a0;
+            y[3 * i + 1] = a1;
+            y[3 * i + 2] = a2;
+            d += x[3 * i] * a0 + x[3 * i + 1] * a1 + x[3 * i + 2] * a2;
+        }
+    }
+    if (dot) {
+        d = block_sum(d, sh);
+        if (threadIdx.x == 0) atomicAdd(dot, d);
+    }
+}
+
 // r = b' (lifted rhs), x = 0, p = z = D^-1 r; rz0 = r.z, bb = r.r
 __global__ void __launch_bounds__(kRedThreads) k_pcg_init(const double *__restrict__ b, const double *__restrict__ dinv,
                                                            double *__restrict__ x, double *__restrict__ r,
@@ -1178,10 +1221,16 @@ void launch_spmv64(sfc_system *s, const double *x, double *y, double *dot, const
 {
     const double avg = (double)s->nnz / (double)std::max<int64_t>(s->N, 1);
     sfc_ctx *ctx = s->ctx;
-    ProfScope ps(ctx, "spmv64", (double)s->nnz * 12 + 4.0 * (s->N + 1) + 16.0 * s->N);
-    const unsigned grid = (unsigned)(ctx->sm_count * 8);
     const int lanes = s->spmv_lanes;  // tuned, else chosen by the mean row length
-    if (lanes == 32 || (lanes == 0 && avg > 24))
+    ProfScope ps(ctx, "spmv64",
+                 (lanes == 0 && s->has_bsr ? (double)s->nblocks * 76 + 4.0 * (s->nodes + 1)
+                                           : (double)s->nnz * 12 + 4.0 * (s->N + 1)) +
+                     16.0 * s->N);
+    const unsigned grid = (unsigned)(ctx->sm_count * 8);
+    if (lanes == 0 && s->has_bsr) {  // 3-dof mesh: node blocks
+        k_bspmv64<<<grid_for(s->nodes * 32, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(
+            s->bptr.p, s->bcol.p, s->bval64.p, x, y, s->nodes, dot, done);
+    } else if (lanes == 32 || (lanes == 0 && avg > 24))
         k_spmv64<32><<<grid_for(s->N * 32, kRedThreads, grid), kRedThreads, 0, ctx->stream>>>(s->row_ptr.p, s->col.p,
                                                                                               s->a_op.p, x, y, s->N, dot, done);
     else if (lanes == 16 || (lanes == 0 && avg > 12))
