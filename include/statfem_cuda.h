@@ -80,11 +80,14 @@ typedef struct sfc_solver_options {
 #define SFC_PRECOND_JACOBI        0 /* point Jacobi                            */
 #define SFC_PRECOND_BLOCK_JACOBI  1 /* nodal 3x3 block Jacobi on 3-dof meshes,
                                        point Jacobi otherwise                  */
-#define SFC_PRECOND_TWO_LEVEL     2 /* nodal 3x3 block Jacobi plus an additive
-                                       coarse correction on the six rigid-body
-                                       modes of box aggregates of the mesh's
-                                       nodes (3-dof meshes assembled from a
-                                       mesh; block Jacobi otherwise)          */
+#define SFC_PRECOND_TWO_LEVEL     2 /* Jacobi smoother plus an additive coarse
+                                       correction on box aggregates of the
+                                       mesh's nodes: nodal 3x3 block Jacobi and
+                                       the six rigid-body modes per aggregate
+                                       on 3-dof meshes, point Jacobi and the
+                                       constant per aggregate on scalar ones
+                                       (systems assembled from a mesh; the
+                                       one-level preconditioner otherwise)    */
 
 typedef struct sfc_solve_stats {
     int32_t iterations;       /* max over right-hand sides, inner iterations   */

@@ -200,11 +200,9 @@ int32_t sfc_autotune_block_solver(sfc_system_t *s, const double *rhs, int32_t nr
         // (preconditioner, coarse size) candidates; the two-level ones only
         // where the system has a coarse space
         std::vector<std::pair<int, int>> pcs{{SFC_PRECOND_JACOBI, 0}};
-        if (dof == 3) {
-            pcs.push_back({SFC_PRECOND_BLOCK_JACOBI, 0});
-            if (s->pattern_mesh)
-                for (int cs : {6, 8, 12}) pcs.push_back({SFC_PRECOND_TWO_LEVEL, cs});
-        }
+        if (dof == 3) pcs.push_back({SFC_PRECOND_BLOCK_JACOBI, 0});
+        if (s->pattern_mesh)
+            for (int cs : {6, 8, 12}) pcs.push_back({SFC_PRECOND_TWO_LEVEL, cs});
         for (int bw : {32, 64, 128}) {
             if (bw > 32 && bw / 2 >= k) continue;  // wider blocks would be mostly padding
             for (auto [pc, csz] : pcs) {

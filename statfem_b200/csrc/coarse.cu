@@ -1,6 +1,7 @@
-// Two-level preconditioner for the 3-dof (elasticity) solves: the nodal 3x3
-// block-Jacobi smoother plus an additive coarse correction on the rigid-body
-// modes of geometric aggregates,
+// Two-level preconditioner: the nodal 3x3 block-Jacobi smoother (elasticity)
+// or point Jacobi (scalar Poisson meshes) plus an additive coarse correction
+// on the rigid-body modes (elasticity) or the constant (Poisson) of
+// geometric aggregates,
 //
 //     M^-1 r = D^-1 r + P A_c^+ P^T r,     A_c = P^T S P,
 //
@@ -43,7 +44,8 @@ namespace {
 namespace cg = cooperative_groups;
 
 constexpr int kSlots = 27;   // 3 x 3 x 3 colour classes of the box grid
-constexpr int kMaxAggs = 512;
+constexpr int kMaxAggs = 512;    // 3-dof meshes: 6 coarse dofs per aggregate
+constexpr int kMaxAggs1 = 2048;  // scalar meshes: 1 coarse dof per aggregate
 
 // R(d): column k is e_k x d (the displacement of rotation mode k at offset d)
 __device__ __forceinline__ void rot_matrix(const float4 m, double (&R)[9])
@@ -60,11 +62,12 @@ __device__ __forceinline__ int mask_bits(const float4 m) { return (int)m.w; }
 // per node: offset from its aggregate's centroid in units of the box edge
 // (x, y, z) and the constrained components as bits in w
 __global__ void k_coarse_modes(const float4 *__restrict__ offset, const unsigned char *__restrict__ mask,
-                               int64_t nodes, float4 *__restrict__ mode)
+                               int64_t nodes, int dof, float4 *__restrict__ mode)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
         float4 m = offset[i];
-        const int bits = (mask[3 * i] ? 1 : 0) | (mask[3 * i + 1] ? 2 : 0) | (mask[3 * i + 2] ? 4 : 0);
+        const int bits = dof == 1 ? (mask[i] ? 1 : 0)
+                                  : (mask[3 * i] ? 1 : 0) | (mask[3 * i + 1] ? 2 : 0) | (mask[3 * i + 2] ? 4 : 0);
         m.w = (float)bits;
         mode[i] = m;
     }
@@ -183,6 +186,62 @@ __global__ void __cluster_dims__(kGalSplit, 1, 1) __launch_bounds__(32 * kGalWar
     cl.sync();  // the other CTAs' accumulators stay alive until every read is done
 }
 
+// Scalar (1-dof) meshes: one constant mode per aggregate, A_c[a][b] = sum of
+// S_ij over free i in a and free j in b.  Same cluster / warp layout as
+// k_coarse_galerkin, lanes over a CSR row's entries.
+__global__ void __cluster_dims__(kGalSplit, 1, 1) __launch_bounds__(32 * kGalWarps)
+    k_coarse_galerkin1(const int32_t *__restrict__ agg_ptr, const int32_t *__restrict__ agg_nodes,
+                       const int32_t *__restrict__ node_agg, const int32_t *__restrict__ agg_slot,
+                       const int32_t *__restrict__ nbr, const float4 *__restrict__ mode,
+                       const int32_t *__restrict__ row_ptr, const int32_t *__restrict__ col,
+                       const double *__restrict__ aval, int64_t nc, double *__restrict__ A)
+{
+    __shared__ double acc[kGalWarps][kSlots];
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    const int a = blockIdx.x / kGalSplit;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int t = threadIdx.x; t < kGalWarps * kSlots; t += blockDim.x) (&acc[0][0])[t] = 0.0;
+    __syncthreads();
+    for (int32_t t = agg_ptr[a] + (int32_t)rank * kGalWarps + w; t < agg_ptr[a + 1]; t += kGalWarps * kGalSplit) {
+        const int32_t i = agg_nodes[t];
+        const bool fi = !(mask_bits(mode[i]) & 1);
+        for (int32_t s0 = row_ptr[i]; s0 < row_ptr[i + 1]; s0 += 32) {
+            const int32_t sl = s0 + lane;
+            const bool has = sl < row_ptr[i + 1];
+            double g = 0.0;
+            int slot = -1;
+            if (has) {
+                const int32_t j = col[sl];
+                slot = agg_slot[node_agg[j]];
+                if (fi && !(mask_bits(mode[j]) & 1)) g = aval[sl];
+            }
+            unsigned left = __ballot_sync(0xffffffffu, has);
+            while (left) {
+                const int leader = __ffs(left) - 1;
+                const int cls = __shfl_sync(0xffffffffu, slot, leader);
+                const bool mine = has && slot == cls;
+                left &= ~__ballot_sync(0xffffffffu, mine);
+                const double v = warp_sum_masked(mine ? g : 0.0);
+                if (lane == 0) acc[w][cls] += v;
+            }
+        }
+    }
+    cl.sync();
+    for (int t = (int)rank * blockDim.x + threadIdx.x; t < kSlots; t += kGalSplit * blockDim.x) {
+        const int32_t b = nbr[kSlots * a + t];
+        if (b < 0) continue;
+        double sum = 0.0;
+        for (unsigned r = 0; r < kGalSplit; ++r) {
+            const double *ra = cl.map_shared_rank(&acc[0][0], r);
+#pragma unroll
+            for (int q = 0; q < kGalWarps; ++q) sum += ra[q * kSlots + t];
+        }
+        A[(int64_t)a * nc + b] = sum;
+    }
+    cl.sync();  // the other CTAs' accumulators stay alive until every read is done
+}
+
 __global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n)
 {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -280,6 +339,52 @@ __global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
         c[(6 * (int64_t)a + t / K) * K + t % K] = sum;
     }
     cl.sync();  // the other CTAs' shared memory stays alive until every read is done
+}
+
+// scalar meshes: c[a][col] = sum of r[i][col] over the free nodes i of a
+template <int V>
+__global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
+    k_coarse_restrict32_1(const float *__restrict__ r, const int32_t *__restrict__ agg_ptr,
+                          const int32_t *__restrict__ agg_nodes, const float4 *__restrict__ mode,
+                          float *__restrict__ c, const int *stop)
+{
+    constexpr int K = 32 * V;
+    __shared__ float red[8][K];
+    if (stop && *stop) return;  // uniform: stop changes only between launches
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    const int a = blockIdx.x / kRestrictSplit;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float acc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = 0.f;
+    const int32_t step = 8 * kRestrictSplit, end = agg_ptr[a + 1];
+    for (int32_t t = agg_ptr[a] + (int32_t)rank * 8 + w; t < end; t += step) {
+        const int32_t i = agg_nodes[t];
+        if ((int)mode[i].w & 1) continue;  // warp-uniform: one node per warp
+        float rv[V];
+        const float *src = r + (int64_t)i * K + lane * V;
+#pragma unroll
+        for (int v = 0; v < V; ++v) rv[v] = src[v];
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] += rv[v];
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) red[w][lane * V + v] = acc[v];
+    __syncthreads();
+    for (int t = threadIdx.x; t < K; t += blockDim.x) {
+        float sum = 0.f;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) sum += red[q][t];
+        red[0][t] = sum;
+    }
+    cl.sync();
+    for (int t = (int)rank * blockDim.x + threadIdx.x; t < K; t += kRestrictSplit * blockDim.x) {
+        float sum = 0.f;
+        for (unsigned j = 0; j < kRestrictSplit; ++j) sum += cl.map_shared_rank(&red[0][0], j)[t];
+        c[(int64_t)a * K + t] = sum;
+    }
+    cl.sync();
 }
 
 // e = A c (A: nc x nc FP32, c and e: [nc][K]); rz[col] += sum_rows c e.
@@ -440,6 +545,32 @@ __global__ void __launch_bounds__(256) k_coarse_restrict64(const double *__restr
     }
 }
 
+// scalar meshes, one FP64 vector: c[a] = sum of r over the free nodes of a
+__global__ void __launch_bounds__(256) k_coarse_restrict64_1(const double *__restrict__ r,
+                                                             const int32_t *__restrict__ agg_ptr,
+                                                             const int32_t *__restrict__ agg_nodes,
+                                                             const float4 *__restrict__ mode, double *__restrict__ c,
+                                                             const int *done)
+{
+    __shared__ double red[8];
+    if (done && *done) return;
+    const int a = blockIdx.x;
+    double acc = 0.0;
+    for (int32_t t = agg_ptr[a] + threadIdx.x; t < agg_ptr[a + 1]; t += blockDim.x) {
+        const int32_t i = agg_nodes[t];
+        if (!((int)mode[i].w & 1)) acc += r[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) sum += red[q];
+        c[a] = sum;
+    }
+}
+
 // e = A c (FP64, warp per row); rz += c.e
 __global__ void __launch_bounds__(256) k_coarse_apply64(const double *__restrict__ A, const double *__restrict__ c,
                                                         double *__restrict__ e, int64_t nc, double *rz, const int *done)
@@ -496,8 +627,15 @@ static bool coarse_aggregate(sfc_system *s, int size)
     const sfc_mesh *m = s->pattern_mesh;
     CoarseSpace &cs = s->coarse;
     cs.built = false;
-    if (!m || m->dof != 3 || !s->has_bsr || m->num_nodes != s->nodes) return false;
+    if (!m) return false;
+    const int dof = m->dof;
+    if (dof == 3) {
+        if (!s->has_bsr || m->num_nodes != s->nodes) return false;
+    } else if (dof != 1 || m->num_dofs != s->N) {
+        return false;
+    }
     const int64_t nodes = m->num_nodes;
+    const int max_aggs = dof == 3 ? kMaxAggs : kMaxAggs1;
     const double *X = m->h_coords.data();
     double lo[3], hi[3];
     for (int d = 0; d < 3; ++d) {
@@ -523,7 +661,7 @@ static bool coarse_aggregate(sfc_system *s, int size)
             vol *= ext[d];
         }
     const double per = std::pow((double)std::max(size, 2), dim);
-    const double target = std::min<double>(kMaxAggs, std::max(1.0, (double)nodes / per));
+    const double target = std::min<double>(max_aggs, std::max(1.0, (double)nodes / per));
     const double hb = std::pow(vol / target, 1.0 / dim);
     int nb[3];
     for (int d = 0; d < 3; ++d) nb[d] = ext[d] > 1e-12 * emax ? std::max(1, (int)std::lround(ext[d] / hb)) : 1;
@@ -617,7 +755,9 @@ static bool coarse_aggregate(sfc_system *s, int size)
                 }
     }
     cs.nagg = nagg;
-    cs.nc = 6 * (int64_t)nagg;
+    cs.dof = dof;
+    cs.nodes = nodes;
+    cs.nc = (dof == 3 ? 6 : 1) * (int64_t)nagg;
     for (int d = 0; d < 3; ++d) cs.nb[d] = nb[d];
     upload(ctx, cs.node_agg, node_agg.data(), nodes);
     upload(ctx, cs.agg_ptr, agg_ptr.data(), agg_ptr.size());
@@ -645,16 +785,21 @@ bool coarse_prepare(sfc_system *s)
     if (cs.op_serial == s->op_serial) return true;
     sfc_ctx *ctx = s->ctx;
     ProfScope ps(ctx, "phase:coarse_setup", 0.0);
-    const int64_t nodes = s->nodes, nc = cs.nc;
-    k_coarse_modes<<<grid_for(nodes, 256), 256, 0, ctx->stream>>>(cs.offset.p, s->mask.p, nodes, cs.mode.p);
+    const int64_t nodes = cs.nodes, nc = cs.nc;
+    k_coarse_modes<<<grid_for(nodes, 256), 256, 0, ctx->stream>>>(cs.offset.p, s->mask.p, nodes, cs.dof, cs.mode.p);
     cs.a64.alloc(nc * nc);
     cs.a32.alloc(nc * nc);
     SFC_CK(cudaMemsetAsync(cs.a64.p, 0, nc * nc * sizeof(double), ctx->stream));
     {
         ProfScope pg(ctx, "coarse_galerkin", 0.0);
-        k_coarse_galerkin<<<(unsigned)(cs.nagg * kGalSplit), 32 * kGalWarps, 0, ctx->stream>>>(cs.agg_ptr.p, cs.agg_nodes.p, cs.node_agg.p,
-                                                                     cs.agg_slot.p, cs.nbr.p, cs.mode.p, s->bptr.p,
-                                                                     s->bcol.p, s->bval64.p, nc, cs.a64.p);
+        if (cs.dof == 3)
+            k_coarse_galerkin<<<(unsigned)(cs.nagg * kGalSplit), 32 * kGalWarps, 0, ctx->stream>>>(
+                cs.agg_ptr.p, cs.agg_nodes.p, cs.node_agg.p, cs.agg_slot.p, cs.nbr.p, cs.mode.p, s->bptr.p, s->bcol.p,
+                s->bval64.p, nc, cs.a64.p);
+        else
+            k_coarse_galerkin1<<<(unsigned)(cs.nagg * kGalSplit), 32 * kGalWarps, 0, ctx->stream>>>(
+                cs.agg_ptr.p, cs.agg_nodes.p, cs.node_agg.p, cs.agg_slot.p, cs.nbr.p, cs.mode.p, s->row_ptr.p,
+                s->col.p, s->a_op.p, nc, cs.a64.p);
     }
     count_launch(ctx, 2);
     cs.gj.reserve(nc);
@@ -679,9 +824,13 @@ void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *st
     cs.c32.reserve(cs.nc * K);
     cs.e32.reserve(cs.nc * K);
     {
-        ProfScope ps(ctx, "coarse_restrict32", 3.0 * s->nodes * K * 4 + 20.0 * s->nodes + 4.0 * cs.nc * K);
-        k_coarse_restrict32<V><<<(unsigned)(cs.nagg * kRestrictSplit), 256, 0, ctx->stream>>>(
-            r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p, cs.c32.p, stop);
+        ProfScope ps(ctx, "coarse_restrict32", (double)cs.dof * cs.nodes * K * 4 + 20.0 * cs.nodes + 4.0 * cs.nc * K);
+        if (cs.dof == 3)
+            k_coarse_restrict32<V><<<(unsigned)(cs.nagg * kRestrictSplit), 256, 0, ctx->stream>>>(
+                r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p, cs.c32.p, stop);
+        else
+            k_coarse_restrict32_1<V><<<(unsigned)(cs.nagg * kRestrictSplit), 256, 0, ctx->stream>>>(
+                r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p, cs.c32.p, stop);
         count_launch(ctx);
     }
     {
@@ -703,9 +852,13 @@ void coarse_vec_apply(sfc_system *s, const double *r, double *rz, const int *don
     cs.c64.reserve(cs.nc);
     cs.e64.reserve(cs.nc);
     {
-        ProfScope ps(ctx, "coarse_restrict64", 3.0 * s->nodes * 8 + 20.0 * s->nodes + 8.0 * cs.nc);
-        k_coarse_restrict64<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p,
-                                                                        cs.c64.p, done);
+        ProfScope ps(ctx, "coarse_restrict64", (double)cs.dof * cs.nodes * 8 + 20.0 * cs.nodes + 8.0 * cs.nc);
+        if (cs.dof == 3)
+            k_coarse_restrict64<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p,
+                                                                            cs.mode.p, cs.c64.p, done);
+        else
+            k_coarse_restrict64_1<<<(unsigned)cs.nagg, 256, 0, ctx->stream>>>(r, cs.agg_ptr.p, cs.agg_nodes.p,
+                                                                              cs.mode.p, cs.c64.p, done);
     }
     {
         ProfScope ps(ctx, "coarse_apply64", 8.0 * cs.nc * cs.nc + 16.0 * cs.nc);

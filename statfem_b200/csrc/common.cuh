@@ -230,7 +230,9 @@ struct CoarseSpace {
     const sfc_mesh *mesh = nullptr;
     int size = 0;                       // nodes per aggregate along each axis (target)
     uint64_t op_serial = 0;             // operator the inverse below belongs to
-    int64_t nagg = 0, nc = 0;           // aggregates, coarse dofs (6 per aggregate)
+    int dof = 3;                        // 3: six rigid-body modes per aggregate; 1: its constant
+    int64_t nodes = 0;
+    int64_t nagg = 0, nc = 0;           // aggregates, coarse dofs
     int nb[3] = {1, 1, 1};              // boxes per axis
     int dropped = 0;                    // dependent coarse dofs left out of the inverse
     DBuf<int32_t> node_agg;             // nodes

@@ -218,6 +218,28 @@ __global__ void k_pcg_pupdate(double *__restrict__ p, const double *__restrict__
         p[i] = dinv[i] * r[i] + beta * p[i];
 }
 
+// scalar two-level variant: p = D^-1 r + e[agg(i)] + beta p (INIT: p = z)
+template <bool INIT>
+__global__ void k_pcg1_pupdate(double *__restrict__ p, const double *__restrict__ r, const double *__restrict__ dinv,
+                               const int32_t *__restrict__ node_agg, const float4 *__restrict__ mode,
+                               const double *__restrict__ e, int64_t N, const double *rz, const double *rz_next,
+                               const double *rr_next, double thr, int it_next, int *done, const int *err)
+{
+    double beta = 0.0;
+    if constexpr (!INIT) {
+        if (*done || *err) return;
+        if (*rr_next <= thr) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *done = it_next;
+            return;
+        }
+        beta = *rz_next / *rz;
+    }
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const double z = dinv[i] * r[i] + (((int)mode[i].w & 1) ? 0.0 : e[node_agg[i]]);
+        p[i] = INIT ? z : z + beta * p[i];
+    }
+}
+
 // lifting of prescribed values: b_f = F_f - sum_{j constrained} a_ref[f,j] g_j,
 // g_j = F_j / a_ref[j,j]; constrained rows keep F.
 __global__ void k_lift(const int32_t *__restrict__ rp, const int32_t *__restrict__ col, const int32_t *__restrict__ diag,
@@ -583,7 +605,7 @@ __global__ void __launch_bounds__(256) k_resid64(const int32_t *__restrict__ rp,
 }
 
 // r32 = r64 * scale_c, x32 = 0, p = z = D^-1 r32 for restarted columns; rz0[c], rr0[c]
-template <int V>
+template <int V, bool SETP = true>
 __global__ void __launch_bounds__(256) k_binit32(const double *__restrict__ R64, const double *__restrict__ scale,
                                                  const float *__restrict__ dinv, const int *__restrict__ restart,
                                                  float *__restrict__ r, float *__restrict__ x, float *__restrict__ p,
@@ -605,7 +627,7 @@ __global__ void __launch_bounds__(256) k_binit32(const double *__restrict__ R64,
             const float zv = di * rv;
             r[o] = rv;
             x[o] = 0.f;
-            if (restart[lane * V + v]) p[o] = zv;
+            if (SETP && restart[lane * V + v]) p[o] = zv;
             a1[v] += (double)rv * zv;
             a2[v] += (double)rv * rv;
         }
@@ -693,6 +715,51 @@ __global__ void __launch_bounds__(256) k_bpupdate32(float *__restrict__ p, const
 #pragma unroll
         for (int v = 0; v < V; ++v)
             if (act[v]) pv[v] = fmaf(beta[v], pv[v], di * rv[v]);
+        stv<V>(p + o, pv);
+    }
+}
+
+// scalar two-level p update: z = D^-1 r + e[agg(i)] (0 on constrained dofs),
+// p = z + beta p for the active columns (INIT: p = z for the restarted ones)
+template <int V, bool INIT>
+__global__ void __launch_bounds__(256) k_cbpupdate32(float *__restrict__ p, const float *__restrict__ r,
+                                                     const float *__restrict__ dinv,
+                                                     const int32_t *__restrict__ node_agg,
+                                                     const float4 *__restrict__ mode, const float *__restrict__ e,
+                                                     int64_t N, const double *rz, const double *rz_next,
+                                                     const double *rr_next, const double *thr, const int *stop,
+                                                     const int *brk, const int *restart)
+{
+    constexpr int K = 32 * V;
+    if (!INIT && *stop) return;
+    const int lane = threadIdx.x & 31;
+    float beta[V];
+    bool act[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int c = lane * V + v;
+        if constexpr (INIT) {
+            act[v] = restart[c] != 0;
+            beta[v] = 0.f;
+        } else {
+            act[v] = rr_next[c] > thr[c] && !brk[c];
+            beta[v] = act[v] ? (float)(rz_next[c] / rz[c]) : 0.f;
+        }
+    }
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const int64_t o = i * K + lane * V;
+        float pv[V], rv[V], ev[V];
+        ldv<V>(p + o, pv);
+        ldv<V>(r + o, rv);
+        const bool free = !((int)mode[i].w & 1);
+        ldv<V>(e + (int64_t)node_agg[i] * K + lane * V, ev);
+        const float di = dinv[i];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const float z = di * rv[v] + (free ? ev[v] : 0.f);
+            if (act[v]) pv[v] = INIT ? z : fmaf(beta[v], pv[v], z);
+        }
         stv<V>(p + o, pv);
     }
 }
@@ -1250,7 +1317,9 @@ void launch_spmv64(sfc_system *s, const double *x, double *y, double *dot, const
 // current operator
 bool use_two_level(sfc_system *s)
 {
-    return s->opt.precond == SFC_PRECOND_TWO_LEVEL && s->has_bsr && s->bdinv32.p && coarse_prepare(s);
+    if (s->opt.precond != SFC_PRECOND_TWO_LEVEL) return false;
+    if (s->has_bsr && !s->bdinv32.p) return false;  // 3-dof mesh without its block-Jacobi smoother
+    return coarse_prepare(s);
 }
 
 // FP64 PCG on S x = b (device vectors, length N): point Jacobi, or with
@@ -1273,7 +1342,15 @@ PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_i
     const int64_t nodes = s->nodes;
     const unsigned gn = grid_for(nodes, kRedThreads, ctx->sm_count * 4);
     const CoarseSpace &cs = s->coarse;
-    if (two) {
+    const bool two1 = two && cs.dof == 1;  // scalar mesh: point Jacobi + constant modes
+    two = two && cs.dof == 3;
+    if (two1) {
+        k_pcg_init<<<g, kRedThreads, 0, ctx->stream>>>(b, s->dinv.p, x, r, p, N, rz, bb);  // rz: Jacobi share
+        count_launch(ctx);
+        coarse_vec_apply(s, r, rz, nullptr);
+        k_pcg1_pupdate<true><<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, cs.node_agg.p, cs.mode.p, cs.e64.p,
+                                                                 N, nullptr, nullptr, nullptr, 0.0, 0, done, err);
+    } else if (two) {
         k_pcg2_init<<<gn, kRedThreads, 0, ctx->stream>>>(b, s->bdinv32.p, x, r, nodes, rz, bb);
         count_launch(ctx);
         coarse_vec_apply(s, r, rz, nullptr);
@@ -1313,12 +1390,20 @@ PcgResult pcg64(sfc_system *s, const double *b, double *x, double tol, int max_i
                 k_pcg_update<<<g, kRedThreads, 0, ctx->stream>>>(x, r, p, q, s->dinv.p, N, pq + it, rz + it,
                                                                  rz + it + 1, rr + it + 1, done, err);
             }
-            {
+            if (two1) {
+                count_launch(ctx);
+                coarse_vec_apply(s, r, rz + it + 1, done);
+                ProfScope ps(ctx, "pcg_pupdate", 32.0 * N + 12.0 * N);
+                k_pcg1_pupdate<false><<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, cs.node_agg.p, cs.mode.p,
+                                                                          cs.e64.p, N, rz + it, rz + it + 1,
+                                                                          rr + it + 1, thr, it + 1, done, err);
+                count_launch(ctx);
+            } else {
                 ProfScope ps(ctx, "pcg_pupdate", 32.0 * N);
                 k_pcg_pupdate<<<g, kRedThreads, 0, ctx->stream>>>(p, r, s->dinv.p, N, rz + it, rz + it + 1,
                                                                   rr + it + 1, thr, it + 1, done, err);
+                count_launch(ctx, 2);
             }
-            count_launch(ctx, 2);
         }
         if ((it + 1) % check == 0 || it + 1 == max_iter) {
             int hf[2];
@@ -1386,9 +1471,11 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     const bool debug = std::getenv("SFC_DEBUG_SOLVER") != nullptr;
     const unsigned gw = (unsigned)(ctx->sm_count * 8);  // warp-per-row kernels: 8 warps/block
     const bool bsr = s->has_bsr;
-    const bool two = use_two_level(s);
-    const bool bj = bsr && (o.precond == SFC_PRECOND_BLOCK_JACOBI || two) && s->bdinv32.p;
+    const bool two_any = use_two_level(s);
     const CoarseSpace &crs = s->coarse;
+    const bool two = two_any && crs.dof == 3;   // block Jacobi + rigid-body modes
+    const bool two1 = two_any && crs.dof == 1;  // point Jacobi + constant modes (scalar mesh)
+    const bool bj = bsr && (o.precond == SFC_PRECOND_BLOCK_JACOBI || two) && s->bdinv32.p;
     // R = B - S X (FP64) and Q = S P (FP32), node-block kernels for 3-dof meshes
     auto resid = [&](const double *X, const double *Bm, double *R, double *out) {
         ProfScope ps(ctx, "resid64",
@@ -1424,6 +1511,14 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                                                                 crs.e32.p, s->nodes, nullptr, nullptr, nullptr,
                                                                 nullptr, nullptr, nullptr, restart.p, nullptr, nullptr,
                                                                 nullptr);
+        } else if (two1) {
+            k_binit32<V, false><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->dinv32.p, restart.p, rr32, xr, pp, N,
+                                                             rz_slot, rr_slot);
+            count_launch(ctx);
+            coarse_block_apply<V>(s, rr32, rz_slot, nullptr);
+            k_cbpupdate32<V, true><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, crs.node_agg.p, crs.mode.p,
+                                                                crs.e32.p, N, nullptr, nullptr, nullptr, nullptr,
+                                                                nullptr, nullptr, restart.p);
         } else if (bj)
             k_ninit32<V><<<gw, 256, 0, ctx->stream>>>(r64.p, scale, s->bdinv32.p, restart.p, rr32, xr, pp, s->nodes,
                                                       rz_slot, rr_slot);
@@ -1497,7 +1592,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                     k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
                                                                 rrs + o0, thr, rz + o1, rrs + o1, stop, err);
             }
-            if (two) coarse_block_apply<V>(s, rr32, rz + o1, stop);
+            if (two_any) coarse_block_apply<V>(s, rr32, rz + o1, stop);
             {
                 ProfScope ps(ctx, "bpupdate32", (bj ? 5.0 : 3.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
                 if (two)
@@ -1507,6 +1602,10 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                 else if (bj)
                     k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz + o0, rz + o1,
                                                                  rrs + o1, thr, stop, err, xr, pq + o0, rrs + o0);
+                else if (two1)
+                    k_cbpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, crs.node_agg.p,
+                                                                         crs.mode.p, crs.e32.p, N, rz + o0, rz + o1,
+                                                                         rrs + o1, thr, stop, err, nullptr);
                 else
                     k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
                                                                  thr, stop, err);
@@ -1619,7 +1718,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             count_launch(ctx);
             const double bn = std::sqrt(hb[c]), r = std::sqrt(rn[c]);
             if (r > tol * bn) {
-                PcgResult pr = pcg64(s, s->tmpN.p, s->tmpN2.p, tol * bn / r, max_iter, check, two);
+                PcgResult pr = pcg64(s, s->tmpN.p, s->tmpN2.p, tol * bn / r, max_iter, check, two_any);
                 if (!pr.converged) all_conv = false;
                 if (debug)
                     std::fprintf(stderr, "[sfc block %d] column %d: FP64 fallback from rel %.3e, %d iterations%s\n", c0,
@@ -1654,7 +1753,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     st.max_rel_residual = worst;
     st.converged = all_conv ? 1 : 0;
     st.fallback_columns = n_fallback;
-    st.coarse_dofs = two ? (int32_t)(crs.nc - crs.dropped) : 0;
+    st.coarse_dofs = two_any ? (int32_t)(crs.nc - crs.dropped) : 0;
 }
 
 }  // namespace

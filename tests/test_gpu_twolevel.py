@@ -137,23 +137,82 @@ def test_rebuilt_after_coefficient_change(ctx):
     assert np.abs(s.giveSolution() - u_ref).max() <= 1e-8 * np.abs(u_ref).max()
 
 
-def test_scalar_mesh_falls_back(ctx):
-    """Poisson (one dof per node) has no rigid-body coarse space: the solver
-    runs with its one-level preconditioner and reports no coarse dofs."""
-    rng = np.random.default_rng(2)
-    mesh = small_mesh(mg.HEX8_POISSON, 6)
-    coeff = coefficients(mesh, rng, mg.HEX8_POISSON)
-    gm = api.Mesh(ctx, mg.HEX8_POISSON, 8, mesh.coords, mesh.conn)
+SCALAR = [(mg.LINE2_POISSON, 200, "x"), (mg.TRI3_POISSON, 24, "all"), (mg.HEX8_POISSON, 10, "all")]
+
+
+def poisson_system(ctx, kind, n, faces, seed):
+    rng = np.random.default_rng(seed)
+    mesh = small_mesh(kind, n, rng, 0.2 if kind != mg.LINE2_POISSON else 0.0)
+    coeff = coefficients(mesh, rng, kind)
+    gm = api.Mesh(ctx, kind, QPS[kind], mesh.coords, mesh.conn)
     gm.set_coefficients(coeff)
     s = api.SystemSolveCuda(ctx, mesh.num_dofs)
     s.assemble(gm)
     s.assemble_load(gm, np.array([1.0]))
+    bc = mg.dirichlet_dofs(mesh, faces)
+    s.applyConstraints((bc, np.zeros(len(bc))))
+    rp, col, val, F = O.fem(mesh, QPS[kind], np.array([1.0]), bc, coeff=coeff)
+    return mesh, s, O.DirectSolver(rp, col, val), F
+
+
+@pytest.mark.parametrize("kind,n,faces", SCALAR)
+def test_scalar_two_level_forward_and_transpose(ctx, kind, n, faces):
+    """Scalar (Poisson) meshes: point Jacobi plus one constant mode per box
+    aggregate, in the FP64 PCG and in the mixed block solver."""
+    mesh, s, ds, F = poisson_system(ctx, kind, n, faces, 30 + kind)
+    u_ref = ds.solve(F)
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-12, precond=api.SFC_PRECOND_JACOBI)
+    s.solveSystem()
+    it_jacobi = s.last_stats()["iterations"]
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-12, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=4)
+    s.solveSystem()
+    st = s.last_stats()
+    assert st["converged"] == 1 and st["coarse_dofs"] > 0
+    assert np.abs(s.giveSolution() - u_ref).max() <= 1e-9 * np.abs(u_ref).max()
+    assert st["iterations"] < it_jacobi, (st["iterations"], it_jacobi)
+    rng = np.random.default_rng(5)
+    Rhs = rng.standard_normal((40, mesh.num_dofs))
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, inner_tol=1e-3, precond=api.SFC_PRECOND_TWO_LEVEL,
+                  coarse_size=4)
+    U = s.solveSystemTranspose(Rhs)
+    st = s.last_stats()
+    assert st["converged"] == 1 and st["coarse_dofs"] > 0 and st["max_rel_residual"] <= 1e-10
+    refs = np.stack([ds.solve_transpose(r) for r in Rhs])
+    assert np.abs(U - refs).max() <= 1e-7 * np.abs(refs).max()
+
+
+def test_scalar_coarse_size_matches_oracle_boxes(ctx):
+    from oracle import coarse_ref as C
+    mesh, s, ds, F = poisson_system(ctx, mg.HEX8_POISSON, 12, "all", 41)
+    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-10, precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=3)
+    s.solveSystem()
+    agg, _ = C.box_aggregates(mesh.coords, 3, max_aggs=2048)
+    assert s.last_stats()["coarse_dofs"] == int(agg.max()) + 1
+
+
+def test_triplet_system_has_no_coarse_space(ctx):
+    """A system assembled from element triplets (no mesh attached) has no
+    aggregates: the solver runs its one-level preconditioner and reports no
+    coarse dofs."""
+    rng = np.random.default_rng(2)
+    kind = mg.TRI3_POISSON
+    mesh = small_mesh(kind, 8, rng, 0.2)
+    coeff = coefficients(mesh, rng, kind)
+    s = api.SystemSolveCuda(ctx, mesh.num_dofs)
+    for e in range(mesh.num_elems):
+        Ke = O.element_matrix(kind, QPS[kind], mesh.coords[mesh.conn[e]], coeff[e], 0.3)
+        dofs = mesh.conn[e].astype(np.int64)
+        s.insertToMatrix(Ke, dofs, dofs)
+        s.insertToRhs(np.full(len(dofs), 0.25), dofs)
+    s.finishAssembly()
     bc = mg.dirichlet_dofs(mesh, "all")
     s.applyConstraints((bc, np.zeros(len(bc))))
     s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, precond=api.SFC_PRECOND_TWO_LEVEL)
     s.solveSystem()
     st = s.last_stats()
-    rp, col, val, F = O.fem(mesh, 8, np.array([1.0]), bc, coeff=coeff)
+    rp, col, val = O.assemble_csr(mesh, QPS[kind], coeff=coeff, nu=0.3)
+    F = 0.25 * np.bincount(mesh.conn.ravel(), minlength=mesh.num_nodes).astype(np.float64)
+    O.apply_constraints(rp, col, val, F, bc)
     u_ref = O.DirectSolver(rp, col, val).solve(F)
     assert st["coarse_dofs"] == 0
     assert np.abs(s.giveSolution() - u_ref).max() <= 1e-8 * np.abs(u_ref).max()
