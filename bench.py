@@ -361,7 +361,8 @@ def run_learned(args, ws, rank, local):
     --c5-train-n^3 grid (the network is local, so it transfers across grid
     sizes), then every held-out 128^3 sample is solved to the true relative
     residual 1e-8 by flexible CG with the network and by plain FP64
-    Jacobi-PCG; value = held-out solves/s of the learned method."""
+    Jacobi-PCG, and (for reference) by FP64 PCG with the two-level
+    preconditioner; value = held-out solves/s of the learned method."""
     from statfem_b200 import api
     from statfem_b200 import learned as L
     ctx = api.Context(local)
@@ -381,12 +382,19 @@ def run_learned(args, ws, rank, local):
         s.solveSystem()
         sp = s.last_stats()
         u_pcg = s.giveSolution()
+        # the classical reference arm: the same FP64 PCG with the two-level
+        # preconditioner (point Jacobi + one constant per box aggregate)
+        s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=50000, check_every=32,
+                      precond=api.SFC_PRECOND_TWO_LEVEL)
+        s.solveSystem()
+        st2 = s.last_stats()
+        d2 = float(np.abs(s.giveSolution() - u_pcg).max() / np.abs(u_pcg).max())
         s.set_options(method=api.SFC_SOLVER_FCG_MPNN, tol=1e-8, max_iter=50000, check_every=8)
         s.solveSystem()
         sf = s.last_stats()
         u = s.giveSolution()
         if k >= args.warmup:
-            rows.append((sp, sf, float(np.abs(u - u_pcg).max() / np.abs(u_pcg).max())))
+            rows.append((sp, sf, float(np.abs(u - u_pcg).max() / np.abs(u_pcg).max()), st2, d2))
     pcg_ms = max_over_ranks(ws, sum(r[0]["device_ms"] for r in rows))
     fcg_ms = max_over_ranks(ws, sum(r[1]["device_ms"] for r in rows))
     n = len(rows)
@@ -406,6 +414,11 @@ def run_learned(args, ws, rank, local):
         "plain_pcg": {"value": round(ws * n / (pcg_ms / 1e3), 4), "unit": "solves/s",
                       "ms_per_step": round(pcg_ms / n, 2),
                       "iterations_mean": float(np.mean([r[0]["iterations"] for r in rows]))},
+        "two_level_pcg": {"value": round(ws * n / (max_over_ranks(ws, sum(r[3]["device_ms"] for r in rows)) / 1e3), 4),
+                          "unit": "solves/s",
+                          "iterations_mean": float(np.mean([r[3]["iterations"] for r in rows])),
+                          "coarse_dofs": int(rows[0][3]["coarse_dofs"]) if rows else 0,
+                          "max_rel_diff_vs_pcg": max(r[4] for r in rows) if rows else None},
         "learned": {"iterations_mean": float(np.mean([r[1]["iterations"] for r in rows])),
                     "max_rel_residual": max(r[1]["max_rel_residual"] for r in rows),
                     "max_rel_diff_vs_pcg": max(r[2] for r in rows)},
