@@ -23,10 +23,13 @@
 //  * k_coarse_apply32: e = A_c^+ c (FP32, dense nc x nc, L2-resident) and the
 //    coarse share c.e of each column's r.z, split over k across a cluster;
 //  * the p update (solvers.cu) adds z += P e on the fly from each node's
-//    aggregate id and centroid offset.
-// Setup per operator: the Galerkin product on the GPU (one CTA per
-// aggregate, FP64), then the inverse by block Gauss-Jordan elimination
-// (FP64, 32-wide panels) with dependent pivots dropped.
+//    aggregate id and centroid offset (k_ncpupdate32; k_cbpupdate32 on scalar
+//    meshes).
+// Setup per operator: the Galerkin product on the GPU (a cluster of CTAs per
+// aggregate, FP64, deterministic), then the inverse by block Gauss-Jordan
+// elimination (dense.cu: FP64, 32-wide panels, one CUDA graph) with dependent
+// pivots dropped.  Scalar meshes take one constant mode per aggregate, point
+// Jacobi as the smoother and the CSR operator in the Galerkin product.
 
 #include <algorithm>
 #include <cmath>
@@ -616,7 +619,8 @@ __global__ void __launch_bounds__(256) k_coarse_apply64(const double *__restrict
 // ---------------------------------------------------------------------------
 
 // Aggregates = the non-empty boxes of a grid laid over the mesh's bounding
-// box, about `size` nodes along each axis (at most kMaxAggs boxes).  The
+// box, about `size` nodes along each axis (about kMaxAggs boxes at most on
+// 3-dof meshes, kMaxAggs1 on scalar ones).  The
 // colour classes (box index mod 3 per axis) make the Galerkin product a
 // single pass; they need every element's nodes to lie in boxes at most one
 // apart per axis, which is checked over the connectivity (the grid is
@@ -774,7 +778,7 @@ static bool coarse_aggregate(sfc_system *s, int size)
 }
 
 // (Re)builds the coarse space for the current operator; false when the
-// system has none (not a 3-dof mesh, or no valid box grid).
+// system has none (no mesh attached, or no valid box grid).
 bool coarse_prepare(sfc_system *s)
 {
     CoarseSpace &cs = s->coarse;

@@ -201,7 +201,7 @@ void make_quadrature(int kind, int qps, QuadTable &t);
 
 // ---------------------------------------------------------------------------
 // coarse space of the two-level preconditioner (coarse.cu): rigid-body modes
-// of box aggregates on 3-dof meshes
+// (3-dof meshes) or the constant (scalar meshes) of box aggregates
 // ---------------------------------------------------------------------------
 struct sfc_mesh;
 namespace sfc {
