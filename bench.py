@@ -196,7 +196,7 @@ def precond_code(api, name):
 
 
 class GpuStatFEM:
-    def __init__(self, wl, device, method, block_width=128, precond=0, coarse_size=0):
+    def __init__(self, wl, device, method, block_width=128, precond=0, coarse_size=0, check_every=32):
         from statfem_b200 import api
         self.api = api
         self.wl = wl
@@ -209,7 +209,7 @@ class GpuStatFEM:
         self.precond = precond
         self.coarse_size = coarse_size
         self.s.set_options(method=method, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=block_width,
-                           check_every=32, precond=precond, coarse_size=coarse_size)
+                           check_every=check_every, precond=precond, coarse_size=coarse_size)
         self.cf = api.CovarianceForcing(self.ctx, self.gm)
         self.cf.applyConstraints(wl["bc"])
         self.fg = api.ForwardGaussRHS(self.s, self.cf, REG)
@@ -252,7 +252,8 @@ def run_ours(args, ws, rank, local):
     from statfem_b200 import api
     method = api.SFC_SOLVER_PCG_MIXED if args.method == "mixed" else api.SFC_SOLVER_PCG_FP64
     wl = make_workload(args.config, seed=1234 + rank, c2_n=args.c2_n)
-    g = GpuStatFEM(wl, local, method, args.block_width, precond_code(api, args.precond), args.coarse_size)
+    g = GpuStatFEM(wl, local, method, args.block_width, precond_code(api, args.precond), args.coarse_size,
+                   args.check_every)
     ctx = g.ctx
     for _ in range(args.warmup):
         g.step()
@@ -909,6 +910,8 @@ def main():
     ap.add_argument("--prof-steps", type=int, default=1)
     ap.add_argument("--block-width", type=int, default=128, choices=[32, 64, 128])
     ap.add_argument("--precond", default="two-level", choices=["jacobi", "block-jacobi", "two-level"])
+    ap.add_argument("--check-every", type=int, default=32,
+                    help="iterations between the solver's convergence checks (c1/c2)")
     ap.add_argument("--coarse-size", type=int, default=0,
                     help="two-level: nodes per aggregate along each axis (0: library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
