@@ -12,12 +12,13 @@ and that PCG with it reaches the direct solution.  Restated here:
   box, nodes assigned by floor of their scaled coordinate;
 * the six rigid-body modes of each aggregate (translations, rotations
   e_k x d about the centroid, d in units of the box edge), zero on
-  constrained dofs;
+  constrained dofs; on scalar meshes the aggregate's constant;
 * the Galerkin matrix A_c = P^T S P;
 * block Gauss-Jordan elimination without pivoting in 32-wide panels with a
   pivot dropped (row and column zeroed) when it is not above rel x its
   original diagonal;
-* M^-1 r = D^-1 r + P A_c^+ P^T r with D the nodal 3 x 3 diagonal blocks.
+* M^-1 r = D^-1 r + P A_c^+ P^T r with D the nodal 3 x 3 diagonal blocks
+  (the diagonal on scalar meshes).
 """
 from __future__ import annotations
 
@@ -112,24 +113,42 @@ def nodal_block_jacobi(S):
     return np.linalg.inv(D)
 
 
-class TwoLevel:
-    """M^-1 = D^-1 + P A_c^+ P^T for the symmetric eliminated operator S."""
+def constant_modes(agg, mask):
+    """P (num_nodes x n_agg) for scalar meshes: the indicator of each
+    aggregate, zero on constrained dofs."""
+    nodes = len(agg)
+    free = ~np.asarray(mask, dtype=bool)
+    i = np.nonzero(free)[0]
+    return sp.csr_matrix((np.ones(len(i)), (i, agg[i])), shape=(nodes, int(agg.max()) + 1))
 
-    def __init__(self, S, coords, mask, size=8, rel=1e-10):
+
+class TwoLevel:
+    """M^-1 = D^-1 + P A_c^+ P^T for the symmetric eliminated operator S:
+    nodal 3 x 3 block Jacobi and rigid-body modes (dof = 3), point Jacobi and
+    aggregate constants (dof = 1)."""
+
+    def __init__(self, S, coords, mask, size=8, rel=1e-10, dof=3):
         self.S = sp.csr_matrix(S)
-        agg, h = box_aggregates(coords, size)
-        self.P = rigid_modes(coords, agg, h, mask)
+        self.dof = dof
+        agg, h = box_aggregates(coords, size, max_aggs=512 if dof == 3 else 2048)
+        self.P = rigid_modes(coords, agg, h, mask) if dof == 3 else constant_modes(agg, mask)
         Ac = (self.P.T @ self.S @ self.P).toarray()
         self.Ac = Ac
         self.Ainv, self.pivots, self.dropped = gauss_jordan_inverse(Ac, rel)
-        self.Dinv = nodal_block_jacobi(self.S)
+        if dof == 3:
+            self.Dinv = nodal_block_jacobi(self.S)
+        else:
+            self.dinv = 1.0 / self.S.diagonal()
 
     @property
     def coarse_dofs(self):
         return self.Ac.shape[0] - self.dropped
 
     def __call__(self, r):
-        z = np.einsum('nij,nj->ni', self.Dinv, r.reshape(-1, 3)).ravel()
+        if self.dof == 3:
+            z = np.einsum('nij,nj->ni', self.Dinv, r.reshape(-1, 3)).ravel()
+        else:
+            z = self.dinv * r
         return z + self.P @ (self.Ainv @ (self.P.T @ r))
 
 

@@ -82,3 +82,30 @@ def test_fully_constrained_boxes_are_dropped():
     u_ref = O.DirectSolver(rp, col, val).solve(F)
     free = ~mask
     assert np.abs(x[free] - u_ref[free]).max() <= 1e-8 * np.abs(u_ref).max()
+
+
+def test_scalar_two_level_pcg_reaches_the_direct_solution():
+    """Poisson: point Jacobi plus one constant per box aggregate."""
+    rng = np.random.default_rng(5)
+    mesh = mg.unit_square_tri(24)
+    coeff = np.exp(0.5 * rng.standard_normal(mesh.num_elems))
+    bc = mg.dirichlet_dofs(mesh, "all")
+    rp, col, val, F = O.fem(mesh, 3, np.array([1.0]), bc, coeff=coeff)
+    N = mesh.num_dofs
+    A = sp.csr_matrix((val, col, rp), shape=(N, N)).tocoo()
+    mask = np.zeros(N, bool)
+    mask[bc] = True
+    keep = ~((mask[A.row] | mask[A.col]) & (A.row != A.col))
+    S = sp.csr_matrix((A.data[keep], (A.row[keep], A.col[keep])), shape=(N, N))
+    b = F.copy()
+    b[mask] = 0.0
+    M = C.TwoLevel(S, mesh.coords, mask, size=4, dof=1)
+    agg, _ = C.box_aggregates(mesh.coords, 4, max_aggs=2048)
+    assert M.Ac.shape[0] == int(agg.max()) + 1
+    x, it2 = C.pcg(S, b, M, tol=1e-10)
+    dinv = 1.0 / S.diagonal()
+    _, it1 = C.pcg(S, b, lambda r: dinv * r, tol=1e-10)
+    u_ref = O.DirectSolver(rp, col, val).solve(F)
+    free = ~mask
+    assert np.abs(x[free] - u_ref[free]).max() <= 1e-8 * np.abs(u_ref).max()
+    assert it2 < 0.7 * it1, (it2, it1)
