@@ -490,6 +490,19 @@ int32_t sfc_autotune_save(const char *path);
 int32_t sfc_autotune_load(const char *path);
 int32_t sfc_autotune_clear(void);
 
+/* ---- two-level preconditioner: the aggregation, on the host --------------- */
+/* No reference counterpart (the reference factorises directly).  The box
+ * aggregation that SFC_PRECOND_TWO_LEVEL builds for a mesh: a grid of about
+ * `size` nodes per axis (0: 8) over the nodes' bounding box, about max_aggs
+ * boxes at most (the library uses 512 on 3-dof meshes, 2048 on scalar ones),
+ * halved per axis until every element's nodes lie in boxes at most one apart;
+ * node_agg[num_nodes] receives each node's aggregate (non-empty boxes in box
+ * order), boxes_per_axis[3] (nullable) the final grid.  Needs no device.
+ * SFC_ERR_BAD_ARG when no grid satisfies the rule (degenerate input). */
+int32_t sfc_coarse_boxes(const double *coords, int64_t num_nodes, const uint32_t *conn, int64_t num_elems,
+                         int32_t nodes_per_elem, int32_t size, int32_t max_aggs, int32_t *node_agg,
+                         int32_t *num_aggs, int32_t *boxes_per_axis);
+
 #ifdef __cplusplus
 }
 #endif

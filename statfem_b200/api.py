@@ -181,6 +181,7 @@ SIGNATURES = {
     "sfc_autotune_save": (_i32, [ctypes.c_char_p]),
     "sfc_autotune_load": (_i32, [ctypes.c_char_p]),
     "sfc_autotune_clear": (_i32, []),
+    "sfc_coarse_boxes": (_i32, [_dp, _i64, _u32p, _i64, _i32, _i32, _i32, _i32p, _i32p, _i32p]),
 }
 
 _lib = None
@@ -818,6 +819,23 @@ def autotune_clear():
     load().sfc_autotune_clear()
 
 
+def coarse_boxes(coords, conn, size=8, max_aggs=512):
+    """The two-level preconditioner's box aggregation of a mesh (host only):
+    (aggregate per node, boxes per axis)."""
+    X = _arr(coords, np.float64).reshape(-1, 3)
+    C = _arr(conn, np.uint32)
+    C2 = C.reshape(C.shape[0], -1) if C.ndim == 2 else C.reshape(-1, 1)
+    agg = np.zeros(X.shape[0], dtype=np.int32)
+    nagg = ctypes.c_int32()
+    nb = np.zeros(3, dtype=np.int32)
+    rc = load().sfc_coarse_boxes(_p(X, _dp), X.shape[0], _p(C2, _u32p), C2.shape[0], C2.shape[1], int(size),
+                                 int(max_aggs), _p(agg, _i32p), ctypes.byref(nagg), _p(nb, _i32p))
+    if rc != 0:
+        raise SfcError(rc, "no box grid satisfies the one-box span rule")
+    return agg, nb
+
+
 __all__ = ["Context", "Mesh", "SystemSolveCuda", "CovarianceForcing", "ForwardGaussRHS", "LikelihoodKOH",
            "LearnedPreconditioner", "BatchStatFEM", "ForwardPerturbation", "SfcError", "SIGNATURES", "load", "meshgen", "SFC_SOLVER_PCG_FP64",
-           "SFC_SOLVER_PCG_MIXED", "SFC_SOLVER_FCG_MPNN", "autotune_save", "autotune_load", "autotune_clear"]
+           "SFC_SOLVER_PCG_MIXED", "SFC_SOLVER_FCG_MPNN", "autotune_save", "autotune_load", "autotune_clear",
+           "coarse_boxes"]

@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <new>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -618,6 +619,95 @@ __global__ void __launch_bounds__(256) k_coarse_apply64(const double *__restrict
 // host side
 // ---------------------------------------------------------------------------
 
+struct BoxGrid {
+    int nb[3] = {1, 1, 1};            // boxes per axis
+    double ext[3] = {0, 0, 0}, emax = 0.0;
+    int32_t nagg = 0;
+    std::vector<int32_t> node_agg;    // aggregate of each node
+    std::vector<int32_t> box_agg;     // aggregate of each box, -1 when empty
+};
+
+// Box grid over a node set: boxes per axis for about `size` nodes along each
+// axis (about max_aggs boxes at most), coarsened (halved per axis) until
+// every element's nodes lie in boxes at most one apart along each axis;
+// aggregates are the non-empty boxes numbered in box order.  Host only.
+bool box_aggregation(const double *X, int64_t nodes, const uint32_t *conn, int64_t num_elems, int nn, int size,
+                     int max_aggs, BoxGrid &g)
+{
+    double lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = INFINITY;
+        hi[d] = -INFINITY;
+    }
+    for (int64_t i = 0; i < nodes; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], X[3 * i + d]);
+            hi[d] = std::max(hi[d], X[3 * i + d]);
+        }
+    double emax = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        g.ext[d] = hi[d] - lo[d];
+        emax = std::max(emax, g.ext[d]);
+    }
+    g.emax = emax;
+    if (!(emax > 0.0)) return false;
+    const double *ext = g.ext;
+    int dim = 0;
+    double vol = 1.0;
+    for (int d = 0; d < 3; ++d)
+        if (ext[d] > 1e-12 * emax) {
+            ++dim;
+            vol *= ext[d];
+        }
+    const double per = std::pow((double)std::max(size, 2), dim);
+    const double target = std::min<double>(max_aggs, std::max(1.0, (double)nodes / per));
+    const double hb = std::pow(vol / target, 1.0 / dim);
+    int *nb = g.nb;
+    for (int d = 0; d < 3; ++d) nb[d] = ext[d] > 1e-12 * emax ? std::max(1, (int)std::lround(ext[d] / hb)) : 1;
+    std::vector<int32_t> box(nodes * 3);
+    bool ok = false;
+    for (int attempt = 0; attempt < 32 && !ok; ++attempt) {
+        for (int64_t i = 0; i < nodes; ++i)
+            for (int d = 0; d < 3; ++d) {
+                int b = ext[d] > 1e-12 * emax ? (int)std::floor((X[3 * i + d] - lo[d]) / ext[d] * nb[d]) : 0;
+                box[3 * i + d] = std::min(std::max(b, 0), nb[d] - 1);
+            }
+        ok = true;
+        for (int64_t e = 0; e < num_elems && ok; ++e)
+            for (int d = 0; d < 3 && ok; ++d) {
+                int bmin = INT32_MAX, bmax = INT32_MIN;
+                for (int k = 0; k < nn; ++k) {
+                    const uint32_t v = conn[(size_t)e * nn + k];
+                    if ((int64_t)v >= nodes) return false;
+                    const int b = box[3 * (int64_t)v + d];
+                    bmin = std::min(bmin, b);
+                    bmax = std::max(bmax, b);
+                }
+                if (bmax - bmin > 1) ok = false;
+            }
+        if (!ok) {
+            if (nb[0] == 1 && nb[1] == 1 && nb[2] == 1) break;
+            for (int d = 0; d < 3; ++d) nb[d] = std::max(1, nb[d] / 2);
+        }
+    }
+    if (!ok) return false;
+    const int64_t nboxes = (int64_t)nb[0] * nb[1] * nb[2];
+    g.box_agg.assign(nboxes, -1);
+    g.node_agg.resize(nodes);
+    int32_t nagg = 0;
+    for (int64_t i = 0; i < nodes; ++i) {
+        const int64_t id = box[3 * i] + (int64_t)nb[0] * (box[3 * i + 1] + (int64_t)nb[1] * box[3 * i + 2]);
+        g.box_agg[id] = 1;
+    }
+    for (int64_t id = 0; id < nboxes; ++id)  // aggregates in box order
+        if (g.box_agg[id] > 0) g.box_agg[id] = nagg++;
+        else g.box_agg[id] = -1;
+    for (int64_t i = 0; i < nodes; ++i)
+        g.node_agg[i] = g.box_agg[box[3 * i] + (int64_t)nb[0] * (box[3 * i + 1] + (int64_t)nb[1] * box[3 * i + 2])];
+    g.nagg = nagg;
+    return true;
+}
+
 // Aggregates = the non-empty boxes of a grid laid over the mesh's bounding
 // box, about `size` nodes along each axis (about kMaxAggs boxes at most on
 // 3-dof meshes, kMaxAggs1 on scalar ones).  The
@@ -641,81 +731,17 @@ static bool coarse_aggregate(sfc_system *s, int size)
     const int64_t nodes = m->num_nodes;
     const int max_aggs = dof == 3 ? kMaxAggs : kMaxAggs1;
     const double *X = m->h_coords.data();
-    double lo[3], hi[3];
-    for (int d = 0; d < 3; ++d) {
-        lo[d] = INFINITY;
-        hi[d] = -INFINITY;
-    }
-    for (int64_t i = 0; i < nodes; ++i)
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = std::min(lo[d], X[3 * i + d]);
-            hi[d] = std::max(hi[d], X[3 * i + d]);
-        }
-    double ext[3], emax = 0.0;
-    for (int d = 0; d < 3; ++d) {
-        ext[d] = hi[d] - lo[d];
-        emax = std::max(emax, ext[d]);
-    }
-    if (!(emax > 0.0)) return false;
-    int dim = 0;
-    double vol = 1.0;
-    for (int d = 0; d < 3; ++d)
-        if (ext[d] > 1e-12 * emax) {
-            ++dim;
-            vol *= ext[d];
-        }
-    const double per = std::pow((double)std::max(size, 2), dim);
-    const double target = std::min<double>(max_aggs, std::max(1.0, (double)nodes / per));
-    const double hb = std::pow(vol / target, 1.0 / dim);
-    int nb[3];
-    for (int d = 0; d < 3; ++d) nb[d] = ext[d] > 1e-12 * emax ? std::max(1, (int)std::lround(ext[d] / hb)) : 1;
     std::vector<uint32_t> conn((size_t)m->num_elems * m->nn);
     download(ctx, conn.data(), m->conn.p, conn.size());
-    std::vector<int32_t> box(nodes * 3);
-    bool ok = false;
-    for (int attempt = 0; attempt < 8 && !ok; ++attempt) {
-        for (int64_t i = 0; i < nodes; ++i)
-            for (int d = 0; d < 3; ++d) {
-                int b = ext[d] > 1e-12 * emax ? (int)std::floor((X[3 * i + d] - lo[d]) / ext[d] * nb[d]) : 0;
-                box[3 * i + d] = std::min(std::max(b, 0), nb[d] - 1);
-            }
-        ok = true;
-        for (int64_t e = 0; e < m->num_elems && ok; ++e)
-            for (int d = 0; d < 3 && ok; ++d) {
-                int bmin = INT32_MAX, bmax = INT32_MIN;
-                for (int k = 0; k < m->nn; ++k) {
-                    const int b = box[3 * (int64_t)conn[(size_t)e * m->nn + k] + d];
-                    bmin = std::min(bmin, b);
-                    bmax = std::max(bmax, b);
-                }
-                if (bmax - bmin > 1) ok = false;
-            }
-        if (!ok) {
-            if (nb[0] == 1 && nb[1] == 1 && nb[2] == 1) break;
-            for (int d = 0; d < 3; ++d) nb[d] = std::max(1, nb[d] / 2);
-        }
-    }
-    if (!ok) return false;
+    BoxGrid g;
+    if (!box_aggregation(X, nodes, conn.data(), m->num_elems, m->nn, size, max_aggs, g)) return false;
+    const int32_t nagg = g.nagg;
+    const int *nb = g.nb;
+    const double *ext = g.ext;
+    const double emax = g.emax;
+    const std::vector<int32_t> &node_agg = g.node_agg;
+    const std::vector<int32_t> &box_agg = g.box_agg;
     const int64_t nboxes = (int64_t)nb[0] * nb[1] * nb[2];
-    std::vector<int32_t> box_agg(nboxes, -1), count;
-    std::vector<int32_t> node_agg(nodes);
-    int32_t nagg = 0;
-    for (int64_t i = 0; i < nodes; ++i) {
-        const int64_t id = box[3 * i] + (int64_t)nb[0] * (box[3 * i + 1] + (int64_t)nb[1] * box[3 * i + 2]);
-        if (box_agg[id] < 0) box_agg[id] = nagg++;
-        node_agg[i] = box_agg[id];
-    }
-    // aggregates in box order (deterministic numbering)
-    {
-        int32_t next = 0;
-        std::vector<int32_t> remap(nagg, -1);
-        for (int64_t id = 0; id < nboxes; ++id)
-            if (box_agg[id] >= 0) {
-                remap[box_agg[id]] = next;
-                box_agg[id] = next++;
-            }
-        for (auto &a : node_agg) a = remap[a];
-    }
     std::vector<int32_t> agg_ptr(nagg + 1, 0), agg_nodes(nodes);
     for (int64_t i = 0; i < nodes; ++i) ++agg_ptr[node_agg[i] + 1];
     for (int32_t a = 0; a < nagg; ++a) agg_ptr[a + 1] += agg_ptr[a];
@@ -873,3 +899,27 @@ void coarse_vec_apply(sfc_system *s, const double *r, double *rz, const int *don
 }
 
 }  // namespace sfc
+
+// Host-only: the box aggregation of the two-level preconditioner for a node
+// set, without a device (for inspection and CPU tests of the grid rule).
+extern "C" int32_t sfc_coarse_boxes(const double *coords, int64_t num_nodes, const uint32_t *conn, int64_t num_elems,
+                                    int32_t nodes_per_elem, int32_t size, int32_t max_aggs, int32_t *node_agg,
+                                    int32_t *num_aggs, int32_t *boxes_per_axis)
+{
+    if (!coords || num_nodes <= 0 || !node_agg || !num_aggs || max_aggs < 1 ||
+        (num_elems > 0 && (!conn || nodes_per_elem < 1)) || num_elems < 0)
+        return SFC_ERR_BAD_ARG;
+    try {
+        sfc::BoxGrid g;
+        if (!sfc::box_aggregation(coords, num_nodes, conn, num_elems, nodes_per_elem, size > 0 ? size : 8, max_aggs,
+                                  g))
+            return SFC_ERR_BAD_ARG;
+        std::copy(g.node_agg.begin(), g.node_agg.end(), node_agg);
+        *num_aggs = g.nagg;
+        if (boxes_per_axis)
+            for (int d = 0; d < 3; ++d) boxes_per_axis[d] = g.nb[d];
+        return SFC_OK;
+    } catch (const std::bad_alloc &) {
+        return SFC_ERR_NO_MEMORY;
+    }
+}

@@ -109,3 +109,43 @@ def test_scalar_two_level_pcg_reaches_the_direct_solution():
     free = ~mask
     assert np.abs(x[free] - u_ref[free]).max() <= 1e-8 * np.abs(u_ref).max()
     assert it2 < 0.7 * it1, (it2, it1)
+
+
+# ---- the library's host-side aggregation (no device needed) ----------------
+import pytest  # noqa: E402
+
+from statfem_b200 import api  # noqa: E402
+
+
+@pytest.mark.parametrize("mesh,size,max_aggs", [
+    (mg.unit_cube_hex(12, mg.HEX8_ELASTIC), 4, 512),
+    (mg.unit_cube_hex(12, mg.HEX8_POISSON), 3, 2048),
+    (mg.unit_square_tri(24), 4, 2048),
+    (mg.bar(200), 4, 2048),
+])
+def test_library_boxes_match_the_oracle(mesh, size, max_aggs):
+    agg, nb = api.coarse_boxes(mesh.coords, mesh.conn, size=size, max_aggs=max_aggs)
+    ref, _ = C.box_aggregates(mesh.coords, size, max_aggs=max_aggs)
+    assert np.array_equal(agg, ref)
+
+
+def test_boxes_coarsen_until_every_element_spans_one_box():
+    """A graded bar whose last element is longer than the boxes: the grid is
+    halved until no element reaches past a neighbouring box."""
+    x = np.concatenate([np.linspace(0.0, 0.1, 41), [1.0]])
+    coords = np.zeros((len(x), 3))
+    coords[:, 0] = x
+    conn = np.stack([np.arange(len(x) - 1), np.arange(1, len(x))], axis=1).astype(np.uint32)
+    agg, nb = api.coarse_boxes(coords, conn, size=2, max_aggs=2048)
+    first = int(np.rint(1.0 / (1.0 / min(2048, len(x) / 2.0))))  # the grid before coarsening
+    assert nb[0] < first and nb[1] == nb[2] == 1
+    box = np.minimum(np.floor(x * nb[0]).astype(int), nb[0] - 1)
+    assert np.all(np.abs(box[conn[:, 0]] - box[conn[:, 1]]) <= 1)
+    assert agg.max() + 1 == len(np.unique(box))
+
+
+def test_boxes_reject_a_degenerate_node_set():
+    coords = np.zeros((4, 3))
+    conn = np.array([[0, 1], [2, 3]], dtype=np.uint32)
+    with pytest.raises(api.SfcError):
+        api.coarse_boxes(coords, conn)
