@@ -346,21 +346,6 @@ __device__ void trsm_lower(int n, const double *L, int ldl, int m, double *B, in
     }
 }
 
-// B = L^-T B (back substitution with the transpose)
-__device__ void trsm_lower_t(int n, const double *L, int ldl, int m, double *B, int ldb)
-{
-    for (int k = n - 1; k >= 0; --k) {
-        const double d = L[(int64_t)k * ldl + k];
-        for (int c = threadIdx.x; c < m; c += blockDim.x) B[(int64_t)k * ldb + c] /= d;
-        __syncthreads();
-        for (int64_t t = threadIdx.x; t < (int64_t)k * m; t += blockDim.x) {
-            const int i = (int)(t / m), c = (int)(t % m);
-            B[(int64_t)i * ldb + c] -= L[(int64_t)k * ldl + i] * B[(int64_t)k * ldb + c];
-        }
-        __syncthreads();
-    }
-}
-
 // MismatchCovariance::giveCovariance (statX/infer/MismatchCovariance.hpp:76-99)
 __device__ void mismatch_cov(int ns, const double *xs, int dim, double sd, double ld, double eps, double *K)
 {
@@ -509,12 +494,6 @@ __global__ void __launch_bounds__(1024) k_koh_loglik_terms(int ns, int n_o, cons
         *out = n_o * (-0.5 * ns * log(2. * M_PI) - 0.5 * logdet) + t3;
         if (!ok) *info = -1;
     }
-}
-
-__global__ void k_lincomb(double *__restrict__ y, double a, const double *__restrict__ x, double b, int64_t n)
-{
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
-        y[t] = a * x[t] + b * y[t];
 }
 
 __global__ void k_identity_minus(double *__restrict__ D, int64_t n)
