@@ -37,41 +37,11 @@ sys.path.insert(0, ROOT)
 
 from statfem_b200 import meshgen as mg  # noqa: E402
 
-HP = {"forcing.sigma": 0.05, "forcing.length": 0.3, "rho": 1.0, "mismatch.sigma": 0.0,
-      "mismatch.length": 0.25, "mismatch.sensorEps": 1e-4}
-REG = 0.001
+from statfem_b200.workloads import C2_HP as HP  # noqa: E402
+from statfem_b200.workloads import C3_HP, REG, make_batch_workload, make_workload, subset_batch  # noqa: E402
 
-
-def make_workload(config, seed, c2_n=48):
-    rng = np.random.default_rng(seed)
-    if config == "c2":
-        n, ns = c2_n, 256
-        mesh = mg.unit_cube_hex(n, mg.HEX8_ELASTIC)
-        ax = mg.cell_centre_axes(n)
-        g = mg.se_field_tensor(rng, [ax, ax, ax], 0.3, 0.25)
-        coeff = np.exp(g)
-        bc = mg.dirichlet_dofs(mesh, "x0")
-        pts = mg.interior_points(rng, ns, 3, margin=0.02)
-        comps = np.arange(ns) % 3
-        P = mg.projection_matrix(mesh, pts, comps)
-        f = np.array([0.0, 0.0, -1.0])
-        hp = dict(HP)
-        desc = "3-D elasticity statFEM, %d^3 hex8 (%d dofs), 256 sensors, rel. residual 1e-8" % (n, mesh.num_dofs)
-        qps = 8
-    elif config == "c1":
-        n, ns = 64, 16
-        mesh = mg.unit_square_tri(n)
-        coeff = np.ones(mesh.num_elems)
-        bc = mg.dirichlet_dofs(mesh, "all")
-        pts = mg.interior_points(rng, ns, 2, margin=0.02)
-        P = mg.projection_matrix(mesh, pts)
-        f = np.array([1.0])
-        hp = dict(HP, **{"forcing.sigma": 0.1, "forcing.length": 0.2, "mismatch.sensorEps": 1e-3})
-        desc = "2-D Poisson statFEM, 64^2 cells x 2 P1 triangles (4,225 dofs), 16 sensors, rel. residual 1e-8"
-        qps = 3
-    else:
-        raise SystemExit("unknown config " + config)
-    return dict(mesh=mesh, coeff=coeff, bc=bc, pts=pts, P=P, f=f, hp=hp, desc=desc, qps=qps, ns=ns, rng=rng)
+# the headline metric, verbatim
+METRIC = "posterior solves/s at rel. residual 1e-8, learned+batched vs plain PCG, 1xB200"
 
 
 class ClockSampler:
@@ -144,6 +114,24 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def relaunch_if_needed(args):
+    """`--gpus N` without a launcher: start N ranks (one process per GPU) with
+    torch.distributed.run on this node and return its exit status; with a
+    launcher, WORLD_SIZE must equal N."""
+    ws = os.environ.get("WORLD_SIZE")
+    if ws is None and args.gpus > 1:
+        import socket
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            port = s.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        return subprocess.call(cmd)
+    if ws is not None and int(ws) != args.gpus:
+        raise SystemExit("--gpus %d but WORLD_SIZE=%s" % (args.gpus, ws))
+    return None
 
 
 def dist_setup():
@@ -325,7 +313,7 @@ def run_ours(args, ws, rank, local):
                 "launches": cnt, "share_of_step": round(tms / max(prof_ms, 1e-9), 4),
                 "timed_over": "%d profiled steps after the timed region" % args.prof_steps}
     out = {
-        "metric": "posterior solves/s at rel. residual 1e-8 (learned+batched vs plain PCG, 1xB200)",
+        "metric": METRIC,
         "value": round(value, 4), "unit": "posterior solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals)",
@@ -346,8 +334,10 @@ def run_ours(args, ws, rank, local):
         "clocks": clk.summary(),
         "loglik": ll,
     }
-    if args.plain_sample > 0 and args.method == "mixed":
-        out["plain_fp64"] = plain_fp64_estimate(g, wl, ms / args.steps, block_stats, stats_fwd, args.plain_sample)
+    if rank == 0 and args.config == "c2" and args.c2_n == 48:
+        out["accuracy_vs_fp64_oracle"] = accuracy_vs_oracle(g, wl)
+    if not args.no_plain and args.plain_sample > 0 and args.method == "mixed":
+        out["plain_fp64"] = plain_fp64_measured(g, wl)
         out["speedup_vs_plain_fp64"] = round(out["value"] / ws / out["plain_fp64"]["value"], 2)
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, wl, g, sample_iters=args.cpu_iters)
@@ -434,8 +424,6 @@ def run_learned(args, ws, rank, local):
         print(json.dumps(out))
 
 
-C3_HP = {"forcing.sigma": 0.1, "forcing.length": 0.2, "rho": 1.0, "mismatch.sigma": 0.0,
-         "mismatch.length": 0.2, "mismatch.sensorEps": 1e-3}
 # algorithmic bytes of one FP32 block-PCG inner iteration per dof, 32 columns:
 # CSR row (7 nnz x 8 B + 4 B), p gather and own row 2 x 128, q write 128,
 # update (x, r, p, q read, x, r write, dinv) 6 x 128 + 4, p update (p, r read,
@@ -443,39 +431,17 @@ C3_HP = {"forcing.sigma": 0.1, "forcing.length": 0.2, "rho": 1.0, "mismatch.sigm
 C3_BYTES_PER_DOF_ITER = 60 + 256 + 128 + 772 + 388
 
 
-def make_batch_workload(seed, n_inst=512, smin=32, smax=256, ns=32):
-    """Config 3: n_inst 2-D Poisson statFEM instances, side s ~ U{smin..smax}
-    cells, P1 triangles, log-conductivity squared-exponential (sigma 0.5,
-    length ~ U[0.05, 0.5]) sampled exactly on the cell-centre grid (both
-    triangles of a cell share the value), ns sensors at seeded interior
-    points, forcing GP sigma_f 0.1 length 0.2, sensor noise 1e-3."""
-    rng = np.random.default_rng(seed)
-    sides = rng.integers(smin, smax + 1, n_inst)
-    meshes, coeffs, bcs, sensors = [], [], [], []
-    for s in sides:
-        s = int(s)
-        mesh = mg.unit_square_tri(s)
-        ax = mg.cell_centre_axes(s)
-        g = mg.se_field_tensor(rng, [ax, ax], 0.5, rng.uniform(0.05, 0.5))
-        coeffs.append(np.repeat(np.exp(g), 2))
-        pts = mg.interior_points(rng, ns, 2, margin=0.02)
-        sensors.append((mg.projection_matrix(mesh, pts), pts))
-        bcs.append(mg.dirichlet_dofs(mesh, "all"))
-        meshes.append(mesh)
-    union, off = mg.disjoint_union(meshes)
-    bc = np.concatenate([b + off[k] for k, b in enumerate(bcs)])
-    return dict(sides=sides, meshes=meshes, coeff=np.concatenate(coeffs), coeffs=coeffs, bcs=bcs,
-                sensors=sensors, union=union, off=off, bc=bc, ns=ns, rng=rng,
-                desc="%d 2-D Poisson statFEM instances, sides U{%d..%d} (P1 triangles, %d dofs in total), "
-                     "%d sensors each, log-likelihood + posterior at the sensors, rel. residual 1e-8"
-                     % (n_inst, smin, smax, int(off[-1]), ns))
-
-
 def run_batch(args, ws, rank, local):
     """Config 3 on our GPU path: every step assembles all instances and runs
     the persistent batch kernel (CUDA graph)."""
     from statfem_b200 import api
-    wl = make_batch_workload(4321 + rank, n_inst=args.c3_instances, smin=args.c3_sides[0], smax=args.c3_sides[1])
+    from statfem_b200 import shard
+    full_wl = make_batch_workload(4321, n_inst=args.c3_instances, smin=args.c3_sides[0], smax=args.c3_sides[1])
+    n_total = len(full_wl["sides"])
+    # one batch split over the ranks: each takes a cost-balanced share of the
+    # instances; the per-instance results are all-gathered every step
+    parts = shard.partition(shard.instance_costs(full_wl["sides"]), ws)
+    wl = subset_batch(full_wl, parts[rank]) if ws > 1 else full_wl
     n = len(wl["sides"])
     ctx = api.Context(local)
     t0 = time.perf_counter()
@@ -505,10 +471,19 @@ def run_batch(args, ws, rank, local):
     barrier(ws)
     cuda_sync(ws)
     l0 = ctx.kernel_launches()
+
+    def gathered():
+        r = b.results()
+        if ws == 1:
+            return r
+        return shard.gather({k: r[k] for k in ("loglik", "post_mean", "post_cov", "status")}, parts, n_total)
+
     with ClockSampler(local) as clk:
         ctx.mark(0)
         for _ in range(args.steps):
             b.run()
+            if ws > 1:
+                gathered()
         ctx.mark(1)
         ctx.synchronize()
     cuda_sync(ws)
@@ -516,6 +491,7 @@ def run_batch(args, ws, rank, local):
     ms = max_over_ranks(ws, ctx.marker_ms(0, 1))
     launches = ctx.kernel_launches() - l0
     res = b.results()
+    status_all = gathered()["status"]
     # phase split and the persistent kernel's own time (one profiled step)
     ctx.set_profiling(True)
     b.run()
@@ -541,19 +517,20 @@ def run_batch(args, ws, rank, local):
     e2e_ms = max_over_ranks(ws, ctx.marker_ms(2, 3))
     h2d = wl["coeff"].nbytes + Y.nbytes
     d2h = 8 * n * (1 + 32 + 32 * 32 + 32 + 32 * 32) + 8 * n
-    value = ws * n * args.steps / (ms / 1e3)
+    value = n_total * args.steps / (ms / 1e3)
     cs, grid = b.launch_shape()
     out = {
         "metric": "posterior solves/s at rel. residual 1e-8 (batched instances, 1xB200)",
         "value": round(value, 3), "unit": "posterior solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 2), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
+        "scaling": "strong", "vs_baseline": None,
         "dtype": "f64 (FP32 inner PCG iterations, FP64 residuals, covariance and Cholesky)",
         "data": "synthetic (seeded)",
-        "config": {"workload": wl["desc"], "cluster_size": cs, "grid_ctas": grid,
-                   "parallelism": "replicas" if ws > 1 else "single GPU",
+        "config": {"workload": full_wl["desc"], "cluster_size": cs, "grid_ctas": grid,
+                   "parallelism": ("instances split over %d ranks (cost-balanced), results all-gathered every step"
+                                   % ws) if ws > 1 else "single GPU",
                    "l2": "inputs larger than L2 (solver vectors 17 GB)"},
-        "e2e": {"value": round(ws * n * args.steps / (e2e_ms / 1e3), 3), "unit": "posterior solves/s",
+        "e2e": {"value": round(n_total * args.steps / (e2e_ms / 1e3), 3), "unit": "posterior solves/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "roofline": {"kernel": "k_batch (persistent)", "bound": "hbm", "achieved": round(achieved, 1),
@@ -564,7 +541,7 @@ def run_batch(args, ws, rank, local):
                                           % C3_BYTES_PER_DOF_ITER},
         "phases_ms_per_step": {"assembly": round(asm_ms, 2), "solve_likelihood_kernel": round(kern_ms, 2)},
         "iterations": {"mean": float(res["iterations"].mean()), "max": int(res["iterations"].max())},
-        "status_ok": int((res["status"] == 0).sum()),
+        "status_ok": int((status_all == 0).sum()),
         "setup_s": round(setup_s, 1),
         "clocks": clk.summary(),
     }
@@ -750,73 +727,150 @@ def run_multi(args, ws, rank, local):
         print(json.dumps(out))
 
 
-def plain_fp64_estimate(g, wl, step_ms, block_stats, fwd_stats, sample):
-    """Posterior solves/s of the plain method on the same GPU: FP64 Jacobi-PCG,
-    one right-hand side at a time.  The forward solve is measured in full;
-    `sample` of the ns adjoint solves are measured and scaled to ns; the
-    non-solve part of the step (assembly, covariance, likelihood, posterior)
-    is taken from the mixed run's step."""
-    from statfem_b200 import api
+def accuracy_vs_oracle(g, wl):
+    """Relative errors of one posterior step against the committed FP64
+    oracle fixture of the 48^3 elasticity workload (tests/golden/
+    c2_oracle.npz: the oracle's Jacobi-PCG to 1e-13 with its own readings;
+    made by tests/golden/make_c2_oracle.py).  Only the fixture's arrays are
+    read here; the oracle itself does not run.  None when the fixture is
+    absent or was made from other inputs."""
+    from statfem_b200.workloads import fingerprint
+    path = os.path.join(ROOT, "tests", "golden", "c2_oracle.npz")
+    if not os.path.exists(path):
+        return None
+    f = np.load(path)
+    if not np.allclose(f["fingerprint"], fingerprint(wl), rtol=1e-12, atol=0):
+        return None
     ns = wl["ns"]
-    ip, ix, dv = wl["P"]
-    rows = np.zeros((sample, wl["mesh"].num_dofs))
-    pick = np.linspace(0, ns - 1, sample).astype(int)
-    for k, a in enumerate(pick):
-        rows[k, ix[ip[a]:ip[a + 1]]] = dv[ip[a]:ip[a + 1]]
-    g.s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=30000, check_every=32)
-    g.s.solveSystem()
-    plain_fwd = g.s.last_stats()
-    g.s.solveSystemTranspose(rows)
+    iu = np.triu_indices(ns)
+
+    def sym(u):
+        M = np.zeros((ns, ns))
+        M[iu] = u
+        return M + np.triu(M, 1).T
+
+    def rel(a, b):
+        return float(np.abs(a - b).max() / np.abs(b).max())
+
+    g.koh.setSensorValues(f["Y"])
+    ll, pm, pc = g.step()
+    out = {"prior_mean": rel(g.fg.giveProjectedMeanU(), f["mean_s"]),
+           "prior_cov": rel(g.fg.giveProjectedCovarU(), sym(f["C_s_upper"])),
+           "posterior_mean": rel(pm, f["post_mean"]), "posterior_cov": rel(pc, sym(f["post_cov_upper"])),
+           "loglik": abs(ll - float(f["loglik"])) / abs(float(f["loglik"])),
+           "oracle": "FP64 Jacobi-PCG to rel. residual 1e-13 (forward + 256 adjoint solves), Kronecker C_f, "
+                     "numpy LikelihoodKOH; oracle's own change from 1e-11 to 1e-13: %.1e"
+                     % float(f["est_rel_change_1e11_to_1e13"].max())}
+    out["max"] = max(out[k] for k in ("prior_mean", "prior_cov", "posterior_mean", "posterior_cov"))
+    g.koh.setSensorValues(g.Y)
+    return out
+
+
+def plain_fp64_measured(g, wl):
+    """Posterior solves/s of the plain method on the same GPU, measured on one
+    whole step: FP64 Jacobi-PCG for the forward solve and for each of the ns
+    adjoint solves (one right-hand side at a time), then the same covariance,
+    likelihood and posterior as the timed step."""
+    from statfem_b200 import api
+    keep = g.s.get_options()
+    g.s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=30000, check_every=32,
+                    precond=api.SFC_PRECOND_JACOBI)
+    g.ctx.synchronize()
+    g.ctx.mark(6)
+    g.step()
+    g.ctx.mark(7)
+    g.ctx.synchronize()
+    ms = g.ctx.marker_ms(6, 7)
     st = g.s.last_stats()
-    g.s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-8, max_iter=30000, inner_tol=1e-4, block_width=g.block_width,
-                    check_every=32, precond=g.precond, coarse_size=g.coarse_size)
-    other_ms = max(0.0, step_ms - block_stats["device_ms"] - fwd_stats["device_ms"])
-    plain_ms = plain_fwd["device_ms"] + st["device_ms"] * ns / sample + other_ms
-    return {"value": round(1e3 / plain_ms, 5), "unit": "posterior solves/s", "ms_per_step": round(plain_ms, 1),
-            "sample": "FP64 Jacobi-PCG one RHS at a time: forward solve measured (%d it), %d of %d adjoint "
-                      "solves measured (%.1f ms, max %d it) and scaled; non-solve work from the timed step"
-                      % (plain_fwd["iterations"], sample, ns, st["device_ms"], st["iterations"])}
+    g.s.set_options(**keep)
+    return {"value": round(1e3 / ms, 5), "unit": "posterior solves/s", "ms_per_step": round(ms, 1),
+            "sample": "measured: one whole posterior step with FP64 Jacobi-PCG (forward solve and %d adjoint "
+                      "solves one right-hand side at a time, max %d iterations per solve)"
+                      % (wl["ns"], st["iterations"])}
 
 
 # ---------------------------------------------------------------------------
 # CPU arms (oracle port)
 # ---------------------------------------------------------------------------
-def cpu_solve_rate(wl, rp, col, val, mask, F, iters_per_solve, sample_iters):
-    """Posterior solves/s of the CPU path, from a bounded sample: the time of
-    `sample_iters` FP64 Jacobi-PCG iterations on the full matrix, times
-    (1 + ns) solves of `iters_per_solve` iterations."""
+CPU_BLOCK = 32  # right-hand sides per CPU block-PCG pass
+
+
+def cpu_setup(wl, rp, col, val, F):
+    """One-off CPU measurements for the posterior-solve model of the CPU path
+    (oracle C restatement, FP64 Jacobi-PCG on all host cores):
+    * assembly: the oracle's element loop + triplet merge on the mesh with
+      half the elements per side, scaled by the element count;
+    * forward solve: A u = F solved in full to the relative residual 1e-8;
+    * covariance: C_s = R C_f R^T through the forcing covariance's Kronecker
+      factors (numpy), in full, on ns unit-norm rows standing in for R."""
     from oracle import oracle as O
+    mesh = wl["mesh"]
+    N = mesh.num_dofs
+    mask = np.zeros(N, dtype=np.uint8)
+    mask[wl["bc"]] = 1
+    n = mesh.grid[0]
+    half = max(2, n // 2)
+    sub = (mg.unit_cube_hex(half, mesh.kind) if mesh.dim == 3 else mg.unit_square_tri(half))
+    sub_coeff = np.ones(sub.num_elems)
     t0 = time.perf_counter()
-    O.pcg(rp, col, val, mask, F, tol=1e-300, max_iter=sample_iters)
-    dt = time.perf_counter() - t0
-    per_iter = dt / sample_iters
-    per_posterior = (1 + wl["ns"]) * iters_per_solve * per_iter
-    return 1.0 / per_posterior, per_iter
+    O.fem(sub, wl["qps"], wl["f"], mg.dirichlet_dofs(sub, "x0" if mesh.dof == 3 else "all"), coeff=sub_coeff, nu=0.3)
+    t_asm = (time.perf_counter() - t0) * mesh.num_elems / sub.num_elems
+    t0 = time.perf_counter()
+    x, its = O.pcg(rp, col, val, mask, F, tol=1e-8, max_iter=60000)
+    t_fwd = time.perf_counter() - t0
+    phibar = O.unit_load(mesh, wl["qps"], wl["bc"])
+    Pd = mg.projection_dense(mesh, *wl["P"])
+    hp = wl["hp"]
+    t0 = time.perf_counter()
+    O.forward_gauss_rhs_grid(Pd, F, Pd, mesh, phibar, hp["forcing.sigma"], hp["forcing.length"], REG)
+    t_cov = time.perf_counter() - t0
+    return dict(mask=mask, Pd=Pd, t_asm=t_asm, t_fwd=t_fwd, fwd_its=int(its), t_cov=t_cov, half=half)
+
+
+def cpu_adjoint_sample(rp, col, val, setup, sample_iters):
+    """Seconds per block-PCG iteration over CPU_BLOCK adjoint right-hand sides
+    (the first CPU_BLOCK sensor rows), timed over sample_iters iterations."""
+    from oracle import oracle as O
+    B = setup["Pd"][:CPU_BLOCK]
+    t0 = time.perf_counter()
+    O.block_pcg(rp, col, val, setup["mask"], B, 1e-300, max_iter=sample_iters)
+    return (time.perf_counter() - t0) / sample_iters
+
+
+def cpu_posterior_seconds(wl, setup, per_block_iter):
+    """assembly + forward solve + ceil(ns / CPU_BLOCK) adjoint blocks of the
+    forward solve's iteration count + covariance."""
+    blocks = -(-wl["ns"] // CPU_BLOCK)
+    return setup["t_asm"] + setup["t_fwd"] + blocks * setup["fwd_its"] * per_block_iter + setup["t_cov"]
+
+
+def cpu_sample_text(wl, setup, per_block_iter, sample_iters, threads):
+    return ("oracle C restatement, FP64 Jacobi-PCG, OpenMP on %d host threads: forward solve to 1e-8 measured "
+            "in full (%d iterations, %.1f s); adjoint solves as %d blocks of %d right-hand sides at %.1f ms "
+            "per block iteration (%d iterations timed) x %d iterations; C_s through the Kronecker factors "
+            "measured in full (%.1f s); assembly measured on the %d^%d mesh and scaled by elements (%.1f s)"
+            % (threads, setup["fwd_its"], setup["t_fwd"], -(-wl["ns"] // CPU_BLOCK), CPU_BLOCK,
+               per_block_iter * 1e3, sample_iters, setup["fwd_its"], setup["t_cov"], setup["half"],
+               wl["mesh"].dim, setup["t_asm"]))
+
+
+def host_threads():
+    try:
+        return int(os.environ.get("OMP_NUM_THREADS") or len(os.sched_getaffinity(0)))
+    except (AttributeError, ValueError):
+        return os.cpu_count() or 1
 
 
 def cpu_baseline(args, wl, g, sample_iters):
-    from oracle import oracle as O
     rp, col, val = g.s.get_csr()
+    rp = rp.astype(np.int64)
     F = g.s.giveForce()
-    mask = np.zeros(len(rp) - 1, dtype=np.uint8)
-    mask[wl["bc"]] = 1
-    # iterations to 1e-8 of the same FP64 Jacobi-PCG, taken from a GPU FP64
-    # Jacobi-PCG forward solve of the identical matrix (avoids a minutes-long
-    # CPU solve)
-    from statfem_b200 import api
-    keep = g.s.get_options()
-    g.s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-8, max_iter=30000, check_every=32,
-                    precond=api.SFC_PRECOND_JACOBI)
-    g.s.solveSystem()
-    its = int(g.s.last_stats()["iterations"])
-    g.s.set_options(**keep)
-    rate, per_iter = cpu_solve_rate(wl, rp, col, val, mask, F, its, sample_iters)
-    threads = 1  # the C port is single-threaded, like the reference path
-    return {"value": round(rate, 6), "unit": "posterior solves/s", "cores": threads, "kind": "port",
-            "sample": "oracle C FP64 Jacobi-PCG on the same assembled matrix: %d iterations timed "
-                      "(%.2f ms/iter), x (1+%d) solves x %d iterations/solve (forward solve to 1e-8 on "
-                      "the CPU); assembly and covariance not counted" % (sample_iters, per_iter * 1e3,
-                                                                         wl["ns"], its)}
+    setup = cpu_setup(wl, rp, col, val, F)
+    per = cpu_adjoint_sample(rp, col, val, setup, sample_iters)
+    sec = cpu_posterior_seconds(wl, setup, per)
+    threads = host_threads()
+    return {"value": round(1.0 / sec, 6), "unit": "posterior solves/s", "cores": threads, "kind": "port",
+            "sample": cpu_sample_text(wl, setup, per, sample_iters, threads)}
 
 
 def run_reference_c5(args):
@@ -849,6 +903,14 @@ def run_reference_c5(args):
 
 
 def run_reference(args, ws, rank):
+    """The CPU path on the host cores (rank 0 only): the oracle's C
+    restatement of the reference's assembly and FP64 Jacobi-PCG standing in
+    for the reference's Eigen SparseLU (which cannot factor this system in
+    any reasonable time), OpenMP on every host thread.  One-off: assembly of
+    the full matrix (not timed: it only provides the operator), a full
+    forward solve, the covariance and a scaled assembly sample; each step
+    then times cpu_iters block-PCG iterations over 32 adjoint right-hand
+    sides, and the step's rate is the posterior-solve model built from them."""
     if rank != 0:
         return
     if args.config == "c5":
@@ -856,29 +918,24 @@ def run_reference(args, ws, rank):
     from oracle import oracle as O
     wl = make_workload(args.config, seed=1234)
     mesh = wl["mesh"]
-    t0 = time.perf_counter()
     rp, col, val, F = O.fem(mesh, wl["qps"], wl["f"], wl["bc"], coeff=wl["coeff"], nu=0.3)
-    t_asm = time.perf_counter() - t0
-    mask = np.zeros(mesh.num_dofs, dtype=np.uint8)
-    mask[wl["bc"]] = 1
-    x, its = O.pcg(rp, col, val, mask, F, tol=1e-8, max_iter=60000)
-    rates = []
+    setup = cpu_setup(wl, rp, col, val, F)
+    rates, pers = [], []
     for k in range(args.warmup + args.steps):
-        r, per_iter = cpu_solve_rate(wl, rp, col, val, mask, F, its, args.cpu_iters)
+        per = cpu_adjoint_sample(rp, col, val, setup, args.cpu_iters)
         if k >= args.warmup:
-            rates.append(r)
+            pers.append(per)
+            rates.append(1.0 / cpu_posterior_seconds(wl, setup, per))
     value = float(np.mean(rates))
-    threads = 1  # the C port is single-threaded, like the reference path
-    out = {"impl": "reference", "metric": "posterior solves/s at rel. residual 1e-8 (learned+batched vs plain "
-           "PCG, 1xB200)", "value": round(value, 6), "unit": "posterior solves/s", "n_gpus": ws,
-           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+    threads = host_threads()
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "posterior solves/s",
+           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-           "config": {"workload": wl["desc"], "method": "CPU FP64 Jacobi-PCG (oracle port)"},
+           "config": {"workload": wl["desc"], "method": "CPU FP64 Jacobi-PCG (oracle port, OpenMP)"},
            "cpu_baseline": {"value": round(value, 6), "unit": "posterior solves/s", "cores": threads,
                             "kind": "port",
-                            "sample": "per step: %d PCG iterations timed on the full matrix, scaled to (1+%d) "
-                                      "solves x %d iterations; oracle assembly took %.1f s (not counted)"
-                                      % (args.cpu_iters, wl["ns"], its, t_asm)},
+                            "sample": "per step: " + cpu_sample_text(wl, setup, float(np.mean(pers)), args.cpu_iters,
+                                                                     threads)},
            "e2e": {"value": round(value, 6), "unit": "posterior solves/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -904,8 +961,11 @@ def main():
     ap.add_argument("--c5-steps", type=int, default=40, help="c5: Adam steps per training sample")
     ap.add_argument("--c5-n", type=int, default=128, help="c5: held-out grid (elements per side)")
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--cpu-iters", type=int, default=100)
-    ap.add_argument("--plain-sample", type=int, default=8)
+    ap.add_argument("--cpu-iters", type=int, default=20,
+                    help="CPU arms: block-PCG iterations timed per sample")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="c2/c1: skip the whole-step plain FP64 Jacobi-PCG measurement")
+    ap.add_argument("--plain-sample", type=int, default=8, help="c3: instances timed through the plain path (0: no plain-method measurement, any config)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--prof-steps", type=int, default=1)
     ap.add_argument("--block-width", type=int, default=128, choices=[32, 64, 128])
@@ -916,6 +976,9 @@ def main():
                     help="two-level: nodes per aggregate along each axis (0: library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    rc = relaunch_if_needed(args)
+    if rc is not None:
+        sys.exit(rc)
     ws, rank, local = dist_setup() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
                                                                 int(os.environ.get("RANK", "0")), 0)
     if args.impl == "reference":

@@ -38,7 +38,12 @@ extern "C" {
 #define SFC_ERR_NO_MEMORY     -6  /* device or host allocation failed         */
 #define SFC_ERR_NEG_JACOBIAN  -7  /* detJ <= 0 in an element (FTL_VERIFY in
                                      corlib/ElementBasic.ipp:199)             */
-#define SFC_ERR_TOO_LARGE     -8  /* problem exceeds a fixed-size scratch area */
+#define SFC_ERR_TOO_LARGE     -8  /* problem exceeds a fixed limit: a fixed-size
+                                     scratch area, or the 32-bit index range
+                                     (dofs < 2^31; element-matrix entries
+                                     E * L^2 < 2^31, L = element dofs: about
+                                     3.7 M hex8 elasticity elements, 33 M
+                                     P1 triangles)                          */
 
 /* ---- element kinds (element type + its integrand) ------------------------ */
 #define SFC_ELEM_LINE2_POISSON  1 /* del2::fem::ElementPotential, 2-node line */
@@ -100,6 +105,11 @@ typedef struct sfc_solve_stats {
                                  Jacobi-PCG after repeated FP32 breakdowns    */
     int32_t coarse_dofs;      /* size of the coarse space used (TWO_LEVEL),
                                  0 when the solve had none                    */
+    int32_t spmm_kernel;      /* FP32 product of the mixed solver: 0 none (FP64
+                                 solve), 1 CSR rows, 2 node blocks (3-dof
+                                 meshes), 3 node blocks staged per lattice
+                                 brick by TMA (3-dof structured lattices)    */
+    int32_t reserved;
 } sfc_solve_stats_t;
 
 /* Hyperparameters; the reference keeps them in std::map<std::string,double>
@@ -350,10 +360,16 @@ int32_t sfc_perturbation_covar(const sfc_perturbation_t *pt, double *cov);
  *                                          -1 for a non-negative quadratic term
  * The kernel is launched on `stream` (a cudaStream_t, NULL = default stream)
  * and nothing is allocated: the scratch is a fixed device array of
- * 2*128*128 + 128*64 doubles (320 KiB, held by every device that loads the
+ * 128*128 + 128*64 doubles (192 KiB, held by every device that loads the
  * library until exit), so num_sensors <= 128 and num_readings <= 64, else
  * SFC_ERR_TOO_LARGE.  The first call on a device looks up that array's device
- * address (with the device current); make it before any stream capture.  All
+ * address (with the device current) and, under CUDA's lazy module loading,
+ * is the call that loads the library's kernels onto the device, which
+ * allocates the array and the code and may synchronise: make one call at
+ * start-up, before any stream capture and outside the loop that must not
+ * allocate.  The address is cached per device for the context current at
+ * that first call (the primary context for runtime-API callers): do not use
+ * this entry point after cudaDeviceReset or from a different context.  All
  * calls share the array: calls that can overlap on the GPU race and must be
  * ordered by the caller. */
 int32_t sfc_koh_log_likelihood_noalloc(const double *mean_dev, const double *cov_dev,

@@ -63,6 +63,8 @@ def lib():
                                                    _dp, ctypes.c_double, ctypes.c_double, _dp]
         L.sfo_pcg.argtypes = [ctypes.c_int64, _i64p, _i32p, _dp, _u8p, _dp, _dp, ctypes.c_double,
                               ctypes.c_int, _dp]
+        L.sfo_block_pcg.argtypes = [ctypes.c_int64, _i64p, _i32p, _dp, _u8p, ctypes.c_int, _dp, _dp,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_int, _i32p]
         _lib = L
     return _lib
 
@@ -162,6 +164,24 @@ def pcg(rp, col, val, mask, b, tol=1e-8, max_iter=100000):
     return x, it
 
 
+def block_pcg(rp, col, val, mask, B, tol, max_iter=100000, X0=None):
+    """FP64 Jacobi-PCG on the symmetric elimination of the row-zeroed matrix
+    for every row of B (k x N) at once, OpenMP over matrix rows (sfo.c
+    sfo_block_pcg).  Starts from X0 (k x N) when given.  Returns (X, its)."""
+    N = len(rp) - 1
+    B = np.atleast_2d(np.asarray(B, dtype=np.float64))
+    k = B.shape[0]
+    Bi = np.ascontiguousarray(B.T)
+    Xi = np.zeros((N, k)) if X0 is None else np.ascontiguousarray(np.atleast_2d(X0).T)
+    its = np.zeros(k, dtype=np.int32)
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    rc = lib().sfo_block_pcg(N, _p(rp, _i64p), _p(col, _i32p), _p(val, _dp), _p(m, _u8p), k, _p(Bi, _dp),
+                             _p(Xi, _dp), tol, max_iter, int(X0 is not None), _p(its, _i32p))
+    if rc == -2:
+        raise MemoryError("sfo_block_pcg: allocation failed")
+    return np.ascontiguousarray(Xi.T), its
+
+
 # --------------------------------------------------------------------------
 # solver: SuperLU on the reference's row-zeroed system
 # --------------------------------------------------------------------------
@@ -248,6 +268,75 @@ def forward_perturbation(mesh, qps, F, rp, col, val, bc_dofs, P, phibar, sigma_f
     add = reg * sigma_m
     C = R @ Cf @ R.T + Cmat + add * add * (P @ P.T)
     return P @ u, C
+
+
+def grid_axes(mesh):
+    """The 1-D node coordinates of a structured mesh (x fastest, then y, z),
+    checked against every node coordinate."""
+    d = mesh.dim
+    axes = [np.unique(mesh.coords[:, a]) for a in range(d)]
+    grid = np.stack(np.meshgrid(*axes[::-1], indexing="ij")[::-1], axis=-1).reshape(-1, d)
+    if grid.shape[0] != mesh.num_nodes or np.abs(grid - mesh.coords[:, :d]).max() > 0:
+        raise ValueError("not a tensor-product node grid")
+    return axes
+
+
+def forcing_covariance_apply_grid(mesh, phibar, sigma, length, W):
+    """C_f W for the nodal forcing covariance of CovarianceForcing::
+    giveProjectedCovar (statX/infer/CovarianceForcing.ipp:38-109) on a
+    tensor-product node grid, without forming the N x N matrix: per
+    component, C_f = diag(phibar) sigma^2 (K_z (x) K_y (x) K_x) diag(phibar),
+    because the squared-exponential kernel factorises over coordinates
+    (exp(-|d|^2/2l^2) = prod_a exp(-d_a^2/2l^2); the same matrix as the
+    dense restatement up to the rounding of that product).  W: N x m."""
+    axes = grid_axes(mesh)
+    dof = mesh.dof
+    W = np.asarray(W, dtype=np.float64)
+    out = np.zeros_like(W)
+    Ks = [np.exp(-(x[:, None] - x[None, :]) ** 2 / (2.0 * length * length)) for x in axes]
+    shape = tuple(len(x) for x in axes[::-1]) + (W.shape[1],)  # (z, y, x, m)
+    for c in range(dof):
+        pb = phibar[c::dof]
+        T = (pb[:, None] * W[c::dof]).reshape(shape)
+        for a, K in enumerate(Ks):
+            ax = len(axes) - 1 - a  # x is the last grid axis
+            T = np.moveaxis(np.tensordot(K, T, axes=([1], [ax])), 0, ax)
+        out[c::dof] = sigma * sigma * pb[:, None] * T.reshape(-1, W.shape[1])
+    return out
+
+
+def forward_gauss_rhs_grid(R, F, Pd, mesh, phibar, sigma_f, length_f, reg):
+    """ForwardGaussRHS::updateSolution (statX/infer/ForwardGaussRHS.hpp:95-139)
+    from given adjoint rows R: mean = R F, C_s = R C_f R^T + (sigma_f reg)^2 P P^T,
+    with C_f applied through its Kronecker factors (tensor-product grids)."""
+    mean = R @ F
+    C = R @ forcing_covariance_apply_grid(mesh, phibar, sigma_f, length_f, R.T)
+    C = 0.5 * (C + C.T)
+    add = sigma_f * reg
+    return mean, C + add * add * (Pd @ Pd.T)
+
+
+def statfem_prior_iterative(mesh, qps, f, bc_dofs, Pd, sigma_f, length_f, reg, coeff=None, nu=0.3, tol=1e-13,
+                            X0=None):
+    """Prior at the sensors for meshes too large for the direct solve: the
+    forward solve A u = F and the ns adjoint solves A^T r_i = P_i by FP64
+    Jacobi-PCG (block_pcg) to the relative residual tol on the symmetric
+    elimination of the row-zeroed system.  With homogeneous Dirichlet data the
+    adjoint rows differ from the reference's A^T solve only on constrained
+    dofs, where F and phibar vanish, so mean and C_s are those of
+    ForwardGaussRHS (SystemSolveEigenSparse.hpp:364-404 with
+    ForwardGaussRHS.hpp:95-139).  Returns the dict of statfem_prior plus the
+    solution block X (rows: u, r_1..r_ns) and the iteration counts."""
+    rp, col, val, F = fem(mesh, qps, f, bc_dofs, coeff=coeff, nu=nu)
+    mask = np.zeros(mesh.num_dofs, dtype=np.uint8)
+    mask[np.asarray(bc_dofs, dtype=np.int64)] = 1
+    B = np.vstack([F[None, :], Pd])
+    X, its = block_pcg(rp, col, val, mask, B, tol, X0=X0)
+    phibar = unit_load(mesh, qps, bc_dofs)
+    R = X[1:]
+    mean_s, C_s = forward_gauss_rhs_grid(R, F, Pd, mesh, phibar, sigma_f, length_f, reg)
+    return dict(rp=rp, col=col, val=val, F=F, u=X[0], phibar=phibar, mean_s=mean_s, C_s=C_s, R=R, X=X,
+                its=its)
 
 
 def mismatch_covariance(sensor_coords, sigma_d, length_d, eps):

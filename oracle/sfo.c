@@ -621,3 +621,155 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
     free(dinv);
     return it > max_iter ? -1 : it;
 }
+
+/*
+ * Block FP64 Jacobi-PCG: k independent right-hand sides solved together so
+ * that one pass over the matrix serves all of them (each column keeps its own
+ * alpha, beta and stopping test; no block-Krylov coupling).  Same operator as
+ * sfo_pcg.  B and X are interleaved [N][k].  When use_x0 != 0 the iteration
+ * starts from the X passed in (r = b - S x), else from zero.  Column c stops
+ * once ||r_c|| <= tol*||b_c||; its_out[c] receives its iteration count (or -1
+ * when max_iter is reached).  Returns the largest count, or -1.
+ * Parallel over rows (OpenMP); the result does not depend on the thread count
+ * except through the order of the dot-product reductions.
+ */
+int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double *val,
+                  const unsigned char *mask, int k, const double *B, double *X, double tol,
+                  int max_iter, int use_x0, int *its_out)
+{
+    const int64_t NK = N * (int64_t)k;
+    double *r = malloc(sizeof(double) * NK), *p = malloc(sizeof(double) * NK);
+    double *q = malloc(sizeof(double) * NK), *dinv = malloc(sizeof(double) * N);
+    double *bb = calloc(k, sizeof(double)), *rz = calloc(k, sizeof(double));
+    double *pq = calloc(k, sizeof(double)), *rr = calloc(k, sizeof(double));
+    double *rz2 = calloc(k, sizeof(double)), *alpha = calloc(k, sizeof(double));
+    double *beta = calloc(k, sizeof(double));
+    char *active = calloc(k, 1);
+    if (!r || !p || !q || !dinv || !bb || !rz || !pq || !rr || !rz2 || !alpha || !beta || !active) return -2;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) {
+        double dg = 1.0;
+        for (int64_t s = row_ptr[i]; s < row_ptr[i + 1]; ++s)
+            if (col[s] == i) dg = val[s];
+        dinv[i] = 1.0 / dg;
+    }
+    /* r = b - S x (x = 0 unless use_x0) */
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < N; ++i) {
+        double *ri = r + i * k;
+        for (int c = 0; c < k; ++c) ri[c] = B[i * k + c];
+        if (!use_x0) {
+            for (int c = 0; c < k; ++c) X[i * k + c] = 0.0;
+        } else if (mask[i]) {
+            for (int c = 0; c < k; ++c) ri[c] -= X[i * k + c] / dinv[i];
+        } else {
+            for (int64_t s = row_ptr[i]; s < row_ptr[i + 1]; ++s) {
+                if (mask[col[s]]) continue;
+                const double v = val[s];
+                const double *xj = X + (int64_t)col[s] * k;
+                for (int c = 0; c < k; ++c) ri[c] -= v * xj[c];
+            }
+        }
+    }
+    for (int64_t i = 0; i < N; ++i)
+        for (int c = 0; c < k; ++c) {
+            const double b = B[i * k + c], rv = r[i * k + c];
+            bb[c] += b * b;
+            p[i * k + c] = dinv[i] * rv;
+            rz[c] += rv * (dinv[i] * rv);
+            rr[c] += rv * rv;
+        }
+    int nact = 0;
+    for (int c = 0; c < k; ++c) {
+        its_out[c] = 0;
+        active[c] = bb[c] > 0 && rr[c] > tol * tol * bb[c];
+        nact += active[c];
+    }
+    int it = 0;
+    while (nact > 0 && it < max_iter) {
+        ++it;
+        for (int c = 0; c < k; ++c) pq[c] = 0;
+#pragma omp parallel
+        {
+            double *acc = malloc(sizeof(double) * k), *lpq = calloc(k, sizeof(double));
+#pragma omp for schedule(static)
+            for (int64_t i = 0; i < N; ++i) {
+                const double *pi = p + i * k;
+                if (mask[i]) {
+                    for (int c = 0; c < k; ++c) acc[c] = pi[c] / dinv[i];
+                } else {
+                    for (int c = 0; c < k; ++c) acc[c] = 0.0;
+                    for (int64_t s = row_ptr[i]; s < row_ptr[i + 1]; ++s) {
+                        if (mask[col[s]]) continue;
+                        const double v = val[s];
+                        const double *pj = p + (int64_t)col[s] * k;
+                        for (int c = 0; c < k; ++c) acc[c] += v * pj[c];
+                    }
+                }
+                double *qi = q + i * k;
+                for (int c = 0; c < k; ++c) {
+                    qi[c] = acc[c];
+                    lpq[c] += pi[c] * acc[c];
+                }
+            }
+#pragma omp critical
+            for (int c = 0; c < k; ++c) pq[c] += lpq[c];
+            free(acc);
+            free(lpq);
+        }
+        for (int c = 0; c < k; ++c) {
+            alpha[c] = active[c] ? rz[c] / pq[c] : 0.0;
+            rr[c] = rz2[c] = 0;
+        }
+#pragma omp parallel
+        {
+            double *lrr = calloc(k, sizeof(double)), *lrz = calloc(k, sizeof(double));
+#pragma omp for schedule(static)
+            for (int64_t i = 0; i < N; ++i) {
+                double *xi = X + i * k, *ri = r + i * k;
+                const double *pi = p + i * k, *qi = q + i * k;
+                for (int c = 0; c < k; ++c) {
+                    xi[c] += alpha[c] * pi[c];
+                    ri[c] -= alpha[c] * qi[c];
+                    lrr[c] += ri[c] * ri[c];
+                    lrz[c] += ri[c] * (dinv[i] * ri[c]);
+                }
+            }
+#pragma omp critical
+            for (int c = 0; c < k; ++c) {
+                rr[c] += lrr[c];
+                rz2[c] += lrz[c];
+            }
+            free(lrr);
+            free(lrz);
+        }
+        for (int c = 0; c < k; ++c) {
+            beta[c] = 0.0;
+            if (!active[c]) continue;
+            if (rr[c] <= tol * tol * bb[c]) {
+                active[c] = 0;
+                its_out[c] = it;
+                --nact;
+                continue;
+            }
+            beta[c] = rz2[c] / rz[c];
+            rz[c] = rz2[c];
+        }
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < N; ++i) {
+            double *pi = p + i * k;
+            const double *ri = r + i * k;
+            for (int c = 0; c < k; ++c)
+                if (active[c]) pi[c] = dinv[i] * ri[c] + beta[c] * pi[c];
+        }
+    }
+    int worst = 0;
+    for (int c = 0; c < k; ++c) {
+        if (active[c]) its_out[c] = -1;
+        if (its_out[c] < 0) worst = -1;
+        else if (worst >= 0 && its_out[c] > worst) worst = its_out[c];
+    }
+    free(r); free(p); free(q); free(dinv); free(bb); free(rz); free(pq); free(rr); free(rz2);
+    free(alpha); free(beta); free(active);
+    return worst;
+}

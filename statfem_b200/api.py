@@ -31,6 +31,15 @@ SFC_SOLVER_FCG_MPNN = 2
 SFC_PRECOND_JACOBI = 0
 SFC_PRECOND_BLOCK_JACOBI = 1
 SFC_PRECOND_TWO_LEVEL = 2
+# status codes of include/statfem_cuda.h
+SFC_ERR_CUDA = -1
+SFC_ERR_BAD_ARG = -2
+SFC_ERR_NOT_SPD = -3
+SFC_ERR_NOT_CONVERGED = -4
+SFC_ERR_TIMEOUT = -5
+SFC_ERR_NO_MEMORY = -6
+SFC_ERR_NEG_JACOBIAN = -7
+SFC_ERR_TOO_LARGE = -8
 
 _ERR = {-1: "CUDA error", -2: "bad argument", -3: "not SPD", -4: "not converged", -5: "timeout",
         -6: "out of memory", -7: "negative Jacobian", -8: "too large for the fixed scratch"}
@@ -53,7 +62,8 @@ class SolveStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int32), ("refinements", ctypes.c_int32),
                 ("num_rhs", ctypes.c_int32), ("converged", ctypes.c_int32),
                 ("max_rel_residual", ctypes.c_double), ("device_ms", ctypes.c_double),
-                ("fallback_columns", ctypes.c_int32), ("coarse_dofs", ctypes.c_int32)]
+                ("fallback_columns", ctypes.c_int32), ("coarse_dofs", ctypes.c_int32),
+                ("spmm_kernel", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

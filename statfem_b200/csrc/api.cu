@@ -208,7 +208,7 @@ int32_t sfc_mesh_create(sfc_ctx_t *ctx, int32_t kind, int32_t qps, const double 
         m->num_nodes = num_nodes;
         m->num_elems = num_elems;
         m->num_dofs = num_nodes * m->dof;
-        SFC_REQUIRE(m->num_dofs < (int64_t)INT32_MAX, "too many dofs");
+        SFC_REQUIRE_SIZE(m->num_dofs < (int64_t)INT32_MAX, "more than 2^31 - 1 dofs (32-bit column indices)");
         make_quadrature(kind, qps, m->quad);
         for (int64_t t = 0; t < num_elems * m->nn; ++t)
             SFC_REQUIRE(conn[t] < (uint64_t)num_nodes, "connectivity refers to a node that does not exist");
@@ -255,6 +255,7 @@ int64_t sfc_mesh_nnz(const sfc_mesh_t *m) { return m ? m->nnz : -1; }
 int32_t sfc_system_create(sfc_ctx_t *ctx, int64_t num_dofs, sfc_system_t **out)
 {
     if (!ctx || !out || num_dofs <= 0) return SFC_ERR_BAD_ARG;
+    if (num_dofs >= (int64_t)INT32_MAX) return SFC_ERR_TOO_LARGE;  // 32-bit column indices
     *out = nullptr;
     sfc_system *s = new (std::nothrow) sfc_system();
     if (!s) return SFC_ERR_NO_MEMORY;

@@ -2,6 +2,7 @@
 // B200 library.  Nothing here is part of the C ABI (include/statfem_cuda.h).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -35,6 +36,13 @@ struct Error {
 #define SFC_REQUIRE(cond, msg)                                                         \
     do {                                                                               \
         if (!(cond)) ::sfc::fail(SFC_ERR_BAD_ARG, msg);                                \
+    } while (0)
+
+// A size beyond a fixed limit of the implementation (32-bit index range,
+// fixed scratch area): SFC_ERR_TOO_LARGE.
+#define SFC_REQUIRE_SIZE(cond, msg)                                                    \
+    do {                                                                               \
+        if (!(cond)) ::sfc::fail(SFC_ERR_TOO_LARGE, msg);                              \
     } while (0)
 
 // Device buffer with RAII ownership.
@@ -311,6 +319,17 @@ struct sfc_system {
     sfc::DBuf<float> bval32;
     sfc::DBuf<double> bval64;
     sfc::DBuf<float> bdinv32;  // inverse of each node's 3x3 diagonal block
+    // lattice view (3-dof meshes whose nodes form an nx x ny x nz lattice
+    // numbered x fastest, blocks coupling lattice neighbours only): every
+    // node's 27 neighbour blocks in canonical slots (dz, dy, dx), zero where
+    // the neighbour is missing, rows padded to 4 floats (lattice.cu)
+    bool has_lattice = false;
+    int lat[3] = {0, 0, 0};
+    sfc::DBuf<float> bq;      // nodes x 27 x 12
+    sfc::DBuf<int> lat_err;   // bounded-wait status of the staged SpMM
+    CUtensorMap pmap{};       // TMA view of the block operand P as (K, 3, nx, ny, nz)
+    const float *pmap_ptr = nullptr;
+    int pmap_K = 0;
     // vectors
     sfc::DBuf<double> F, X;
     sfc::DBuf<unsigned char> mask;   // 1 for constrained dofs
@@ -406,6 +425,10 @@ void apply_constraints_dev(sfc_system *s, const uint32_t *idx_dev, const double 
 // require_positive_diag: fail on a non-positive (or NaN) diagonal entry; the
 // batch path passes false and lets the affected instance fail alone
 void build_operator(sfc_system *s, bool require_positive_diag = true);
+// lattice.cu
+void build_lattice_blocks(sfc_system *s);
+void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop);
+void lattice_check(sfc_system *s);
 void flush_staged(sfc_system *s);
 void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);
 void element_matrices_unit(const sfc_mesh *m, double *ke0);

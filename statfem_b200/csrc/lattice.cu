@@ -1,0 +1,340 @@
+// Staged block SpMM Q = S P for 3-dof meshes on a structured node lattice
+// (trilinear hexahedra on an nx x ny x nz grid, nodes numbered x fastest):
+// the FP32 product at the heart of the mixed block PCG, replacing the sparse
+// direct solve of corlib/SystemSolveEigenSparse.hpp:273-404 for the many
+// adjoint right-hand sides of statX/infer/ForwardGaussRHS.hpp:104-112.
+//
+// S is held as each node's 27 neighbour blocks in canonical slots
+// (dz, dy, dx) (zero where the lattice has no neighbour), rows padded to four
+// floats so a warp reads a block with three 16-byte broadcast loads.  P and Q
+// are the block solver's RHS-interleaved [N][K] FP32 arrays.
+//
+// A work item is a brick of 4 x 2 x 2 output nodes and a 64-column slice of
+// the block.  One elected thread issues a single 5-D TMA tensor load of the
+// brick's halo (6 x 4 x 4 column nodes x 3 rows x 64 columns, zero-filled
+// outside the lattice: 72 KiB) and 1-D bulk copies of the brick's block rows
+// (up to 4 x 5 KiB) into shared memory, completing on one mbarrier.  Each of
+// the four warps then owns one x-line of four output nodes and two columns
+// per lane: for every column node of its 3 x 3 neighbour lines it reads the
+// node's three P rows from shared memory once and applies them to every
+// output node of the line that couples to it (up to three), so a P row read
+// feeds 1.8 outputs on average and the FMA pipe, not the load path, bounds
+// the kernel.  The p.q column dots are accumulated in FP64 per lane across
+// all of a CTA's work items and reduced once at the end.
+//
+// Two CTAs (94.5 KiB of shared memory each) share an SM, so one computes
+// while the other waits for its copies.  Waits on the mbarrier are bounded:
+// a wait that gives up sets lat_err (the solver then fails with
+// SFC_ERR_TIMEOUT), waits once more (bounded) for the copies in flight and
+// leaves the kernel.  No multicast, no clusters: every copy reads this
+// GPU's own memory.
+
+#include <cudaTypedefs.h>
+
+#include <cstdlib>
+
+#include "common.cuh"
+
+namespace sfc {
+namespace {
+
+constexpr int BX = 4, BY = 2, BZ = 2;  // output nodes per brick
+constexpr int HX = BX + 2, HY = BY + 2, HZ = BZ + 2;
+constexpr int CS = 64;                 // columns per slice (2 per lane)
+constexpr int SLOT = 12;               // floats per padded 3x3 block
+constexpr int NODE_FLOATS = 27 * SLOT; // 324 floats = 1296 bytes per node
+constexpr int HALO_FLOATS = HZ * HY * HX * 3 * CS;
+constexpr int BLK_FLOATS = BX * BY * BZ * NODE_FLOATS;
+constexpr int HALO_BYTES = HALO_FLOATS * 4;                 // 73,728
+constexpr size_t SMEM_BYTES = (size_t)(HALO_FLOATS + BLK_FLOATS) * 4 + 16;  // + mbarrier
+constexpr int THREADS = 128;
+constexpr uint32_t WAIT_TRIES = 1u << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// bounded wait for the phase with the given parity to complete
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < WAIT_TRIES; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int c0, int c1, int c2,
+                                            int c3, int c4)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(THREADS, 2)
+    k_lspmm32(const __grid_constant__ CUtensorMap pmap, const float *__restrict__ bq, float *__restrict__ Q, int nx,
+              int ny, int nz, int K, int slices, int64_t work, double *pq, const int *stop, int *err)
+{
+    if (*stop) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *halo = reinterpret_cast<float *>(smem);
+    float *blk = halo + HALO_FLOATS;
+    uint64_t *barp = reinterpret_cast<uint64_t *>(blk + BLK_FLOATS);
+    const uint32_t bar = smem_u32(barp);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wy = warp & 1, wz = warp >> 1;
+    const int tx_n = (nx + BX - 1) / BX, ty_n = (ny + BY - 1) / BY;
+    const int slice = (int)(blockIdx.x % slices);  // gridDim.x is a multiple of slices
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    double dacc0 = 0.0, dacc1 = 0.0;
+    uint32_t parity = 0;
+    for (int64_t w = blockIdx.x; w < work; w += gridDim.x) {
+        const int64_t t = w / slices;
+        const int tx = (int)(t % tx_n);
+        const int64_t tr = t / tx_n;
+        const int ty = (int)(tr % ty_n), tz = (int)(tr / ty_n);
+        const int x0 = tx * BX, y0 = ty * BY, z0 = tz * BZ;
+        const int nvx = min(BX, nx - x0);
+        if (threadIdx.x == 0) {
+            uint32_t bytes = HALO_BYTES;
+            for (int l = 0; l < BY * BZ; ++l)
+                if (y0 + (l & 1) < ny && z0 + (l >> 1) < nz) bytes += (uint32_t)nvx * NODE_FLOATS * 4;
+            mbar_expect_tx(bar, bytes);
+            tma_load_5d(smem_u32(halo), &pmap, bar, slice * CS, 0, x0 - 1, y0 - 1, z0 - 1);
+            for (int l = 0; l < BY * BZ; ++l) {
+                const int y = y0 + (l & 1), z = z0 + (l >> 1);
+                if (y >= ny || z >= nz) continue;
+                const int64_t node = ((int64_t)z * ny + y) * nx + x0;
+                bulk_load(smem_u32(blk + l * BX * NODE_FLOATS), bq + node * NODE_FLOATS,
+                          (uint32_t)nvx * NODE_FLOATS * 4, bar);
+            }
+        }
+        const bool got = mbar_wait(bar, parity);
+        if (__syncthreads_or(!got)) {
+            // the copies did not complete in time: record it, give the copies
+            // in flight one more bounded wait, and leave (uniformly)
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            mbar_wait(bar, parity);
+            return;
+        }
+        parity ^= 1u;
+        float acc[BX][3][2];
+#pragma unroll
+        for (int o = 0; o < BX; ++o)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) acc[o][r][0] = acc[o][r][1] = 0.f;
+        const float *hb = halo + 2 * lane;
+        const float *bb = blk + warp * BX * NODE_FLOATS;
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy) {
+                const float *line = hb + ((wz + dz) * HY + (wy + dy)) * HX * 3 * CS;
+#pragma unroll
+                for (int cx = 0; cx < HX; ++cx) {
+                    const float2 p0 = *reinterpret_cast<const float2 *>(line + (cx * 3 + 0) * CS);
+                    const float2 p1 = *reinterpret_cast<const float2 *>(line + (cx * 3 + 1) * CS);
+                    const float2 p2 = *reinterpret_cast<const float2 *>(line + (cx * 3 + 2) * CS);
+#pragma unroll
+                    for (int ox = 0; ox < BX; ++ox) {
+                        const int dx = cx - ox;  // lattice offset dx - 1
+                        if (dx < 0 || dx > 2) continue;
+                        const float *b = bb + ox * NODE_FLOATS + (dz * 9 + dy * 3 + dx) * SLOT;
+                        const float4 b0 = *reinterpret_cast<const float4 *>(b);
+                        const float4 b1 = *reinterpret_cast<const float4 *>(b + 4);
+                        const float4 b2 = *reinterpret_cast<const float4 *>(b + 8);
+                        acc[ox][0][0] = fmaf(b0.z, p2.x, fmaf(b0.y, p1.x, fmaf(b0.x, p0.x, acc[ox][0][0])));
+                        acc[ox][0][1] = fmaf(b0.z, p2.y, fmaf(b0.y, p1.y, fmaf(b0.x, p0.y, acc[ox][0][1])));
+                        acc[ox][1][0] = fmaf(b1.z, p2.x, fmaf(b1.y, p1.x, fmaf(b1.x, p0.x, acc[ox][1][0])));
+                        acc[ox][1][1] = fmaf(b1.z, p2.y, fmaf(b1.y, p1.y, fmaf(b1.x, p0.y, acc[ox][1][1])));
+                        acc[ox][2][0] = fmaf(b2.z, p2.x, fmaf(b2.y, p1.x, fmaf(b2.x, p0.x, acc[ox][2][0])));
+                        acc[ox][2][1] = fmaf(b2.z, p2.y, fmaf(b2.y, p1.y, fmaf(b2.x, p0.y, acc[ox][2][1])));
+                    }
+                }
+            }
+        const int y = y0 + wy, z = z0 + wz;
+        if (y < ny && z < nz) {
+            // own rows of P sit at halo (ox + 1, wy + 1, wz + 1)
+            const float *own = hb + ((wz + 1) * HY + (wy + 1)) * HX * 3 * CS;
+#pragma unroll
+            for (int ox = 0; ox < BX; ++ox) {
+                if (ox >= nvx) break;
+                const int64_t node = ((int64_t)z * ny + y) * nx + x0 + ox;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const float2 pv = *reinterpret_cast<const float2 *>(own + ((ox + 1) * 3 + r) * CS);
+                    *reinterpret_cast<float2 *>(Q + (3 * node + r) * K + slice * CS + 2 * lane) =
+                        make_float2(acc[ox][r][0], acc[ox][r][1]);
+                    dacc0 += (double)pv.x * (double)acc[ox][r][0];
+                    dacc1 += (double)pv.y * (double)acc[ox][r][1];
+                }
+            }
+        }
+        __syncthreads();  // every warp is done with the staged tiles before the next copies land
+    }
+    // column dots: the four warps' lanes hold the same 64 columns
+    double *red = reinterpret_cast<double *>(smem);
+    red[warp * CS + 2 * lane] = dacc0;
+    red[warp * CS + 2 * lane + 1] = dacc1;
+    __syncthreads();
+    if (threadIdx.x < CS) {
+        const double s = red[threadIdx.x] + red[CS + threadIdx.x] + red[2 * CS + threadIdx.x] + red[3 * CS + threadIdx.x];
+        atomicAdd(pq + slice * CS + threadIdx.x, s);
+    }
+}
+
+// canonical 27-slot blocks from the node-block (BSR) view; a block whose
+// column node is not a lattice neighbour sets *err
+__global__ void k_lattice_fill(const int32_t *__restrict__ bptr, const int32_t *__restrict__ bcol,
+                               const float *__restrict__ b32, int64_t nodes, int nx, int ny, float *__restrict__ bq,
+                               int *err)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t plane = (int64_t)nx * ny;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nodes; i += warps) {
+        const int32_t b0 = bptr[i], nb = bptr[i + 1] - b0;
+        const int xi = (int)(i % nx), yi = (int)((i / nx) % ny), zi = (int)(i / plane);
+        for (int32_t e = lane; e < 9 * nb; e += 32) {
+            const int32_t t = e / 9, k = e % 9;
+            const int64_t j = bcol[b0 + t];
+            const int dx = (int)(j % nx) - xi, dy = (int)((j / nx) % ny) - yi, dz = (int)(j / plane) - zi;
+            if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
+                atomicExch(err, 1);
+                continue;
+            }
+            const int slot = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+            bq[i * NODE_FLOATS + slot * SLOT + (k / 3) * 4 + k % 3] = b32[(int64_t)(b0 + t) * 9 + k];
+        }
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SFC_CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(SFC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+}  // namespace
+
+// Installs the lattice view when the system's pattern comes from a 3-dof
+// mesh whose nodes form a lattice (numbered x fastest) and every block
+// couples lattice neighbours; otherwise the node-block (BSR) kernels are used.
+// SFC_SPMM=bsr in the environment keeps the BSR kernel (for comparisons).
+void build_lattice_blocks(sfc_system *s)
+{
+    sfc_ctx *ctx = s->ctx;
+    s->has_lattice = false;
+    const sfc_mesh *m = s->pattern_mesh;
+    const char *force = std::getenv("SFC_SPMM");
+    if (force && std::string(force) == "bsr") return;
+    if (!s->has_bsr || !m || !m->is_grid || m->dim != 3 || m->dof != 3) return;
+    const int nx = m->gn[0], ny = m->gn[1], nz = m->gn[2];
+    if ((int64_t)nx * ny * nz != s->nodes || nx < 2 || ny < 2 || nz < 2) return;
+    s->bq.alloc((size_t)s->nodes * NODE_FLOATS);  // same size on every rebuild: no reallocation
+    if (!s->lat_err.p) {
+        s->lat_err.alloc(1);
+        SFC_CK(cudaMemsetAsync(s->lat_err.p, 0, sizeof(int), ctx->stream));
+    }
+    s->pmap_ptr = nullptr;  // the lattice may differ from the one the cached map was made for
+    SFC_CK(cudaMemsetAsync(s->bq.p, 0, (size_t)s->nodes * NODE_FLOATS * 4, ctx->stream));
+    DevInt err = status_word(ctx);
+    SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
+    k_lattice_fill<<<grid_for(s->nodes * 32, 256), 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval32.p, s->nodes,
+                                                                       nx, ny, s->bq.p, err.p);
+    count_launch(ctx);
+    int h = 0;
+    download(ctx, &h, err.p, 1);
+    if (h) return;
+    s->lat[0] = nx;
+    s->lat[1] = ny;
+    s->lat[2] = nz;
+    s->has_lattice = true;
+}
+
+void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop)
+{
+    sfc_ctx *ctx = s->ctx;
+    const int nx = s->lat[0], ny = s->lat[1], nz = s->lat[2];
+    SFC_REQUIRE(K % CS == 0, "lattice SpMM needs a multiple of 64 columns");
+    if (s->pmap_ptr != P || s->pmap_K != K) {
+        const cuuint64_t dims[5] = {(cuuint64_t)K, 3, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+        const cuuint64_t strides[4] = {(cuuint64_t)K * 4, (cuuint64_t)3 * K * 4, (cuuint64_t)3 * K * 4 * nx,
+                                       (cuuint64_t)3 * K * 4 * nx * ny};
+        const cuuint32_t box[5] = {CS, 3, HX, HY, HZ};
+        const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+        const CUresult r = encode_fn()(&s->pmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<float *>(P), dims,
+                                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                       CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) fail(SFC_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+        s->pmap_ptr = P;
+        s->pmap_K = K;
+    }
+    static int occ = 0;
+    if (!occ) {
+        SFC_CK(cudaFuncSetAttribute(k_lspmm32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+        SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_lspmm32, THREADS, SMEM_BYTES));
+        if (occ < 1) occ = 1;
+    }
+    const int slices = K / CS;
+    const int64_t tiles = (int64_t)((nx + BX - 1) / BX) * ((ny + BY - 1) / BY) * ((nz + BZ - 1) / BZ);
+    const int64_t work = tiles * slices;
+    int64_t grid = std::min<int64_t>(work, (int64_t)occ * ctx->sm_count);
+    grid = std::max<int64_t>(slices, grid - grid % slices);
+    k_lspmm32<<<(unsigned)grid, THREADS, SMEM_BYTES, ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K, slices, work,
+                                                                     pq, stop, s->lat_err.p);
+    count_launch(ctx);
+}
+
+// after a solve: a staged SpMM whose bounded wait gave up fails the solve
+void lattice_check(sfc_system *s)
+{
+    if (!s->has_lattice || !s->lat_err.p) return;
+    int h = 0;
+    download(s->ctx, &h, s->lat_err.p, 1);
+    if (h) {
+        SFC_CK(cudaMemsetAsync(s->lat_err.p, 0, sizeof(int), s->ctx->stream));
+        fail(SFC_ERR_TIMEOUT, "staged SpMM: a bounded wait for its shared-memory copies gave up");
+    }
+}
+
+}  // namespace sfc

@@ -28,9 +28,9 @@ namespace {
 constexpr int kMaxSensors = 128;
 constexpr int kMaxReadings = 64;
 constexpr int kMaxDevices = 64;
-constexpr size_t kScratchDoubles = 2 * (size_t)kMaxSensors * kMaxSensors + (size_t)kMaxSensors * kMaxReadings;
+constexpr size_t kScratchDoubles = (size_t)kMaxSensors * kMaxSensors + (size_t)kMaxSensors * kMaxReadings;
 
-// 2 * 128 * 128 + 128 * 64 doubles = 320 KiB per device
+// [C (ns x ns) | D (ns x n_o)]: 128 * 128 + 128 * 64 doubles = 192 KiB per device
 static __device__ __align__(256) double g_koh_scratch[kScratchDoubles];
 
 __device__ __forceinline__ double se_kernel(const double *x, const double *y, int dim, double sigma, double length)
@@ -142,7 +142,11 @@ __global__ void __launch_bounds__(1024) k_koh_loglik_fixed(int ns, int n_o, cons
     }
 }
 
-// per-device address of g_koh_scratch, looked up once with the device current
+// per-device address of g_koh_scratch, looked up once with the device current.
+// The address belongs to the context that was current at the lookup (the
+// device's primary context for runtime-API callers); after cudaDeviceReset,
+// or for a caller that makes another context current, it is stale, so both
+// are documented as unsupported in the public header.
 std::mutex g_sym_mutex;
 void *g_sym_addr[kMaxDevices] = {};
 
@@ -178,6 +182,11 @@ extern "C" int32_t sfc_koh_log_likelihood_noalloc(const double *mean_dev, const 
     k_koh_loglik_fixed<<<1, 1024, 0, (cudaStream_t)stream>>>(num_sensors, num_readings, mean_dev, cov_dev,
                                                               sensor_coords_dev, dim, y_dev, *hp, (double *)scratch,
                                                               loglik_dev, info_dev);
-    if (cudaGetLastError() != cudaSuccess) return SFC_ERR_CUDA;
+    // check this launch without consuming an error that earlier, unrelated
+    // runtime work left for its owner: only a failed launch is cleared
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();
+        return SFC_ERR_CUDA;
+    }
     return SFC_OK;
 }

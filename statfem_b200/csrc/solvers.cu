@@ -1491,6 +1491,10 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         ProfScope ps(ctx, "spmm32",
                      bsr ? (double)s->nblocks * 40 + 4.0 * (s->nodes + 1) + 2.0 * N * K * 4
                          : (double)s->nnz * 8 + 4.0 * (N + 1) + 2.0 * N * K * 4);
+        if (bsr && s->has_lattice && K >= 64) {
+            lattice_spmm32(s, Pm, Qm, K, out, stop);
+            return;
+        }
         if (bsr)
             k_bspmm32<V><<<gw, 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval32.p, Pm, Qm, s->nodes, out, stop);
         else
@@ -1747,6 +1751,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         max_updates = std::max(max_updates, updates);
     }
     SFC_CK(cudaStreamSynchronize(ctx->stream));
+    lattice_check(s);
     st.iterations = max_inner;
     st.refinements = max_updates;
     st.num_rhs = nrhs;
@@ -1754,6 +1759,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     st.converged = all_conv ? 1 : 0;
     st.fallback_columns = n_fallback;
     st.coarse_dofs = two_any ? (int32_t)(crs.nc - crs.dropped) : 0;
+    st.spmm_kernel = bsr ? (s->has_lattice && K >= 64 ? 3 : 2) : 1;
 }
 
 }  // namespace
@@ -1826,10 +1832,20 @@ void solve_forward(sfc_system *s)
     SFC_CK(cudaEventRecord(e0, ctx->stream));
     PcgResult r;
     bool two = false;
+    sfc_solve_stats_t mst{};
+    const bool mixed = o.method == SFC_SOLVER_PCG_MIXED;
     {
         ProfScope ps(ctx, "phase:forward_solve", 0.0);
         two = use_two_level(s);
-        r = pcg64(s, b.p, s->X.p, tol, max_iter, check, two);
+        if (mixed) {
+            // the forward system as a one-column block of the mixed solver:
+            // FP32 iterations, FP64 residual replacement, same preconditioner
+            block_mixed<1>(s, b.p, s->X.p, 1, 1, mst);
+            r.iters = mst.iterations;
+            r.converged = mst.converged != 0;
+        } else {
+            r = pcg64(s, b.p, s->X.p, tol, max_iter, check, two);
+        }
     }
     SFC_CK(cudaEventRecord(e1, ctx->stream));
     const double rel = true_rel_residual(s, b.p, s->X.p);
@@ -1845,6 +1861,11 @@ void solve_forward(sfc_system *s)
     s->stats.max_rel_residual = rel;
     s->stats.device_ms = ms;
     s->stats.coarse_dofs = two ? (int32_t)(s->coarse.nc - s->coarse.dropped) : 0;
+    if (mixed) {
+        s->stats.refinements = mst.refinements;
+        s->stats.fallback_columns = mst.fallback_columns;
+        s->stats.spmm_kernel = mst.spmm_kernel;
+    }
     if (!r.converged) fail(SFC_ERR_NOT_CONVERGED, "PCG did not converge within max_iter");
 }
 

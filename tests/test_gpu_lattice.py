@@ -1,0 +1,62 @@
+"""The staged lattice SpMM of the mixed block solver (3-dof meshes on a
+structured node lattice: TMA-staged halo bricks in shared memory) against the
+node-block kernel it replaces and against the oracle's LU of A^T, on lattices
+whose sides are not multiples of the brick (ragged bricks on every face), for
+one and two 64-column slices per block; and the 32-bit size limit."""
+import os
+
+import numpy as np
+import pytest
+
+from statfem_b200 import api
+from statfem_b200 import meshgen as mg
+from tests.test_gpu_solve import setup
+
+pytestmark = pytest.mark.gpu
+
+
+def solve(ctx, n, bw, precond, rhs_seed=4, nrhs=130, force_bsr=False):
+    if force_bsr:
+        os.environ["SFC_SPMM"] = "bsr"
+    try:
+        mesh, s, ds, F, bc = setup(ctx, mg.HEX8_ELASTIC, n, 17, amount=0.0, faces="x0")
+    finally:
+        os.environ.pop("SFC_SPMM", None)
+    rng = np.random.default_rng(rhs_seed)
+    Rhs = rng.standard_normal((nrhs, mesh.num_dofs))
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, block_width=bw, precond=precond)
+    U = s.solveSystemTranspose(Rhs)
+    st = s.last_stats()
+    return U, st, ds, Rhs
+
+
+@pytest.mark.parametrize("n,bw", [(6, 128), (6, 64), (9, 128), (4, 64)])
+@pytest.mark.parametrize("precond", [api.SFC_PRECOND_BLOCK_JACOBI, api.SFC_PRECOND_TWO_LEVEL])
+def test_lattice_spmm_matches_lu_and_node_blocks(ctx, n, bw, precond):
+    U, st, ds, Rhs = solve(ctx, n, bw, precond)
+    assert st["spmm_kernel"] == 3, st
+    assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
+    refs = np.stack([ds.solve_transpose(r) for r in Rhs])
+    assert np.abs(U - refs).max() <= 1e-7 * np.abs(refs).max()
+    U2, st2, _, _ = solve(ctx, n, bw, precond, force_bsr=True)
+    assert st2["spmm_kernel"] == 2, st2
+    assert np.abs(U2 - refs).max() <= 1e-7 * np.abs(refs).max()
+    # the two FP32 products differ only in summation order: iteration counts stay close
+    assert abs(st["iterations"] - st2["iterations"]) <= max(8, st2["iterations"] // 5)
+
+
+def test_distorted_mesh_keeps_node_blocks(ctx):
+    """A mesh whose nodes are not a lattice uses the node-block kernel."""
+    mesh, s, ds, F, bc = setup(ctx, mg.HEX8_ELASTIC, 4, 3, amount=0.3, faces="x0")
+    Rhs = np.random.default_rng(1).standard_normal((64, mesh.num_dofs))
+    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, block_width=64, precond=api.SFC_PRECOND_BLOCK_JACOBI)
+    U = s.solveSystemTranspose(Rhs)
+    assert s.last_stats()["spmm_kernel"] == 2
+    refs = np.stack([ds.solve_transpose(r) for r in Rhs])
+    assert np.abs(U - refs).max() <= 1e-7 * np.abs(refs).max()
+
+
+def test_system_beyond_32bit_indices_is_rejected(ctx):
+    with pytest.raises(api.SfcError) as e:
+        api.SystemSolveCuda(ctx, 2 ** 31)
+    assert e.value.code == api.SFC_ERR_TOO_LARGE

@@ -79,8 +79,8 @@ def test_prior_posterior_loglik(ctx, kind, n, ns, amount, method):
     assert abs(ll - ll_ref) <= 1e-7 * max(1.0, abs(ll_ref))
     pm, pc = koh.giveProjFEconditionedData(HP)
     pm_ref, pc_ref = O.koh_proj_conditioned(o["mean_s"], o["C_s"], Ks, Y, HP["rho"])
-    assert rel_err(pm, pm_ref) < 1e-6
-    assert rel_err(pc, pc_ref) < 1e-6
+    assert rel_err(pm, pm_ref) < REL
+    assert rel_err(pc, pc_ref) < REL
 
 
 def test_kronecker_and_dense_covariance_agree(ctx):
@@ -169,5 +169,9 @@ def test_woodbury_mean_at_sensor_cost(ctx, kind, n, ns, amount, method):
     u_mean, C_u, _ = O.forward_gauss_rhs(o["solver"], o["F"], I, mesh.coords, o["phibar"], mesh.dim, mesh.dof,
                                          HP["forcing.sigma"], HP["forcing.length"], reg)
     Ks = O.mismatch_covariance(prob["pts"], HP["mismatch.sigma"], HP["mismatch.length"], HP["mismatch.sensorEps"])
-    m_ref, _ = O.koh_woodbury(o["C_s"], Ks, Y, HP["rho"], Pd, C_u, u_mean)
-    assert np.abs(m - m_ref).max() <= 1e-7 * np.abs(m_ref).max()
+    m_ref, cov_ref = O.koh_woodbury(o["C_s"], Ks, Y, HP["rho"], Pd, C_u, u_mean)
+    assert np.abs(m - m_ref).max() <= REL * np.abs(m_ref).max()
+    # the full-field Woodbury covariance Sigma = D C_u (LikelihoodKOH.ipp:442-508)
+    m_full2, cov = koh.giveFEconditionedDataWoodbury(HP, with_cov=True)
+    assert np.abs(m_full2 - m_ref).max() <= REL * np.abs(m_ref).max()
+    assert rel_err(cov, cov_ref) < REL

@@ -1,6 +1,6 @@
 """Reference file formats (no GPU): SMF meshes, property files, parameter
-maps and the app's data files; when the reference tree is present, its
-laplaceRHSinfer inputs parse to the committed fixture."""
+maps and the app's data files; when STATFEM_REFERENCE names a checkout of the
+reference tree, its laplaceRHSinfer inputs parse to the committed fixture."""
 import os
 
 import numpy as np
@@ -10,7 +10,9 @@ from statfem_b200 import io as sio
 from statfem_b200 import meshgen as mg
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_APP = "/root/reference/del2/apps/reference/laplaceRHSinfer"
+# a checkout of the reference tree, when one is available (skipped otherwise)
+REF_TREE = os.environ.get("STATFEM_REFERENCE", "")
+REF_APP = os.path.join(REF_TREE, "del2", "apps", "reference", "laplaceRHSinfer") if REF_TREE else ""
 
 
 @pytest.mark.parametrize("mesh", [mg.bar(7), mg.unit_square_tri(3), mg.unit_cube_hex(2)])
@@ -58,7 +60,7 @@ def test_data_files(tmp_path):
     np.testing.assert_allclose(sio.read_vector(tmp_path / "v.dat"), v, rtol=1e-6)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_APP), reason="reference tree not present")
+@pytest.mark.skipif(not REF_APP or not os.path.isdir(REF_APP), reason="STATFEM_REFERENCE not set")
 def test_reference_app_inputs_parse_to_fixture():
     k = np.load(os.path.join(ROOT, "tests", "golden", "kat1_laplaceRHSinfer.npz"))
     top = sio.read_properties(os.path.join(REF_APP, "input.dat"))
