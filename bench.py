@@ -38,7 +38,8 @@ sys.path.insert(0, ROOT)
 from statfem_b200 import meshgen as mg  # noqa: E402
 
 from statfem_b200.workloads import C2_HP as HP  # noqa: E402
-from statfem_b200.workloads import C3_HP, REG, make_batch_workload, make_workload, subset_batch  # noqa: E402
+from statfem_b200.workloads import C3_HP, REG, make_batch_workload, make_workload, multi_rhs_columns  # noqa: E402
+from statfem_b200.workloads import subset_batch  # noqa: E402
 
 # the headline metric, verbatim
 METRIC = "posterior solves/s at rel. residual 1e-8, learned+batched vs plain PCG, 1xB200"
@@ -252,7 +253,7 @@ def run_ours(args, ws, rank, local):
     barrier(ws)
     cuda_sync(ws)
     ctx.synchronize()
-    l0 = ctx.kernel_launches()
+    l0, gl0 = ctx.kernel_launches(), ctx.graph_launches()
     with ClockSampler(local) as clk:
         ctx.mark(0)
         for _ in range(args.steps):
@@ -263,6 +264,7 @@ def run_ours(args, ws, rank, local):
     barrier(ws)
     ms = ctx.marker_ms(0, 1)
     launches = ctx.kernel_launches() - l0
+    graph_launches = ctx.graph_launches() - gl0
     block_stats = g.s.last_stats()
     ms_max = max_over_ranks(ws, ms)
     # kernel timing: the same steps again with an event pair around every hot
@@ -326,6 +328,7 @@ def run_ours(args, ws, rank, local):
                  "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                  "wall_s": round(e2e_wall, 3)} if e2e_steps else None),
         "gpu_launches": int(launches),
+        "graph_launches": int(graph_launches),
         "roofline": roof,
         "kernels": {k: {"launches": v[0], "ms": round(v[1], 3), "GBps": round(v[2] / max(v[1], 1e-9) / 1e6, 1)}
                     for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
@@ -606,44 +609,30 @@ def batch_plain_estimate(ctx, wl, sample):
                          len(sides))}
 
 
-def pivoted_cholesky(K, rel=1e-12):
-    """Greedy (largest remaining diagonal) pivoted Cholesky K ~ L L^T, stopped
-    when the largest remaining diagonal drops below rel * max(diag K)."""
-    n = K.shape[0]
-    d = np.diag(K).astype(np.float64).copy()
-    L = np.zeros((n, 0))
-    stop = rel * d.max()
-    while L.shape[1] < n and d.max() > stop:
-        j = int(np.argmax(d))
-        col = (K[:, j] - L @ L[j]) / np.sqrt(d[j])
-        L = np.column_stack([L, col])
-        d = np.maximum(d - col * col, 0.0)
-        d[j] = 0.0
-    return L
-
-
-def multi_rhs_columns(wl, nrhs, sigma, length):
-    """The nrhs leading columns of the forcing covariance's factor on the c2
-    grid: diag(phibar) (Lz (x) Ly (x) Lx) with L_a the pivoted Cholesky factor
-    of exp(-d^2/(2 l^2)) on axis a (numerical rank to 1e-12), the Kronecker
-    columns ordered by decreasing norm, one displacement component per column
-    (cycling x, y, z), scaled by sigma.  Returns nrhs x num_dofs."""
-    mesh = wl["mesh"]
-    n = mesh.grid[0] + 1
-    x = np.arange(n) / (n - 1)
-    L = pivoted_cholesky(np.exp(-(x[:, None] - x[None, :]) ** 2 / (2 * length * length)))
-    nrm = np.linalg.norm(L, axis=0)
-    r = L.shape[1]
-    w = np.einsum("i,j,k->ijk", nrm, nrm, nrm).ravel()
-    order = np.argsort(-w, kind="stable")
-    phibar = wl["phibar"]
-    out = np.zeros((nrhs, mesh.num_dofs))
-    for c in range(nrhs):
-        t = order[c // 3] if c // 3 < len(order) else order[-1]
-        kz, ky, kx = t // (r * r), (t // r) % r, t % r
-        v = sigma * np.einsum("i,j,k->ijk", L[:, kz], L[:, ky], L[:, kx]).ravel()  # z slowest, x fastest
-        out[c, c % 3::3] = v
-    return out * phibar[None, :]
+def c4_accuracy(wl, B, U):
+    """Per-column errors of the multi-RHS solutions against the committed
+    FP64 oracle fixture (tests/golden/c4_oracle.npz: 16 columns solved by the
+    oracle's Jacobi-PCG to 1e-13; made by tests/golden/make_c4_oracle.py),
+    through the functionals the fixture keeps: the values at the 256 sensor
+    rows and the energy u^T b.  Only the fixture's arrays are read here."""
+    from statfem_b200.workloads import fingerprint
+    path = os.path.join(ROOT, "tests", "golden", "c4_oracle.npz")
+    if not os.path.exists(path):
+        return None
+    f = np.load(path)
+    pick = f["pick"]
+    if (not np.allclose(f["fingerprint"], fingerprint(wl), rtol=1e-12, atol=0)
+            or not np.allclose(f["b_sums"], B[pick].sum(axis=1), rtol=1e-12, atol=1e-300)):
+        return None
+    Pd = mg.projection_dense(wl["mesh"], *wl["P"])
+    pu = Pd @ U[pick].T
+    en = np.einsum("ij,ij->i", U[pick], B[pick])
+    sens = np.abs(pu - f["Pu"]).max(axis=0) / np.abs(f["Pu"]).max(axis=0)
+    ener = np.abs(en - f["energy"]) / np.abs(f["energy"])
+    return {"columns": int(len(pick)), "sensor_values_max_rel": float(sens.max()),
+            "energy_max_rel": float(ener.max()),
+            "oracle": "FP64 Jacobi-PCG to rel. residual 1e-13 on 16 evenly spaced columns; oracle's own change "
+                      "from 1e-11 to 1e-13: %.1e" % float(f["est_rel_change_1e11_to_1e13"])}
 
 
 def run_multi(args, ws, rank, local):
@@ -682,12 +671,9 @@ def run_multi(args, ws, rank, local):
     launches = ctx.kernel_launches() - l0
     st = s.last_stats()
     U = Ud.cpu().numpy().T
-    # per-column error against FP64 Jacobi-PCG to 1e-13 on a sample of columns
+    accuracy = c4_accuracy(wl, B, U) if rank == 0 and nrhs == 1024 else None
     pick = np.linspace(0, nrhs - 1, args.c4_check).astype(int)
-    s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-13, max_iter=200000, check_every=32)
-    Uref = s.solveSystemMulti(B[pick])
-    errs = [float(np.linalg.norm(U[k] - Uref[t]) / np.linalg.norm(Uref[t])) for t, k in enumerate(pick)]
-    # plain FP64 PCG at 1e-10, one column at a time, on the sample
+    # plain FP64 PCG at 1e-10, one column at a time, on a sample of columns
     s.set_options(method=api.SFC_SOLVER_PCG_FP64, tol=1e-10, max_iter=200000, check_every=32)
     s.solveSystemMulti(B[pick])
     plain = s.last_stats()
@@ -715,8 +701,7 @@ def run_multi(args, ws, rank, local):
                 "h2d_bytes_per_step": int(B.nbytes), "d2h_bytes_per_step": int(B.nbytes)},
         "gpu_launches": int(launches),
         "solver": st,
-        "column_error_vs_fp64_pcg_1e-13": {"max": max(errs), "median": float(np.median(errs)),
-                                           "columns": len(errs)},
+        "accuracy_vs_fp64_oracle": accuracy,
         "plain_fp64": {"value": round(len(pick) / (plain["device_ms"] / 1e3), 3), "unit": "RHS solves/s",
                        "sample": "%d columns, FP64 Jacobi-PCG one at a time to 1e-10, max %d iterations"
                                  % (len(pick), plain["iterations"])},

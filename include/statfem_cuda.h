@@ -133,8 +133,12 @@ int32_t sfc_ctx_create(int32_t device, sfc_ctx_t **out);
 int32_t sfc_ctx_destroy(sfc_ctx_t *ctx);
 const char *sfc_last_error(const sfc_ctx_t *ctx);
 int32_t sfc_ctx_synchronize(sfc_ctx_t *ctx);
-/* Number of kernels this library has launched on the context. */
+/* Number of kernels this library has launched on the context (kernels inside
+ * a replayed CUDA graph included). */
 int32_t sfc_ctx_kernel_launches(const sfc_ctx_t *ctx, int64_t *count);
+/* Number of CUDA graphs this library has launched on the context (the mixed
+ * block solver's captured check intervals, batch steps, dense inverses). */
+int32_t sfc_ctx_graph_launches(const sfc_ctx_t *ctx, int64_t *count);
 /* Device time between two markers recorded on the context stream. */
 int32_t sfc_ctx_mark(sfc_ctx_t *ctx, int32_t slot);
 int32_t sfc_ctx_marker_ms(sfc_ctx_t *ctx, int32_t slot_begin, int32_t slot_end, double *ms);

@@ -105,6 +105,7 @@ SIGNATURES = {
     "sfc_last_error": (ctypes.c_char_p, [_vp]),
     "sfc_ctx_synchronize": (_i32, [_vp]),
     "sfc_ctx_kernel_launches": (_i32, [_vp, _i64p]),
+    "sfc_ctx_graph_launches": (_i32, [_vp, _i64p]),
     "sfc_ctx_mark": (_i32, [_vp, _i32]),
     "sfc_ctx_marker_ms": (_i32, [_vp, _i32, _i32, _dp]),
     "sfc_ctx_set_profiling": (_i32, [_vp, _i32]),
@@ -240,6 +241,11 @@ class Context:
         c = ctypes.c_int64()
         self.check(self.lib.sfc_ctx_kernel_launches(self.h, ctypes.byref(c)))
         return c.value
+
+    def graph_launches(self):
+        v = ctypes.c_int64()
+        self.check(self.lib.sfc_ctx_graph_launches(self.h, ctypes.byref(v)))
+        return v.value
 
     def mark(self, slot):
         self.check(self.lib.sfc_ctx_mark(self.h, slot))

@@ -127,6 +127,13 @@ int32_t sfc_ctx_kernel_launches(const sfc_ctx_t *ctx, int64_t *count)
     return SFC_OK;
 }
 
+int32_t sfc_ctx_graph_launches(const sfc_ctx_t *ctx, int64_t *count)
+{
+    if (!ctx || !count) return SFC_ERR_BAD_ARG;
+    *count = ctx->graph_replays;
+    return SFC_OK;
+}
+
 int32_t sfc_ctx_mark(sfc_ctx_t *ctx, int32_t slot)
 {
     if (!ctx || slot < 0 || slot >= 16) return SFC_ERR_BAD_ARG;

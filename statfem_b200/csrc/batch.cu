@@ -861,6 +861,7 @@ void batch_run(sfc_batch *b)
     ProfScope ps(ctx, "phase:batch_solve_likelihood", 0.0);
     SFC_CK(cudaGraphLaunch(b->gexec, ctx->stream));
     count_launch(ctx);
+    ++ctx->graph_replays;
 }
 
 }  // namespace sfc

@@ -92,7 +92,8 @@ struct sfc_ctx {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     std::string err;
-    int64_t launches = 0;
+    int64_t launches = 0;        // kernels launched (also those inside graph replays)
+    int64_t graph_replays = 0;   // graph launches (each counted once here)
     cudaEvent_t marks[16] = {};
     // pinned host scratch for small device->host reads
     void *pinned = nullptr;
@@ -233,6 +234,25 @@ struct GjScratch {
     void drop_graphs();
 };
 
+// An instantiated CUDA graph of a captured launch sequence, with the key
+// (pointers and sizes baked into its launches) it was captured for.
+struct GraphExec {
+    std::vector<uintptr_t> key;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;  // kernel launches per replay
+    GraphExec() = default;
+    GraphExec(const GraphExec &) = delete;
+    GraphExec &operator=(const GraphExec &) = delete;
+    ~GraphExec() { reset(); }
+    void reset()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+        kernels = 0;
+    }
+};
+
 struct CoarseSpace {
     bool built = false;                 // aggregates for (mesh, size)
     const sfc_mesh *mesh = nullptr;
@@ -360,6 +380,9 @@ struct sfc_system {
     int spmv_lanes = 0;               // lanes per row of the FP64 SpMV (0: by row length; set by the tuner)
     uint64_t op_serial = 0;           // bumped by every operator (re)build
     sfc::CoarseSpace coarse;          // SFC_PRECOND_TWO_LEVEL
+    // the mixed block solver's check interval of iterations, captured once
+    // per launch configuration (block widths 32, 64, 128)
+    sfc::GraphExec blk_graph[3];
 };
 
 // ---------------------------------------------------------------------------
@@ -428,6 +451,7 @@ void build_operator(sfc_system *s, bool require_positive_diag = true);
 // lattice.cu
 void build_lattice_blocks(sfc_system *s);
 void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop);
+void lattice_prepare(sfc_system *s, const float *P, int K);
 void lattice_check(sfc_system *s);
 void flush_staged(sfc_system *s);
 void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);

@@ -237,6 +237,7 @@ void spd_inverse_gj(sfc_ctx *ctx, double *A, int64_t n, double rel, GjScratch &w
     }
     SFC_CK(cudaGraphLaunch(g->exec, ctx->stream));
     count_launch(ctx, nlaunch);
+    ++ctx->graph_replays;
     int h = 0;
     download(ctx, &h, w.word.p, 1);
     if (dropped) *dropped = h;

@@ -241,6 +241,8 @@ __global__ void k_lattice_fill(const int32_t *__restrict__ bptr, const int32_t *
     }
 }
 
+int g_occ = 0;  // resident CTAs per SM of k_lspmm32
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -291,9 +293,10 @@ void build_lattice_blocks(sfc_system *s)
     s->has_lattice = true;
 }
 
-void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop)
+// the tensor map of P and the kernel's attributes, set up outside any
+// stream capture
+void lattice_prepare(sfc_system *s, const float *P, int K)
 {
-    sfc_ctx *ctx = s->ctx;
     const int nx = s->lat[0], ny = s->lat[1], nz = s->lat[2];
     SFC_REQUIRE(K % CS == 0, "lattice SpMM needs a multiple of 64 columns");
     if (s->pmap_ptr != P || s->pmap_K != K) {
@@ -309,12 +312,19 @@ void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, 
         s->pmap_ptr = P;
         s->pmap_K = K;
     }
-    static int occ = 0;
-    if (!occ) {
+    if (!g_occ) {
         SFC_CK(cudaFuncSetAttribute(k_lspmm32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-        SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_lspmm32, THREADS, SMEM_BYTES));
-        if (occ < 1) occ = 1;
+        SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32, THREADS, SMEM_BYTES));
+        if (g_occ < 1) g_occ = 1;
     }
+}
+
+void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop)
+{
+    sfc_ctx *ctx = s->ctx;
+    const int nx = s->lat[0], ny = s->lat[1], nz = s->lat[2];
+    lattice_prepare(s, P, K);
+    const int occ = g_occ;
     const int slices = K / CS;
     const int64_t tiles = (int64_t)((nx + BX - 1) / BX) * ((ny + BY - 1) / BY) * ((nz + BZ - 1) / BZ);
     const int64_t work = tiles * slices;

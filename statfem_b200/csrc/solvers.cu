@@ -1458,9 +1458,25 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         double *p;
     } b64{s->blk64.p}, x64{s->blk64.p + N * K}, r64{s->blk64.p + 2 * N * K}, cs{s->colsc.p};
     float *xr = s->blk32.p, *rr32 = xr + N * K, *pp = rr32 + N * K, *qq = pp + N * K;
-    const int64_t nsc = 3 * (int64_t)(max_iter + 2) * K;
+    // per-iteration column scalars p.q, r.z, r.r in a ring of R slots:
+    // iteration it reads slot it % R and accumulates into (it + 1) % R.  With
+    // R = check every check-interval chunk uses the same slots, so one
+    // captured graph serves every chunk.
+    const int R = check >= 2 ? check : 2;
+    const int64_t nsc = 3 * (int64_t)R * K;
     s->scal.reserve(nsc);
-    double *pq = s->scal.p, *rz = pq + (int64_t)(max_iter + 2) * K, *rrs = rz + (int64_t)(max_iter + 2) * K;
+    double *pq = s->scal.p, *rz = pq + (int64_t)R * K, *rrs = rz + (int64_t)R * K;
+    auto slot = [&](int i) { return (int64_t)(i % R) * K; };
+    // before a chunk: every p.q slot and every r.z / r.r slot except `keep`
+    // (the chunk's first iteration reads it) start at zero
+    auto zero_ring = [&](int keep) {
+        SFC_CK(cudaMemsetAsync(pq, 0, (size_t)R * K * 8, ctx->stream));
+        for (double *a : {rz, rrs}) {
+            if (keep > 0) SFC_CK(cudaMemsetAsync(a, 0, (size_t)keep * K * 8, ctx->stream));
+            if (keep + 1 < R)
+                SFC_CK(cudaMemsetAsync(a + (int64_t)(keep + 1) * K, 0, (size_t)(R - keep - 1) * K * 8, ctx->stream));
+        }
+    };
     double *bn2 = cs.p, *rn2 = bn2 + K, *scale = rn2 + K, *norm = scale + K, *thr = norm + K;
     // flags[0]: all columns below their thresholds; flags[1 + c]: breakdown
     // (p^T A p <= 0) in column c
@@ -1531,6 +1547,111 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                                                       rr_slot);
         count_launch(ctx);
     };
+    // one inner iteration: Q = S P, alpha, x/r update with r.z and r.r,
+    // coarse correction, beta and the p update
+    auto iterate = [&](int it) {
+        const int64_t o0 = slot(it), o1 = slot(it + 1);
+        spmm(pp, qq, pq + o0);
+        {
+            ProfScope ps(ctx, "bupdate32", (bj ? 3.0 : 6.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N);
+            if (bj)
+                k_nupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pq + o0,
+                                                                   rz + o0, rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+            else
+                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
+                                                            rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+        }
+        if (two_any) coarse_block_apply<V>(s, rr32, rz + o1, stop);
+        {
+            ProfScope ps(ctx, "bpupdate32",
+                         (bj ? 5.0 : 3.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
+            if (two)
+                k_ncpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, crs.node_agg.p,
+                                                                     crs.mode.p, crs.e32.p, s->nodes, rz + o0, rz + o1,
+                                                                     rrs + o1, thr, stop, err, nullptr, xr, pq + o0,
+                                                                     rrs + o0);
+            else if (bj)
+                k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz + o0, rz + o1,
+                                                             rrs + o1, thr, stop, err, xr, pq + o0, rrs + o0);
+            else if (two1)
+                k_cbpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, crs.node_agg.p,
+                                                                     crs.mode.p, crs.e32.p, N, rz + o0, rz + o1,
+                                                                     rrs + o1, thr, stop, err, nullptr);
+            else
+                k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
+                                                             thr, stop, err);
+        }
+        count_launch(ctx, 2);
+    };
+    // A whole check interval as one CUDA graph: the ring's zeroing, `check`
+    // iterations and the convergence flag, captured once per launch
+    // configuration (the key lists every pointer and size baked into the
+    // launches) and replayed for every later interval.  Not used while kernel
+    // profiling records events around each launch, nor with
+    // SFC_BLOCK_GRAPH=0 in the environment.
+    const char *genv = std::getenv("SFC_BLOCK_GRAPH");
+    const bool use_graph = !ctx->prof && check >= 2 && !(genv && genv[0] == '0');
+    const bool lattice = bsr && s->has_lattice && K >= 64;
+    auto launch_chunk_graph = [&]() {
+        GraphExec &g = s->blk_graph[V == 1 ? 0 : V == 2 ? 1 : 2];
+        // everything the captured launches allocate or set up, done outside the capture
+        if (two_any) {
+            s->coarse.c32.reserve(crs.nc * K);
+            s->coarse.e32.reserve(crs.nc * K);
+        }
+        if (lattice) lattice_prepare(s, pp, K);
+        const std::vector<uintptr_t> key = {
+            (uintptr_t)K, (uintptr_t)check, (uintptr_t)N, (uintptr_t)s->nodes, (uintptr_t)gw,
+            (uintptr_t)(bsr | (bj << 1) | (two << 2) | (two1 << 3) | (lattice << 4)), (uintptr_t)s->scal.p,
+            (uintptr_t)s->blk32.p, (uintptr_t)s->colsc.p, (uintptr_t)s->flags.p, (uintptr_t)s->bdinv32.p,
+            (uintptr_t)s->dinv32.p, (uintptr_t)s->bptr.p, (uintptr_t)s->bcol.p, (uintptr_t)s->bval32.p,
+            (uintptr_t)s->row_ptr.p, (uintptr_t)s->col.p, (uintptr_t)s->a_op32.p, (uintptr_t)s->bq.p,
+            (uintptr_t)s->lat_err.p, (uintptr_t)s->lat[0], (uintptr_t)s->lat[1], (uintptr_t)s->lat[2],
+            (uintptr_t)s->pmap_ptr, (uintptr_t)crs.agg_ptr.p, (uintptr_t)crs.agg_nodes.p, (uintptr_t)crs.mode.p,
+            (uintptr_t)crs.c32.p, (uintptr_t)crs.e32.p, (uintptr_t)crs.a32.p, (uintptr_t)crs.node_agg.p,
+            (uintptr_t)crs.nagg, (uintptr_t)crs.nc, (uintptr_t)crs.dof};
+        if (!g.exec || g.key != key) {
+            g.reset();
+            cudaStream_t st;
+            SFC_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            const cudaStream_t keep = ctx->stream;
+            const int64_t l0 = ctx->launches;
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                ctx->stream = st;
+                try {
+                    zero_ring(0);
+                    for (int j = 0; j < check; ++j) iterate(j);
+                    k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + slot(check), thr, stop);
+                    count_launch(ctx);
+                } catch (...) {
+                    ctx->stream = keep;
+                    cudaStreamEndCapture(st, &graph);
+                    if (graph) cudaGraphDestroy(graph);
+                    cudaStreamDestroy(st);
+                    ctx->launches = l0;
+                    throw;
+                }
+                ctx->stream = keep;
+                e = cudaStreamEndCapture(st, &graph);
+            }
+            cudaStreamDestroy(st);
+            const int64_t captured = ctx->launches - l0;
+            ctx->launches = l0;
+            SFC_CK(e);
+            cudaGraphExec_t exec = nullptr;
+            e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            SFC_CK(e);
+            g.exec = exec;
+            g.key = key;
+            g.kernels = captured;
+        }
+        SFC_CK(cudaGraphLaunch(g.exec, ctx->stream));
+        ctx->launches += g.kernels;
+        ++ctx->graph_replays;
+    };
     // Reliable-update mixed-precision block PCG.  Each column is scaled to
     // ||b|| = 1 and iterated in FP32; whenever every active column's recurrence
     // residual has dropped by a decade since the last update (or has fallen
@@ -1585,41 +1706,23 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             init32(rz, rrs);
         }
         while (nactive > 0) {
-            const int64_t o0 = (int64_t)it * K, o1 = (int64_t)(it + 1) * K;
-            spmm(pp, qq, pq + o0);
-            {
-                ProfScope ps(ctx, "bupdate32", (bj ? 3.0 : 6.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N);
-                if (bj)
-                    k_nupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pq + o0,
-                                                                rz + o0, rrs + o0, thr, rz + o1, rrs + o1, stop, err);
-                else
-                    k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
-                                                                rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+            bool ran_graph = false;
+            if (it % check == 0 && use_graph && it + check <= max_iter) {
+                launch_chunk_graph();
+                it += check;
+                ran_graph = true;
+            } else {
+                if (it % check == 0) zero_ring((int)(it % R));
+                iterate(it);
+                ++it;
             }
-            if (two_any) coarse_block_apply<V>(s, rr32, rz + o1, stop);
-            {
-                ProfScope ps(ctx, "bpupdate32", (bj ? 5.0 : 3.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
-                if (two)
-                    k_ncpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, crs.node_agg.p,
-                                                                         crs.mode.p, crs.e32.p, s->nodes, rz + o0,
-                                                                         rz + o1, rrs + o1, thr, stop, err, nullptr, xr, pq + o0, rrs + o0);
-                else if (bj)
-                    k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz + o0, rz + o1,
-                                                                 rrs + o1, thr, stop, err, xr, pq + o0, rrs + o0);
-                else if (two1)
-                    k_cbpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, crs.node_agg.p,
-                                                                         crs.mode.p, crs.e32.p, N, rz + o0, rz + o1,
-                                                                         rrs + o1, thr, stop, err, nullptr);
-                else
-                    k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
-                                                                 thr, stop, err);
-            }
-            count_launch(ctx, 2);
-            ++it;
+            const int64_t o1 = slot(it);
             const bool at_cap = it >= max_iter;
-            if (it % check != 0 && !at_cap) continue;
-            k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + o1, thr, stop);
-            count_launch(ctx);
+            if (!ran_graph) {
+                if (it % check != 0 && !at_cap) continue;
+                k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + o1, thr, stop);
+                count_launch(ctx);
+            }
             download(ctx, hflags.data(), s->flags.p, 1 + K);
             download(ctx, rr_now.data(), rrs + o1, K);
             bool update = hflags[0] || at_cap;

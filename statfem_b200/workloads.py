@@ -130,3 +130,45 @@ def fingerprint(wl):
     ip, ix, dv = wl["P"]
     return np.array([wl["coeff"].sum(), float(np.dot(wl["coeff"], np.arange(len(wl["coeff"])) % 97)),
                      dv.sum(), float(ix.sum()), wl["pts"].sum(), float(len(wl["bc"]))])
+
+
+def pivoted_cholesky(K, rel=1e-12):
+    """Greedy (largest remaining diagonal) pivoted Cholesky K ~ L L^T, stopped
+    when the largest remaining diagonal drops below rel * max(diag K)."""
+    n = K.shape[0]
+    d = np.diag(K).astype(np.float64).copy()
+    L = np.zeros((n, 0))
+    stop = rel * d.max()
+    while L.shape[1] < n and d.max() > stop:
+        j = int(np.argmax(d))
+        col = (K[:, j] - L @ L[j]) / np.sqrt(d[j])
+        L = np.column_stack([L, col])
+        d = np.maximum(d - col * col, 0.0)
+        d[j] = 0.0
+    return L
+
+
+def multi_rhs_columns(wl, nrhs, sigma, length, cols=None):
+    """The nrhs leading columns of the forcing covariance's factor on the c2
+    grid: diag(phibar) (Lz (x) Ly (x) Lx) with L_a the pivoted Cholesky factor
+    of exp(-d^2/(2 l^2)) on axis a (numerical rank to 1e-12), the Kronecker
+    columns ordered by decreasing norm, one displacement component per column
+    (cycling x, y, z), scaled by sigma.  Returns nrhs x num_dofs, or only the
+    rows `cols` of it (len(cols) x num_dofs)."""
+    mesh = wl["mesh"]
+    n = mesh.grid[0] + 1
+    x = np.arange(n) / (n - 1)
+    L = pivoted_cholesky(np.exp(-(x[:, None] - x[None, :]) ** 2 / (2 * length * length)))
+    nrm = np.linalg.norm(L, axis=0)
+    r = L.shape[1]
+    w = np.einsum("i,j,k->ijk", nrm, nrm, nrm).ravel()
+    order = np.argsort(-w, kind="stable")
+    phibar = wl["phibar"]
+    cols = range(nrhs) if cols is None else [int(c) for c in cols]
+    out = np.zeros((len(cols), mesh.num_dofs))
+    for row, c in enumerate(cols):
+        t = order[c // 3] if c // 3 < len(order) else order[-1]
+        kz, ky, kx = t // (r * r), (t // r) % r, t % r
+        v = sigma * np.einsum("i,j,k->ijk", L[:, kz], L[:, ky], L[:, kx]).ravel()  # z slowest, x fastest
+        out[row, c % 3::3] = v
+    return out * phibar[None, :]

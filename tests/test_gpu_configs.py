@@ -129,3 +129,34 @@ def test_c2_headline_against_fp64_oracle():
                post_cov=pc)
     errs = check_all(got, ref)
     print("c2 relative errors against the FP64 oracle:", errs)
+
+
+GOLDEN_C4 = os.path.join(os.path.dirname(__file__), "golden", "c4_oracle.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(GOLDEN_C4), reason="c4 oracle fixture not generated")
+def test_c4_columns_against_fp64_oracle():
+    """Multi-RHS prior covariance columns on the 48^3 elasticity mesh (mixed
+    block PCG with the two-level preconditioner, rel. residual 1e-10): the
+    oracle fixture's 16 columns, compared through the functionals it keeps
+    (values at the 256 sensor rows, energy u^T b)."""
+    from statfem_b200.workloads import fingerprint, multi_rhs_columns
+    f = np.load(GOLDEN_C4)
+    wl = make_workload("c2", seed=1234)
+    assert np.allclose(f["fingerprint"], fingerprint(wl), rtol=1e-12, atol=0), "workload generator changed"
+    g = bench.GpuStatFEM(wl, 0, api.SFC_SOLVER_PCG_MIXED, 128, api.SFC_PRECOND_TWO_LEVEL)
+    wl["phibar"] = g.cf.phibar()
+    pick = f["pick"]
+    B = multi_rhs_columns(wl, 1024, wl["hp"]["forcing.sigma"], wl["hp"]["forcing.length"], cols=pick)
+    assert np.allclose(f["b_sums"], B.sum(axis=1), rtol=1e-12, atol=0)
+    g.s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, max_iter=30000, inner_tol=1e-4, block_width=128,
+                    check_every=32, precond=api.SFC_PRECOND_TWO_LEVEL)
+    U = g.s.solveSystemMulti(B)
+    st = g.s.last_stats()
+    assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
+    Pd = mg.projection_dense(wl["mesh"], *wl["P"])
+    pu = Pd @ U.T
+    en = np.einsum("ij,ij->i", U, B)
+    sens = (np.abs(pu - f["Pu"]).max(axis=0) / np.abs(f["Pu"]).max(axis=0)).max()
+    ener = (np.abs(en - f["energy"]) / np.abs(f["energy"])).max()
+    assert sens < 1e-7 and ener < 1e-7, (sens, ener)

@@ -60,3 +60,32 @@ def test_system_beyond_32bit_indices_is_rejected(ctx):
     with pytest.raises(api.SfcError) as e:
         api.SystemSolveCuda(ctx, 2 ** 31)
     assert e.value.code == api.SFC_ERR_TOO_LARGE
+
+
+@pytest.mark.parametrize("precond", [api.SFC_PRECOND_BLOCK_JACOBI, api.SFC_PRECOND_TWO_LEVEL])
+def test_check_interval_graph_matches_eager_launches(ctx, precond):
+    """The mixed solver's check intervals replayed from a captured CUDA graph
+    give the eager launch sequence's answer (the same kernels in the same
+    order), with one graph launch per interval instead of a launch per
+    kernel."""
+    results = {}
+    for mode in ("graph", "eager"):
+        if mode == "eager":
+            os.environ["SFC_BLOCK_GRAPH"] = "0"
+        try:
+            g0, k0 = ctx.graph_launches(), ctx.kernel_launches()
+            U, st, ds, Rhs = solve(ctx, 5, 128, precond, nrhs=100)
+            results[mode] = (U, st, ctx.graph_launches() - g0, ctx.kernel_launches() - k0)
+        finally:
+            os.environ.pop("SFC_BLOCK_GRAPH", None)
+    Ug, stg, gg, kg = results["graph"]
+    Ue, ste, ge, ke = results["eager"]
+    refs = np.stack([ds.solve_transpose(r) for r in Rhs])
+    for U in (Ug, Ue):
+        assert np.abs(U - refs).max() <= 1e-7 * np.abs(refs).max()
+    assert stg["converged"] == ste["converged"] == 1
+    assert abs(stg["iterations"] - ste["iterations"]) <= 32
+    # check_every is 16 here: one replay per 16 iterations (the coarse
+    # inverse's own graphs are launched in both modes)
+    assert gg - ge >= max(1, stg["iterations"] // 16 - 1)
+    assert kg > 0 and ke > 0

@@ -83,3 +83,22 @@ def test_c2_fixture_is_consistent():
     assert np.abs(pm - g["post_mean"]).max() <= 1e-12 * np.abs(pm).max()
     ll = O.koh_log_likelihood(g["mean_s"], C, Ks, g["Y"], hp["rho"])
     assert abs(ll - float(g["loglik"])) <= 1e-10 * abs(ll)
+
+
+GOLDEN_C4 = os.path.join(os.path.dirname(__file__), "golden", "c4_oracle.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(GOLDEN_C4), reason="c4 oracle fixture not generated")
+def test_c4_fixture_is_consistent():
+    """The multi-RHS oracle fixture was made from the workload generator's
+    columns, and its oracle error estimate is far below 1e-7."""
+    from statfem_b200.workloads import fingerprint, make_workload, multi_rhs_columns
+    f = np.load(GOLDEN_C4)
+    wl = make_workload("c2", seed=1234)
+    assert np.allclose(f["fingerprint"], fingerprint(wl), rtol=1e-12, atol=0)
+    wl["phibar"] = O.unit_load(wl["mesh"], wl["qps"], wl["bc"])
+    B = multi_rhs_columns(wl, 1024, wl["hp"]["forcing.sigma"], wl["hp"]["forcing.length"], cols=f["pick"])
+    assert np.allclose(f["b_sums"], B.sum(axis=1), rtol=1e-12, atol=0)
+    assert np.allclose(f["b_norms"], np.linalg.norm(B, axis=1), rtol=1e-12, atol=0)
+    assert float(f["est_rel_change_1e11_to_1e13"]) < 1e-9
+    assert (f["energy"] > 0).all()
