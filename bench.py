@@ -323,6 +323,9 @@ def run_ours(args, ws, rank, local):
         "config": {"workload": wl["desc"], "block_width": args.block_width, "precond": args.precond,
                    "method": "mixed block PCG (%s preconditioner)" % args.precond if args.method == "mixed"
                    else "plain FP64 Jacobi-PCG", "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "learned_part": "not in this step: the learned preconditioner (FCG + message-passing "
+                                   "network, --config c5) gains iterations over Jacobi but loses wall time "
+                                   "to this step's two-level preconditioner",
                    "l2": "inputs larger than L2 (matrix 220+ MB)"},
         "e2e": ({"value": round(ws * e2e_steps / (e2e_ms / 1e3), 4), "unit": "posterior solves/s",
                  "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

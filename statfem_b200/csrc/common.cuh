@@ -374,6 +374,7 @@ struct sfc_system {
     sfc::DBuf<double> colsc;   // per-column scalars
     sfc::DBuf<int> restart;    // per-column restart flags
     sfc::DBuf<double> tmpN, tmpN2;
+    sfc::DBuf<double> fwd_rhs;  // lifted forward right-hand side (the mixed solver uses tmpN itself)
     sfc::DBuf<uint32_t> cidx;  // constraint upload buffers
     sfc::DBuf<double> cval;
     struct sfc_mpnn *mpnn = nullptr;  // learned preconditioner for SFC_SOLVER_FCG_MPNN

@@ -829,7 +829,7 @@ __global__ void __launch_bounds__(256) k_ninit32(const double *__restrict__ R64,
 // XUPD = false: x is left to the p update (k_npupdate32 / k_ncpupdate32 with
 // x given), so this pass reads r and q only
 template <int V, bool XUPD = true>
-__global__ void __launch_bounds__(256) k_nupdate32(float *__restrict__ x, float *__restrict__ r,
+__global__ void __launch_bounds__(256, 4) k_nupdate32(float *__restrict__ x, float *__restrict__ r,
                                                    const float *__restrict__ p, const float *__restrict__ q,
                                                    const float *__restrict__ bdinv, int64_t nodes, const double *pq,
                                                    const double *rz, const double *rr, const double *thr,
@@ -945,8 +945,9 @@ __global__ void __launch_bounds__(256) k_npupdate32(float *__restrict__ p, const
 // correction e of the node's aggregate a, M_n = diag(free) [I | R(d_n)]:
 // translation t plus rotation w x d), then p = z + beta p for the active
 // columns.  INIT: p = z for the restarted columns, others keep p.
+// (four 256-thread CTAs per SM: at most 64 registers)
 template <int V, bool INIT>
-__global__ void __launch_bounds__(256) k_ncpupdate32(float *__restrict__ p, const float *__restrict__ r,
+__global__ void __launch_bounds__(256, 4) k_ncpupdate32(float *__restrict__ p, const float *__restrict__ r,
                                                      const float *__restrict__ bdinv,
                                                      const int32_t *__restrict__ node_agg,
                                                      const float4 *__restrict__ mode, const float *__restrict__ e,
@@ -982,17 +983,32 @@ __global__ void __launch_bounds__(256) k_ncpupdate32(float *__restrict__ p, cons
         const int32_t a = node_agg[n];
         const float4 m = mode[n];
         const int bits = (int)m.w;
-        float ev[6][V];
+        // M_n e_a streamed one mode row at a time (translations, then the
+        // rotations w x d), so that only one row of e is live
+        const float *ea = e + 6 * (int64_t)a * K + lane * V;
+        float cc[3][V], t[V];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) ldv<V>(e + (6 * (int64_t)a + k) * K + lane * V, ev[k]);
+        for (int k = 0; k < 3; ++k) ldv<V>(ea + k * K, cc[k]);
+        ldv<V>(ea + 3 * K, t);
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-            const float c0 = ev[0][v] + ev[4][v] * m.z - ev[5][v] * m.y;
-            const float c1 = ev[1][v] + ev[5][v] * m.x - ev[3][v] * m.z;
-            const float c2 = ev[2][v] + ev[3][v] * m.y - ev[4][v] * m.x;
-            if (!(bits & 1)) zv[0][v] += c0;
-            if (!(bits & 2)) zv[1][v] += c1;
-            if (!(bits & 4)) zv[2][v] += c2;
+            cc[1][v] -= t[v] * m.z;
+            cc[2][v] += t[v] * m.y;
+        }
+        ldv<V>(ea + 4 * K, t);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            cc[0][v] += t[v] * m.z;
+            cc[2][v] -= t[v] * m.x;
+        }
+        ldv<V>(ea + 5 * K, t);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            cc[0][v] -= t[v] * m.y;
+            cc[1][v] += t[v] * m.x;
+            if (!(bits & 1)) zv[0][v] += cc[0][v];
+            if (!(bits & 2)) zv[1][v] += cc[1][v];
+            if (!(bits & 4)) zv[2][v] += cc[2][v];
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
@@ -1920,8 +1936,8 @@ void solve_forward(sfc_system *s)
     build_operator(s);
     const int64_t N = s->N;
     s->X.alloc(N);
-    s->tmpN.reserve(N);
-    DBuf<double> &b = s->tmpN;
+    s->fwd_rhs.reserve(N);
+    DBuf<double> &b = s->fwd_rhs;
     k_lift<<<grid_for(N, 256), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, s->diag.p, s->a_ref.p, s->mask.p, s->F.p,
                                                       N, b.p);
     count_launch(ctx);
