@@ -253,6 +253,25 @@ struct GraphExec {
     }
 };
 
+// A pair of CUDA events kept for the life of their owner (timing of repeated
+// solves without creating events per call).
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() = default;
+    EventPair(const EventPair &) = delete;
+    EventPair &operator=(const EventPair &) = delete;
+    ~EventPair()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    void ensure()
+    {
+        if (!a) SFC_CK(cudaEventCreate(&a));
+        if (!b) SFC_CK(cudaEventCreate(&b));
+    }
+};
+
 struct CoarseSpace {
     bool built = false;                 // aggregates for (mesh, size)
     const sfc_mesh *mesh = nullptr;
@@ -384,6 +403,7 @@ struct sfc_system {
     // the mixed block solver's check interval of iterations, captured once
     // per launch configuration (block widths 32, 64, 128)
     sfc::GraphExec blk_graph[3];
+    sfc::EventPair solve_ev;  // device time of the last solve call
 };
 
 // ---------------------------------------------------------------------------

@@ -1945,9 +1945,8 @@ void solve_forward(sfc_system *s)
     const int max_iter = o.max_iter > 0 ? o.max_iter : 20000;
     const int check = o.check_every > 0 ? o.check_every : 16;
     const double tol = o.tol > 0 ? o.tol : 1e-8;
-    cudaEvent_t e0, e1;
-    SFC_CK(cudaEventCreate(&e0));
-    SFC_CK(cudaEventCreate(&e1));
+    s->solve_ev.ensure();
+    cudaEvent_t e0 = s->solve_ev.a, e1 = s->solve_ev.b;
     SFC_CK(cudaEventRecord(e0, ctx->stream));
     PcgResult r;
     bool two = false;
@@ -1971,8 +1970,6 @@ void solve_forward(sfc_system *s)
     float ms = 0;
     SFC_CK(cudaEventSynchronize(e1));
     SFC_CK(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     s->stats = {};
     s->stats.iterations = r.iters;
     s->stats.num_rhs = 1;
@@ -1995,9 +1992,8 @@ void solve_block(sfc_system *s, const double *B, double *X, int nrhs, int ld)
     sfc_ctx *ctx = s->ctx;
     build_operator(s);
     const int64_t N = s->N;
-    cudaEvent_t e0, e1;
-    SFC_CK(cudaEventCreate(&e0));
-    SFC_CK(cudaEventCreate(&e1));
+    s->solve_ev.ensure();
+    cudaEvent_t e0 = s->solve_ev.a, e1 = s->solve_ev.b;
     SFC_CK(cudaEventRecord(e0, ctx->stream));
     sfc_solve_stats_t st{};
     const auto &o = s->opt;
@@ -2037,8 +2033,6 @@ void solve_block(sfc_system *s, const double *B, double *X, int nrhs, int ld)
     float ms = 0;
     SFC_CK(cudaEventSynchronize(e1));
     SFC_CK(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     st.device_ms = ms;
     s->stats = st;
     if (!st.converged) fail(SFC_ERR_NOT_CONVERGED, "block PCG did not converge within max_iter");
