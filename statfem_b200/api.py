@@ -242,6 +242,11 @@ class Context:
         self.check(self.lib.sfc_ctx_kernel_launches(self.h, ctypes.byref(c)))
         return c.value
 
+    def last_message(self):
+        """The context's last message (the last error, or a note such as a
+        graph capture that fell back to separate launches)."""
+        return self.lib.sfc_last_error(self.h).decode()
+
     def graph_launches(self):
         v = ctypes.c_int64()
         self.check(self.lib.sfc_ctx_graph_launches(self.h, ctypes.byref(v)))

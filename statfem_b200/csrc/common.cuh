@@ -240,6 +240,7 @@ struct GraphExec {
     std::vector<uintptr_t> key;
     cudaGraphExec_t exec = nullptr;
     int64_t kernels = 0;  // kernel launches per replay
+    std::vector<uintptr_t> failed_key;  // a configuration whose capture failed (launched eagerly)
     GraphExec() = default;
     GraphExec(const GraphExec &) = delete;
     GraphExec &operator=(const GraphExec &) = delete;

@@ -1474,25 +1474,16 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         double *p;
     } b64{s->blk64.p}, x64{s->blk64.p + N * K}, r64{s->blk64.p + 2 * N * K}, cs{s->colsc.p};
     float *xr = s->blk32.p, *rr32 = xr + N * K, *pp = rr32 + N * K, *qq = pp + N * K;
-    // per-iteration column scalars p.q, r.z, r.r in a ring of R slots:
-    // iteration it reads slot it % R and accumulates into (it + 1) % R.  With
-    // R = check every check-interval chunk uses the same slots, so one
-    // captured graph serves every chunk.
+    // Per-iteration column scalars in a ring of R slots of 3K doubles
+    // (p.q | r.z | r.r).  Iteration it reads r.z and r.r of slot it % R and
+    // accumulates its p.q, the new r.z and the new r.r into slot (it+1) % R,
+    // which it zeroes first (the slot's last reader, iteration it+1-R, is
+    // done).  With R = check every check interval uses the same slots, so
+    // one captured graph serves every interval.
     const int R = check >= 2 ? check : 2;
     const int64_t nsc = 3 * (int64_t)R * K;
     s->scal.reserve(nsc);
-    double *pq = s->scal.p, *rz = pq + (int64_t)R * K, *rrs = rz + (int64_t)R * K;
-    auto slot = [&](int i) { return (int64_t)(i % R) * K; };
-    // before a chunk: every p.q slot and every r.z / r.r slot except `keep`
-    // (the chunk's first iteration reads it) start at zero
-    auto zero_ring = [&](int keep) {
-        SFC_CK(cudaMemsetAsync(pq, 0, (size_t)R * K * 8, ctx->stream));
-        for (double *a : {rz, rrs}) {
-            if (keep > 0) SFC_CK(cudaMemsetAsync(a, 0, (size_t)keep * K * 8, ctx->stream));
-            if (keep + 1 < R)
-                SFC_CK(cudaMemsetAsync(a + (int64_t)(keep + 1) * K, 0, (size_t)(R - keep - 1) * K * 8, ctx->stream));
-        }
-    };
+    auto sl = [&](int i) { return s->scal.p + (int64_t)(i % R) * 3 * K; };
     double *bn2 = cs.p, *rn2 = bn2 + K, *scale = rn2 + K, *norm = scale + K, *thr = norm + K;
     // flags[0]: all columns below their thresholds; flags[1 + c]: breakdown
     // (p^T A p <= 0) in column c
@@ -1566,35 +1557,37 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     // one inner iteration: Q = S P, alpha, x/r update with r.z and r.r,
     // coarse correction, beta and the p update
     auto iterate = [&](int it) {
-        const int64_t o0 = slot(it), o1 = slot(it + 1);
-        spmm(pp, qq, pq + o0);
+        double *cur = sl(it), *nxt = sl(it + 1);
+        SFC_CK(cudaMemsetAsync(nxt, 0, (size_t)3 * K * 8, ctx->stream));
+        double *pqi = nxt, *rz0 = cur + K, *rr0 = cur + 2 * K, *rz1 = nxt + K, *rr1 = nxt + 2 * K;
+        spmm(pp, qq, pqi);
         {
             ProfScope ps(ctx, "bupdate32", (bj ? 3.0 : 6.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N);
             if (bj)
-                k_nupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pq + o0,
-                                                                   rz + o0, rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+                k_nupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pqi,
+                                                                   rz0, rr0, thr, rz1, rr1, stop, err);
             else
-                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pq + o0, rz + o0,
-                                                            rrs + o0, thr, rz + o1, rrs + o1, stop, err);
+                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pqi, rz0,
+                                                            rr0, thr, rz1, rr1, stop, err);
         }
-        if (two_any) coarse_block_apply<V>(s, rr32, rz + o1, stop);
+        if (two_any) coarse_block_apply<V>(s, rr32, rz1, stop);
         {
             ProfScope ps(ctx, "bpupdate32",
                          (bj ? 5.0 : 3.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
             if (two)
                 k_ncpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, crs.node_agg.p,
-                                                                     crs.mode.p, crs.e32.p, s->nodes, rz + o0, rz + o1,
-                                                                     rrs + o1, thr, stop, err, nullptr, xr, pq + o0,
-                                                                     rrs + o0);
+                                                                     crs.mode.p, crs.e32.p, s->nodes, rz0, rz1,
+                                                                     rr1, thr, stop, err, nullptr, xr, pqi,
+                                                                     rr0);
             else if (bj)
-                k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz + o0, rz + o1,
-                                                             rrs + o1, thr, stop, err, xr, pq + o0, rrs + o0);
+                k_npupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->bdinv32.p, s->nodes, rz0, rz1,
+                                                             rr1, thr, stop, err, xr, pqi, rr0);
             else if (two1)
                 k_cbpupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, crs.node_agg.p,
-                                                                     crs.mode.p, crs.e32.p, N, rz + o0, rz + o1,
-                                                                     rrs + o1, thr, stop, err, nullptr);
+                                                                     crs.mode.p, crs.e32.p, N, rz0, rz1,
+                                                                     rr1, thr, stop, err, nullptr);
             else
-                k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz + o0, rz + o1, rrs + o1,
+                k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz0, rz1, rr1,
                                                              thr, stop, err);
         }
         count_launch(ctx, 2);
@@ -1608,7 +1601,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     const char *genv = std::getenv("SFC_BLOCK_GRAPH");
     const bool use_graph = !ctx->prof && check >= 2 && !(genv && genv[0] == '0');
     const bool lattice = bsr && s->has_lattice && K >= 64;
-    auto launch_chunk_graph = [&]() {
+    auto launch_chunk_graph = [&]() -> bool {
         GraphExec &g = s->blk_graph[V == 1 ? 0 : V == 2 ? 1 : 2];
         // everything the captured launches allocate or set up, done outside the capture
         if (two_any) {
@@ -1628,18 +1621,19 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             (uintptr_t)crs.nagg, (uintptr_t)crs.nc, (uintptr_t)crs.dof};
         if (!g.exec || g.key != key) {
             g.reset();
+            if (g.failed_key == key) return false;  // this configuration could not be captured: eager
             cudaStream_t st;
             SFC_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
             const cudaStream_t keep = ctx->stream;
             const int64_t l0 = ctx->launches;
             cudaGraph_t graph = nullptr;
+            const char *where = "cudaStreamBeginCapture";
             cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
                 ctx->stream = st;
                 try {
-                    zero_ring(0);
                     for (int j = 0; j < check; ++j) iterate(j);
-                    k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + slot(check), thr, stop);
+                    k_bcheck<K><<<1, 128, 0, ctx->stream>>>(sl(check) + 2 * K, thr, stop);
                     count_launch(ctx);
                 } catch (...) {
                     ctx->stream = keep;
@@ -1650,16 +1644,27 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                     throw;
                 }
                 ctx->stream = keep;
+                where = "cudaStreamEndCapture";
                 e = cudaStreamEndCapture(st, &graph);
             }
             cudaStreamDestroy(st);
             const int64_t captured = ctx->launches - l0;
             ctx->launches = l0;
-            SFC_CK(e);
             cudaGraphExec_t exec = nullptr;
-            e = cudaGraphInstantiate(&exec, graph, 0);
-            cudaGraphDestroy(graph);
-            SFC_CK(e);
+            if (e == cudaSuccess) {
+                where = "cudaGraphInstantiate";
+                e = cudaGraphInstantiate(&exec, graph, 0);
+            }
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                // not fatal: the same launches go out one by one; the reason
+                // is kept as the context's message (sfc_last_error)
+                cudaGetLastError();
+                g.failed_key = key;
+                ctx->err = std::string("block solver graph not used: ") + where + ": " + cudaGetErrorString(e);
+                if (debug) std::fprintf(stderr, "[sfc] %s\n", ctx->err.c_str());
+                return false;
+            }
             g.exec = exec;
             g.key = key;
             g.kernels = captured;
@@ -1667,6 +1672,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         SFC_CK(cudaGraphLaunch(g.exec, ctx->stream));
         ctx->launches += g.kernels;
         ++ctx->graph_replays;
+        return true;
     };
     // Reliable-update mixed-precision block PCG.  Each column is scaled to
     // ||b|| = 1 and iterated in FP32; whenever every active column's recurrence
@@ -1719,28 +1725,26 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             SFC_CK(cudaMemcpyAsync(norm, hn.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(thr, ht.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(restart.p, hrestart.data(), K * 4, cudaMemcpyHostToDevice, ctx->stream));
-            init32(rz, rrs);
+            init32(sl(0) + K, sl(0) + 2 * K);
         }
         while (nactive > 0) {
             bool ran_graph = false;
-            if (it % check == 0 && use_graph && it + check <= max_iter) {
-                launch_chunk_graph();
+            if (it % check == 0 && use_graph && it + check <= max_iter && launch_chunk_graph()) {
                 it += check;
                 ran_graph = true;
             } else {
-                if (it % check == 0) zero_ring((int)(it % R));
                 iterate(it);
                 ++it;
             }
-            const int64_t o1 = slot(it);
+            double *rz1 = sl(it) + K, *rr1 = sl(it) + 2 * K;
             const bool at_cap = it >= max_iter;
             if (!ran_graph) {
                 if (it % check != 0 && !at_cap) continue;
-                k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rrs + o1, thr, stop);
+                k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rr1, thr, stop);
                 count_launch(ctx);
             }
             download(ctx, hflags.data(), s->flags.p, 1 + K);
-            download(ctx, rr_now.data(), rrs + o1, K);
+            download(ctx, rr_now.data(), rr1, K);
             bool update = hflags[0] || at_cap;
             for (int c = 0; c < K; ++c)
                 if (active[c] && hflags[1 + c]) {
@@ -1822,11 +1826,10 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             if (nactive == 0 || at_cap) break;
             SFC_CK(cudaMemcpyAsync(thr, ht.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(restart.p, hrestart.data(), K * 4, cudaMemcpyHostToDevice, ctx->stream));
-            SFC_CK(cudaMemsetAsync(rz + o1, 0, K * 8, ctx->stream));
-            SFC_CK(cudaMemsetAsync(rrs + o1, 0, K * 8, ctx->stream));
+            SFC_CK(cudaMemsetAsync(sl(it), 0, (size_t)3 * K * 8, ctx->stream));
             SFC_CK(cudaMemsetAsync(s->flags.p, 0, (1 + K) * sizeof(int), ctx->stream));
             // r32 <- scaled true residual, x32 <- 0, p kept (restarted columns: p = z)
-            init32(rz + o1, rrs + o1);
+            init32(rz1, rr1);
         }
         // FP64 fallback: S d = r_c (the column's true residual) by Jacobi-PCG
         // to tol ||b_c|| / ||r_c||, then x_c += d

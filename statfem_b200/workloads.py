@@ -95,7 +95,7 @@ def make_batch_workload(seed, n_inst=512, smin=32, smax=256, ns=32, sides=None):
     return dict(sides=sides, meshes=meshes, coeff=np.concatenate(coeffs), coeffs=coeffs, bcs=bcs,
                 sensors=sensors, union=union, off=off, bc=bc, ns=ns, rng=rng,
                 desc="%d 2-D Poisson statFEM instances, sides U{%d..%d} (P1 triangles, %d dofs in total), "
-                     "%d sensors each, log-likelihood + posterior at the sensors, rel. residual 1e-8"
+                     "%d sensors each, log-likelihood + posterior at the sensors"
                      % (len(sides), int(sides.min()), int(sides.max()), int(off[-1]), ns))
 
 

@@ -67,13 +67,14 @@ def test_c1_at_config_size(method, precond):
 
 def test_c3_sides_32_to_256():
     """Instances at both ends and inside the config's side range, through the
-    persistent batch kernel with the benchmark's tolerances."""
+    persistent batch kernel with the benchmark's tolerances (rel. residual
+    1e-9, FP32 reduction 1e-2 between FP64 residuals)."""
     sides = [32, 256, 77, 141, 203, 45]
     wl = make_batch_workload(4321, sides=sides)
     ctx = api.Context(0)
     gm = api.Mesh(ctx, mg.TRI3_POISSON, 3, wl["union"].coords, wl["union"].conn)
     b = api.BatchStatFEM(ctx, gm, wl["off"], wl["sides"], wl["bc"], wl["sensors"], 1.0)
-    b.set_solver(tol=1e-8, inner_tol=1e-2)
+    b.set_solver(tol=1e-9, inner_tol=1e-2)  # the bench's c3 setting (at 1e-8 the worst instance is at 1.1e-7)
     b.set_coefficients(wl["coeff"])
     b.set_hparams(C3_HP, REG)
     refs, Ys = [], []

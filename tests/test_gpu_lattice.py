@@ -87,5 +87,5 @@ def test_check_interval_graph_matches_eager_launches(ctx, precond):
     assert abs(stg["iterations"] - ste["iterations"]) <= 32
     # check_every is 16 here: one replay per 16 iterations (the coarse
     # inverse's own graphs are launched in both modes)
-    assert gg - ge >= max(1, stg["iterations"] // 16 - 1)
+    assert gg - ge >= max(1, stg["iterations"] // 16 - 1), ctx.last_message()
     assert kg > 0 and ke > 0
