@@ -1953,20 +1953,10 @@ void solve_forward(sfc_system *s)
     SFC_CK(cudaEventRecord(e0, ctx->stream));
     PcgResult r;
     bool two = false;
-    sfc_solve_stats_t mst{};
-    const bool mixed = o.method == SFC_SOLVER_PCG_MIXED;
     {
         ProfScope ps(ctx, "phase:forward_solve", 0.0);
         two = use_two_level(s);
-        if (mixed) {
-            // the forward system as a one-column block of the mixed solver:
-            // FP32 iterations, FP64 residual replacement, same preconditioner
-            block_mixed<1>(s, b.p, s->X.p, 1, 1, mst);
-            r.iters = mst.iterations;
-            r.converged = mst.converged != 0;
-        } else {
-            r = pcg64(s, b.p, s->X.p, tol, max_iter, check, two);
-        }
+        r = pcg64(s, b.p, s->X.p, tol, max_iter, check, two);
     }
     SFC_CK(cudaEventRecord(e1, ctx->stream));
     const double rel = true_rel_residual(s, b.p, s->X.p);
@@ -1980,11 +1970,6 @@ void solve_forward(sfc_system *s)
     s->stats.max_rel_residual = rel;
     s->stats.device_ms = ms;
     s->stats.coarse_dofs = two ? (int32_t)(s->coarse.nc - s->coarse.dropped) : 0;
-    if (mixed) {
-        s->stats.refinements = mst.refinements;
-        s->stats.fallback_columns = mst.fallback_columns;
-        s->stats.spmm_kernel = mst.spmm_kernel;
-    }
     if (!r.converged) fail(SFC_ERR_NOT_CONVERGED, "PCG did not converge within max_iter");
 }
 

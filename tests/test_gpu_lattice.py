@@ -16,16 +16,17 @@ pytestmark = pytest.mark.gpu
 
 
 def solve(ctx, n, bw, precond, rhs_seed=4, nrhs=130, force_bsr=False):
+    # the operator (and with it the choice of SpMM) is built at solve time
     if force_bsr:
         os.environ["SFC_SPMM"] = "bsr"
     try:
         mesh, s, ds, F, bc = setup(ctx, mg.HEX8_ELASTIC, n, 17, amount=0.0, faces="x0")
+        rng = np.random.default_rng(rhs_seed)
+        Rhs = rng.standard_normal((nrhs, mesh.num_dofs))
+        s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, block_width=bw, precond=precond)
+        U = s.solveSystemTranspose(Rhs)
     finally:
         os.environ.pop("SFC_SPMM", None)
-    rng = np.random.default_rng(rhs_seed)
-    Rhs = rng.standard_normal((nrhs, mesh.num_dofs))
-    s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, block_width=bw, precond=precond)
-    U = s.solveSystemTranspose(Rhs)
     st = s.last_stats()
     return U, st, ds, Rhs
 
