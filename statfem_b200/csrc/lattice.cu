@@ -22,8 +22,10 @@
 // the kernel.  The p.q column dots are accumulated in FP64 per lane across
 // all of a CTA's work items and reduced once at the end.
 //
-// Two CTAs (94.5 KiB of shared memory each) share an SM, so one computes
-// while the other waits for its copies.  Waits on the mbarrier are bounded:
+// Each CTA (one per SM) keeps two stages of 94.5 KiB: the next brick's copies
+// are issued into the other stage before this one is computed, so the TMA
+// traffic overlaps the FMAs (SFC_LATTICE_STAGES=1 selects a single-stage
+// version, two CTAs per SM).  Waits on the mbarrier are bounded:
 // a wait that gives up sets lat_err (the solver then fails with
 // SFC_ERR_TIMEOUT), waits once more (bounded) for the copies in flight and
 // leaves the kernel.  No multicast, no clusters: every copy reads this
@@ -46,7 +48,9 @@ constexpr int NODE_FLOATS = 27 * SLOT; // 324 floats = 1296 bytes per node
 constexpr int HALO_FLOATS = HZ * HY * HX * 3 * CS;
 constexpr int BLK_FLOATS = BX * BY * BZ * NODE_FLOATS;
 constexpr int HALO_BYTES = HALO_FLOATS * 4;                 // 73,728
-constexpr size_t SMEM_BYTES = (size_t)(HALO_FLOATS + BLK_FLOATS) * 4 + 16;  // + mbarrier
+constexpr int STAGE_FLOATS = HALO_FLOATS + BLK_FLOATS;       // 94,464 bytes per stage
+template <int STAGES>
+constexpr size_t smem_bytes() { return (size_t)STAGES * STAGE_FLOATS * 4 + 16 * STAGES; }  // + mbarriers
 constexpr int THREADS = 128;
 constexpr uint32_t WAIT_TRIES = 1u << 20;
 
@@ -99,57 +103,99 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
                  : "memory");
 }
 
-__global__ void __launch_bounds__(THREADS, 2)
+struct Brick {
+    int x0, y0, z0, nvx;
+};
+
+__device__ __forceinline__ Brick brick_of(int64_t w, int slices, int tx_n, int ty_n, int nx)
+{
+    const int64_t t = w / slices;
+    const int tx = (int)(t % tx_n);
+    const int64_t tr = t / tx_n;
+    Brick b;
+    b.x0 = tx * BX;
+    b.y0 = (int)(tr % ty_n) * BY;
+    b.z0 = (int)(tr / ty_n) * BZ;
+    b.nvx = min(BX, nx - b.x0);
+    return b;
+}
+
+// one thread: the brick's halo (one 5-D tensor copy) and its block rows (one
+// bulk copy per x-line inside the lattice), all completing on `bar`
+__device__ __forceinline__ void issue_brick(const CUtensorMap *pmap, const float *__restrict__ bq, float *halo,
+                                            float *blk, uint32_t bar, const Brick &b, int slice, int nx, int ny,
+                                            int nz)
+{
+    uint32_t bytes = HALO_BYTES;
+    for (int l = 0; l < BY * BZ; ++l)
+        if (b.y0 + (l & 1) < ny && b.z0 + (l >> 1) < nz) bytes += (uint32_t)b.nvx * NODE_FLOATS * 4;
+    mbar_expect_tx(bar, bytes);
+    tma_load_5d(smem_u32(halo), pmap, bar, slice * CS, 0, b.x0 - 1, b.y0 - 1, b.z0 - 1);
+    for (int l = 0; l < BY * BZ; ++l) {
+        const int y = b.y0 + (l & 1), z = b.z0 + (l >> 1);
+        if (y >= ny || z >= nz) continue;
+        const int64_t node = ((int64_t)z * ny + y) * nx + b.x0;
+        bulk_load(smem_u32(blk + l * BX * NODE_FLOATS), bq + node * NODE_FLOATS, (uint32_t)b.nvx * NODE_FLOATS * 4,
+                  bar);
+    }
+}
+
+// STAGES = 2: one CTA per SM, the next brick's copies land in the other stage
+// while this one is computed.  STAGES = 1: two CTAs per SM, each waiting for
+// its own copies.
+template <int STAGES>
+__global__ void __launch_bounds__(THREADS, 3 - STAGES)
     k_lspmm32(const __grid_constant__ CUtensorMap pmap, const float *__restrict__ bq, float *__restrict__ Q, int nx,
               int ny, int nz, int K, int slices, int64_t work, double *pq, const int *stop, int *err)
 {
     if (*stop) return;
     extern __shared__ __align__(128) unsigned char smem[];
-    float *halo = reinterpret_cast<float *>(smem);
-    float *blk = halo + HALO_FLOATS;
-    uint64_t *barp = reinterpret_cast<uint64_t *>(blk + BLK_FLOATS);
-    const uint32_t bar = smem_u32(barp);
+    float *stage_base = reinterpret_cast<float *>(smem);
+    uint64_t *barp = reinterpret_cast<uint64_t *>(stage_base + STAGES * STAGE_FLOATS);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wy = warp & 1, wz = warp >> 1;
     const int tx_n = (nx + BX - 1) / BX, ty_n = (ny + BY - 1) / BY;
     const int slice = (int)(blockIdx.x % slices);  // gridDim.x is a multiple of slices
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
+        for (int st = 0; st < STAGES; ++st) mbar_init(smem_u32(barp + st), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // bit s: stage s has copies issued and not yet waited for / the parity to wait for
+    uint32_t pending = 0, phase = 0;
+    if ((int64_t)blockIdx.x < work) {
+        if (threadIdx.x == 0)
+            issue_brick(&pmap, bq, stage_base, stage_base + HALO_FLOATS, smem_u32(barp),
+                        brick_of(blockIdx.x, slices, tx_n, ty_n, nx), slice, nx, ny, nz);
+        pending = 1u;
+    }
     double dacc0 = 0.0, dacc1 = 0.0;
-    uint32_t parity = 0;
-    for (int64_t w = blockIdx.x; w < work; w += gridDim.x) {
-        const int64_t t = w / slices;
-        const int tx = (int)(t % tx_n);
-        const int64_t tr = t / tx_n;
-        const int ty = (int)(tr % ty_n), tz = (int)(tr / ty_n);
-        const int x0 = tx * BX, y0 = ty * BY, z0 = tz * BZ;
-        const int nvx = min(BX, nx - x0);
-        if (threadIdx.x == 0) {
-            uint32_t bytes = HALO_BYTES;
-            for (int l = 0; l < BY * BZ; ++l)
-                if (y0 + (l & 1) < ny && z0 + (l >> 1) < nz) bytes += (uint32_t)nvx * NODE_FLOATS * 4;
-            mbar_expect_tx(bar, bytes);
-            tma_load_5d(smem_u32(halo), &pmap, bar, slice * CS, 0, x0 - 1, y0 - 1, z0 - 1);
-            for (int l = 0; l < BY * BZ; ++l) {
-                const int y = y0 + (l & 1), z = z0 + (l >> 1);
-                if (y >= ny || z >= nz) continue;
-                const int64_t node = ((int64_t)z * ny + y) * nx + x0;
-                bulk_load(smem_u32(blk + l * BX * NODE_FLOATS), bq + node * NODE_FLOATS,
-                          (uint32_t)nvx * NODE_FLOATS * 4, bar);
-            }
+    int k = 0;
+    for (int64_t w = blockIdx.x; w < work; w += gridDim.x, ++k) {
+        const int st = STAGES == 1 ? 0 : (k & 1);
+        float *halo = stage_base + st * STAGE_FLOATS;
+        float *blk = halo + HALO_FLOATS;
+        const Brick b = brick_of(w, slices, tx_n, ty_n, nx);
+        if (STAGES == 2 && w + gridDim.x < work) {
+            // the other stage was released by the barrier that ended the previous brick
+            const int sn = st ^ 1;
+            if (threadIdx.x == 0)
+                issue_brick(&pmap, bq, stage_base + sn * STAGE_FLOATS, stage_base + sn * STAGE_FLOATS + HALO_FLOATS,
+                            smem_u32(barp + sn), brick_of(w + gridDim.x, slices, tx_n, ty_n, nx), slice, nx, ny, nz);
+            pending |= 1u << sn;
         }
-        const bool got = mbar_wait(bar, parity);
+        const bool got = mbar_wait(smem_u32(barp + st), (phase >> st) & 1u);
         if (__syncthreads_or(!got)) {
-            // the copies did not complete in time: record it, give the copies
-            // in flight one more bounded wait, and leave (uniformly)
+            // the copies did not complete in time: record it, give every copy
+            // still in flight one more bounded wait, and leave (uniformly)
             if (threadIdx.x == 0) atomicExch(err, 1);
-            mbar_wait(bar, parity);
+#pragma unroll
+            for (int s2 = 0; s2 < STAGES; ++s2)
+                if ((pending >> s2) & 1u) mbar_wait(smem_u32(barp + s2), (phase >> s2) & 1u);
             return;
         }
-        parity ^= 1u;
+        pending &= ~(1u << st);
+        phase ^= 1u << st;
         float acc[BX][3][2];
 #pragma unroll
         for (int o = 0; o < BX; ++o)
@@ -171,10 +217,10 @@ __global__ void __launch_bounds__(THREADS, 2)
                     for (int ox = 0; ox < BX; ++ox) {
                         const int dx = cx - ox;  // lattice offset dx - 1
                         if (dx < 0 || dx > 2) continue;
-                        const float *b = bb + ox * NODE_FLOATS + (dz * 9 + dy * 3 + dx) * SLOT;
-                        const float4 b0 = *reinterpret_cast<const float4 *>(b);
-                        const float4 b1 = *reinterpret_cast<const float4 *>(b + 4);
-                        const float4 b2 = *reinterpret_cast<const float4 *>(b + 8);
+                        const float *bp = bb + ox * NODE_FLOATS + (dz * 9 + dy * 3 + dx) * SLOT;
+                        const float4 b0 = *reinterpret_cast<const float4 *>(bp);
+                        const float4 b1 = *reinterpret_cast<const float4 *>(bp + 4);
+                        const float4 b2 = *reinterpret_cast<const float4 *>(bp + 8);
                         acc[ox][0][0] = fmaf(b0.z, p2.x, fmaf(b0.y, p1.x, fmaf(b0.x, p0.x, acc[ox][0][0])));
                         acc[ox][0][1] = fmaf(b0.z, p2.y, fmaf(b0.y, p1.y, fmaf(b0.x, p0.y, acc[ox][0][1])));
                         acc[ox][1][0] = fmaf(b1.z, p2.x, fmaf(b1.y, p1.x, fmaf(b1.x, p0.x, acc[ox][1][0])));
@@ -184,14 +230,14 @@ __global__ void __launch_bounds__(THREADS, 2)
                     }
                 }
             }
-        const int y = y0 + wy, z = z0 + wz;
+        const int y = b.y0 + wy, z = b.z0 + wz;
         if (y < ny && z < nz) {
             // own rows of P sit at halo (ox + 1, wy + 1, wz + 1)
             const float *own = hb + ((wz + 1) * HY + (wy + 1)) * HX * 3 * CS;
 #pragma unroll
             for (int ox = 0; ox < BX; ++ox) {
-                if (ox >= nvx) break;
-                const int64_t node = ((int64_t)z * ny + y) * nx + x0 + ox;
+                if (ox >= b.nvx) break;
+                const int64_t node = ((int64_t)z * ny + y) * nx + b.x0 + ox;
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
                     const float2 pv = *reinterpret_cast<const float2 *>(own + ((ox + 1) * 3 + r) * CS);
@@ -202,7 +248,13 @@ __global__ void __launch_bounds__(THREADS, 2)
                 }
             }
         }
-        __syncthreads();  // every warp is done with the staged tiles before the next copies land
+        __syncthreads();  // every warp is done with this stage before it is refilled
+        if (STAGES == 1 && w + gridDim.x < work) {
+            if (threadIdx.x == 0)
+                issue_brick(&pmap, bq, stage_base, stage_base + HALO_FLOATS, smem_u32(barp),
+                            brick_of(w + gridDim.x, slices, tx_n, ty_n, nx), slice, nx, ny, nz);
+            pending = 1u;
+        }
     }
     // column dots: the four warps' lanes hold the same 64 columns
     double *red = reinterpret_cast<double *>(smem);
@@ -241,7 +293,8 @@ __global__ void k_lattice_fill(const int32_t *__restrict__ bptr, const int32_t *
     }
 }
 
-int g_occ = 0;  // resident CTAs per SM of k_lspmm32
+int g_occ = 0;     // resident CTAs per SM of the k_lspmm32 instantiation in use
+int g_stages = 0;  // its shared-memory stages (SFC_LATTICE_STAGES=1 selects the single-stage kernel)
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
@@ -312,9 +365,18 @@ void lattice_prepare(sfc_system *s, const float *P, int K)
         s->pmap_ptr = P;
         s->pmap_K = K;
     }
-    if (!g_occ) {
-        SFC_CK(cudaFuncSetAttribute(k_lspmm32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
-        SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32, THREADS, SMEM_BYTES));
+    if (!g_stages) {
+        const char *e = std::getenv("SFC_LATTICE_STAGES");
+        g_stages = (e && e[0] == '1') ? 1 : 2;
+        if (g_stages == 2) {
+            SFC_CK(cudaFuncSetAttribute(k_lspmm32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_bytes<2>()));
+            SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32<2>, THREADS, smem_bytes<2>()));
+        } else {
+            SFC_CK(cudaFuncSetAttribute(k_lspmm32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem_bytes<1>()));
+            SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32<1>, THREADS, smem_bytes<1>()));
+        }
         if (g_occ < 1) g_occ = 1;
     }
 }
@@ -330,8 +392,12 @@ void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, 
     const int64_t work = tiles * slices;
     int64_t grid = std::min<int64_t>(work, (int64_t)occ * ctx->sm_count);
     grid = std::max<int64_t>(slices, grid - grid % slices);
-    k_lspmm32<<<(unsigned)grid, THREADS, SMEM_BYTES, ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K, slices, work,
-                                                                     pq, stop, s->lat_err.p);
+    if (g_stages == 2)
+        k_lspmm32<2><<<(unsigned)grid, THREADS, smem_bytes<2>(), ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K,
+                                                                               slices, work, pq, stop, s->lat_err.p);
+    else
+        k_lspmm32<1><<<(unsigned)grid, THREADS, smem_bytes<1>(), ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K,
+                                                                               slices, work, pq, stop, s->lat_err.p);
     count_launch(ctx);
 }
 
