@@ -13,19 +13,19 @@
 // the block.  One elected thread issues a single 5-D TMA tensor load of the
 // brick's halo (6 x 4 x 4 column nodes x 3 rows x 64 columns, zero-filled
 // outside the lattice: 72 KiB) and 1-D bulk copies of the brick's block rows
-// (up to 4 x 5 KiB) into shared memory, completing on one mbarrier.  Each of
-// the four warps then owns one x-line of four output nodes and two columns
-// per lane: for every column node of its 3 x 3 neighbour lines it reads the
-// node's three P rows from shared memory once and applies them to every
+// (up to 4 x 5 KiB) into shared memory, completing on one mbarrier.  Each
+// x-line of four output nodes belongs to two warps (32 columns each, one
+// per lane): for every column node of its 3 x 3 neighbour lines a warp reads
+// the node's three P rows from shared memory once and applies them to every
 // output node of the line that couples to it (up to three), so a P row read
 // feeds 1.8 outputs on average and the FMA pipe, not the load path, bounds
 // the kernel.  The p.q column dots are accumulated in FP64 per lane across
 // all of a CTA's work items and reduced once at the end.
 //
-// Each CTA (one per SM) keeps two stages of 94.5 KiB: the next brick's copies
-// are issued into the other stage before this one is computed, so the TMA
-// traffic overlaps the FMAs (SFC_LATTICE_STAGES=1 selects a single-stage
-// version, two CTAs per SM).  Waits on the mbarrier are bounded:
+// Two CTAs share an SM (94.5 KiB of shared memory each); each x-line is
+// split over two warps by columns (8 warps per CTA) for latency hiding
+// (SFC_LATTICE_WARPS=4 keeps one warp per x-line).  Waits on the mbarrier
+// are bounded:
 // a wait that gives up sets lat_err (the solver then fails with
 // SFC_ERR_TIMEOUT), waits once more (bounded) for the copies in flight and
 // leaves the kernel.  No multicast, no clusters: every copy reads this
@@ -48,10 +48,7 @@ constexpr int NODE_FLOATS = 27 * SLOT; // 324 floats = 1296 bytes per node
 constexpr int HALO_FLOATS = HZ * HY * HX * 3 * CS;
 constexpr int BLK_FLOATS = BX * BY * BZ * NODE_FLOATS;
 constexpr int HALO_BYTES = HALO_FLOATS * 4;                 // 73,728
-constexpr int STAGE_FLOATS = HALO_FLOATS + BLK_FLOATS;       // 94,464 bytes per stage
-template <int STAGES>
-constexpr size_t smem_bytes() { return (size_t)STAGES * STAGE_FLOATS * 4 + 16 * STAGES; }  // + mbarriers
-constexpr int THREADS = 128;
+constexpr size_t SMEM_BYTES = (size_t)(HALO_FLOATS + BLK_FLOATS) * 4 + 16;  // 94,480: + mbarrier
 constexpr uint32_t WAIT_TRIES = 1u << 20;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -140,69 +137,57 @@ __device__ __forceinline__ void issue_brick(const CUtensorMap *pmap, const float
     }
 }
 
-// STAGES = 2: one CTA per SM, the next brick's copies land in the other stage
-// while this one is computed.  STAGES = 1: two CTAs per SM, each waiting for
-// its own copies.
-template <int STAGES>
-__global__ void __launch_bounds__(THREADS, 3 - STAGES)
+// H column groups per x-line: 4 H warps, warp (xl, g) owns x-line xl (wy =
+// xl & 1, wz = xl >> 1) and V = 2 / H columns per lane of the slice's group g.
+// Two CTAs per SM (94.5 KiB of shared memory each).
+template <int H>
+__global__ void __launch_bounds__(128 * H, 2)
     k_lspmm32(const __grid_constant__ CUtensorMap pmap, const float *__restrict__ bq, float *__restrict__ Q, int nx,
               int ny, int nz, int K, int slices, int64_t work, double *pq, const int *stop, int *err)
 {
+    constexpr int V = 2 / H, GC = CS / H;  // columns per lane, per group
     if (*stop) return;
     extern __shared__ __align__(128) unsigned char smem[];
-    float *stage_base = reinterpret_cast<float *>(smem);
-    uint64_t *barp = reinterpret_cast<uint64_t *>(stage_base + STAGES * STAGE_FLOATS);
+    float *halo = reinterpret_cast<float *>(smem);
+    float *blk = halo + HALO_FLOATS;
+    uint64_t *barp = reinterpret_cast<uint64_t *>(blk + BLK_FLOATS);
+    const uint32_t bar = smem_u32(barp);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wy = warp & 1, wz = warp >> 1;
+    const int xl = warp & 3, grp = warp >> 2;
+    const int wy = xl & 1, wz = xl >> 1;
+    const int col = grp * GC + lane * V;  // first column of this lane within the slice
     const int tx_n = (nx + BX - 1) / BX, ty_n = (ny + BY - 1) / BY;
     const int slice = (int)(blockIdx.x % slices);  // gridDim.x is a multiple of slices
     if (threadIdx.x == 0) {
-        for (int st = 0; st < STAGES; ++st) mbar_init(smem_u32(barp + st), 1);
+        mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    // bit s: stage s has copies issued and not yet waited for / the parity to wait for
-    uint32_t pending = 0, phase = 0;
-    if ((int64_t)blockIdx.x < work) {
-        if (threadIdx.x == 0)
-            issue_brick(&pmap, bq, stage_base, stage_base + HALO_FLOATS, smem_u32(barp),
-                        brick_of(blockIdx.x, slices, tx_n, ty_n, nx), slice, nx, ny, nz);
-        pending = 1u;
-    }
-    double dacc0 = 0.0, dacc1 = 0.0;
-    int k = 0;
-    for (int64_t w = blockIdx.x; w < work; w += gridDim.x, ++k) {
-        const int st = STAGES == 1 ? 0 : (k & 1);
-        float *halo = stage_base + st * STAGE_FLOATS;
-        float *blk = halo + HALO_FLOATS;
-        const Brick b = brick_of(w, slices, tx_n, ty_n, nx);
-        if (STAGES == 2 && w + gridDim.x < work) {
-            // the other stage was released by the barrier that ended the previous brick
-            const int sn = st ^ 1;
-            if (threadIdx.x == 0)
-                issue_brick(&pmap, bq, stage_base + sn * STAGE_FLOATS, stage_base + sn * STAGE_FLOATS + HALO_FLOATS,
-                            smem_u32(barp + sn), brick_of(w + gridDim.x, slices, tx_n, ty_n, nx), slice, nx, ny, nz);
-            pending |= 1u << sn;
-        }
-        const bool got = mbar_wait(smem_u32(barp + st), (phase >> st) & 1u);
-        if (__syncthreads_or(!got)) {
-            // the copies did not complete in time: record it, give every copy
-            // still in flight one more bounded wait, and leave (uniformly)
-            if (threadIdx.x == 0) atomicExch(err, 1);
+    double dacc[V];
 #pragma unroll
-            for (int s2 = 0; s2 < STAGES; ++s2)
-                if ((pending >> s2) & 1u) mbar_wait(smem_u32(barp + s2), (phase >> s2) & 1u);
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    uint32_t parity = 0;
+    for (int64_t w = blockIdx.x; w < work; w += gridDim.x) {
+        const Brick b = brick_of(w, slices, tx_n, ty_n, nx);
+        if (threadIdx.x == 0) issue_brick(&pmap, bq, halo, blk, bar, b, slice, nx, ny, nz);
+        const bool got = mbar_wait(bar, parity);
+        if (__syncthreads_or(!got)) {
+            // the copies did not complete in time: record it, give the copies
+            // in flight one more bounded wait, and leave (uniformly)
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            mbar_wait(bar, parity);
             return;
         }
-        pending &= ~(1u << st);
-        phase ^= 1u << st;
-        float acc[BX][3][2];
+        parity ^= 1u;
+        float acc[BX][3][V];
 #pragma unroll
         for (int o = 0; o < BX; ++o)
 #pragma unroll
-            for (int r = 0; r < 3; ++r) acc[o][r][0] = acc[o][r][1] = 0.f;
-        const float *hb = halo + 2 * lane;
-        const float *bb = blk + warp * BX * NODE_FLOATS;
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[o][r][v] = 0.f;
+        const float *hb = halo + col;
+        const float *bb = blk + xl * BX * NODE_FLOATS;
 #pragma unroll
         for (int dz = 0; dz < 3; ++dz)
 #pragma unroll
@@ -210,23 +195,31 @@ __global__ void __launch_bounds__(THREADS, 3 - STAGES)
                 const float *line = hb + ((wz + dz) * HY + (wy + dy)) * HX * 3 * CS;
 #pragma unroll
                 for (int cx = 0; cx < HX; ++cx) {
-                    const float2 p0 = *reinterpret_cast<const float2 *>(line + (cx * 3 + 0) * CS);
-                    const float2 p1 = *reinterpret_cast<const float2 *>(line + (cx * 3 + 1) * CS);
-                    const float2 p2 = *reinterpret_cast<const float2 *>(line + (cx * 3 + 2) * CS);
+                    float p[3][V];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) {
+                        if constexpr (V == 2) {
+                            const float2 t = *reinterpret_cast<const float2 *>(line + (cx * 3 + r) * CS);
+                            p[r][0] = t.x;
+                            p[r][1] = t.y;
+                        } else {
+                            p[r][0] = line[(cx * 3 + r) * CS];
+                        }
+                    }
 #pragma unroll
                     for (int ox = 0; ox < BX; ++ox) {
                         const int dx = cx - ox;  // lattice offset dx - 1
                         if (dx < 0 || dx > 2) continue;
                         const float *bp = bb + ox * NODE_FLOATS + (dz * 9 + dy * 3 + dx) * SLOT;
-                        const float4 b0 = *reinterpret_cast<const float4 *>(bp);
-                        const float4 b1 = *reinterpret_cast<const float4 *>(bp + 4);
-                        const float4 b2 = *reinterpret_cast<const float4 *>(bp + 8);
-                        acc[ox][0][0] = fmaf(b0.z, p2.x, fmaf(b0.y, p1.x, fmaf(b0.x, p0.x, acc[ox][0][0])));
-                        acc[ox][0][1] = fmaf(b0.z, p2.y, fmaf(b0.y, p1.y, fmaf(b0.x, p0.y, acc[ox][0][1])));
-                        acc[ox][1][0] = fmaf(b1.z, p2.x, fmaf(b1.y, p1.x, fmaf(b1.x, p0.x, acc[ox][1][0])));
-                        acc[ox][1][1] = fmaf(b1.z, p2.y, fmaf(b1.y, p1.y, fmaf(b1.x, p0.y, acc[ox][1][1])));
-                        acc[ox][2][0] = fmaf(b2.z, p2.x, fmaf(b2.y, p1.x, fmaf(b2.x, p0.x, acc[ox][2][0])));
-                        acc[ox][2][1] = fmaf(b2.z, p2.y, fmaf(b2.y, p1.y, fmaf(b2.x, p0.y, acc[ox][2][1])));
+                        const float4 bm[3] = {*reinterpret_cast<const float4 *>(bp),
+                                              *reinterpret_cast<const float4 *>(bp + 4),
+                                              *reinterpret_cast<const float4 *>(bp + 8)};
+#pragma unroll
+                        for (int r = 0; r < 3; ++r)
+#pragma unroll
+                            for (int v = 0; v < V; ++v)
+                                acc[ox][r][v] =
+                                    fmaf(bm[r].z, p[2][v], fmaf(bm[r].y, p[1][v], fmaf(bm[r].x, p[0][v], acc[ox][r][v])));
                     }
                 }
             }
@@ -240,30 +233,27 @@ __global__ void __launch_bounds__(THREADS, 3 - STAGES)
                 const int64_t node = ((int64_t)z * ny + y) * nx + b.x0 + ox;
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
-                    const float2 pv = *reinterpret_cast<const float2 *>(own + ((ox + 1) * 3 + r) * CS);
-                    *reinterpret_cast<float2 *>(Q + (3 * node + r) * K + slice * CS + 2 * lane) =
-                        make_float2(acc[ox][r][0], acc[ox][r][1]);
-                    dacc0 += (double)pv.x * (double)acc[ox][r][0];
-                    dacc1 += (double)pv.y * (double)acc[ox][r][1];
+                    float *q = Q + (3 * node + r) * K + slice * CS + col;
+                    const float *pv = own + ((ox + 1) * 3 + r) * CS;
+                    if constexpr (V == 2)
+                        *reinterpret_cast<float2 *>(q) = make_float2(acc[ox][r][0], acc[ox][r][1]);
+                    else
+                        *q = acc[ox][r][0];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) dacc[v] += (double)pv[v] * (double)acc[ox][r][v];
                 }
             }
         }
-        __syncthreads();  // every warp is done with this stage before it is refilled
-        if (STAGES == 1 && w + gridDim.x < work) {
-            if (threadIdx.x == 0)
-                issue_brick(&pmap, bq, stage_base, stage_base + HALO_FLOATS, smem_u32(barp),
-                            brick_of(w + gridDim.x, slices, tx_n, ty_n, nx), slice, nx, ny, nz);
-            pending = 1u;
-        }
+        __syncthreads();  // every warp is done with the staged tiles before the next copies land
     }
-    // column dots: the four warps' lanes hold the same 64 columns
+    // column dots: red[xl][c], the four x-lines' partials of slice column c
     double *red = reinterpret_cast<double *>(smem);
-    red[warp * CS + 2 * lane] = dacc0;
-    red[warp * CS + 2 * lane + 1] = dacc1;
+#pragma unroll
+    for (int v = 0; v < V; ++v) red[xl * CS + col + v] = dacc[v];
     __syncthreads();
     if (threadIdx.x < CS) {
-        const double s = red[threadIdx.x] + red[CS + threadIdx.x] + red[2 * CS + threadIdx.x] + red[3 * CS + threadIdx.x];
-        atomicAdd(pq + slice * CS + threadIdx.x, s);
+        const double sum = red[threadIdx.x] + red[CS + threadIdx.x] + red[2 * CS + threadIdx.x] + red[3 * CS + threadIdx.x];
+        atomicAdd(pq + slice * CS + threadIdx.x, sum);
     }
 }
 
@@ -294,7 +284,7 @@ __global__ void k_lattice_fill(const int32_t *__restrict__ bptr, const int32_t *
 }
 
 int g_occ = 0;     // resident CTAs per SM of the k_lspmm32 instantiation in use
-int g_stages = 0;  // its shared-memory stages (SFC_LATTICE_STAGES=1 selects the single-stage kernel)
+int g_groups = 0;  // column groups per x-line: 2 (8 warps per CTA) or 1 (SFC_LATTICE_WARPS=4)
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
@@ -311,17 +301,19 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 }  // namespace
 
-// Installs the lattice view when the system's pattern comes from a 3-dof
-// mesh whose nodes form a lattice (numbered x fastest) and every block
-// couples lattice neighbours; otherwise the node-block (BSR) kernels are used.
-// SFC_SPMM=bsr in the environment keeps the BSR kernel (for comparisons).
+// With SFC_SPMM=lattice in the environment, installs the lattice view when
+// the system's pattern comes from a 3-dof mesh whose nodes form a lattice
+// (numbered x fastest) and every block couples lattice neighbours.  Without
+// it (the default: the node-block kernel measured faster at 48^3, 285 against
+// 363 us per 128-column product) and on other meshes, the node-block (BSR)
+// kernels are used.
 void build_lattice_blocks(sfc_system *s)
 {
     sfc_ctx *ctx = s->ctx;
     s->has_lattice = false;
     const sfc_mesh *m = s->pattern_mesh;
-    const char *force = std::getenv("SFC_SPMM");
-    if (force && std::string(force) == "bsr") return;
+    const char *want = std::getenv("SFC_SPMM");
+    if (!want || std::string(want) != "lattice") return;
     if (!s->has_bsr || !m || !m->is_grid || m->dim != 3 || m->dof != 3) return;
     const int nx = m->gn[0], ny = m->gn[1], nz = m->gn[2];
     if ((int64_t)nx * ny * nz != s->nodes || nx < 2 || ny < 2 || nz < 2) return;
@@ -365,17 +357,15 @@ void lattice_prepare(sfc_system *s, const float *P, int K)
         s->pmap_ptr = P;
         s->pmap_K = K;
     }
-    if (!g_stages) {
-        const char *e = std::getenv("SFC_LATTICE_STAGES");
-        g_stages = (e && e[0] == '1') ? 1 : 2;
-        if (g_stages == 2) {
-            SFC_CK(cudaFuncSetAttribute(k_lspmm32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem_bytes<2>()));
-            SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32<2>, THREADS, smem_bytes<2>()));
+    if (!g_groups) {
+        const char *e = std::getenv("SFC_LATTICE_WARPS");
+        g_groups = (e && std::string(e) == "4") ? 1 : 2;
+        if (g_groups == 2) {
+            SFC_CK(cudaFuncSetAttribute(k_lspmm32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+            SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32<2>, 256, SMEM_BYTES));
         } else {
-            SFC_CK(cudaFuncSetAttribute(k_lspmm32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem_bytes<1>()));
-            SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32<1>, THREADS, smem_bytes<1>()));
+            SFC_CK(cudaFuncSetAttribute(k_lspmm32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES));
+            SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ, k_lspmm32<1>, 128, SMEM_BYTES));
         }
         if (g_occ < 1) g_occ = 1;
     }
@@ -392,12 +382,12 @@ void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, 
     const int64_t work = tiles * slices;
     int64_t grid = std::min<int64_t>(work, (int64_t)occ * ctx->sm_count);
     grid = std::max<int64_t>(slices, grid - grid % slices);
-    if (g_stages == 2)
-        k_lspmm32<2><<<(unsigned)grid, THREADS, smem_bytes<2>(), ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K,
-                                                                               slices, work, pq, stop, s->lat_err.p);
+    if (g_groups == 2)
+        k_lspmm32<2><<<(unsigned)grid, 256, SMEM_BYTES, ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K, slices,
+                                                                       work, pq, stop, s->lat_err.p);
     else
-        k_lspmm32<1><<<(unsigned)grid, THREADS, smem_bytes<1>(), ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K,
-                                                                               slices, work, pq, stop, s->lat_err.p);
+        k_lspmm32<1><<<(unsigned)grid, 128, SMEM_BYTES, ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K, slices,
+                                                                       work, pq, stop, s->lat_err.p);
     count_launch(ctx);
 }
 

@@ -15,10 +15,11 @@ from tests.test_gpu_solve import setup
 pytestmark = pytest.mark.gpu
 
 
-def solve(ctx, n, bw, precond, rhs_seed=4, nrhs=130, force_bsr=False):
-    # the operator (and with it the choice of SpMM) is built at solve time
-    if force_bsr:
-        os.environ["SFC_SPMM"] = "bsr"
+def solve(ctx, n, bw, precond, rhs_seed=4, nrhs=130, lattice=True):
+    # the operator (and with it the choice of SpMM) is built at solve time;
+    # the lattice product is opt-in (SFC_SPMM=lattice)
+    if lattice:
+        os.environ["SFC_SPMM"] = "lattice"
     try:
         mesh, s, ds, F, bc = setup(ctx, mg.HEX8_ELASTIC, n, 17, amount=0.0, faces="x0")
         rng = np.random.default_rng(rhs_seed)
@@ -39,7 +40,7 @@ def test_lattice_spmm_matches_lu_and_node_blocks(ctx, n, bw, precond):
     assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
     refs = np.stack([ds.solve_transpose(r) for r in Rhs])
     assert np.abs(U - refs).max() <= 1e-7 * np.abs(refs).max()
-    U2, st2, _, _ = solve(ctx, n, bw, precond, force_bsr=True)
+    U2, st2, _, _ = solve(ctx, n, bw, precond, lattice=False)
     assert st2["spmm_kernel"] == 2, st2
     assert np.abs(U2 - refs).max() <= 1e-7 * np.abs(refs).max()
     # the two FP32 products differ only in summation order: iteration counts stay close
