@@ -873,36 +873,118 @@ void koh_loglik_batch(sfc_koh *k, const sfc_hparams_t *hps, int n, double *out)
 // m = Sigma (rho K_s^-1 sum_k y_k + C_s^-1 mean) with three explicit inverses.
 // The same Sigma and m follow from the Woodbury identity the reference uses in
 // giveFEconditionedDataWoodbury (:442-508) with P = I:
-//   S = C_s + K_s / (rho^2 n_o) = L L^T,  X = L^-1 C_s,
-//   Sigma = C_s - X^T X,  m = mean + X^T L^-1 (ybar - rho mean) / rho,
+//   S = C_s + K_s / (rho^2 n_o) = L L^T,  [X | z] = L^-1 [C_s | ybar - rho mean],
+//   Sigma = C_s - X^T X,  m = mean + X^T z / rho,
 // which needs one Cholesky factor and triangular solves (backward stable)
 // instead of the inverse of the ill-conditioned C_s: at the 48^3 elasticity
 // configuration (cond C_s ~ 3e8, sensor noise 1e-4) Gauss-Jordan inverses of
 // the three-inverse form left Sigma 8e-7 from the exact value, this form about
-// 1e-9.  One CTA: S, X and z = ybar - rho mean in `work`; L overwrites S.
-__global__ void __launch_bounds__(1024) k_koh_proj_factor(int ns, int n_o, const double *__restrict__ mean,
-                                                          const double *__restrict__ Cs,
-                                                          const double *__restrict__ xs, int dim,
-                                                          const double *__restrict__ Y, sfc_hparams_t hp,
-                                                          double *__restrict__ S, double *__restrict__ X,
-                                                          double *__restrict__ z, int *info)
+// 1e-9.  The factor and the solve are blocked by 32 (kChB): a one-CTA kernel
+// per diagonal block, a row-parallel kernel per panel, the trailing updates
+// on the multi-CTA gemm.
+constexpr int kChB = 32;
+
+// S = K_s / (rho^2 n_o) + C_s (ns x ns); W = [C_s | ybar - rho mean] (ns x (ns+1))
+__global__ void k_koh_proj_setup(int ns, int n_o, const double *__restrict__ mean, const double *__restrict__ Cs,
+                                 const double *__restrict__ xs, int dim, const double *__restrict__ Y,
+                                 sfc_hparams_t hp, double *__restrict__ S, double *__restrict__ W)
 {
-    mismatch_cov(ns, xs, dim, hp.mismatch_sigma, hp.mismatch_length, hp.mismatch_sensor_eps, S);
     const double sc = 1.0 / (hp.rho * hp.rho * n_o);
-    for (int64_t t = threadIdx.x; t < (int64_t)ns * ns; t += blockDim.x) {
-        S[t] = S[t] * sc + Cs[t];
-        X[t] = Cs[t];
+    const int64_t nn = (int64_t)ns * ns;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nn + ns; t += (int64_t)gridDim.x * blockDim.x) {
+        if (t < nn) {
+            const int k = (int)(t / ns), l = (int)(t % ns);
+            double kv = se_value(xs + 3 * k, xs + 3 * l, dim, hp.mismatch_sigma, hp.mismatch_length);
+            if (k == l) kv += hp.mismatch_sensor_eps * hp.mismatch_sensor_eps;
+            S[t] = kv * sc + Cs[t];
+            W[(int64_t)k * (ns + 1) + l] = Cs[t];
+        } else {
+            const int i = (int)(t - nn);
+            double ys = 0.0;
+            for (int c = 0; c < n_o; ++c) ys += Y[(int64_t)i * n_o + c];
+            W[(int64_t)i * (ns + 1) + ns] = ys / n_o - hp.rho * mean[i];
+        }
     }
-    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-        double ys = 0.0;
-        for (int c = 0; c < n_o; ++c) ys += Y[(int64_t)i * n_o + c];
-        z[i] = ys / n_o - hp.rho * mean[i];
-    }
+}
+
+// in-place lower Cholesky of the kb x kb diagonal block at (k0, k0) of the
+// n x n row-major A; a non-positive pivot sets *info (one CTA of 256)
+__global__ void __launch_bounds__(256) k_chol_diag(double *A, int64_t n, int64_t k0, int kb, int *info)
+{
+    __shared__ double D[kChB][kChB + 1];
+    __shared__ int bad;
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) D[t / kb][t % kb] = A[(k0 + t / kb) * n + k0 + t % kb];
+    if (threadIdx.x == 0) bad = 0;
     __syncthreads();
-    chol_lower(ns, S, ns, info);
-    if (*info) return;  // uniform: chol_lower ends with a barrier after writing info
-    trsm_lower(ns, S, ns, ns, X, ns);
-    trsm_lower(ns, S, ns, 1, z, 1);
+    for (int k = 0; k < kb; ++k) {
+        if (threadIdx.x == 0) {
+            const double d = D[k][k];
+            if (!(d > 0.0)) bad = 1;
+            D[k][k] = d > 0.0 ? sqrt(d) : 1.0;
+        }
+        __syncthreads();
+        for (int i = k + 1 + threadIdx.x; i < kb; i += blockDim.x) D[i][k] /= D[k][k];
+        __syncthreads();
+        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+            const int i = t / kb, j = t % kb;
+            if (i > k && j > k && j <= i) D[i][j] -= D[i][k] * D[j][k];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int i = t / kb, j = t % kb;
+        if (j <= i) A[(k0 + i) * n + k0 + j] = D[i][j];
+    }
+    if (threadIdx.x == 0 && bad) atomicExch(info, 1);
+}
+
+// rows i >= k0 + kb of the panel: A[i, k0:k0+kb] <- A[i, k0:k0+kb] L_kk^-T
+// (thread per row, L_kk staged in shared memory)
+__global__ void __launch_bounds__(256) k_chol_panel(double *A, int64_t n, int64_t k0, int kb)
+{
+    __shared__ double L[kChB][kChB + 1];
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) L[t / kb][t % kb] = A[(k0 + t / kb) * n + k0 + t % kb];
+    __syncthreads();
+    const int64_t i = k0 + kb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x[kChB];
+#pragma unroll
+    for (int m = 0; m < kChB; ++m) x[m] = m < kb ? A[i * n + k0 + m] : 0.0;
+#pragma unroll
+    for (int m = 0; m < kChB; ++m) {
+        if (m >= kb) break;
+        double v = x[m];
+        for (int q = 0; q < m; ++q) v -= x[q] * L[m][q];
+        x[m] = v / L[m][m];
+    }
+#pragma unroll
+    for (int m = 0; m < kChB; ++m)
+        if (m < kb) A[i * n + k0 + m] = x[m];
+}
+
+// rows k0..k0+kb of W (ncols columns, leading dimension ldw):
+// W_k <- L_kk^-1 W_k (thread per column)
+__global__ void __launch_bounds__(256) k_trsm_block_rows(const double *A, int64_t n, int64_t k0, int kb, double *W,
+                                                         int64_t ldw, int64_t ncols)
+{
+    __shared__ double L[kChB][kChB + 1];
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) L[t / kb][t % kb] = A[(k0 + t / kb) * n + k0 + t % kb];
+    __syncthreads();
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncols) return;
+    double x[kChB];
+#pragma unroll
+    for (int m = 0; m < kChB; ++m) x[m] = m < kb ? W[(k0 + m) * ldw + c] : 0.0;
+#pragma unroll
+    for (int m = 0; m < kChB; ++m) {
+        if (m >= kb) break;
+        double v = x[m];
+        for (int q = 0; q < m; ++q) v -= L[m][q] * x[q];
+        x[m] = v / L[m][m];
+    }
+#pragma unroll
+    for (int m = 0; m < kChB; ++m)
+        if (m < kb) W[(k0 + m) * ldw + c] = x[m];
 }
 
 void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
@@ -913,29 +995,48 @@ void koh_proj(sfc_koh *k, const sfc_hparams_t *hp, double *mean, double *cov)
     SFC_REQUIRE(k->n_o > 0, "sensor values not set");
     const int ns = (int)k->ns, n_o = k->n_o;
     const int64_t nn = (int64_t)ns * ns;
-    k->work.reserve((size_t)2 * nn + 2 * (size_t)ns + 16);
+    k->work.reserve((size_t)nn + (size_t)ns * (ns + 1) + 16);
     k->outv.reserve((size_t)ns + (size_t)nn);
-    double *Ksi = k->work.p, *Cui = Ksi + nn, *ysum = Cui + nn, *v = ysum + ns;
     double *pm = k->outv.p, *pc = k->outv.p + ns;
     const double rho = hp->rho;
     {
         ProfScope ps(ctx, "phase:koh_posterior", 0.0);
-        // S = C_s + K_s/(rho^2 n_o) = L L^T, X = L^-1 C_s, z = L^-1 (ybar - rho mean);
+        // S = C_s + K_s/(rho^2 n_o) = L L^T, [X | z] = L^-1 [C_s | ybar - rho mean];
         // Sigma = C_s - X^T X, m = mean + X^T z / rho
-        double *S = Ksi, *X = Cui, *z = ysum;
         SFC_REQUIRE(rho != 0.0, "rho must be nonzero");
+        const int64_t ld = ns + 1;
+        double *S = k->work.p, *W = S + nn;
         k->info.reserve(1);
-        k_koh_proj_factor<<<1, 1024, 0, ctx->stream>>>(ns, n_o, fg->mean.p, fg->cov.p, k->sensor_coords.p, k->dim,
-                                                       k->Y.p, *hp, S, X, z, k->info.p);
+        SFC_CK(cudaMemsetAsync(k->info.p, 0, sizeof(int), ctx->stream));
+        k_koh_proj_setup<<<grid_for(nn + ns, 256), 256, 0, ctx->stream>>>(ns, n_o, fg->mean.p, fg->cov.p,
+                                                                         k->sensor_coords.p, k->dim, k->Y.p, *hp, S, W);
         count_launch(ctx);
+        for (int64_t k0 = 0; k0 < ns; k0 += kChB) {
+            const int kb = (int)std::min<int64_t>(kChB, ns - k0);
+            const int64_t k1 = k0 + kb;
+            k_chol_diag<<<1, 256, 0, ctx->stream>>>(S, ns, k0, kb, k->info.p);
+            count_launch(ctx);
+            if (k1 < ns) {
+                k_chol_panel<<<grid_for(ns - k1, 256), 256, 0, ctx->stream>>>(S, ns, k0, kb);
+                count_launch(ctx);
+                gemm(ctx, 0, 1, ns - k1, ns - k1, kb, -1.0, S + k1 * ns + k0, ns, S + k1 * ns + k0, ns, 1.0,
+                     S + k1 * ns + k1, ns);
+            }
+        }
+        for (int64_t k0 = 0; k0 < ns; k0 += kChB) {
+            const int kb = (int)std::min<int64_t>(kChB, ns - k0);
+            const int64_t k1 = k0 + kb;
+            k_trsm_block_rows<<<grid_for(ld, 256), 256, 0, ctx->stream>>>(S, ns, k0, kb, W, ld, ld);
+            count_launch(ctx);
+            if (k1 < ns) gemm(ctx, 0, 0, ns - k1, ld, kb, -1.0, S + k1 * ns + k0, ns, W + k0 * ld, ld, 1.0, W + k1 * ld, ld);
+        }
         int bad = 0;
         download(ctx, &bad, k->info.p, 1);
         if (bad) fail(SFC_ERR_NOT_SPD, "sensor-space matrix not positive definite (C_s + K_s / (rho^2 n_o))");
         SFC_CK(cudaMemcpyAsync(pc, fg->cov.p, nn * 8, cudaMemcpyDeviceToDevice, ctx->stream));
         SFC_CK(cudaMemcpyAsync(pm, fg->mean.p, ns * 8, cudaMemcpyDeviceToDevice, ctx->stream));
-        gemm(ctx, 1, 0, ns, ns, ns, -1.0, X, ns, X, ns, 1.0, pc, ns);
-        gemm(ctx, 1, 0, ns, 1, ns, 1.0 / rho, X, ns, z, 1, 1.0, pm, 1);
-        (void)v;
+        gemm(ctx, 1, 0, ns, ns, ns, -1.0, W, ld, W, ld, 1.0, pc, ns);
+        gemm(ctx, 1, 0, ns, 1, ns, 1.0 / rho, W, ld, W + ns, ld, 1.0, pm, 1);
     }
     if (mean) download(ctx, mean, pm, ns);
     if (cov) download(ctx, cov, pc, (size_t)nn);
