@@ -26,6 +26,9 @@
  */
 #include <math.h>
 #include <stdint.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <stdlib.h>
 #include <string.h>
 
@@ -591,7 +594,7 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
     int it;
     for (it = 1; it <= max_iter; ++it) {
         double pq = 0, rr = 0, rz2 = 0;
-#pragma omp parallel for reduction(+ : pq) schedule(static)
+#pragma omp parallel for reduction(+ : pq) schedule(static) if (N >= 20000)
         for (int64_t i = 0; i < N; ++i) {
             double acc = 0;
             if (mask[i]) {
@@ -604,7 +607,7 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
             pq += p[i] * acc;
         }
         double alpha = rz / pq;
-#pragma omp parallel for reduction(+ : rr, rz2) schedule(static)
+#pragma omp parallel for reduction(+ : rr, rz2) schedule(static) if (N >= 20000)
         for (int64_t i = 0; i < N; ++i) {
             x[i] += alpha * p[i];
             r[i] -= alpha * q[i];
@@ -615,7 +618,7 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
         if (rr <= tol * tol * bb) break;
         double beta = rz2 / rz;
         rz = rz2;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (N >= 20000)
         for (int64_t i = 0; i < N; ++i) p[i] = z[i] + beta * p[i];
     }
     free(dinv);
@@ -633,6 +636,24 @@ int sfo_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double 
  * Parallel over rows (OpenMP); the result does not depend on the thread count
  * except through the order of the dot-product reductions.
  */
+static int max_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+static int thread_id(void)
+{
+#ifdef _OPENMP
+    return omp_get_thread_num();
+#else
+    return 0;
+#endif
+}
+
 int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const double *val,
                   const unsigned char *mask, int k, const double *B, double *X, double tol,
                   int max_iter, int use_x0, int *its_out)
@@ -645,8 +666,15 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
     double *rz2 = calloc(k, sizeof(double)), *alpha = calloc(k, sizeof(double));
     double *beta = calloc(k, sizeof(double));
     char *active = calloc(k, 1);
-    if (!r || !p || !q || !dinv || !bb || !rz || !pq || !rr || !rz2 || !alpha || !beta || !active) return -2;
-#pragma omp parallel for schedule(static)
+    /* per-thread partial sums, allocated once; small systems run serially */
+    const int par = N * (int64_t)k >= (1 << 20);
+    const int nthr = max_threads();
+    double *tl_acc = malloc(sizeof(double) * nthr * k), *tl_pq = malloc(sizeof(double) * nthr * k);
+    double *tl_rr = malloc(sizeof(double) * nthr * k), *tl_rz = malloc(sizeof(double) * nthr * k);
+    if (!r || !p || !q || !dinv || !bb || !rz || !pq || !rr || !rz2 || !alpha || !beta || !active || !tl_acc ||
+        !tl_pq || !tl_rr || !tl_rz)
+        return -2;
+#pragma omp parallel for schedule(static) if (par)
     for (int64_t i = 0; i < N; ++i) {
         double dg = 1.0;
         for (int64_t s = row_ptr[i]; s < row_ptr[i + 1]; ++s)
@@ -654,7 +682,7 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
         dinv[i] = 1.0 / dg;
     }
     /* r = b - S x (x = 0 unless use_x0) */
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (par)
     for (int64_t i = 0; i < N; ++i) {
         double *ri = r + i * k;
         for (int c = 0; c < k; ++c) ri[c] = B[i * k + c];
@@ -689,9 +717,11 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
     while (nact > 0 && it < max_iter) {
         ++it;
         for (int c = 0; c < k; ++c) pq[c] = 0;
-#pragma omp parallel
+        for (int64_t t = 0; t < (int64_t)nthr * k; ++t) tl_pq[t] = 0.0;
+#pragma omp parallel if (par)
         {
-            double *acc = malloc(sizeof(double) * k), *lpq = calloc(k, sizeof(double));
+            const int tid = thread_id();
+            double *acc = tl_acc + (int64_t)tid * k, *lpq = tl_pq + (int64_t)tid * k;
 #pragma omp for schedule(static)
             for (int64_t i = 0; i < N; ++i) {
                 const double *pi = p + i * k;
@@ -712,18 +742,18 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
                     lpq[c] += pi[c] * acc[c];
                 }
             }
-#pragma omp critical
-            for (int c = 0; c < k; ++c) pq[c] += lpq[c];
-            free(acc);
-            free(lpq);
         }
+        for (int t = 0; t < nthr; ++t)
+            for (int c = 0; c < k; ++c) pq[c] += tl_pq[(int64_t)t * k + c];
         for (int c = 0; c < k; ++c) {
             alpha[c] = active[c] ? rz[c] / pq[c] : 0.0;
             rr[c] = rz2[c] = 0;
         }
-#pragma omp parallel
+        for (int64_t t = 0; t < (int64_t)nthr * k; ++t) tl_rr[t] = tl_rz[t] = 0.0;
+#pragma omp parallel if (par)
         {
-            double *lrr = calloc(k, sizeof(double)), *lrz = calloc(k, sizeof(double));
+            const int tid = thread_id();
+            double *lrr = tl_rr + (int64_t)tid * k, *lrz = tl_rz + (int64_t)tid * k;
 #pragma omp for schedule(static)
             for (int64_t i = 0; i < N; ++i) {
                 double *xi = X + i * k, *ri = r + i * k;
@@ -735,14 +765,12 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
                     lrz[c] += ri[c] * (dinv[i] * ri[c]);
                 }
             }
-#pragma omp critical
-            for (int c = 0; c < k; ++c) {
-                rr[c] += lrr[c];
-                rz2[c] += lrz[c];
-            }
-            free(lrr);
-            free(lrz);
         }
+        for (int t = 0; t < nthr; ++t)
+            for (int c = 0; c < k; ++c) {
+                rr[c] += tl_rr[(int64_t)t * k + c];
+                rz2[c] += tl_rz[(int64_t)t * k + c];
+            }
         for (int c = 0; c < k; ++c) {
             beta[c] = 0.0;
             if (!active[c]) continue;
@@ -755,7 +783,7 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
             beta[c] = rz2[c] / rz[c];
             rz[c] = rz2[c];
         }
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (par)
         for (int64_t i = 0; i < N; ++i) {
             double *pi = p + i * k;
             const double *ri = r + i * k;
@@ -771,5 +799,6 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
     }
     free(r); free(p); free(q); free(dinv); free(bb); free(rz); free(pq); free(rr); free(rz2);
     free(alpha); free(beta); free(active);
+    free(tl_acc); free(tl_pq); free(tl_rr); free(tl_rz);
     return worst;
 }
