@@ -981,7 +981,7 @@ def main():
     ap.add_argument("--prof-steps", type=int, default=1)
     ap.add_argument("--block-width", type=int, default=128, choices=[32, 64, 128])
     ap.add_argument("--precond", default="two-level", choices=["jacobi", "block-jacobi", "two-level"])
-    ap.add_argument("--check-every", type=int, default=32,
+    ap.add_argument("--check-every", type=int, default=16,
                     help="iterations between the solver's convergence checks (c1/c2)")
     ap.add_argument("--coarse-size", type=int, default=0,
                     help="two-level: nodes per aggregate along each axis (0: library default)")
