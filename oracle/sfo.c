@@ -666,14 +666,18 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
     double *rz2 = calloc(k, sizeof(double)), *alpha = calloc(k, sizeof(double));
     double *beta = calloc(k, sizeof(double));
     char *active = calloc(k, 1);
-    /* per-thread partial sums, allocated once; small systems run serially */
+    /* Small systems run serially.  Each thread's row scratch and partial sums
+     * are its own allocations (a pointer into a shared array would keep the
+     * compiler from proving that the scratch row aliases no operand, and the
+     * column loops would not vectorise); the partial sums are merged in
+     * thread order after the loop, so the reductions do not depend on which
+     * thread finishes first. */
     const int par = N * (int64_t)k >= (1 << 20);
     const int nthr = max_threads();
-    double *tl_acc = malloc(sizeof(double) * nthr * k), *tl_pq = malloc(sizeof(double) * nthr * k);
-    double *tl_rr = malloc(sizeof(double) * nthr * k), *tl_rz = malloc(sizeof(double) * nthr * k);
-    if (!r || !p || !q || !dinv || !bb || !rz || !pq || !rr || !rz2 || !alpha || !beta || !active || !tl_acc ||
-        !tl_pq || !tl_rr || !tl_rz)
+    double **part = calloc(2 * (size_t)nthr, sizeof(double *));
+    if (!r || !p || !q || !dinv || !bb || !rz || !pq || !rr || !rz2 || !alpha || !beta || !active || !part)
         return -2;
+    int fail = 0;
 #pragma omp parallel for schedule(static) if (par)
     for (int64_t i = 0; i < N; ++i) {
         double dg = 1.0;
@@ -717,13 +721,17 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
     while (nact > 0 && it < max_iter) {
         ++it;
         for (int c = 0; c < k; ++c) pq[c] = 0;
-        for (int64_t t = 0; t < (int64_t)nthr * k; ++t) tl_pq[t] = 0.0;
 #pragma omp parallel if (par)
         {
-            const int tid = thread_id();
-            double *acc = tl_acc + (int64_t)tid * k, *lpq = tl_pq + (int64_t)tid * k;
+            double *acc = malloc(sizeof(double) * k), *lpq = calloc(k, sizeof(double));
+            part[thread_id()] = lpq;
+            if (!acc || !lpq) {
+#pragma omp atomic write
+                fail = 1;
+            }
 #pragma omp for schedule(static)
             for (int64_t i = 0; i < N; ++i) {
+                if (!acc || !lpq) continue;
                 const double *pi = p + i * k;
                 if (mask[i]) {
                     for (int c = 0; c < k; ++c) acc[c] = pi[c] / dinv[i];
@@ -742,20 +750,31 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
                     lpq[c] += pi[c] * acc[c];
                 }
             }
+            free(acc);
         }
-        for (int t = 0; t < nthr; ++t)
-            for (int c = 0; c < k; ++c) pq[c] += tl_pq[(int64_t)t * k + c];
+        for (int t = 0; t < nthr; ++t) {
+            if (part[t])
+                for (int c = 0; c < k; ++c) pq[c] += part[t][c];
+            free(part[t]);
+            part[t] = NULL;
+        }
+        if (fail) break;
         for (int c = 0; c < k; ++c) {
             alpha[c] = active[c] ? rz[c] / pq[c] : 0.0;
             rr[c] = rz2[c] = 0;
         }
-        for (int64_t t = 0; t < (int64_t)nthr * k; ++t) tl_rr[t] = tl_rz[t] = 0.0;
 #pragma omp parallel if (par)
         {
-            const int tid = thread_id();
-            double *lrr = tl_rr + (int64_t)tid * k, *lrz = tl_rz + (int64_t)tid * k;
+            double *lrr = calloc(k, sizeof(double)), *lrz = calloc(k, sizeof(double));
+            part[2 * thread_id()] = lrr;
+            part[2 * thread_id() + 1] = lrz;
+            if (!lrr || !lrz) {
+#pragma omp atomic write
+                fail = 1;
+            }
 #pragma omp for schedule(static)
             for (int64_t i = 0; i < N; ++i) {
+                if (!lrr || !lrz) continue;
                 double *xi = X + i * k, *ri = r + i * k;
                 const double *pi = p + i * k, *qi = q + i * k;
                 for (int c = 0; c < k; ++c) {
@@ -766,11 +785,17 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
                 }
             }
         }
-        for (int t = 0; t < nthr; ++t)
-            for (int c = 0; c < k; ++c) {
-                rr[c] += tl_rr[(int64_t)t * k + c];
-                rz2[c] += tl_rz[(int64_t)t * k + c];
-            }
+        for (int t = 0; t < nthr; ++t) {
+            if (part[2 * t] && part[2 * t + 1])
+                for (int c = 0; c < k; ++c) {
+                    rr[c] += part[2 * t][c];
+                    rz2[c] += part[2 * t + 1][c];
+                }
+            free(part[2 * t]);
+            free(part[2 * t + 1]);
+            part[2 * t] = part[2 * t + 1] = NULL;
+        }
+        if (fail) break;
         for (int c = 0; c < k; ++c) {
             beta[c] = 0.0;
             if (!active[c]) continue;
@@ -799,6 +824,7 @@ int sfo_block_pcg(int64_t N, const int64_t *row_ptr, const int32_t *col, const d
     }
     free(r); free(p); free(q); free(dinv); free(bb); free(rz); free(pq); free(rr); free(rz2);
     free(alpha); free(beta); free(active);
-    free(tl_acc); free(tl_pq); free(tl_rr); free(tl_rz);
+    free(part);
+    if (fail) return -2;
     return worst;
 }
