@@ -96,14 +96,18 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def ncu_traffic(kernel, block_width):
+# the CUDA kernel behind the solver's "spmm32" step, by last_stats()["spmm_kernel"]
+SPMM_KERNELS = {1: "k_spmm32", 2: "k_bspmm32", 3: "k_lspmm32", 4: "k_xspmm32"}
+
+
+def ncu_traffic(kernel, block_width, impl=None):
     """Per-launch DRAM bytes of `kernel` from the committed ncu summary, when
-    it was captured at this block width."""
+    it was captured at this block width on the same CUDA kernel."""
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
             d = json.load(f)
         e = d.get(kernel)
-        if e and e.get("block_width") == block_width:
+        if e and e.get("block_width") == block_width and (impl is None or e.get("kernel", "").startswith(impl)):
             return float(e["traffic_bytes"])
     except (OSError, ValueError):
         pass
@@ -323,8 +327,10 @@ def run_ours(args, ws, rank, local):
         per_launch_bytes = tbytes / cnt
         per_launch_s = tms / 1e3 / cnt
         achieved = per_launch_bytes / per_launch_s / 1e9
-        roof = {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": ncu_traffic(name, args.block_width),
+        impl = SPMM_KERNELS.get(block_stats.get("spmm_kernel")) if name == "spmm32" else None
+        roof = {"kernel": name, "cuda_kernel": impl, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": ncu_traffic(name, args.block_width, impl),
                 "traffic_source": "profiles/ncu_traffic.json (ncu --set full, same workload)",
                 "peak_source": peak_kind,
                 "bytes_per_launch": per_launch_bytes, "avg_launch_us": round(per_launch_s * 1e6, 2),

@@ -295,6 +295,65 @@ struct CoarseSpace {
     DBuf<float> c32, e32;               // [nc][K] restriction and correction (block)
     DBuf<double> c64, e64;              // single FP64 vector
 };
+
+// vectors of V consecutive columns of a K = 32*V column block (lane owns
+// columns lane*V .. lane*V+V-1)
+template <int V>
+struct VecT;
+template <> struct VecT<1> { using f = float; using d = double; };
+template <> struct VecT<2> { using f = float2; using d = double2; };
+template <> struct VecT<4> { using f = float4; using d = double4; };
+
+template <int V>
+__device__ __forceinline__ void ldv(const float *p, float (&v)[V])
+{
+    if constexpr (V == 1) v[0] = *p;
+    if constexpr (V == 2) { const float2 t = *reinterpret_cast<const float2 *>(p); v[0] = t.x; v[1] = t.y; }
+    if constexpr (V == 4) {
+        const float4 t = *reinterpret_cast<const float4 *>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    }
+}
+template <int V>
+__device__ __forceinline__ void stv(float *p, const float (&v)[V])
+{
+    if constexpr (V == 1) *p = v[0];
+    if constexpr (V == 2) *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+    if constexpr (V == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// V consecutive doubles (16-byte loads where V >= 2; the rows are 16-byte aligned)
+template <int V>
+__device__ __forceinline__ void ldv64(const double *p, double (&v)[V])
+{
+    if constexpr (V == 1) {
+        v[0] = *p;
+    } else {
+#pragma unroll
+        for (int k = 0; k < V; k += 2) {
+            const double2 t = *reinterpret_cast<const double2 *>(p + k);
+            v[k] = t.x;
+            v[k + 1] = t.y;
+        }
+    }
+}
+
+// reduce per-lane column partials acc[V] (column lane*V+v) over the block's
+// warps and add them to out[K]
+template <int V>
+__device__ __forceinline__ void block_cols_add(const double (&acc)[V], double *sh, double *out)
+{
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    constexpr int K = 32 * V;
+#pragma unroll
+    for (int v = 0; v < V; ++v) sh[w * K + l * V + v] = acc[v];
+    __syncthreads();
+    for (int c = threadIdx.x; c < K; c += blockDim.x) {
+        double s = 0;
+        for (int j = 0; j < nw; ++j) s += sh[j * K + c];
+        atomicAdd(out + c, s);
+    }
+}
 }  // namespace sfc
 
 // ---------------------------------------------------------------------------
@@ -364,6 +423,7 @@ struct sfc_system {
     // node's 27 neighbour blocks in canonical slots (dz, dy, dx), zero where
     // the neighbour is missing, rows padded to 4 floats (lattice.cu)
     bool has_lattice = false;
+    int lat_mode = 0;         // product on the lattice view: 1 staged bricks, 2 streamed x-lines
     int lat[3] = {0, 0, 0};
     sfc::DBuf<float> bq;      // nodes x 27 x 12
     sfc::DBuf<int> lat_err;   // bounded-wait status of the staged SpMM
@@ -475,6 +535,8 @@ void build_lattice_blocks(sfc_system *s);
 void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop);
 void lattice_prepare(sfc_system *s, const float *P, int K);
 void lattice_check(sfc_system *s);
+void xline_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop);
+void xline_prepare(int K);
 void flush_staged(sfc_system *s);
 void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);
 void element_matrices_unit(const sfc_mesh *m, double *ke0);

@@ -1,4 +1,4 @@
-// Staged block SpMM Q = S P for 3-dof meshes on a structured node lattice
+// Block SpMM Q = S P for 3-dof meshes on a structured node lattice
 // (trilinear hexahedra on an nx x ny x nz grid, nodes numbered x fastest):
 // the FP32 product at the heart of the mixed block PCG, replacing the sparse
 // direct solve of corlib/SystemSolveEigenSparse.hpp:273-404 for the many
@@ -7,10 +7,14 @@
 // S is held as each node's 27 neighbour blocks in canonical slots
 // (dz, dy, dx) (zero where the lattice has no neighbour), rows padded to four
 // floats so a warp reads a block with three 16-byte broadcast loads.  P and Q
-// are the block solver's RHS-interleaved [N][K] FP32 arrays.
+// are the block solver's RHS-interleaved [N][K] FP32 arrays.  Two products
+// use this view: the streamed x-line kernel k_xspmm32 (the default; described
+// at the kernel) and the TMA-staged brick kernel k_lspmm32 below
+// (SFC_SPMM=lattice).
 //
-// A work item is a brick of 4 x 2 x 2 output nodes and a 64-column slice of
-// the block.  One elected thread issues a single 5-D TMA tensor load of the
+// Staged bricks.  A work item is a brick of 4 x 2 x 2 output nodes and a
+// 64-column slice of the block.  One elected thread issues a single 5-D TMA
+// tensor load of the
 // brick's halo (6 x 4 x 4 column nodes x 3 rows x 64 columns, zero-filled
 // outside the lattice: 72 KiB) and 1-D bulk copies of the brick's block rows
 // (up to 4 x 5 KiB) into shared memory, completing on one mbarrier.  Each
@@ -18,15 +22,15 @@
 // per lane): for every column node of its 3 x 3 neighbour lines a warp reads
 // the node's three P rows from shared memory once and applies them to every
 // output node of the line that couples to it (up to three), so a P row read
-// feeds 1.8 outputs on average and the FMA pipe, not the load path, bounds
-// the kernel.  The p.q column dots are accumulated in FP64 per lane across
-// all of a CTA's work items and reduced once at the end.
+// feeds 1.8 outputs on average.  Measured, the shared-memory load path bounds
+// it: both warps of an x-line load the same block values for their two
+// columns per lane.  The p.q column dots are accumulated in FP64 per lane
+// across all of a CTA's work items and reduced once at the end.
 //
 // Two CTAs share an SM (94.5 KiB of shared memory each); each x-line is
 // split over two warps by columns (8 warps per CTA) for latency hiding
 // (SFC_LATTICE_WARPS=4 keeps one warp per x-line).  Waits on the mbarrier
-// are bounded:
-// a wait that gives up sets lat_err (the solver then fails with
+// are bounded: a wait that gives up sets lat_err (the solver then fails with
 // SFC_ERR_TIMEOUT), waits once more (bounded) for the copies in flight and
 // leaves the kernel.  No multicast, no clusters: every copy reads this
 // GPU's own memory.
@@ -283,6 +287,162 @@ __global__ void k_lattice_fill(const int32_t *__restrict__ bptr, const int32_t *
     }
 }
 
+// Streamed lattice product (the default on lattices): one warp per
+// contiguous run of output nodes (numbered x fastest, so a run is a few x-line
+// segments), all K = 32 V columns of the block, V per lane.  The warp walks
+// each segment's column positions cx along x; at each it loads the P rows of
+// the nine neighbour lines (y + dy, z + dz) once and applies them to the
+// three output nodes cx - 1, cx, cx + 1 that couple to them, keeping a
+// sliding window of three output nodes' accumulators in registers.  Output
+// cx - 1 then has all its columns and is stored.  Every P row read from L1
+// therefore feeds three outputs (against one in the node-block kernel), and a
+// block's nine values (three 16-byte shared loads, the same address in every
+// lane) feed 9 V FMAs per lane.
+//
+// Each block is read exactly once, so a load of it from global memory would
+// miss L1 and stall the FMAs that follow it.  Every output node's 27 blocks
+// (1296 bytes) are instead copied by cp.async into a per-warp ring of four
+// rows in shared memory one position before their first use (the three rows
+// in use and the one in flight), and the FMAs read them there.  Neighbour
+// lines outside the lattice are clamped to a line inside it: their blocks are
+// zero, so they add nothing; outputs outside the segment are computed from
+// stale ring rows and never stored.  p.q column dots in FP64.
+constexpr int XR = 4;  // block ring rows per warp
+
+template <int V>
+constexpr size_t xsmem()
+{
+    return (size_t)8 * 32 * V * sizeof(double) + (size_t)8 * XR * NODE_FLOATS * sizeof(float);
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <int V>
+__global__ void __launch_bounds__(256, 2)
+    k_xspmm32(const float *__restrict__ bq, const float *__restrict__ P, float *__restrict__ Q, int nx, int ny,
+              int nz, int64_t nodes, int64_t per_warp, double *pq, const int *stop)
+{
+    constexpr int K = 32 * V;
+    constexpr int64_t RS = 3 * (int64_t)K;  // floats per node of P and Q
+    extern __shared__ __align__(16) unsigned char xs[];
+    double *sh = reinterpret_cast<double *>(xs);
+    if (*stop) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float *ring = reinterpret_cast<float *>(xs + 8 * K * sizeof(double)) + warp * XR * NODE_FLOATS;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    double dacc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    const int64_t end = min(nodes, (gw + 1) * per_warp);
+    const int64_t row = (int64_t)nx * RS;
+    for (int64_t a = gw * per_warp; a < end;) {
+        const int64_t line = a / nx;
+        const int x0 = (int)(a - line * nx);
+        const int x1 = (int)(min(end, (line + 1) * nx) - 1 - line * nx);
+        const int y = (int)(line % ny), z = (int)(line / ny);
+        // the nine neighbour lines (index z * ny + y), clamped into the lattice
+        int nl[9];
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy)
+                nl[dz * 3 + dy] = min(max(z + dz - 1, 0), nz - 1) * ny + min(max(y + dy - 1, 0), ny - 1);
+        const float *pb = P + lane * V;
+        const float *bl = bq + line * nx * NODE_FLOATS;
+        const float *own = P + line * row + lane * V;
+        float *ql = Q + line * row + lane * V;
+        const int c0 = max(0, x0 - 1), c1 = min(nx - 1, x1 + 1);
+        // output ox's blocks into ring row ox % XR (nothing outside the segment)
+        auto fetch = [&](int ox) {
+            if (ox < x0 || ox > x1) return;
+            const float4 *src = reinterpret_cast<const float4 *>(bl + (int64_t)ox * NODE_FLOATS);
+            float4 *dst = reinterpret_cast<float4 *>(ring + (ox % XR) * NODE_FLOATS);
+            for (int t = lane; t < NODE_FLOATS / 4; t += 32) cp_async16(dst + t, src + t);
+        };
+        // every lane is done with the previous segment's ring; the outputs
+        // that the first position needs
+        __syncwarp();
+        for (int ox = x0; ox <= c0 + 1; ++ox) fetch(ox);
+        cp_async_commit();
+        float acc[3][3][V];
+#pragma unroll
+        for (int o = 0; o < 3; ++o)
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[o][r][v] = 0.f;
+        for (int cx = c0; cx <= c1; ++cx) {
+            // outputs up to cx + 1 have landed; then the copy for output cx + 2
+            // (into the row of output cx - 2, which no lane reads any more)
+            cp_async_wait_all();
+            __syncwarp();
+            fetch(cx + 2);
+            cp_async_commit();
+#pragma unroll
+            for (int l = 0; l < 9; ++l) {
+                const float *pj = pb + ((int64_t)nl[l] * nx + cx) * RS;
+                float p[3][V];
+                ldv<V>(pj, p[0]);
+                ldv<V>(pj + K, p[1]);
+                ldv<V>(pj + 2 * K, p[2]);
+#pragma unroll
+                for (int o = 0; o < 3; ++o) {
+                    // output cx - 1 + o couples to column cx at dx = 1 - o (slot 2 - o)
+                    const int slot = (cx - 1 + o + XR) % XR;  // cx - 1 + o >= -1
+                    const float4 *bp =
+                        reinterpret_cast<const float4 *>(ring + slot * NODE_FLOATS + (l * 3 + 2 - o) * SLOT);
+                    const float4 m[3] = {bp[0], bp[1], bp[2]};
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+#pragma unroll
+                        for (int v = 0; v < V; ++v)
+                            acc[o][r][v] = fmaf(m[r].z, p[2][v], fmaf(m[r].y, p[1][v], fmaf(m[r].x, p[0][v], acc[o][r][v])));
+                }
+            }
+            // output cx - 1 has all three of its column positions
+            if (cx - 1 >= x0) {
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const int64_t off = (int64_t)(cx - 1) * RS + r * K;
+                    stv<V>(ql + off, acc[0][r]);
+                    float pv[V];
+                    ldv<V>(own + off, pv);
+#pragma unroll
+                    for (int v = 0; v < V; ++v) dacc[v] += (double)pv[v] * (double)acc[0][r][v];
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    acc[0][r][v] = acc[1][r][v];
+                    acc[1][r][v] = acc[2][r][v];
+                    acc[2][r][v] = 0.f;
+                }
+        }
+        if (c1 == x1) {
+            // the segment ends on the lattice face: its last output is in slot 0
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int64_t off = (int64_t)x1 * RS + r * K;
+                stv<V>(ql + off, acc[0][r]);
+                float pv[V];
+                ldv<V>(own + off, pv);
+#pragma unroll
+                for (int v = 0; v < V; ++v) dacc[v] += (double)pv[v] * (double)acc[0][r][v];
+            }
+        }
+        a = line * nx + x1 + 1;
+    }
+    cp_async_wait_all();  // no copy outlives the kernel (they are all empty by now)
+    block_cols_add<V>(dacc, sh, pq);
+}
+
 int g_occ = 0;     // resident CTAs per SM of the k_lspmm32 instantiation in use
 int g_groups = 0;  // column groups per x-line: 2 (8 warps per CTA) or 1 (SFC_LATTICE_WARPS=4)
 
@@ -301,19 +461,21 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 
 }  // namespace
 
-// With SFC_SPMM=lattice in the environment, installs the lattice view when
-// the system's pattern comes from a 3-dof mesh whose nodes form a lattice
-// (numbered x fastest) and every block couples lattice neighbours.  Without
-// it (the default: the node-block kernel measured faster at 48^3, 285 against
-// 363 us per 128-column product) and on other meshes, the node-block (BSR)
-// kernels are used.
+// Installs the lattice view when the system's pattern comes from a 3-dof
+// mesh whose nodes form a lattice (numbered x fastest) and every block couples
+// lattice neighbours, and picks the product that uses it: the streamed
+// x-line kernel by default, the TMA-staged brick kernel with SFC_SPMM=lattice
+// in the environment.  SFC_SPMM=bsr, and every other mesh, keep the
+// node-block (BSR) kernels.
 void build_lattice_blocks(sfc_system *s)
 {
     sfc_ctx *ctx = s->ctx;
     s->has_lattice = false;
+    s->lat_mode = 0;
     const sfc_mesh *m = s->pattern_mesh;
-    const char *want = std::getenv("SFC_SPMM");
-    if (!want || std::string(want) != "lattice") return;
+    const char *e = std::getenv("SFC_SPMM");
+    const std::string want = e ? e : "";
+    if (want == "bsr") return;
     if (!s->has_bsr || !m || !m->is_grid || m->dim != 3 || m->dof != 3) return;
     const int nx = m->gn[0], ny = m->gn[1], nz = m->gn[2];
     if ((int64_t)nx * ny * nz != s->nodes || nx < 2 || ny < 2 || nz < 2) return;
@@ -336,6 +498,7 @@ void build_lattice_blocks(sfc_system *s)
     s->lat[1] = ny;
     s->lat[2] = nz;
     s->has_lattice = true;
+    s->lat_mode = want == "lattice" ? 1 : 2;
 }
 
 // the tensor map of P and the kernel's attributes, set up outside any
@@ -389,6 +552,49 @@ void lattice_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, 
         k_lspmm32<1><<<(unsigned)grid, 128, SMEM_BYTES, ctx->stream>>>(s->pmap, s->bq.p, Q, nx, ny, nz, K, slices,
                                                                        work, pq, stop, s->lat_err.p);
     count_launch(ctx);
+}
+
+// the streamed x-line product (k_xspmm32): contiguous runs of output nodes,
+// one per warp, of equal length, over every resident warp of the GPU
+template <int V>
+int xline_occ()
+{
+    static int occ = 0;
+    if (!occ) {
+        SFC_CK(cudaFuncSetAttribute(k_xspmm32<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsmem<V>()));
+        SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xspmm32<V>, 256, xsmem<V>()));
+        if (occ < 1) occ = 1;
+    }
+    return occ;
+}
+
+template <int V>
+void xline_launch(sfc_system *s, const float *P, float *Q, double *pq, const int *stop)
+{
+    sfc_ctx *ctx = s->ctx;
+    const int64_t warps = (int64_t)xline_occ<V>() * ctx->sm_count * 8;
+    const int64_t per_warp = (s->nodes + warps - 1) / warps;
+    const unsigned grid = (unsigned)((s->nodes + per_warp * 8 - 1) / (per_warp * 8));
+    k_xspmm32<V><<<grid, 256, xsmem<V>(), ctx->stream>>>(s->bq.p, P, Q, s->lat[0], s->lat[1], s->lat[2], s->nodes,
+                                                           per_warp, pq, stop);
+    count_launch(ctx);
+}
+
+// kernel attributes of the streamed product for K columns, set up outside any
+// stream capture
+void xline_prepare(int K)
+{
+    if (K == 32) xline_occ<1>();
+    else if (K == 64) xline_occ<2>();
+    else if (K == 128) xline_occ<4>();
+}
+
+void xline_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop)
+{
+    SFC_REQUIRE(K == 32 || K == 64 || K == 128, "streamed lattice SpMM needs 32, 64 or 128 columns");
+    if (K == 32) xline_launch<1>(s, P, Q, pq, stop);
+    else if (K == 64) xline_launch<2>(s, P, Q, pq, stop);
+    else xline_launch<4>(s, P, Q, pq, stop);
 }
 
 // after a solve: a staged SpMM whose bounded wait gave up fails the solve

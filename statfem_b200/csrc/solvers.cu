@@ -296,63 +296,6 @@ __global__ void __launch_bounds__(kRedThreads) k_dot(const double *__restrict__ 
 // ---------------------------------------------------------------------------
 // block of K = 32*V right-hand sides, RHS-interleaved [N][K]
 // ---------------------------------------------------------------------------
-template <int V>
-struct VecT;
-template <> struct VecT<1> { using f = float; using d = double; };
-template <> struct VecT<2> { using f = float2; using d = double2; };
-template <> struct VecT<4> { using f = float4; using d = double4; };
-
-template <int V>
-__device__ __forceinline__ void ldv(const float *p, float (&v)[V])
-{
-    if constexpr (V == 1) v[0] = *p;
-    if constexpr (V == 2) { const float2 t = *reinterpret_cast<const float2 *>(p); v[0] = t.x; v[1] = t.y; }
-    if constexpr (V == 4) {
-        const float4 t = *reinterpret_cast<const float4 *>(p);
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    }
-}
-template <int V>
-__device__ __forceinline__ void stv(float *p, const float (&v)[V])
-{
-    if constexpr (V == 1) *p = v[0];
-    if constexpr (V == 2) *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
-    if constexpr (V == 4) *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
-}
-
-// V consecutive doubles (16-byte loads where V >= 2; the rows are 16-byte aligned)
-template <int V>
-__device__ __forceinline__ void ldv64(const double *p, double (&v)[V])
-{
-    if constexpr (V == 1) {
-        v[0] = *p;
-    } else {
-#pragma unroll
-        for (int k = 0; k < V; k += 2) {
-            const double2 t = *reinterpret_cast<const double2 *>(p + k);
-            v[k] = t.x;
-            v[k + 1] = t.y;
-        }
-    }
-}
-
-// reduce per-lane column partials acc[V] (column lane*V+v) over the block's
-// warps and add them to out[K]
-template <int V>
-__device__ __forceinline__ void block_cols_add(const double (&acc)[V], double *sh, double *out)
-{
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
-    constexpr int K = 32 * V;
-#pragma unroll
-    for (int v = 0; v < V; ++v) sh[w * K + l * V + v] = acc[v];
-    __syncthreads();
-    for (int c = threadIdx.x; c < K; c += blockDim.x) {
-        double s = 0;
-        for (int j = 0; j < nw; ++j) s += sh[j * K + c];
-        atomicAdd(out + c, s);
-    }
-}
-
 // Q = S P (FP32 values, FP32 vectors, FP32 accumulate), warp per row;
 // pq[c] += sum_i P[i][c] Q[i][c] in FP64
 template <int V>
@@ -1514,7 +1457,11 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         ProfScope ps(ctx, "spmm32",
                      bsr ? (double)s->nblocks * 40 + 4.0 * (s->nodes + 1) + 2.0 * N * K * 4
                          : (double)s->nnz * 8 + 4.0 * (N + 1) + 2.0 * N * K * 4);
-        if (bsr && s->has_lattice && K >= 64) {
+        if (bsr && s->has_lattice && s->lat_mode == 2) {
+            xline_spmm32(s, Pm, Qm, K, out, stop);
+            return;
+        }
+        if (bsr && s->has_lattice && s->lat_mode == 1 && K >= 64) {
             lattice_spmm32(s, Pm, Qm, K, out, stop);
             return;
         }
@@ -1600,7 +1547,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     // SFC_BLOCK_GRAPH=0 in the environment.
     const char *genv = std::getenv("SFC_BLOCK_GRAPH");
     const bool use_graph = !ctx->prof && check >= 2 && !(genv && genv[0] == '0');
-    const bool lattice = bsr && s->has_lattice && K >= 64;
+    const bool lattice = bsr && s->has_lattice && s->lat_mode == 1 && K >= 64;
     auto launch_chunk_graph = [&]() -> bool {
         GraphExec &g = s->blk_graph[V == 1 ? 0 : V == 2 ? 1 : 2];
         // everything the captured launches allocate or set up, done outside the capture
@@ -1609,13 +1556,14 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             s->coarse.e32.reserve(crs.nc * K);
         }
         if (lattice) lattice_prepare(s, pp, K);
+        if (bsr && s->has_lattice && s->lat_mode == 2) xline_prepare(K);
         const std::vector<uintptr_t> key = {
             (uintptr_t)K, (uintptr_t)check, (uintptr_t)N, (uintptr_t)s->nodes, (uintptr_t)gw,
             (uintptr_t)(bsr | (bj << 1) | (two << 2) | (two1 << 3) | (lattice << 4)), (uintptr_t)s->scal.p,
             (uintptr_t)s->blk32.p, (uintptr_t)s->colsc.p, (uintptr_t)s->flags.p, (uintptr_t)s->bdinv32.p,
             (uintptr_t)s->dinv32.p, (uintptr_t)s->bptr.p, (uintptr_t)s->bcol.p, (uintptr_t)s->bval32.p,
             (uintptr_t)s->row_ptr.p, (uintptr_t)s->col.p, (uintptr_t)s->a_op32.p, (uintptr_t)s->bq.p,
-            (uintptr_t)s->lat_err.p, (uintptr_t)s->lat[0], (uintptr_t)s->lat[1], (uintptr_t)s->lat[2],
+            (uintptr_t)s->lat_err.p, (uintptr_t)s->lat_mode, (uintptr_t)s->lat[0], (uintptr_t)s->lat[1], (uintptr_t)s->lat[2],
             (uintptr_t)s->pmap_ptr, (uintptr_t)crs.agg_ptr.p, (uintptr_t)crs.agg_nodes.p, (uintptr_t)crs.mode.p,
             (uintptr_t)crs.c32.p, (uintptr_t)crs.e32.p, (uintptr_t)crs.a32.p, (uintptr_t)crs.node_agg.p,
             (uintptr_t)crs.nagg, (uintptr_t)crs.nc, (uintptr_t)crs.dof};
@@ -1881,7 +1829,10 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     st.converged = all_conv ? 1 : 0;
     st.fallback_columns = n_fallback;
     st.coarse_dofs = two_any ? (int32_t)(crs.nc - crs.dropped) : 0;
-    st.spmm_kernel = bsr ? (s->has_lattice && K >= 64 ? 3 : 2) : 1;
+    st.spmm_kernel = !bsr ? 1
+                     : s->has_lattice && s->lat_mode == 2 ? 4
+                     : s->has_lattice && s->lat_mode == 1 && K >= 64 ? 3
+                                                                    : 2;
 }
 
 }  // namespace
