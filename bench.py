@@ -331,7 +331,7 @@ def run_ours(args, ws, rank, local):
         roof = {"kernel": name, "cuda_kernel": impl, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": ncu_traffic(name, args.block_width, impl),
-                "traffic_source": "profiles/ncu_traffic.json (ncu --set full, same workload)",
+                "traffic_source": "profiles/ncu_traffic.json (ncu DRAM bytes of the same kernel on the same workload)",
                 "peak_source": peak_kind,
                 "bytes_per_launch": per_launch_bytes, "avg_launch_us": round(per_launch_s * 1e6, 2),
                 "launches": cnt, "share_of_step": round(tms / max(prof_ms, 1e-9), 4),
