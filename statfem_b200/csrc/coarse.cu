@@ -20,8 +20,9 @@
 //  * k_coarse_restrict32: c = P^T r, a cluster of CTAs per aggregate (a
 //    version fused into the x/r update ran slower: its register count halved
 //    the resident warps);
-//  * k_coarse_apply32: e = A_c^+ c (FP32, dense nc x nc, L2-resident) and the
-//    coarse share c.e of each column's r.z, split over k across a cluster;
+//  * k_coarse_gemm32: e = A_c^+ c (FP32, dense, L2-resident, a tiled product
+//    split over k across a cluster) and the coarse share c.e of each
+//    column's r.z;
 //  * the p update (solvers.cu) adds z += P e on the fly from each node's
 //    aggregate id and centroid offset (k_ncpupdate32; k_cbpupdate32 on scalar
 //    meshes).
@@ -46,6 +47,15 @@ namespace sfc {
 namespace {
 
 namespace cg = cooperative_groups;
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 constexpr int kSlots = 27;   // 3 x 3 x 3 colour classes of the box grid
 constexpr int kMaxAggs = 512;    // 3-dof meshes: 6 coarse dofs per aggregate
@@ -246,10 +256,13 @@ __global__ void __cluster_dims__(kGalSplit, 1, 1) __launch_bounds__(32 * kGalWar
     cl.sync();  // the other CTAs' accumulators stay alive until every read is done
 }
 
-__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n)
+// b = (a + a^T) / 2 in FP32 with row stride ldb >= n (the padding stays as it is)
+__global__ void k_to_f32_sym(const double *__restrict__ a, float *__restrict__ b, int64_t n, int64_t ldb)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / n, j = t % n;
+        b[i * ldb + j] = (float)(0.5 * (a[t] + a[j * n + i]));
+    }
 }
 
 // c[6a + m][col] = (P^T r)[6a + m][col] for K = 32 V interleaved columns: a
@@ -391,122 +404,99 @@ __global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
     cl.sync();
 }
 
-// e = A c (A: nc x nc FP32, c and e: [nc][K]); rz[col] += sum_rows c e.
-// Split over k: a cluster of kSplitK CTAs shares one block of ROWS output
-// rows, each CTA takes a quarter of the k range (register-prefetched 32-wide
-// chunks of A's rows and of c), and the partial tiles are added in rank
-// order through distributed shared memory, each CTA finishing ROWS/kSplitK
-// of the rows.
-constexpr int kSplitK = 4;
+// e = A c with A the coarse inverse (FP32, symmetric, lda x lda, zero past
+// nc) and c, e [lda][K]; rz[col] += sum_rows c e in FP64.  A tiled FP32
+// product on CUDA cores: a CTA owns 64 rows x 32 columns of e and a quarter
+// of the k range, with 4 x 4 outputs per thread from shared-memory tiles
+// (the A tile is read as rows k of A, i.e. already transposed, because A is
+// symmetric) filled by cp.async one 32-wide k chunk ahead; the four k
+// quarters form a cluster and are added in rank order through distributed
+// shared memory, so the result does not depend on scheduling.
+constexpr int kGemmRows = 64, kGemmCols = 32, kGemmK = 32, kGemmSplit = 4;
 
 template <int V>
-__global__ void __cluster_dims__(1, kSplitK, 1) __launch_bounds__(256)
-    k_coarse_apply32(const float *__restrict__ A, const float *__restrict__ c, float *__restrict__ e, int64_t nc,
-                     double *rz, const int *stop)
+__global__ void __cluster_dims__(1, 1, kGemmSplit) __launch_bounds__(128)
+    k_coarse_gemm32(const float *__restrict__ A, const float *__restrict__ c, float *__restrict__ e, int64_t lda,
+                    int64_t nc, double *rz, const int *stop)
 {
     constexpr int K = 32 * V;
-    constexpr int CG = K / 4;         // float4 column groups
-    constexpr int RS = 256 / CG;      // row sets
-    constexpr int R = 2;              // rows per thread
-    constexpr int ROWS = RS * R;      // 16, 32, 64 for V = 4, 2, 1
-    constexpr int NA = ROWS * 32 / 256;  // A values per thread and chunk
-    constexpr int NC = 32 * CG / 256;    // c float4 per thread and chunk
-    __shared__ float sa[ROWS][33];
-    __shared__ __align__(16) float4 sc[32][CG];
-    __shared__ __align__(16) float part[ROWS][K];
-    __shared__ double sred[RS][K];
-    if (stop && *stop) return;
+    __shared__ __align__(16) float sa[2][kGemmK][kGemmRows];
+    __shared__ __align__(16) float sc[2][kGemmK][kGemmCols];
+    __shared__ __align__(16) float part[kGemmRows][kGemmCols];
+    __shared__ double sred[4][kGemmCols];
+    if (stop && *stop) return;  // uniform: stop changes only between launches
     cg::cluster_group cl = cg::this_cluster();
     const unsigned rank = cl.block_rank();
-    const int g = threadIdx.x % CG, rs = threadIdx.x / CG;
-    const int64_t row0 = (int64_t)blockIdx.x * ROWS;
-    const int64_t nchunks = (nc + 31) / 32, per = (nchunks + kSplitK - 1) / kSplitK;
-    const int64_t kc0 = (int64_t)rank * per, kc1 = kc0 + per < nchunks ? kc0 + per : nchunks;
-    float acc[R][4];
+    const int tid = threadIdx.x, rg = tid % 16, cgp = tid / 16;  // rows 4 rg.., columns 4 cgp..
+    const int64_t row0 = (int64_t)blockIdx.x * kGemmRows;
+    const int col0 = blockIdx.y * kGemmCols;
+    const int64_t nchunks = lda / kGemmK, per = (nchunks + kGemmSplit - 1) / kGemmSplit;
+    const int64_t kc0 = min((int64_t)rank * per, nchunks), kc1 = min(kc0 + per, nchunks);
+    auto fetch = [&](int64_t kc, int buf) {
+        const int64_t k0 = kc * kGemmK;
+        // A rows k0.., columns row0..row0+63: 512 16-byte pieces, 4 per thread
 #pragma unroll
-    for (int u = 0; u < R; ++u)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[u][q] = 0.f;
-    float pa[NA];
-    float4 pc[NC];
-    auto fetch = [&](int64_t kc) {
-        const int64_t k0 = kc * 32;
-#pragma unroll
-        for (int j = 0; j < NA; ++j) {
-            const int t = threadIdx.x + 256 * j, rr = t / 32, kk = t % 32;
-            const int64_t row = row0 + rr, k = k0 + kk;
-            pa[j] = (row < nc && k < nc) ? A[row * nc + k] : 0.f;
+        for (int j = 0; j < 4; ++j) {
+            const int q = tid + 128 * j, kr = q / 16, cc = q % 16;
+            cp_async16(&sa[buf][kr][cc * 4], A + (k0 + kr) * lda + row0 + cc * 4);
         }
+        // c rows k0.., columns col0..col0+31: 256 pieces, 2 per thread
 #pragma unroll
-        for (int j = 0; j < NC; ++j) {
-            const int t = threadIdx.x + 256 * j, kk = t / CG, gg = t % CG;
-            pc[j] = (k0 + kk < nc) ? *reinterpret_cast<const float4 *>(c + (k0 + kk) * K + 4 * gg)
-                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j = 0; j < 2; ++j) {
+            const int q = tid + 128 * j, kr = q / 8, cc = q % 8;
+            cp_async16(&sc[buf][kr][cc * 4], c + (k0 + kr) * K + col0 + cc * 4);
         }
+        cp_async_commit();
     };
-    if (kc0 < kc1) fetch(kc0);
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+    if (kc0 < kc1) fetch(kc0, 0);
     for (int64_t kc = kc0; kc < kc1; ++kc) {
-#pragma unroll
-        for (int j = 0; j < NA; ++j) {
-            const int t = threadIdx.x + 256 * j;
-            sa[t / 32][t % 32] = pa[j];
-        }
-#pragma unroll
-        for (int j = 0; j < NC; ++j) {
-            const int t = threadIdx.x + 256 * j;
-            sc[t / CG][t % CG] = pc[j];
+        const int buf = (int)((kc - kc0) & 1);
+        if (kc + 1 < kc1) {
+            fetch(kc + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
         __syncthreads();
-        if (kc + 1 < kc1) fetch(kc + 1);  // in flight during the products below
 #pragma unroll 8
-        for (int kk = 0; kk < 32; ++kk) {
-            const float4 cv = sc[kk][g];
+        for (int kk = 0; kk < kGemmK; ++kk) {
+            const float4 a4 = *reinterpret_cast<const float4 *>(&sa[buf][kk][rg * 4]);
+            const float4 c4 = *reinterpret_cast<const float4 *>(&sc[buf][kk][cgp * 4]);
+            const float av[4] = {a4.x, a4.y, a4.z, a4.w}, cv[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
-            for (int u = 0; u < R; ++u) {
-                const float av = sa[rs * R + u][kk];
-                acc[u][0] = fmaf(av, cv.x, acc[u][0]);
-                acc[u][1] = fmaf(av, cv.y, acc[u][1]);
-                acc[u][2] = fmaf(av, cv.z, acc[u][2]);
-                acc[u][3] = fmaf(av, cv.w, acc[u][3]);
-            }
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], cv[j], acc[i][j]);
         }
-        __syncthreads();
+        __syncthreads();  // the buffer is refilled by the next iteration's fetch
     }
 #pragma unroll
-    for (int u = 0; u < R; ++u)
-        *reinterpret_cast<float4 *>(&part[rs * R + u][4 * g]) = make_float4(acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+    for (int i = 0; i < 4; ++i)
+        *reinterpret_cast<float4 *>(&part[rg * 4 + i][cgp * 4]) = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
     cl.sync();
-    // this CTA finishes rows [rank ROWS/kSplitK, (rank + 1) ROWS/kSplitK) of the block
-    constexpr int MY = ROWS / kSplitK;
-    double d[(MY * K + 255) / 256];
+    // this CTA finishes rows [16 rank, 16 rank + 16) of the tile: column tid % 32, rows 4 apart
+    constexpr int MY = kGemmRows / kGemmSplit;
+    const int col = tid % kGemmCols;
+    double d = 0.0;
 #pragma unroll
-    for (int j = 0; j < (MY * K + 255) / 256; ++j) {
-        d[j] = 0.0;
-        const int t = threadIdx.x + 256 * j;
-        if (t >= MY * K) continue;
-        const int lr = (int)rank * MY + t / K, col = t % K;
-        const int64_t row = row0 + lr;
+    for (int j = 0; j < MY / 4; ++j) {
+        const int lr = (int)rank * MY + tid / kGemmCols + 4 * j;
         float sum = 0.f;
-        for (unsigned q = 0; q < kSplitK; ++q) sum += cl.map_shared_rank(&part[0][0], q)[lr * K + col];
-        if (row < nc) {
-            e[row * K + col] = sum;
-            d[j] = (double)c[row * K + col] * sum;
-        }
+        for (unsigned q = 0; q < kGemmSplit; ++q) sum += cl.map_shared_rank(&part[0][0], q)[lr * kGemmCols + col];
+        const int64_t row = row0 + lr;
+        e[row * K + col0 + col] = sum;
+        if (row < nc) d += (double)c[row * K + col0 + col] * sum;
     }
     cl.sync();  // partial tiles stay alive until every CTA has read them
     if (!rz) return;
-    // column sums of c.e over this CTA's rows: threads t and t + 256 j share column t % K
-#pragma unroll
-    for (int j = 1; j < (MY * K + 255) / 256; ++j) d[0] += d[j];
-    // (MY K is a multiple of 256 for V = 1, 2, 4: every thread holds one column's partial)
-    double *sd = &sred[0][0];
-    sd[threadIdx.x] = d[0];
+    sred[tid / kGemmCols][col] = d;
     __syncthreads();
-    for (int col = threadIdx.x; col < K; col += 256) {
-        double sum = 0.0;
-        for (int t = col; t < 256; t += K) sum += sd[t];
-        atomicAdd(rz + col, sum);
-    }
+    if (tid < kGemmCols) atomicAdd(rz + col0 + tid, sred[0][tid] + sred[1][tid] + sred[2][tid] + sred[3][tid]);
 }
 
 // single FP64 vector: c[6a + m] = (P^T r)[6a + m]
@@ -818,7 +808,9 @@ bool coarse_prepare(sfc_system *s)
     const int64_t nodes = cs.nodes, nc = cs.nc;
     k_coarse_modes<<<grid_for(nodes, 256), 256, 0, ctx->stream>>>(cs.offset.p, s->mask.p, nodes, cs.dof, cs.mode.p);
     cs.a64.alloc(nc * nc);
-    cs.a32.alloc(nc * nc);
+    cs.lda = (nc + 63) / 64 * 64;
+    cs.a32.alloc(cs.lda * cs.lda);
+    SFC_CK(cudaMemsetAsync(cs.a32.p, 0, cs.lda * cs.lda * sizeof(float), ctx->stream));
     SFC_CK(cudaMemsetAsync(cs.a64.p, 0, nc * nc * sizeof(double), ctx->stream));
     {
         ProfScope pg(ctx, "coarse_galerkin", 0.0);
@@ -838,11 +830,30 @@ bool coarse_prepare(sfc_system *s)
         ProfScope pg(ctx, "coarse_inverse", 0.0);
         spd_inverse_gj(ctx, cs.a64.p, nc, 1e-10, cs.gj, nullptr, &dropped);
     }
-    k_to_f32<<<grid_for(nc * nc, 256), 256, 0, ctx->stream>>>(cs.a64.p, cs.a32.p, nc * nc);
+    k_to_f32_sym<<<grid_for(nc * nc, 256), 256, 0, ctx->stream>>>(cs.a64.p, cs.a32.p, nc, cs.lda);
     count_launch(ctx);
     cs.dropped = dropped;
     cs.op_serial = s->op_serial;
     return true;
+}
+
+// c32 / e32 for K columns: lda rows, c32's rows past nc zero (the product
+// multiplies them by A's zero padding); called outside stream capture before
+// a block solve, so inside a captured interval nothing is allocated or set
+void coarse_block_reserve(sfc_system *s, int K)
+{
+    CoarseSpace &cs = s->coarse;
+    cs.c32.reserve(cs.lda * K);
+    cs.e32.reserve(cs.lda * K);
+    // the padding rows of the [lda][K] layout (a block of another K may have
+    // written there): zeroed again whenever the allocation or K changes
+    if (cs.c32_zeroed != cs.c32.p || cs.c32_zeroed_K != K || cs.c32_zeroed_lda != cs.lda) {
+        SFC_CK(cudaMemsetAsync(cs.c32.p + cs.nc * K, 0, (size_t)(cs.lda - cs.nc) * K * sizeof(float),
+                               s->ctx->stream));
+        cs.c32_zeroed = cs.c32.p;
+        cs.c32_zeroed_K = K;
+        cs.c32_zeroed_lda = cs.lda;
+    }
 }
 
 template <int V>
@@ -851,8 +862,7 @@ void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *st
     constexpr int K = 32 * V;
     CoarseSpace &cs = s->coarse;
     sfc_ctx *ctx = s->ctx;
-    cs.c32.reserve(cs.nc * K);
-    cs.e32.reserve(cs.nc * K);
+    coarse_block_reserve(s, K);
     {
         ProfScope ps(ctx, "coarse_restrict32", (double)cs.dof * cs.nodes * K * 4 + 20.0 * cs.nodes + 4.0 * cs.nc * K);
         if (cs.dof == 3)
@@ -864,10 +874,9 @@ void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *st
         count_launch(ctx);
     }
     {
-        constexpr int ROWS = (256 / (K / 4)) * 2;
         ProfScope ps(ctx, "coarse_apply32", 4.0 * cs.nc * cs.nc + 8.0 * cs.nc * K);
-        const dim3 grid((unsigned)((cs.nc + ROWS - 1) / ROWS), kSplitK);
-        k_coarse_apply32<V><<<grid, 256, 0, ctx->stream>>>(cs.a32.p, cs.c32.p, cs.e32.p, cs.nc, rz, stop);
+        const dim3 grid((unsigned)(cs.lda / kGemmRows), K / kGemmCols, kGemmSplit);
+        k_coarse_gemm32<V><<<grid, 128, 0, ctx->stream>>>(cs.a32.p, cs.c32.p, cs.e32.p, cs.lda, cs.nc, rz, stop);
         count_launch(ctx);
     }
 }

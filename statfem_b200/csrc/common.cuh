@@ -290,9 +290,13 @@ struct CoarseSpace {
     DBuf<float4> offset;                // node offset from the centroid / box edge
     DBuf<float4> mode;                  // offset + constrained components (bits in w)
     DBuf<double> a64;                   // nc x nc: Galerkin matrix, inverted in place
-    DBuf<float> a32;                    // FP32 copy of the inverse
+    DBuf<float> a32;                    // FP32 copy of the inverse, symmetrised, lda x lda zero-padded
+    int64_t lda = 0;                    // nc rounded up to 64: row stride of a32, rows of c32 / e32
     GjScratch gj;                       // inverse scratch
-    DBuf<float> c32, e32;               // [nc][K] restriction and correction (block)
+    DBuf<float> c32, e32;               // [lda][K] restriction and correction (block; rows past nc zero in c32)
+    const float *c32_zeroed = nullptr;  // c32 allocation, K and lda whose padding rows are zero
+    int c32_zeroed_K = 0;
+    int64_t c32_zeroed_lda = 0;
     DBuf<double> c64, e64;              // single FP64 vector
 };
 
@@ -537,6 +541,7 @@ void lattice_prepare(sfc_system *s, const float *P, int K);
 void lattice_check(sfc_system *s);
 void xline_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop);
 void xline_prepare(int K);
+void coarse_block_reserve(sfc_system *s, int K);
 void flush_staged(sfc_system *s);
 void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);
 void element_matrices_unit(const sfc_mesh *m, double *ke0);

@@ -1551,10 +1551,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     auto launch_chunk_graph = [&]() -> bool {
         GraphExec &g = s->blk_graph[V == 1 ? 0 : V == 2 ? 1 : 2];
         // everything the captured launches allocate or set up, done outside the capture
-        if (two_any) {
-            s->coarse.c32.reserve(crs.nc * K);
-            s->coarse.e32.reserve(crs.nc * K);
-        }
+        if (two_any) coarse_block_reserve(s, K);
         if (lattice) lattice_prepare(s, pp, K);
         if (bsr && s->has_lattice && s->lat_mode == 2) xline_prepare(K);
         const std::vector<uintptr_t> key = {
