@@ -430,6 +430,7 @@ struct sfc_system {
     int lat_mode = 0;         // product on the lattice view: 1 staged bricks, 2 streamed x-lines
     int lat[3] = {0, 0, 0};
     sfc::DBuf<float> bq;      // nodes x 27 x 12
+    sfc::DBuf<double> bq64;   // the same in FP64 (true residuals)
     sfc::DBuf<int> lat_err;   // bounded-wait status of the staged SpMM
     CUtensorMap pmap{};       // TMA view of the block operand P as (K, 3, nx, ny, nz)
     const float *pmap_ptr = nullptr;
@@ -541,6 +542,8 @@ void lattice_prepare(sfc_system *s, const float *P, int K);
 void lattice_check(sfc_system *s);
 void xline_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, const int *stop);
 void xline_prepare(int K);
+void xline_resid64(sfc_system *s, const double *X, const double *B, double *R, int K, double *rr);
+void xresid_prepare(int K);
 void coarse_block_reserve(sfc_system *s, int K);
 void flush_staged(sfc_system *s);
 void ensure_pattern_from_mesh(sfc_system *s, const sfc_mesh *m);

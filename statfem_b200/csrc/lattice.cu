@@ -261,10 +261,11 @@ __global__ void __launch_bounds__(128 * H, 2)
     }
 }
 
-// canonical 27-slot blocks from the node-block (BSR) view; a block whose
-// column node is not a lattice neighbour sets *err
+// canonical 27-slot blocks (FP32 or FP64) from the node-block (BSR) view; a
+// block whose column node is not a lattice neighbour sets *err
+template <typename T>
 __global__ void k_lattice_fill(const int32_t *__restrict__ bptr, const int32_t *__restrict__ bcol,
-                               const float *__restrict__ b32, int64_t nodes, int nx, int ny, float *__restrict__ bq,
+                               const T *__restrict__ b32, int64_t nodes, int nx, int ny, T *__restrict__ bq,
                                int *err)
 {
     const int lane = threadIdx.x & 31;
@@ -443,6 +444,133 @@ __global__ void __launch_bounds__(256, 2)
     block_cols_add<V>(dacc, sh, pq);
 }
 
+// R = B - S X in FP64 on the lattice view (the true residual of the mixed
+// block solver's reliable updates; rr[c] += sum R^2 per column): the same
+// streamed x-line walk as k_xspmm32 over FP64 canonical blocks (12 doubles
+// per 3x3 block, rows padded to four), each run of output nodes split over H
+// warps by columns (V doubles per lane) so that the FP64 accumulators fit two
+// CTAs per SM; the blocks of output cx + 2 are copied by cp.async into the
+// warp's ring while position cx is computed.
+template <int V, int H>
+constexpr size_t xrsmem()
+{
+    return (size_t)8 * 32 * V * H * sizeof(double) + (size_t)8 * XR * NODE_FLOATS * sizeof(double);
+}
+
+template <int V, int H>
+__global__ void __launch_bounds__(256, 2)
+    k_xresid64(const double *__restrict__ bq, const double *__restrict__ X, const double *__restrict__ B,
+               double *__restrict__ R, int nx, int ny, int nz, int64_t nodes, int64_t per_run, double *rr)
+{
+    constexpr int K = 32 * V * H;
+    constexpr int64_t RS = 3 * (int64_t)K;  // doubles per node of X, B and R
+    extern __shared__ __align__(16) unsigned char xs[];
+    double *sh = reinterpret_cast<double *>(xs);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int colv = (warp % H) * 32 * V + lane * V;  // first column of this lane
+    double *ring = reinterpret_cast<double *>(xs + 8 * K * sizeof(double)) + warp * XR * NODE_FLOATS;
+    const int64_t run = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) / H;
+    double dacc[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dacc[v] = 0.0;
+    const int64_t end = min(nodes, (run + 1) * per_run);
+    const int64_t row = (int64_t)nx * RS;
+    for (int64_t a = run * per_run; a < end;) {
+        const int64_t line = a / nx;
+        const int x0 = (int)(a - line * nx);
+        const int x1 = (int)(min(end, (line + 1) * nx) - 1 - line * nx);
+        const int y = (int)(line % ny), z = (int)(line / ny);
+        int nl[9];
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy)
+                nl[dz * 3 + dy] = min(max(z + dz - 1, 0), nz - 1) * ny + min(max(y + dy - 1, 0), ny - 1);
+        const double *xb = X + colv;
+        const double *bl = bq + line * nx * NODE_FLOATS;
+        const int64_t own = line * row + colv;
+        const int c0 = max(0, x0 - 1), c1 = min(nx - 1, x1 + 1);
+        auto fetch = [&](int ox) {
+            if (ox < x0 || ox > x1) return;
+            const double2 *src = reinterpret_cast<const double2 *>(bl + (int64_t)ox * NODE_FLOATS);
+            double2 *dst = reinterpret_cast<double2 *>(ring + (ox % XR) * NODE_FLOATS);
+            for (int t = lane; t < NODE_FLOATS / 2; t += 32) cp_async16(dst + t, src + t);
+        };
+        auto store = [&](int ox, const double (&acc)[3][V]) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int64_t off = own + (int64_t)ox * RS + r * K;
+                double bv[V];
+                ldv64<V>(B + off, bv);
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    const double rv = bv[v] - acc[r][v];
+                    R[off + v] = rv;
+                    dacc[v] += rv * rv;
+                }
+            }
+        };
+        __syncwarp();
+        for (int ox = x0; ox <= c0 + 1; ++ox) fetch(ox);
+        cp_async_commit();
+        double acc[3][3][V];
+#pragma unroll
+        for (int o = 0; o < 3; ++o)
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[o][r][v] = 0.0;
+        for (int cx = c0; cx <= c1; ++cx) {
+            cp_async_wait_all();
+            __syncwarp();
+            fetch(cx + 2);
+            cp_async_commit();
+#pragma unroll
+            for (int l = 0; l < 9; ++l) {
+                const double *xj = xb + ((int64_t)nl[l] * nx + cx) * RS;
+                double p[3][V];
+                ldv64<V>(xj, p[0]);
+                ldv64<V>(xj + K, p[1]);
+                ldv64<V>(xj + 2 * K, p[2]);
+#pragma unroll
+                for (int o = 0; o < 3; ++o) {
+                    const int slot = (cx - 1 + o + XR) % XR;
+                    const double *bp = ring + slot * NODE_FLOATS + (l * 3 + 2 - o) * SLOT;
+#pragma unroll
+                    for (int r = 0; r < 3; ++r) {
+                        const double2 m01 = *reinterpret_cast<const double2 *>(bp + 4 * r);
+                        const double m2 = bp[4 * r + 2];
+#pragma unroll
+                        for (int v = 0; v < V; ++v)
+                            acc[o][r][v] = fma(m2, p[2][v], fma(m01.y, p[1][v], fma(m01.x, p[0][v], acc[o][r][v])));
+                    }
+                }
+            }
+            if (cx - 1 >= x0) store(cx - 1, acc[0]);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    acc[0][r][v] = acc[1][r][v];
+                    acc[1][r][v] = acc[2][r][v];
+                    acc[2][r][v] = 0.0;
+                }
+        }
+        if (c1 == x1) store(x1, acc[0]);
+        a = line * nx + x1 + 1;
+    }
+    cp_async_wait_all();
+    // the 8 / H runs' partials of column c sit at sh[run][c]
+#pragma unroll
+    for (int v = 0; v < V; ++v) sh[(warp / H) * K + colv + v] = dacc[v];
+    __syncthreads();
+    for (int c = threadIdx.x; c < K; c += blockDim.x) {
+        double sum = 0;
+        for (int j = 0; j < 8 / H; ++j) sum += sh[j * K + c];
+        atomicAdd(rr + c, sum);
+    }
+}
+
 int g_occ = 0;     // resident CTAs per SM of the k_lspmm32 instantiation in use
 int g_groups = 0;  // column groups per x-line: 2 (8 warps per CTA) or 1 (SFC_LATTICE_WARPS=4)
 
@@ -488,9 +616,14 @@ void build_lattice_blocks(sfc_system *s)
     SFC_CK(cudaMemsetAsync(s->bq.p, 0, (size_t)s->nodes * NODE_FLOATS * 4, ctx->stream));
     DevInt err = status_word(ctx);
     SFC_CK(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
-    k_lattice_fill<<<grid_for(s->nodes * 32, 256), 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval32.p, s->nodes,
-                                                                       nx, ny, s->bq.p, err.p);
-    count_launch(ctx);
+    k_lattice_fill<float><<<grid_for(s->nodes * 32, 256), 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval32.p,
+                                                                              s->nodes, nx, ny, s->bq.p, err.p);
+    // the FP64 view for the true residual (k_xresid64)
+    s->bq64.alloc((size_t)s->nodes * NODE_FLOATS);
+    SFC_CK(cudaMemsetAsync(s->bq64.p, 0, (size_t)s->nodes * NODE_FLOATS * 8, ctx->stream));
+    k_lattice_fill<double><<<grid_for(s->nodes * 32, 256), 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval64.p,
+                                                                               s->nodes, nx, ny, s->bq64.p, err.p);
+    count_launch(ctx, 2);
     int h = 0;
     download(ctx, &h, err.p, 1);
     if (h) return;
@@ -595,6 +728,48 @@ void xline_spmm32(sfc_system *s, const float *P, float *Q, int K, double *pq, co
     if (K == 32) xline_launch<1>(s, P, Q, pq, stop);
     else if (K == 64) xline_launch<2>(s, P, Q, pq, stop);
     else xline_launch<4>(s, P, Q, pq, stop);
+}
+
+// the FP64 residual on the lattice view (k_xresid64): K = 128 as two
+// 64-column warps per run, K = 64 and 32 as one warp
+template <int V, int H>
+int xresid_occ()
+{
+    static int occ = 0;
+    if (!occ) {
+        SFC_CK(cudaFuncSetAttribute(k_xresid64<V, H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)xrsmem<V, H>()));
+        SFC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_xresid64<V, H>, 256, xrsmem<V, H>()));
+        if (occ < 1) occ = 1;
+    }
+    return occ;
+}
+
+template <int V, int H>
+void xresid_launch(sfc_system *s, const double *X, const double *B, double *R, double *rr)
+{
+    sfc_ctx *ctx = s->ctx;
+    const int64_t runs = (int64_t)xresid_occ<V, H>() * ctx->sm_count * (8 / H);
+    const int64_t per_run = (s->nodes + runs - 1) / runs;
+    const unsigned grid = (unsigned)((s->nodes + per_run * (8 / H) - 1) / (per_run * (8 / H)));
+    k_xresid64<V, H><<<grid, 256, xrsmem<V, H>(), ctx->stream>>>(s->bq64.p, X, B, R, s->lat[0], s->lat[1], s->lat[2],
+                                                                   s->nodes, per_run, rr);
+    count_launch(ctx);
+}
+
+void xresid_prepare(int K)
+{
+    if (K == 32) xresid_occ<1, 1>();
+    else if (K == 64) xresid_occ<2, 1>();
+    else if (K == 128) xresid_occ<2, 2>();
+}
+
+void xline_resid64(sfc_system *s, const double *X, const double *B, double *R, int K, double *rr)
+{
+    SFC_REQUIRE(K == 32 || K == 64 || K == 128, "lattice residual needs 32, 64 or 128 columns");
+    if (K == 32) xresid_launch<1, 1>(s, X, B, R, rr);
+    else if (K == 64) xresid_launch<2, 1>(s, X, B, R, rr);
+    else xresid_launch<2, 2>(s, X, B, R, rr);
 }
 
 // after a solve: a staged SpMM whose bounded wait gave up fails the solve

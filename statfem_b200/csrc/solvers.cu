@@ -1443,10 +1443,18 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     const bool two1 = two_any && crs.dof == 1;  // point Jacobi + constant modes (scalar mesh)
     const bool bj = bsr && (o.precond == SFC_PRECOND_BLOCK_JACOBI || two) && s->bdinv32.p;
     // R = B - S X (FP64) and Q = S P (FP32), node-block kernels for 3-dof meshes
+    // the true residual on the lattice view unless SFC_RESID=bsr
+    const char *renv = std::getenv("SFC_RESID");
+    const bool xresid_off = renv && std::string(renv) == "bsr";
+    if (bsr && s->has_lattice && s->bq64.p && !xresid_off) xresid_prepare(K);
     auto resid = [&](const double *X, const double *Bm, double *R, double *out) {
         ProfScope ps(ctx, "resid64",
                      bsr ? (double)s->nblocks * 76 + 4.0 * (s->nodes + 1) + 3.0 * N * K * 8
                          : (double)s->nnz * 12 + 4.0 * (N + 1) + 3.0 * N * K * 8);
+        if (bsr && s->has_lattice && s->bq64.p && !xresid_off) {
+            xline_resid64(s, X, Bm, R, K, out);
+            return;
+        }
         if (bsr)
             k_bresid64<V><<<gw, 256, 0, ctx->stream>>>(s->bptr.p, s->bcol.p, s->bval64.p, X, Bm, R, s->nodes, out);
         else
@@ -1559,7 +1567,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             (uintptr_t)(bsr | (bj << 1) | (two << 2) | (two1 << 3) | (lattice << 4)), (uintptr_t)s->scal.p,
             (uintptr_t)s->blk32.p, (uintptr_t)s->colsc.p, (uintptr_t)s->flags.p, (uintptr_t)s->bdinv32.p,
             (uintptr_t)s->dinv32.p, (uintptr_t)s->bptr.p, (uintptr_t)s->bcol.p, (uintptr_t)s->bval32.p,
-            (uintptr_t)s->row_ptr.p, (uintptr_t)s->col.p, (uintptr_t)s->a_op32.p, (uintptr_t)s->bq.p,
+            (uintptr_t)s->row_ptr.p, (uintptr_t)s->col.p, (uintptr_t)s->a_op32.p, (uintptr_t)s->bq.p, (uintptr_t)s->bq64.p,
             (uintptr_t)s->lat_err.p, (uintptr_t)s->lat_mode, (uintptr_t)s->lat[0], (uintptr_t)s->lat[1], (uintptr_t)s->lat[2],
             (uintptr_t)s->pmap_ptr, (uintptr_t)crs.agg_ptr.p, (uintptr_t)crs.agg_nodes.p, (uintptr_t)crs.mode.p,
             (uintptr_t)crs.c32.p, (uintptr_t)crs.e32.p, (uintptr_t)crs.a32.p, (uintptr_t)crs.node_agg.p,
