@@ -267,11 +267,13 @@ __global__ void k_to_f32_sym(const double *__restrict__ a, float *__restrict__ b
 
 // c[6a + m][col] = (P^T r)[6a + m][col] for K = 32 V interleaved columns: a
 // cluster of kRestrictSplit CTAs per aggregate (warp per node), partial sums
-// added in rank order through distributed shared memory
-constexpr int kRestrictSplit = 4;
+// added in rank order through distributed shared memory.  Two CTAs per
+// aggregate keep the c2 grid (216 aggregates) within one wave of resident
+// CTAs; four left a half-empty second wave (51 against 50 us per launch).
+constexpr int kRestrictSplit = 2;
 
 template <int V>
-__global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
+__global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256, 4)
     k_coarse_restrict32(const float *__restrict__ r, const int32_t *__restrict__ agg_ptr,
                         const int32_t *__restrict__ agg_nodes, const float4 *__restrict__ mode, float *__restrict__ c,
                         const int *stop)
@@ -288,10 +290,9 @@ __global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
     for (int m = 0; m < 6; ++m)
 #pragma unroll
         for (int v = 0; v < V; ++v) acc[m][v] = 0.f;
-    // two nodes per trip: six row loads in flight per warp
-    auto load_node = [&](int32_t t, float4 &m, float (&rv)[3][V]) {
-        const int32_t i = agg_nodes[t];
-        m = mode[i];
+    // two nodes per trip: six row loads in flight per warp; the nodes' ids
+    // and modes are fetched one per lane ahead of the trips and broadcast
+    auto load_node = [&](int32_t i, const float4 &m, float (&rv)[3][V]) {
         const int bits = (int)m.w;
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -322,20 +323,37 @@ __global__ void __cluster_dims__(kRestrictSplit, 1, 1) __launch_bounds__(256)
         }
     };
     const int32_t step = 8 * kRestrictSplit, end = agg_ptr[a + 1];
-    int32_t t = agg_ptr[a] + (int32_t)rank * 8 + w;
-    for (; t + step < end; t += 2 * step) {
-        float4 m0, m1;
-        float r0[3][V], r1[3][V];
-        load_node(t, m0, r0);
-        load_node(t + step, m1, r1);
-        add_node(m0, r0);
-        add_node(m1, r1);
-    }
-    if (t < end) {
-        float4 m0;
-        float r0[3][V];
-        load_node(t, m0, r0);
-        add_node(m0, r0);
+    const int32_t first = agg_ptr[a] + (int32_t)rank * 8 + w;  // this warp's nodes: first + k step
+    const int mine = first < end ? (end - 1 - first) / step + 1 : 0;
+    auto bcast = [&](const float4 &m, int k) {
+        return make_float4(__shfl_sync(0xffffffffu, m.x, k), __shfl_sync(0xffffffffu, m.y, k),
+                           __shfl_sync(0xffffffffu, m.z, k), __shfl_sync(0xffffffffu, m.w, k));
+    };
+    for (int base = 0; base < mine; base += 32) {
+        int32_t li = 0;
+        float4 lm = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (base + lane < mine) {
+            li = agg_nodes[first + (base + lane) * step];
+            lm = mode[li];
+        }
+        const int cnt = min(32, mine - base);
+        int k = 0;
+        for (; k + 1 < cnt; k += 2) {
+            const int32_t i0 = __shfl_sync(0xffffffffu, li, k), i1 = __shfl_sync(0xffffffffu, li, k + 1);
+            const float4 m0 = bcast(lm, k), m1 = bcast(lm, k + 1);
+            float r0[3][V], r1[3][V];
+            load_node(i0, m0, r0);
+            load_node(i1, m1, r1);
+            add_node(m0, r0);
+            add_node(m1, r1);
+        }
+        if (k < cnt) {
+            const int32_t i0 = __shfl_sync(0xffffffffu, li, k);
+            const float4 m0 = bcast(lm, k);
+            float r0[3][V];
+            load_node(i0, m0, r0);
+            add_node(m0, r0);
+        }
     }
 #pragma unroll
     for (int m = 0; m < 6; ++m)
