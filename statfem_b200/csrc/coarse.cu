@@ -269,7 +269,7 @@ __global__ void k_to_f32_sym(const double *__restrict__ a, float *__restrict__ b
 // cluster of kRestrictSplit CTAs per aggregate (warp per node), partial sums
 // added in rank order through distributed shared memory.  Two CTAs per
 // aggregate keep the c2 grid (216 aggregates) within one wave of resident
-// CTAs; four left a half-empty second wave (51 against 50 us per launch).
+// CTAs; four left a half-empty second wave (52 against 50 us per launch).
 constexpr int kRestrictSplit = 2;
 
 template <int V>
