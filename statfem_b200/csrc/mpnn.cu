@@ -11,10 +11,13 @@
 //   M(r) = s D^-1/2 (x0 + y) = D^-1 r + s D^-1/2 y    Jacobi + learned correction
 // (y = 0 on constrained dofs, whose rows of S are diagonal: Jacobi is exact).
 // The RMS normalisation keeps the node features O(1) whatever the mesh size.
-// The aggregation Ahat H is a 64-column SpMM on the operator's pattern; the
-// dense transforms run on BF16 tensor-core fragments (mma.sync m16n8k16,
-// FP32 accumulate) with the inputs rounded to BF16 on the fly; activations,
-// master weights, gradients and Adam state are FP32.
+// The aggregation Ahat H is a 64-column SpMM on the operator's pattern.  In
+// inference (the flexible-CG application) the dense transforms run on the
+// 5th-generation tensor cores (tcgen05.mma, BF16 x BF16 -> FP32 in tensor
+// memory, k_layer_tc; SFC_MPNN_TC=0 selects the mma.sync form k_layer_inf);
+// the training kernels use BF16 mma.sync fragments (m16n8k16, FP32
+// accumulate) with the inputs rounded to BF16 on the fly.  Activations in
+// training, master weights, gradients and Adam state are FP32.
 //
 // Training pair (r, e) with S e = r: target t = D^1/2 e / s, d = x0 + y - t,
 // loss L = d^T Ahat d / N (the S-norm of the error of M(r) scaled by 1/(N s^2)).
@@ -25,6 +28,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <new>
@@ -59,6 +63,7 @@ struct sfc_mpnn {
     // activations and gradients
     sfc::DBuf<float> x0, ax0, yhat, tgt, dvec, qvec, H[LAYERS + 1], Y[LAYERS + 1], dH0, dH1, dY;
     sfc::DBuf<__nv_bfloat16> hb[2];  // inference activations (BF16, ping-pong)
+    sfc::DBuf<int> tc_err;           // bounded-wait status of the tensor-core layers
     sfc::DBuf<double> fcg_sc;        // flexible-CG scalars, per iteration
     sfc::DBuf<int> fcg_flags;        // done, breakdown
     sfc::DBuf<double> scal;  // [0]: N s^2 = |D^-1/2 r|^2, [1]: loss
@@ -655,6 +660,231 @@ __global__ void __launch_bounds__(128) k_layer_inf(const int32_t *__restrict__ r
     }
 }
 
+// ---- inference on the 5th-generation tensor cores (tcgen05) ---------------------
+// A CTA of eight warps takes 128 nodes at a time: the warps gather the tile's
+// [Hin | Ahat Hin] rows (BF16, K = 128) into shared memory in the canonical
+// K-major layout without swizzle (8-row x 16-byte core matrices: core (row
+// group g, K chunk c) at byte (16 g + c) * 128, so the next K chunk is 128
+// bytes on (LBO) and the next 8-row group 2,048 bytes on (SBO)); W (64 x 128,
+// K-major) sits beside it in the same layout for the whole kernel.  One thread
+// issues eight tcgen05.mma (M = 128, N = 64, K = 16, BF16 x BF16 -> FP32)
+// into a 64-column accumulator in tensor memory and commits them to an
+// mbarrier; warps w and w + 4 then read the 32 rows of TMEM lanes 32 (w % 4)
+// .. with tcgen05.ld, columns 0-31 and 32-63 respectively, add the bias, apply
+// relu and store BF16 rows (or, DECODE, the decoded correction z).  The mbarrier wait is bounded: on a timeout the
+// kernel sets *err, waits once more (bounded) for the MMAs in flight, frees
+// its tensor memory and leaves.
+constexpr int kTcRows = 128;           // nodes per tile (MMA M)
+constexpr uint32_t kTcCols = 64;       // accumulator columns (MMA N), tensor-memory columns allocated
+constexpr int kTcBBytes = H * 2 * H * 2;      // W: 16 KiB
+constexpr int kTcABytes = kTcRows * 2 * H * 2;  // A tile: 32 KiB
+constexpr size_t kTcSmem = (size_t)kTcABytes + kTcBBytes + 16;  // + mbarrier + tensor-memory address
+constexpr uint32_t kTcWaitTries = 1u << 22;
+// instruction descriptor: FP32 accumulator (bits 4-5 = 1), A and B BF16 (bits
+// 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kTcCols >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+
+__device__ __forceinline__ uint32_t tc_off(int row, int chunk)
+{
+    return (uint32_t)(((row >> 3) * 16 + chunk) * 128 + (row & 7) * 16);
+}
+
+// shared-memory matrix descriptor: start address, LBO = 128 B, SBO = 2,048 B
+// (all in 16-byte units), descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(2048u >> 4) << 32) |
+           (1ull << 46);
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < kTcWaitTries; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t u[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7]),
+          "=r"(u[8]), "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]), "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(u[j]);
+}
+
+template <bool DECODE>
+__global__ void __launch_bounds__(256, 4) k_layer_tc(const int32_t *__restrict__ rp, const int32_t *__restrict__ col,
+                                                     const float *__restrict__ v, const uint32_t *__restrict__ Hin,
+                                                     const __nv_bfloat16 *__restrict__ W,
+                                                     const float *__restrict__ bias, int64_t N,
+                                                     uint32_t *__restrict__ Hout, const float *__restrict__ P,
+                                                     const float *__restrict__ x0, const float *__restrict__ sdinv,
+                                                     const unsigned char *__restrict__ mask, const double *scal,
+                                                     double *__restrict__ z, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    unsigned char *sA = tsm, *sB = tsm + kTcABytes;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(tsm + kTcABytes + kTcBBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(tsm + kTcABytes + kTcBBytes + 8);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA), sB_u = (uint32_t)__cvta_generic_to_shared(sB);
+    const uint32_t bar_u = (uint32_t)__cvta_generic_to_shared(bar);
+    // W (row n = output feature, 16 chunks of 8 K values) into the canonical layout
+    const uint4 *W4 = reinterpret_cast<const uint4 *>(W);
+    for (int t = threadIdx.x; t < H * 16; t += blockDim.x)
+        *reinterpret_cast<uint4 *>(sB + tc_off(t / 16, t % 16)) = W4[t];
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(tslot)),
+                     "r"(kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_u) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // W visible to the tensor cores
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __shared__ float ypart[kTcRows];  // DECODE: the upper 32 columns' share of each row's w . H
+    const uint32_t tmem = *tslot;
+    // warps w and w + 4 share TMEM lanes 32 (w % 4) ..: w < 4 reads columns 0-31, w >= 4 columns 32-63
+    const int quad = warp & 3, half = warp >> 2;
+    const uint32_t trow = tmem + ((uint32_t)(32 * quad) << 16) + 32u * half;
+    const int64_t tiles = (N + kTcRows - 1) / kTcRows;
+    const uint4 *Hin4 = reinterpret_cast<const uint4 *>(Hin);
+    const int sub = lane >> 3, fl = lane & 7;
+    uint32_t parity = 0;
+    bool ok = !(*err), pending = false;  // pending: MMAs committed and not yet waited for
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        // gather: warp w fills rows 16 w .. 16 w + 15, four rows per pass, 8 lanes per row
+        for (int pass = 0; pass < 4; ++pass) {
+            const int rr = 16 * warp + pass * 4 + sub;
+            const int64_t i = tile * kTcRows + rr;
+            const bool valid = i < N;
+            const int32_t b = valid ? rp[i] : 0;
+            const int len = valid ? rp[i + 1] - b : 0;
+            int maxlen = len;
+            maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, 8));
+            maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, 16));
+            float acc[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) acc[q] = 0.f;
+            for (int s0 = 0; s0 < maxlen; s0 += 8) {
+                const int sl = s0 + fl;
+                const int32_t cv = sl < len ? col[b + sl] : 0;  // padding: row 0 with weight 0
+                const float av = sl < len ? v[b + sl] : 0.f;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int32_t cj = __shfl_sync(0xffffffffu, cv, j, 8);
+                    const float aj = __shfl_sync(0xffffffffu, av, j, 8);
+                    const uint4 u = Hin4[(int64_t)cj * 8 + fl];
+                    const float2 f0 = bf16x2_to_f2(u.x), f1 = bf16x2_to_f2(u.y), f2 = bf16x2_to_f2(u.z),
+                                 f3 = bf16x2_to_f2(u.w);
+                    acc[0] = fmaf(aj, f0.x, acc[0]);
+                    acc[1] = fmaf(aj, f0.y, acc[1]);
+                    acc[2] = fmaf(aj, f1.x, acc[2]);
+                    acc[3] = fmaf(aj, f1.y, acc[3]);
+                    acc[4] = fmaf(aj, f2.x, acc[4]);
+                    acc[5] = fmaf(aj, f2.y, acc[5]);
+                    acc[6] = fmaf(aj, f3.x, acc[6]);
+                    acc[7] = fmaf(aj, f3.y, acc[7]);
+                }
+            }
+            const uint4 hv = valid ? Hin4[i * 8 + fl] : make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4 *>(sA + tc_off(rr, fl)) = hv;
+            *reinterpret_cast<uint4 *>(sA + tc_off(rr, 8 + fl)) =
+                make_uint4(pack_bf16(acc[0], acc[1]), pack_bf16(acc[2], acc[3]), pack_bf16(acc[4], acc[5]),
+                           pack_bf16(acc[6], acc[7]));
+        }
+        // the tile is visible to the tensor cores, and every warp has read the
+        // previous tile's accumulator
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) {
+                const uint64_t da = tc_desc(sA_u + 256u * ks), db = tc_desc(sB_u + 256u * ks);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(kTcIdesc), "r"(ks), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_u)
+                         : "memory");
+        }
+        pending = true;
+        ok = __syncthreads_and(tc_wait(bar_u, parity));
+        if (!ok) break;
+        pending = false;
+        parity ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int64_t i = tile * kTcRows + 32 * quad + lane;  // this thread's row
+        const int c0 = 32 * half;                              // and its first column
+        float y = 0.f;
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            float d[16];
+            tc_ld16(trow + 16u * part, d);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int cb = c0 + 16 * part;
+            if constexpr (!DECODE) {
+                uint32_t w[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    w[j] = pack_bf16(fmaxf(d[2 * j] + bias[cb + 2 * j], 0.f),
+                                     fmaxf(d[2 * j + 1] + bias[cb + 2 * j + 1], 0.f));
+                if (i < N) {
+                    uint4 *dst = reinterpret_cast<uint4 *>(Hout + i * (H / 2) + cb / 2);
+                    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) y = fmaf(P[OFF_DW + cb + j], fmaxf(d[j] + bias[cb + j], 0.f), y);
+            }
+        }
+        if constexpr (DECODE) {
+            if (half) ypart[32 * quad + lane] = y;
+            __syncthreads();
+            if (!half && i < N) {
+                y += ypart[32 * quad + lane];
+                const double sc = sqrt(scal[0] / (double)N);
+                z[i] = sc * (double)sdinv[i] * (double)(mask[i] ? x0[i] : x0[i] + y + P[OFF_DB]);
+            }
+        }
+    }
+    if (!ok && pending) {
+        // a wait gave up: record it and let the MMAs in flight finish (bounded)
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        tc_wait(bar_u, parity);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
+}
+
 // ---- host side -------------------------------------------------------------------
 void refresh_bf16(sfc_mpnn *m)
 {
@@ -787,6 +1017,30 @@ double loss_grad(sfc_mpnn *m, const double *r, const double *e, double w)
     return hl;
 }
 
+// the tensor-core (tcgen05) layers unless SFC_MPNN_TC=0 selects the mma.sync ones
+bool use_tc()
+{
+    static int m = -1;
+    if (m < 0) {
+        const char *e = std::getenv("SFC_MPNN_TC");
+        m = (e && e[0] == '0') ? 0 : 1;
+    }
+    return m == 1;
+}
+
+// after a batch of applications: a tensor-core layer whose bounded wait gave
+// up fails the call
+void check_tc(sfc_mpnn *m)
+{
+    if (!m->tc_err.p) return;
+    int h = 0;
+    download(m->ctx, &h, m->tc_err.p, 1);
+    if (h) {
+        SFC_CK(cudaMemsetAsync(m->tc_err.p, 0, sizeof(int), m->ctx->stream));
+        fail(SFC_ERR_TIMEOUT, "learned preconditioner: a bounded wait for the tensor-core products gave up");
+    }
+}
+
 // z = M(r) (device FP64 vectors): the inference kernels, no host synchronisation
 void apply(sfc_mpnn *m, const double *r, double *z)
 {
@@ -800,6 +1054,43 @@ void apply(sfc_mpnn *m, const double *r, double *z)
     k_encoder_inf<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->ax0.p, m->scal.p,
                                                        m->params.p, N, m->x0.p, reinterpret_cast<uint4 *>(m->hb[0].p));
     count_launch(ctx, 2);
+    if (use_tc()) {
+        if (!m->tc_err.p) {
+            m->tc_err.alloc(1);
+            SFC_CK(cudaMemsetAsync(m->tc_err.p, 0, sizeof(int), ctx->stream));
+        }
+        static int occ = 0;
+        if (!occ) {
+            // all of the unified L1 / shared memory as shared memory, so that
+            // four 48 KiB CTAs fit per SM
+            for (const void *f : {(const void *)k_layer_tc<false>, (const void *)k_layer_tc<true>}) {
+                SFC_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+                SFC_CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            }
+            // four CTAs per SM by their resources (4 x 49 KiB of shared memory,
+            // 4 x 256 threads x 64 registers, 4 x 64 tensor-memory columns); the
+            // runtime's occupancy query answers 1 for this kernel, and the
+            // grid-stride loop is correct for any number of resident CTAs
+            occ = 4;
+        }
+        const unsigned gt = (unsigned)std::min<int64_t>((N + kTcRows - 1) / kTcRows, (int64_t)ctx->sm_count * occ);
+        for (int l = 0; l < LAYERS; ++l) {
+            const uint32_t *hin = reinterpret_cast<const uint32_t *>(m->hb[l & 1].p);
+            uint32_t *hout = reinterpret_cast<uint32_t *>(m->hb[(l + 1) & 1].p);
+            const __nv_bfloat16 *W = m->wbf.p + l * H * 2 * H;
+            const float *b = m->params.p + OFF_L + l * LSZ + H * 2 * H;
+            if (l + 1 < LAYERS)
+                k_layer_tc<false><<<gt, 256, kTcSmem, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, hin, W, b, N,
+                                                                     hout, m->params.p, m->x0.p, m->sdinv.p,
+                                                                     s->mask.p, m->scal.p, nullptr, m->tc_err.p);
+            else
+                k_layer_tc<true><<<gt, 256, kTcSmem, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, hin, W, b, N,
+                                                                    nullptr, m->params.p, m->x0.p, m->sdinv.p,
+                                                                    s->mask.p, m->scal.p, z, m->tc_err.p);
+            count_launch(ctx);
+        }
+        return;
+    }
     const unsigned g = (unsigned)std::min<int64_t>((N + 63) / 64, (int64_t)ctx->sm_count * 12);
     for (int l = 0; l < LAYERS; ++l) {
         const uint32_t *hin = reinterpret_cast<const uint32_t *>(m->hb[l & 1].p);
@@ -1094,6 +1385,7 @@ void solve_forward_fcg(sfc_system *s)
     SFC_CK(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    check_tc(m);
     s->stats = {};
     s->stats.iterations = iters;
     s->stats.num_rhs = 1;
@@ -1255,6 +1547,7 @@ int32_t sfc_mpnn_apply(sfc_mpnn_t *m, sfc_system_t *s, const double *r, double *
         dz.alloc(s->N);
         apply(m, dr.p, dz.p);
         download(m->ctx, z, dz.p, s->N);
+        check_tc(m);
     });
 }
 
