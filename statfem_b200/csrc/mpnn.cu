@@ -11,13 +11,14 @@
 //   M(r) = s D^-1/2 (x0 + y) = D^-1 r + s D^-1/2 y    Jacobi + learned correction
 // (y = 0 on constrained dofs, whose rows of S are diagonal: Jacobi is exact).
 // The RMS normalisation keeps the node features O(1) whatever the mesh size.
-// The aggregation Ahat H is a 64-column SpMM on the operator's pattern.  In
-// inference (the flexible-CG application) the dense transforms run on the
-// 5th-generation tensor cores (tcgen05.mma, BF16 x BF16 -> FP32 in tensor
-// memory, k_layer_tc; SFC_MPNN_TC=0 selects the mma.sync form k_layer_inf);
-// the training kernels use BF16 mma.sync fragments (m16n8k16, FP32
-// accumulate) with the inputs rounded to BF16 on the fly.  Activations in
-// training, master weights, gradients and Adam state are FP32.
+// The aggregation Ahat H is a 64-column SpMM on the operator's pattern.  The
+// dense transforms run on the 5th-generation tensor cores (tcgen05.mma,
+// BF16 x BF16 -> FP32 in tensor memory): k_layer_tc in inference (gather
+// fused), k_dense_fwd_tc and k_dense_bwd_x_tc in training, with the inputs
+// rounded to BF16 on the fly; SFC_MPNN_TC=0 selects the earlier mma.sync
+// forms (k_layer_inf, k_dense_fwd, k_dense_bwd_x) for comparison.  The
+// weight gradient (k_dense_bwd_w) is an FP32 reduction over the nodes.
+// Activations in training, master weights, gradients and Adam state are FP32.
 //
 // Training pair (r, e) with S e = r: target t = D^1/2 e / s, d = x0 + y - t,
 // loss L = d^T Ahat d / N (the S-norm of the error of M(r) scaled by 1/(N s^2)).
@@ -683,18 +684,31 @@ constexpr uint32_t kTcWaitTries = 1u << 22;
 // instruction descriptor: FP32 accumulator (bits 4-5 = 1), A and B BF16 (bits
 // 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((kTcCols >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+static_assert(kTcIdesc == (1u << 4) + (1u << 7) + (1u << 10) + (8u << 17) + (8u << 24), "M = 128, N = 64");
 
+// byte offset of the 16-byte piece (row, K chunk) of a K-major operand with KC
+// chunks of 8 BF16 per row in the canonical layout (core matrix = 8 rows of
+// one chunk, 128 bytes; next chunk +128 B; next 8-row group + 128 KC B)
+template <int KC = 16>
 __device__ __forceinline__ uint32_t tc_off(int row, int chunk)
 {
-    return (uint32_t)(((row >> 3) * 16 + chunk) * 128 + (row & 7) * 16);
+    return (uint32_t)(((row >> 3) * KC + chunk) * 128 + (row & 7) * 16);
 }
 
-// shared-memory matrix descriptor: start address, LBO = 128 B, SBO = 2,048 B
-// (all in 16-byte units), descriptor version 1, no swizzle
+// shared-memory matrix descriptor: start address, LBO = 128 B (next K chunk),
+// SBO = 128 KC B (next 8-row group), all in 16-byte units; descriptor version
+// 1, no swizzle
+template <int KC = 16>
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr)
 {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(2048u >> 4) << 32) |
-           (1ull << 46);
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+           ((uint64_t)((128u * KC) >> 4) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of a BF16 x BF16 -> FP32 MMA, both operands K-major
+constexpr uint32_t tc_idesc(uint32_t M, uint32_t N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }
 
 __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity)
@@ -885,7 +899,266 @@ __global__ void __launch_bounds__(256, 4) k_layer_tc(const int32_t *__restrict__
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
 }
 
+// ---- training products on tcgen05 --------------------------------------------------
+// Shared steps of the tensor-core kernels below: warp 0 allocates NCOLS
+// tensor-memory columns and thread 0 initialises the mbarrier; tc_product
+// makes the staged operands visible to the tensor cores, lets thread 0 issue
+// the KS K-steps (16 each) and commit them, and waits for them (bounded);
+// tc_finish frees the tensor memory after a last bounded wait when a product
+// is still in flight.
+template <uint32_t NCOLS>
+__device__ __forceinline__ uint32_t tc_setup(uint32_t *tslot, uint32_t bar_u)
+{
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(tslot)),
+                     "r"(NCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_u) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return *tslot;
+}
+
+template <int KCA, int KCB, int KS, uint32_t IDESC>
+__device__ __forceinline__ bool tc_product(uint32_t sA_u, uint32_t sB_u, uint32_t tmem, uint32_t bar_u,
+                                           uint32_t parity)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+            const uint64_t da = tc_desc<KCA>(sA_u + 256u * ks), db = tc_desc<KCB>(sB_u + 256u * ks);
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                :
+                : "r"(tmem), "l"(da), "l"(db), "r"(IDESC), "r"(ks), "r"(0u)
+                : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_u)
+                     : "memory");
+    }
+    const bool ok = __syncthreads_and(tc_wait(bar_u, parity));
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return ok;
+}
+
+template <uint32_t NCOLS>
+__device__ __forceinline__ void tc_finish(uint32_t tmem, uint32_t bar_u, uint32_t parity, bool ok, bool pending,
+                                          int *err)
+{
+    if (!ok && pending) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        tc_wait(bar_u, parity);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS));
+}
+
+// Hout = relu([Hin | Yin] W^T + b) on tcgen05: 128 nodes per tile, the FP32
+// inputs rounded to BF16 into the canonical K-major layout (K = 128), W
+// (64 x 128) staged once; M = 128, N = 64, eight K-steps into 64 TMEM columns.
+// Eight warps; warps w and w + 4 read back TMEM lanes 32 (w % 4) .., columns
+// 0-31 and 32-63.
+constexpr size_t kTcFwdSmem = (size_t)kTcABytes + kTcBBytes + 16;
+
+__global__ void __launch_bounds__(256, 4) k_dense_fwd_tc(const float *__restrict__ Hin, const float *__restrict__ Yin,
+                                                         const __nv_bfloat16 *__restrict__ W,
+                                                         const float *__restrict__ bias, int64_t N,
+                                                         float *__restrict__ Hout, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    unsigned char *sA = tsm, *sB = tsm + kTcABytes;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(tsm + kTcABytes + kTcBBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(tsm + kTcABytes + kTcBBytes + 8);
+    const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA), sB_u = (uint32_t)__cvta_generic_to_shared(sB);
+    const uint32_t bar_u = (uint32_t)__cvta_generic_to_shared(bar);
+    const uint4 *W4 = reinterpret_cast<const uint4 *>(W);
+    for (int t = threadIdx.x; t < H * 16; t += blockDim.x) *reinterpret_cast<uint4 *>(sB + tc_off(t / 16, t % 16)) = W4[t];
+    const uint32_t tmem = tc_setup<64>(tslot, bar_u);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quad = warp & 3, half = warp >> 2;
+    const uint32_t trow = tmem + ((uint32_t)(32 * quad) << 16) + 32u * half;
+    const int64_t tiles = (N + kTcRows - 1) / kTcRows;
+    uint32_t parity = 0;
+    bool ok = !(*err), pending = false;
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        // 128 rows x 16 pieces of 8 inputs: 8 pieces per thread
+        for (int t = threadIdx.x; t < kTcRows * 16; t += blockDim.x) {
+            const int rr = t >> 4, c = t & 15;
+            const int64_t i = tile * kTcRows + rr;
+            uint4 u = make_uint4(0, 0, 0, 0);
+            if (i < N) {
+                const float4 *src = reinterpret_cast<const float4 *>((c < 8 ? Hin : Yin) + i * H + (c & 7) * 8);
+                const float4 a = src[0], b = src[1];
+                u = make_uint4(pack_bf16(a.x, a.y), pack_bf16(a.z, a.w), pack_bf16(b.x, b.y), pack_bf16(b.z, b.w));
+            }
+            *reinterpret_cast<uint4 *>(sA + tc_off(rr, c)) = u;
+        }
+        pending = true;
+        ok = tc_product<16, 16, 8, tc_idesc(128, 64)>(sA_u, sB_u, tmem, bar_u, parity);
+        if (!ok) break;
+        pending = false;
+        parity ^= 1u;
+        const int64_t i = tile * kTcRows + 32 * quad + lane;
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            float d[16];
+            tc_ld16(trow + 16u * part, d);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int cb = 32 * half + 16 * part;
+            if (i < N) {
+                float4 *dst = reinterpret_cast<float4 *>(Hout + i * H + cb);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    dst[q] = make_float4(fmaxf(d[4 * q] + bias[cb + 4 * q], 0.f),
+                                         fmaxf(d[4 * q + 1] + bias[cb + 4 * q + 1], 0.f),
+                                         fmaxf(d[4 * q + 2] + bias[cb + 4 * q + 2], 0.f),
+                                         fmaxf(d[4 * q + 3] + bias[cb + 4 * q + 3], 0.f));
+            }
+        }
+    }
+    tc_finish<64>(tmem, bar_u, parity, ok, pending, err);
+}
+
+// [dHprev | dY] = dZ W with dZ = dH * (Hl > 0) on tcgen05: A = dZ rounded to
+// BF16 (128 x 64, K = 64 over the layer's outputs), B = W^T (128 x 64, staged
+// once from W by columns); M = 128, N = 128, four K-steps into 128 TMEM
+// columns.  Warps w and w + 4 read back TMEM lanes 32 (w % 4) .., columns
+// 0-63 (dHprev) and 64-127 (dY).
+constexpr int kTcXABytes = kTcRows * H * 2;   // 16 KiB
+constexpr int kTcXBBytes = 2 * H * H * 2;     // 16 KiB
+constexpr size_t kTcBwdSmem = (size_t)kTcXABytes + kTcXBBytes + 16;
+
+__global__ void __launch_bounds__(256, 4) k_dense_bwd_x_tc(const float *__restrict__ dH, const float *__restrict__ Hl,
+                                                           const __nv_bfloat16 *__restrict__ W, int64_t N,
+                                                           float *__restrict__ dHprev, float *__restrict__ dY,
+                                                           int *err)
+{
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    unsigned char *sA = tsm, *sB = tsm + kTcXABytes;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(tsm + kTcXABytes + kTcXBBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(tsm + kTcXABytes + kTcXBBytes + 8);
+    const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA), sB_u = (uint32_t)__cvta_generic_to_shared(sB);
+    const uint32_t bar_u = (uint32_t)__cvta_generic_to_shared(bar);
+    // B[j][o] = W[o][j]: 128 rows j x 8 pieces of 8 outputs o
+    const uint16_t *W16 = reinterpret_cast<const uint16_t *>(W);
+    for (int t = threadIdx.x; t < 2 * H * 8; t += blockDim.x) {
+        const int j = t >> 3, c = t & 7;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            w[q] = (uint32_t)W16[(8 * c + 2 * q) * 2 * H + j] | ((uint32_t)W16[(8 * c + 2 * q + 1) * 2 * H + j] << 16);
+        *reinterpret_cast<uint4 *>(sB + tc_off<8>(j, c)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    const uint32_t tmem = tc_setup<128>(tslot, bar_u);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quad = warp & 3, half = warp >> 2;
+    const uint32_t trow = tmem + ((uint32_t)(32 * quad) << 16) + 64u * half;
+    float *out = half ? dY : dHprev;
+    const int64_t tiles = (N + kTcRows - 1) / kTcRows;
+    uint32_t parity = 0;
+    bool ok = !(*err), pending = false;
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        // 128 rows x 8 pieces of 8 outputs: 4 pieces per thread
+        for (int t = threadIdx.x; t < kTcRows * 8; t += blockDim.x) {
+            const int rr = t >> 3, c = t & 7;
+            const int64_t i = tile * kTcRows + rr;
+            uint4 u = make_uint4(0, 0, 0, 0);
+            if (i < N) {
+                const float4 *d4 = reinterpret_cast<const float4 *>(dH + i * H + 8 * c);
+                const float4 *h4 = reinterpret_cast<const float4 *>(Hl + i * H + 8 * c);
+                const float4 a = d4[0], b = d4[1], ha = h4[0], hb = h4[1];
+                u = make_uint4(pack_bf16(ha.x > 0.f ? a.x : 0.f, ha.y > 0.f ? a.y : 0.f),
+                               pack_bf16(ha.z > 0.f ? a.z : 0.f, ha.w > 0.f ? a.w : 0.f),
+                               pack_bf16(hb.x > 0.f ? b.x : 0.f, hb.y > 0.f ? b.y : 0.f),
+                               pack_bf16(hb.z > 0.f ? b.z : 0.f, hb.w > 0.f ? b.w : 0.f));
+            }
+            *reinterpret_cast<uint4 *>(sA + tc_off<8>(rr, c)) = u;
+        }
+        pending = true;
+        ok = tc_product<8, 8, 4, tc_idesc(128, 128)>(sA_u, sB_u, tmem, bar_u, parity);
+        if (!ok) break;
+        pending = false;
+        parity ^= 1u;
+        const int64_t i = tile * kTcRows + 32 * quad + lane;
+#pragma unroll
+        for (int part = 0; part < 4; ++part) {
+            float d[16];
+            tc_ld16(trow + 16u * part, d);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (i < N) {
+                float4 *dst = reinterpret_cast<float4 *>(out + i * H + 16 * part);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dst[q] = make_float4(d[4 * q], d[4 * q + 1], d[4 * q + 2], d[4 * q + 3]);
+            }
+        }
+    }
+    tc_finish<128>(tmem, bar_u, parity, ok, pending, err);
+}
+
 // ---- host side -------------------------------------------------------------------
+// the tensor-core (tcgen05) kernels unless SFC_MPNN_TC=0 selects the mma.sync ones
+bool use_tc()
+{
+    static int m = -1;
+    if (m < 0) {
+        const char *e = std::getenv("SFC_MPNN_TC");
+        m = (e && e[0] == '0') ? 0 : 1;
+    }
+    return m == 1;
+}
+
+// grid of the tensor-core kernels (four CTAs per SM by their resources, at
+// most 4 x 128 tensor-memory columns; the grid-stride loops take any number of
+// tiles); sets their attributes and the error word on first use
+unsigned tc_grid(sfc_mpnn *m, int64_t N)
+{
+    sfc_ctx *ctx = m->ctx;
+    if (!m->tc_err.p) {
+        m->tc_err.alloc(1);
+        SFC_CK(cudaMemsetAsync(m->tc_err.p, 0, sizeof(int), ctx->stream));
+    }
+    static bool attr = false;
+    if (!attr) {
+        const std::pair<const void *, size_t> ks[] = {{(const void *)k_layer_tc<false>, kTcSmem},
+                                                      {(const void *)k_layer_tc<true>, kTcSmem},
+                                                      {(const void *)k_dense_fwd_tc, kTcFwdSmem},
+                                                      {(const void *)k_dense_bwd_x_tc, kTcBwdSmem}};
+        for (const auto &k : ks) {
+            SFC_CK(cudaFuncSetAttribute(k.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.second));
+            SFC_CK(cudaFuncSetAttribute(k.first, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        }
+        attr = true;
+    }
+    return (unsigned)std::min<int64_t>((N + kTcRows - 1) / kTcRows, (int64_t)ctx->sm_count * 4);
+}
+
+// after a batch of applications: a tensor-core layer whose bounded wait gave
+// up fails the call
+void check_tc(sfc_mpnn *m)
+{
+    if (!m->tc_err.p) return;
+    int h = 0;
+    download(m->ctx, &h, m->tc_err.p, 1);
+    if (h) {
+        SFC_CK(cudaMemsetAsync(m->tc_err.p, 0, sizeof(int), m->ctx->stream));
+        fail(SFC_ERR_TIMEOUT, "learned preconditioner: a bounded wait for the tensor-core products gave up");
+    }
+}
+
 void refresh_bf16(sfc_mpnn *m)
 {
     k_to_bf16<<<64, 256, 0, m->ctx->stream>>>(m->params.p, m->wbf.p);
@@ -943,9 +1216,14 @@ void forward(sfc_mpnn *m, const double *r)
     count_launch(ctx, 3);
     for (int l = 1; l <= LAYERS; ++l) {
         k_agg64<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->H[l - 1].p, m->Y[l].p, N, 0);
-        k_dense_fwd<<<gwarp(ctx), 256, 0, ctx->stream>>>(m->H[l - 1].p, m->Y[l].p, m->wbf.p + (l - 1) * H * 2 * H,
-                                                        m->params.p + OFF_L + (l - 1) * LSZ + H * 2 * H, N,
-                                                        m->H[l].p);
+        if (use_tc())
+            k_dense_fwd_tc<<<tc_grid(m, N), 256, kTcFwdSmem, ctx->stream>>>(
+                m->H[l - 1].p, m->Y[l].p, m->wbf.p + (l - 1) * H * 2 * H, m->params.p + OFF_L + (l - 1) * LSZ + H * 2 * H,
+                N, m->H[l].p, m->tc_err.p);
+        else
+            k_dense_fwd<<<gwarp(ctx), 256, 0, ctx->stream>>>(m->H[l - 1].p, m->Y[l].p, m->wbf.p + (l - 1) * H * 2 * H,
+                                                            m->params.p + OFF_L + (l - 1) * LSZ + H * 2 * H, N,
+                                                            m->H[l].p);
         count_launch(ctx, 2);
     }
     k_decoder<<<gwarp(ctx), 256, 0, ctx->stream>>>(m->H[LAYERS].p, m->params.p, m->x0.p, s->mask.p, N, m->yhat.p);
@@ -980,6 +1258,7 @@ double jacobi_loss(sfc_mpnn *m, const double *r, const double *e)
     pair_residual(m, e, m->x0.p, 1.0);
     double hl = 0;
     download(ctx, &hl, m->scal.p + 1, 1);
+    check_tc(m);
     return hl;
 }
 
@@ -1003,7 +1282,11 @@ double loss_grad(sfc_mpnn *m, const double *r, const double *e, double w)
         float *GW = m->grads.p + OFF_L + (l - 1) * LSZ;
         k_dense_bwd_w<<<(unsigned)(ctx->sm_count * 2), 256, 0, ctx->stream>>>(dHa, m->H[l].p, m->H[l - 1].p, m->Y[l].p,
                                                                               N, GW, GW + H * 2 * H);
-        k_dense_bwd_x<<<gwarp(ctx), 256, 0, ctx->stream>>>(dHa, m->H[l].p, W, N, dHb, m->dY.p);
+        if (use_tc())
+            k_dense_bwd_x_tc<<<tc_grid(m, N), 256, kTcBwdSmem, ctx->stream>>>(dHa, m->H[l].p, W, N, dHb, m->dY.p,
+                                                                               m->tc_err.p);
+        else
+            k_dense_bwd_x<<<gwarp(ctx), 256, 0, ctx->stream>>>(dHa, m->H[l].p, W, N, dHb, m->dY.p);
         // dH(l-1) += Ahat^T dY (Ahat is symmetric)
         k_agg64<<<gwarp(ctx), 256, 0, ctx->stream>>>(s->row_ptr.p, s->col.p, m->ahat.p, m->dY.p, dHb, N, 1);
         count_launch(ctx, 3);
@@ -1014,31 +1297,8 @@ double loss_grad(sfc_mpnn *m, const double *r, const double *e, double w)
     count_launch(ctx);
     double hl = 0;
     download(ctx, &hl, m->scal.p + 1, 1);
+    check_tc(m);
     return hl;
-}
-
-// the tensor-core (tcgen05) layers unless SFC_MPNN_TC=0 selects the mma.sync ones
-bool use_tc()
-{
-    static int m = -1;
-    if (m < 0) {
-        const char *e = std::getenv("SFC_MPNN_TC");
-        m = (e && e[0] == '0') ? 0 : 1;
-    }
-    return m == 1;
-}
-
-// after a batch of applications: a tensor-core layer whose bounded wait gave
-// up fails the call
-void check_tc(sfc_mpnn *m)
-{
-    if (!m->tc_err.p) return;
-    int h = 0;
-    download(m->ctx, &h, m->tc_err.p, 1);
-    if (h) {
-        SFC_CK(cudaMemsetAsync(m->tc_err.p, 0, sizeof(int), m->ctx->stream));
-        fail(SFC_ERR_TIMEOUT, "learned preconditioner: a bounded wait for the tensor-core products gave up");
-    }
 }
 
 // z = M(r) (device FP64 vectors): the inference kernels, no host synchronisation
@@ -1055,25 +1315,7 @@ void apply(sfc_mpnn *m, const double *r, double *z)
                                                        m->params.p, N, m->x0.p, reinterpret_cast<uint4 *>(m->hb[0].p));
     count_launch(ctx, 2);
     if (use_tc()) {
-        if (!m->tc_err.p) {
-            m->tc_err.alloc(1);
-            SFC_CK(cudaMemsetAsync(m->tc_err.p, 0, sizeof(int), ctx->stream));
-        }
-        static int occ = 0;
-        if (!occ) {
-            // all of the unified L1 / shared memory as shared memory, so that
-            // four 48 KiB CTAs fit per SM
-            for (const void *f : {(const void *)k_layer_tc<false>, (const void *)k_layer_tc<true>}) {
-                SFC_CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-                SFC_CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-            }
-            // four CTAs per SM by their resources (4 x 49 KiB of shared memory,
-            // 4 x 256 threads x 64 registers, 4 x 64 tensor-memory columns); the
-            // runtime's occupancy query answers 1 for this kernel, and the
-            // grid-stride loop is correct for any number of resident CTAs
-            occ = 4;
-        }
-        const unsigned gt = (unsigned)std::min<int64_t>((N + kTcRows - 1) / kTcRows, (int64_t)ctx->sm_count * occ);
+        const unsigned gt = tc_grid(m, N);
         for (int l = 0; l < LAYERS; ++l) {
             const uint32_t *hin = reinterpret_cast<const uint32_t *>(m->hb[l & 1].p);
             uint32_t *hout = reinterpret_cast<uint32_t *>(m->hb[(l + 1) & 1].p);
