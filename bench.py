@@ -385,6 +385,35 @@ def run_learned(args, ws, rank, local):
     from statfem_b200 import api
     from statfem_b200 import learned as L
     ctx = api.Context(local)
+    if args.mpnn_apply:
+        # profiling aid: only the network's application M(r) on one held-out
+        # system (random parameters, no training), --mpnn-apply times
+        te = L.PoissonSamples(ctx, args.c5_n, seed0=900_000)
+        s = te.assemble(0, te.coefficients(0))
+        net = api.LearnedPreconditioner(ctx, seed=0)
+        r = np.random.default_rng(0).standard_normal(te.mesh.num_dofs)
+        for _ in range(args.warmup):
+            net.apply(s, r)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.mpnn_apply):
+            z = net.apply(s, r)
+        ctx.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / args.mpnn_apply
+        # the device time of the same applications, kernel by kernel
+        ctx.set_profiling(True)
+        for _ in range(args.mpnn_apply):
+            net.apply(s, r)
+        ctx.synchronize()
+        ctx.set_profiling(False)
+        prof = ctx.profile_report()
+        if rank == 0:
+            print(json.dumps({"metric": "network applications (host wall, with the host copies of r and z)",
+                              "ms_per_application": round(ms, 3), "n": args.c5_n, "applications": args.mpnn_apply,
+                              "device_ms_per_application": {k: round(v[1] / args.mpnn_apply, 3)
+                                                            for k, v in prof.items()},
+                              "checksum": float(np.abs(z).sum())}))
+        return
     # the network is local: train on smaller grids whose fields have the same
     # correlation length in cells as the 128^3 target (length 0.1 x 128 / n)
     tr = L.PoissonSamples(ctx, args.c5_train_n, length=0.1 * 128 / args.c5_train_n, seed0=10_000 + 1000 * rank)
@@ -979,6 +1008,8 @@ def main():
     ap.add_argument("--c5-train-n", type=int, default=32, help="c5: training grid (elements per side)")
     ap.add_argument("--c5-steps", type=int, default=40, help="c5: Adam steps per training sample")
     ap.add_argument("--c5-n", type=int, default=128, help="c5: held-out grid (elements per side)")
+    ap.add_argument("--mpnn-apply", type=int, default=0,
+                    help="c5 profiling aid: time this many network applications on one held-out system and exit")
     ap.add_argument("--method", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cpu-iters", type=int, default=20,
                     help="CPU arms: block-PCG iterations timed per sample")
