@@ -107,8 +107,10 @@ typedef struct sfc_solve_stats {
                                  0 when the solve had none                    */
     int32_t spmm_kernel;      /* FP32 product of the mixed solver: 0 none (FP64
                                  solve), 1 CSR rows, 2 node blocks (3-dof
-                                 meshes), 3 node blocks staged per lattice
-                                 brick by TMA (3-dof structured lattices)    */
+                                 meshes), 3 lattice bricks staged by TMA
+                                 (SFC_SPMM=lattice), 4 streamed lattice
+                                 x-lines (the default on 3-dof structured
+                                 lattices)                                    */
     int32_t reserved;
 } sfc_solve_stats_t;
 
