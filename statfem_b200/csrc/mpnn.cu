@@ -15,9 +15,10 @@
 // dense transforms run on the 5th-generation tensor cores (tcgen05.mma,
 // BF16 x BF16 -> FP32 in tensor memory): k_layer_tc in inference (gather
 // fused), k_dense_fwd_tc and k_dense_bwd_x_tc in training, with the inputs
-// rounded to BF16 on the fly; SFC_MPNN_TC=0 selects the earlier mma.sync
-// forms (k_layer_inf, k_dense_fwd, k_dense_bwd_x) for comparison.  The
-// weight gradient (k_dense_bwd_w) is an FP32 reduction over the nodes.
+// rounded to BF16 on the fly, and the weight gradient k_dense_bwd_w_tc as the
+// transposed product accumulated over a CTA's node tiles; SFC_MPNN_TC=0
+// selects the earlier forms (mma.sync k_layer_inf, k_dense_fwd,
+// k_dense_bwd_x, and the FP32 reduction k_dense_bwd_w) for comparison.
 // Activations in training, master weights, gradients and Adam state are FP32.
 //
 // Training pair (r, e) with S e = r: target t = D^1/2 e / s, d = x0 + y - t,
@@ -1109,6 +1110,120 @@ __global__ void __launch_bounds__(256, 4) k_dense_bwd_x_tc(const float *__restri
     tc_finish<128>(tmem, bar_u, parity, ok, pending, err);
 }
 
+// dW[o][j] += sum_i dZ[i][o] Xc[i][j] (Xc = [Hin | Yin]) and db[o] += sum_i
+// dZ[i][o] on tcgen05: the transposed product dW^T = Xc^T dZ with M = 128 (the
+// inputs j), N = 64 (the outputs o) and K = the 128 nodes of a tile, both
+// operands MN-major as they lie in memory (a node's 8 consecutive features
+// are one 16-byte piece: piece (feature group g, node group kg) at byte
+// (16 g + kg) * 128 + (node % 8) * 16, so the next node group is 128 B on
+// (LBO) and the next feature group 2,048 B on (SBO)), rounded to BF16 like
+// the forward products.  A CTA accumulates all its tiles in 64 TMEM columns
+// and adds the result to GW once; db (unrounded dZ) is summed on the way.
+constexpr uint32_t kTcIdescWgrad = tc_idesc(128, 64) | (1u << 15) | (1u << 16);  // A and B MN-major
+
+__global__ void __launch_bounds__(256, 4) k_dense_bwd_w_tc(const float *__restrict__ dH, const float *__restrict__ Hl,
+                                                           const float *__restrict__ Hin,
+                                                           const float *__restrict__ Yin, int64_t N,
+                                                           float *__restrict__ GW, float *__restrict__ Gb, int *err)
+{
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    unsigned char *sA = tsm, *sB = tsm + kTcABytes;  // Xc^T: 128 x 128 (32 KiB); dZ^T: 64 x 128 (16 KiB)
+    uint64_t *bar = reinterpret_cast<uint64_t *>(tsm + kTcABytes + kTcBBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(tsm + kTcABytes + kTcBBytes + 8);
+    __shared__ float sdb[H];
+    const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA), sB_u = (uint32_t)__cvta_generic_to_shared(sB);
+    const uint32_t bar_u = (uint32_t)__cvta_generic_to_shared(bar);
+    for (int t = threadIdx.x; t < H; t += blockDim.x) sdb[t] = 0.f;
+    const uint32_t tmem = tc_setup<64>(tslot, bar_u);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quad = warp & 3, half = warp >> 2;
+    const int64_t tiles = (N + kTcRows - 1) / kTcRows;
+    uint32_t parity = 0;
+    bool ok = !(*err), pending = false, any = false;
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        // Xc: 128 nodes x 16 feature groups; dZ: 128 nodes x 8 output groups
+        for (int t = threadIdx.x; t < kTcRows * 24; t += blockDim.x) {
+            const int node = t / 24, g = t % 24;
+            const int64_t i = tile * kTcRows + node;
+            uint4 u = make_uint4(0, 0, 0, 0);
+            if (i < N) {
+                float4 a, b;
+                if (g < 16) {
+                    const float4 *src = reinterpret_cast<const float4 *>((g < 8 ? Hin : Yin) + i * H + (g & 7) * 8);
+                    a = src[0];
+                    b = src[1];
+                } else {
+                    const float4 *d4 = reinterpret_cast<const float4 *>(dH + i * H + (g - 16) * 8);
+                    const float4 *h4 = reinterpret_cast<const float4 *>(Hl + i * H + (g - 16) * 8);
+                    const float4 da = d4[0], dbv = d4[1], ha = h4[0], hb = h4[1];
+                    a = make_float4(ha.x > 0.f ? da.x : 0.f, ha.y > 0.f ? da.y : 0.f, ha.z > 0.f ? da.z : 0.f,
+                                    ha.w > 0.f ? da.w : 0.f);
+                    b = make_float4(hb.x > 0.f ? dbv.x : 0.f, hb.y > 0.f ? dbv.y : 0.f, hb.z > 0.f ? dbv.z : 0.f,
+                                    hb.w > 0.f ? dbv.w : 0.f);
+                    // db: unrounded dZ, one shared-memory add per output and piece
+                    const int o0 = (g - 16) * 8;
+                    atomicAdd(&sdb[o0], a.x);
+                    atomicAdd(&sdb[o0 + 1], a.y);
+                    atomicAdd(&sdb[o0 + 2], a.z);
+                    atomicAdd(&sdb[o0 + 3], a.w);
+                    atomicAdd(&sdb[o0 + 4], b.x);
+                    atomicAdd(&sdb[o0 + 5], b.y);
+                    atomicAdd(&sdb[o0 + 6], b.z);
+                    atomicAdd(&sdb[o0 + 7], b.w);
+                }
+                u = make_uint4(pack_bf16(a.x, a.y), pack_bf16(a.z, a.w), pack_bf16(b.x, b.y), pack_bf16(b.z, b.w));
+            }
+            const uint32_t off = (uint32_t)((((g < 16 ? g : g - 16) * 16) + (node >> 3)) * 128 + (node & 7) * 16);
+            *reinterpret_cast<uint4 *>((g < 16 ? sA : sB) + off) = u;
+        }
+        pending = true;
+        // K-steps of 16 nodes: the descriptors advance by two node groups (256 B);
+        // the first tile's first step overwrites the accumulator
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks) {
+                const uint64_t da = tc_desc<16>(sA_u + 256u * ks), dbd = tc_desc<16>(sB_u + 256u * ks);
+                const uint32_t acc = (any || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                    :
+                    : "r"(tmem), "l"(da), "l"(dbd), "r"(kTcIdescWgrad), "r"(acc), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_u)
+                         : "memory");
+        }
+        ok = __syncthreads_and(tc_wait(bar_u, parity));
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!ok) break;
+        pending = false;
+        any = true;
+        parity ^= 1u;
+    }
+    if (ok && any) {
+        // D[j][o]: warps w and w + 4 hold inputs j = 32 (w % 4) + lane, outputs 0-31 / 32-63
+        const int j = 32 * quad + lane;
+        const uint32_t trow = tmem + ((uint32_t)(32 * quad) << 16) + 32u * half;
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            float d[16];
+            tc_ld16(trow + 16u * part, d);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 16; ++q) atomicAdd(&GW[(32 * half + 16 * part + q) * 2 * H + j], d[q]);
+        }
+    }
+    __syncthreads();
+    if (ok && any)
+        for (int t = threadIdx.x; t < H; t += blockDim.x) atomicAdd(&Gb[t], sdb[t]);
+    tc_finish<64>(tmem, bar_u, parity, ok, pending, err);
+}
+
 // ---- host side -------------------------------------------------------------------
 // the tensor-core (tcgen05) kernels unless SFC_MPNN_TC=0 selects the mma.sync ones
 bool use_tc()
@@ -1136,7 +1251,8 @@ unsigned tc_grid(sfc_mpnn *m, int64_t N)
         const std::pair<const void *, size_t> ks[] = {{(const void *)k_layer_tc<false>, kTcSmem},
                                                       {(const void *)k_layer_tc<true>, kTcSmem},
                                                       {(const void *)k_dense_fwd_tc, kTcFwdSmem},
-                                                      {(const void *)k_dense_bwd_x_tc, kTcBwdSmem}};
+                                                      {(const void *)k_dense_bwd_x_tc, kTcBwdSmem},
+                                                      {(const void *)k_dense_bwd_w_tc, kTcFwdSmem}};
         for (const auto &k : ks) {
             SFC_CK(cudaFuncSetAttribute(k.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.second));
             SFC_CK(cudaFuncSetAttribute(k.first, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
@@ -1280,8 +1396,13 @@ double loss_grad(sfc_mpnn *m, const double *r, const double *e, double w)
     for (int l = LAYERS; l >= 1; --l) {
         const __nv_bfloat16 *W = m->wbf.p + (l - 1) * H * 2 * H;
         float *GW = m->grads.p + OFF_L + (l - 1) * LSZ;
-        k_dense_bwd_w<<<(unsigned)(ctx->sm_count * 2), 256, 0, ctx->stream>>>(dHa, m->H[l].p, m->H[l - 1].p, m->Y[l].p,
-                                                                              N, GW, GW + H * 2 * H);
+        if (use_tc())
+            k_dense_bwd_w_tc<<<tc_grid(m, N), 256, kTcFwdSmem, ctx->stream>>>(dHa, m->H[l].p, m->H[l - 1].p,
+                                                                               m->Y[l].p, N, GW, GW + H * 2 * H,
+                                                                               m->tc_err.p);
+        else
+            k_dense_bwd_w<<<(unsigned)(ctx->sm_count * 2), 256, 0, ctx->stream>>>(dHa, m->H[l].p, m->H[l - 1].p,
+                                                                                  m->Y[l].p, N, GW, GW + H * 2 * H);
         if (use_tc())
             k_dense_bwd_x_tc<<<tc_grid(m, N), 256, kTcBwdSmem, ctx->stream>>>(dHa, m->H[l].p, W, N, dHb, m->dY.p,
                                                                                m->tc_err.p);
