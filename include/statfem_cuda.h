@@ -368,16 +368,13 @@ int32_t sfc_perturbation_covar(const sfc_perturbation_t *pt, double *cov);
  * and nothing is allocated: the scratch is a fixed device array of
  * 128*128 + 128*64 doubles (192 KiB, held by every device that loads the
  * library until exit), so num_sensors <= 128 and num_readings <= 64, else
- * SFC_ERR_TOO_LARGE.  The first call on a device looks up that array's device
- * address (with the device current) and, under CUDA's lazy module loading,
- * is the call that loads the library's kernels onto the device, which
+ * SFC_ERR_TOO_LARGE.  Every call looks up that array's address in the
+ * current context (a host-side lookup); under CUDA's lazy module loading the
+ * first call in a context is the one that loads the library's kernels, which
  * allocates the array and the code and may synchronise: make one call at
  * start-up, before any stream capture and outside the loop that must not
- * allocate.  The address is cached per device for the context current at
- * that first call (the primary context for runtime-API callers): do not use
- * this entry point after cudaDeviceReset or from a different context.  All
- * calls share the array: calls that can overlap on the GPU race and must be
- * ordered by the caller. */
+ * allocate (and again after cudaDeviceReset).  All calls share the array:
+ * calls that can overlap on the GPU race and must be ordered by the caller. */
 int32_t sfc_koh_log_likelihood_noalloc(const double *mean_dev, const double *cov_dev,
                                        const double *sensor_coords_dev, int32_t dim,
                                        const double *y_dev, int32_t num_sensors,
