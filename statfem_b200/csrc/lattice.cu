@@ -14,12 +14,12 @@
 //
 // Staged bricks.  A work item is a brick of 4 x 2 x 2 output nodes and a
 // 64-column slice of the block.  One elected thread issues a single 5-D TMA
-// tensor load of the
-// brick's halo (6 x 4 x 4 column nodes x 3 rows x 64 columns, zero-filled
-// outside the lattice: 72 KiB) and 1-D bulk copies of the brick's block rows
-// (up to 4 x 5 KiB) into shared memory, completing on one mbarrier.  Each
-// x-line of four output nodes belongs to two warps (32 columns each, one
-// per lane): for every column node of its 3 x 3 neighbour lines a warp reads
+// tensor load of the brick's halo (6 x 4 x 4 column nodes x 3 rows x 64
+// columns, zero-filled outside the lattice: 72 KiB) and 1-D bulk copies of
+// the brick's block rows (up to 4 x 5 KiB) into shared memory, completing on
+// one mbarrier.  Each x-line of four output nodes belongs to two warps (32
+// columns each, one per lane): for every column node of its 3 x 3 neighbour
+// lines a warp reads
 // the node's three P rows from shared memory once and applies them to every
 // output node of the line that couples to it (up to three), so a P row read
 // feeds 1.8 outputs on average.  Measured, the shared-memory load path bounds
