@@ -19,10 +19,9 @@
 // the brick's block rows (up to 4 x 5 KiB) into shared memory, completing on
 // one mbarrier.  Each x-line of four output nodes belongs to two warps (32
 // columns each, one per lane): for every column node of its 3 x 3 neighbour
-// lines a warp reads
-// the node's three P rows from shared memory once and applies them to every
-// output node of the line that couples to it (up to three), so a P row read
-// feeds 1.8 outputs on average.  Measured, the shared-memory load path bounds
+// lines a warp reads the node's three P rows from shared memory once and
+// applies them to every output node of the line that couples to it (up to
+// three), so a P row read feeds 1.8 outputs on average.  Measured, the shared-memory load path bounds
 // it: both warps of an x-line load the same block values for their two
 // columns per lane.  The p.q column dots are accumulated in FP64 per lane
 // across all of a CTA's work items and reduced once at the end.
