@@ -55,6 +55,32 @@ int guard(sfc_ctx *ctx, const std::function<void()> &fn)
     }
 }
 
+// out[c][r] = in[r][c] for an rows x cols row-major FP64 matrix: 32 x 32
+// tiles through shared memory (padded against bank conflicts), so both the
+// reads and the writes are coalesced
+__global__ void k_transpose64(const double *__restrict__ in, double *__restrict__ out, int64_t rows, int64_t cols)
+{
+    __shared__ double tile[32][33];
+    const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t r = r0 + j, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[j][threadIdx.x] = in[r * cols + c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int64_t c = c0 + j, r = r0 + threadIdx.x;
+        if (c < cols && r < rows) out[c * rows + r] = tile[threadIdx.x][j];
+    }
+}
+
+void transpose64(sfc_ctx *ctx, const double *in, double *out, int64_t rows, int64_t cols)
+{
+    const dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+    SFC_REQUIRE(grid.y <= 65535u, "transpose: too many rows");
+    k_transpose64<<<grid, dim3(32, 8), 0, ctx->stream>>>(in, out, rows, cols);
+    count_launch(ctx);
+}
+
 void ensure_vectors(sfc_system *s)
 {
     if (!s->F.p) {
@@ -446,16 +472,16 @@ int32_t sfc_solve_multi(sfc_system_t *s, const double *rhs, double *u, int32_t n
     return guard(s->ctx, [&] {
         flush_staged(s);
         const int64_t N = s->N;
-        std::vector<double> Bt((size_t)N * nrhs);
-        for (int a = 0; a < nrhs; ++a)
-            for (int64_t i = 0; i < N; ++i) Bt[(size_t)i * nrhs + a] = rhs[(size_t)a * N + i];
-        DBuf<double> B, X;
-        upload(s->ctx, B, Bt.data(), Bt.size());
+        // the caller's [nrhs][N] columns go up as they are and are transposed
+        // to the interleaved [N][nrhs] layout on the GPU (and back)
+        DBuf<double> C, B, X;
+        upload(s->ctx, C, rhs, (size_t)N * nrhs);
+        B.alloc((size_t)N * nrhs);
+        transpose64(s->ctx, C.p, B.p, nrhs, N);
         X.alloc((size_t)N * nrhs);
         solve_multi(s, B.p, X.p, nrhs, nrhs);
-        download(s->ctx, Bt.data(), X.p, Bt.size());
-        for (int a = 0; a < nrhs; ++a)
-            for (int64_t i = 0; i < N; ++i) u[(size_t)a * N + i] = Bt[(size_t)i * nrhs + a];
+        transpose64(s->ctx, X.p, C.p, N, nrhs);
+        download(s->ctx, u, C.p, (size_t)N * nrhs);
     });
 }
 
