@@ -61,7 +61,8 @@ int guard(sfc_ctx *ctx, const std::function<void()> &fn)
 __global__ void k_transpose64(const double *__restrict__ in, double *__restrict__ out, int64_t rows, int64_t cols)
 {
     __shared__ double tile[32][33];
-    const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+    const int64_t ct = (cols + 31) / 32;  // tiles along the columns; the grid is one tile per CTA
+    const int64_t r0 = ((int64_t)blockIdx.x / ct) * 32, c0 = ((int64_t)blockIdx.x % ct) * 32;
     for (int j = threadIdx.y; j < 32; j += blockDim.y) {
         const int64_t r = r0 + j, c = c0 + threadIdx.x;
         if (r < rows && c < cols) tile[j][threadIdx.x] = in[r * cols + c];
@@ -75,9 +76,9 @@ __global__ void k_transpose64(const double *__restrict__ in, double *__restrict_
 
 void transpose64(sfc_ctx *ctx, const double *in, double *out, int64_t rows, int64_t cols)
 {
-    const dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
-    SFC_REQUIRE(grid.y <= 65535u, "transpose: too many rows");
-    k_transpose64<<<grid, dim3(32, 8), 0, ctx->stream>>>(in, out, rows, cols);
+    const int64_t tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
+    SFC_REQUIRE(tiles <= 0x7fffffff, "transpose: too many tiles");
+    k_transpose64<<<(unsigned)tiles, dim3(32, 8), 0, ctx->stream>>>(in, out, rows, cols);
     count_launch(ctx);
 }
 
