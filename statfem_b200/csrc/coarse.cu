@@ -891,16 +891,28 @@ void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *st
                 r, cs.agg_ptr.p, cs.agg_nodes.p, cs.mode.p, cs.c32.p, stop);
         count_launch(ctx);
     }
-    {
-        ProfScope ps(ctx, "coarse_apply32", 4.0 * cs.nc * cs.nc + 8.0 * cs.nc * K);
-        const dim3 grid((unsigned)(cs.lda / kGemmRows), K / kGemmCols, kGemmSplit);
-        k_coarse_gemm32<V><<<grid, 128, 0, ctx->stream>>>(cs.a32.p, cs.c32.p, cs.e32.p, cs.lda, cs.nc, rz, stop);
-        count_launch(ctx);
-    }
+    coarse_block_gemm<V>(s, rz, stop);
 }
 template void coarse_block_apply<1>(sfc_system *, const float *, double *, const int *);
 template void coarse_block_apply<2>(sfc_system *, const float *, double *, const int *);
 template void coarse_block_apply<4>(sfc_system *, const float *, double *, const int *);
+
+// e = A_c^+ c for a restriction c already in cs.c32 (the fused r update and
+// restriction of the block solver writes it)
+template <int V>
+void coarse_block_gemm(sfc_system *s, double *rz, const int *stop)
+{
+    constexpr int K = 32 * V;
+    CoarseSpace &cs = s->coarse;
+    sfc_ctx *ctx = s->ctx;
+    ProfScope ps(ctx, "coarse_apply32", 4.0 * cs.nc * cs.nc + 8.0 * cs.nc * K);
+    const dim3 grid((unsigned)(cs.lda / kGemmRows), K / kGemmCols, kGemmSplit);
+    k_coarse_gemm32<V><<<grid, 128, 0, ctx->stream>>>(cs.a32.p, cs.c32.p, cs.e32.p, cs.lda, cs.nc, rz, stop);
+    count_launch(ctx);
+}
+template void coarse_block_gemm<1>(sfc_system *, double *, const int *);
+template void coarse_block_gemm<2>(sfc_system *, double *, const int *);
+template void coarse_block_gemm<4>(sfc_system *, double *, const int *);
 
 void coarse_vec_apply(sfc_system *s, const double *r, double *rz, const int *done)
 {

@@ -578,6 +578,8 @@ void spd_inverse_gj(sfc_ctx *ctx, double *A, int64_t n, double rel, GjScratch &w
 bool coarse_prepare(sfc_system *s);
 template <int V>
 void coarse_block_apply(sfc_system *s, const float *r, double *rz, const int *stop);
+template <int V>
+void coarse_block_gemm(sfc_system *s, double *rz, const int *stop);  // e = A_c^+ c of cs.c32
 void coarse_vec_apply(sfc_system *s, const double *r, double *rz, const int *done);
 // stats.cu
 void forward_gauss_update(sfc_forward_gauss *fg, const sfc_hparams_t *hp);

@@ -829,6 +829,136 @@ __global__ void __launch_bounds__(256, 4) k_nupdate32(float *__restrict__ x, flo
     block_cols_add<V>(a2, sh, rr_next);
 }
 
+// Two-level r update fused with the coarse restriction: r -= alpha q, r.z and
+// r.r with z the nodal block-Jacobi share (k_nupdate32<V, false>), and the
+// restriction c[6a + m][col] = (P^T r)[6a + m][col] of the updated r
+// (k_coarse_restrict32), so r is read once per iteration instead of twice.
+// The nodes are visited by aggregate: a cluster of kNrSplit CTAs per
+// aggregate, a warp per node, node ids and modes fetched one per lane ahead
+// of the trips; the restriction's partial sums are added in rank order
+// through distributed shared memory (no atomics, the same sums on every
+// run), the dots as in k_nupdate32.
+constexpr int kNrSplit = 2;
+
+template <int V>
+__global__ void __cluster_dims__(kNrSplit, 1, 1) __launch_bounds__(256, 3)
+    k_nrupdate32(float *__restrict__ r, const float *__restrict__ q, const float *__restrict__ bdinv,
+                 const int32_t *__restrict__ agg_ptr, const int32_t *__restrict__ agg_nodes,
+                 const float4 *__restrict__ mode, float *__restrict__ c, const double *pq, const double *rz,
+                 const double *rr, const double *thr, double *rz_next, double *rr_next, const int *stop, int *err)
+{
+    constexpr int K = 32 * V;
+    __shared__ float red[8][6][K];
+    __shared__ double sh[8 * K];
+    if (*stop) return;  // uniform: stop changes only between launches
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    const int a = blockIdx.x / kNrSplit;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float alpha[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int col = lane * V + v;
+        const bool frozen = rr[col] <= thr[col] || err[col];
+        const double den = pq[col];
+        if (!frozen && !(den > 0.0) && rank == 0 && a == 0) err[col] = 1;
+        alpha[v] = (frozen || !(den > 0.0)) ? 0.f : (float)(rz[col] / den);
+    }
+    // r.z and r.r over this warp's nodes (a few dozen) in FP32, then FP64
+    // across warps and CTAs
+    float a1f[V], a2f[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) a1f[v] = a2f[v] = 0.f;
+    // the warp's restriction partial sums live in its own rows of red (each
+    // lane its own columns), which keeps the trip within 80 registers
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+#pragma unroll
+        for (int v = 0; v < V; ++v) red[w][m][lane * V + v] = 0.f;
+    const int32_t step = 8 * kNrSplit, end = agg_ptr[a + 1];
+    const int32_t first = agg_ptr[a] + (int32_t)rank * 8 + w;  // this warp's nodes: first + k step
+    const int mine = first < end ? (end - 1 - first) / step + 1 : 0;
+    for (int base = 0; base < mine; base += 32) {
+        int32_t li = 0;
+        float4 lm = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (base + lane < mine) {
+            li = agg_nodes[first + (base + lane) * step];
+            lm = mode[li];
+        }
+        const int cnt = min(32, mine - base);
+#pragma unroll 1
+        for (int k = 0; k < cnt; ++k) {
+            const int64_t n = __shfl_sync(0xffffffffu, li, k);
+            const float mx = __shfl_sync(0xffffffffu, lm.x, k), my = __shfl_sync(0xffffffffu, lm.y, k),
+                        mz = __shfl_sync(0xffffffffu, lm.z, k);
+            const int bits = (int)__shfl_sync(0xffffffffu, lm.w, k);
+            float rv[3][V], zv[3][V];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int64_t o = (3 * n + i) * K + lane * V;
+                float qv[V];
+                ldv<V>(r + o, rv[i]);
+                ldv<V>(q + o, qv);
+#pragma unroll
+                for (int v = 0; v < V; ++v) rv[i][v] = fmaf(-alpha[v], qv[v], rv[i][v]);
+                stv<V>(r + o, rv[i]);
+            }
+            bj_apply<V>(bdinv + 9 * n, rv, zv);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    a1f[v] = fmaf(rv[i][v], zv[i][v], a1f[v]);
+                    a2f[v] = fmaf(rv[i][v], rv[i][v], a2f[v]);
+                }
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                if ((bits >> i) & 1)
+#pragma unroll
+                    for (int v = 0; v < V; ++v) rv[i][v] = 0.f;
+            float acc[V];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) {
+                float *row = &red[w][m][lane * V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    const float t = m < 3    ? rv[m][v]
+                                    : m == 3 ? my * rv[2][v] - mz * rv[1][v]
+                                    : m == 4 ? mz * rv[0][v] - mx * rv[2][v]
+                                             : mx * rv[1][v] - my * rv[0][v];
+                    acc[v] = row[v] + t;
+                }
+#pragma unroll
+                for (int v = 0; v < V; ++v) row[v] = acc[v];
+            }
+        }
+    }
+    double a1[V], a2[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        a1[v] = a1f[v];
+        a2[v] = a2f[v];
+    }
+    block_cols_add<V>(a1, sh, rz_next);
+    __syncthreads();
+    block_cols_add<V>(a2, sh, rr_next);
+    __syncthreads();
+    for (int t = threadIdx.x; t < 6 * K; t += blockDim.x) {
+        const int m = t / K, col = t % K;
+        float sum = 0.f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) sum += red[j][m][col];
+        red[0][m][col] = sum;  // entry (m, col) is read and written by this thread only
+    }
+    cl.sync();
+    for (int t = (int)rank * blockDim.x + threadIdx.x; t < 6 * K; t += kNrSplit * blockDim.x) {
+        float sum = 0.f;
+        for (unsigned j = 0; j < kNrSplit; ++j) sum += cl.map_shared_rank(&red[0][0][0], j)[t];
+        c[(6 * (int64_t)a + t / K) * K + t % K] = sum;
+    }
+    cl.sync();  // the other CTAs' shared memory stays alive until every read is done
+}
+
 // x (nullable): x += alpha p with this iteration's alpha (computed as in
 // k_nupdate32) before p is overwritten
 __device__ __forceinline__ float iter_alpha(int c, const double *pq, const double *rz, const double *rr,
@@ -1088,17 +1218,24 @@ __global__ void k_pcg2_pupdate(double *__restrict__ p, const double *__restrict_
     }
 }
 
-// all columns converged at iteration it -> *stop = 1
+// Convergence test after every inner iteration of a check interval: the
+// first iteration after which all columns are below their thresholds sets
+// *stop (every later kernel of the interval returns at once) and records in
+// *ran how many of the interval's iterations ran (it_local + 1).
 template <int K>
-__global__ void k_bcheck(const double *rr, const double *thr, int *stop)
+__global__ void k_bcheck_it(const double *rr, const double *thr, int *stop, int *ran, int it_local)
 {
     __shared__ int any;
+    if (*stop) return;  // uniform: only check kernels set it, and none runs beside this one
     if (threadIdx.x == 0) any = 0;
     __syncthreads();
     for (int c = threadIdx.x; c < K; c += blockDim.x)
         if (rr[c] > thr[c]) any = 1;
     __syncthreads();
-    if (threadIdx.x == 0 && !any) *stop = 1;
+    if (threadIdx.x == 0 && !any) {
+        *stop = 1;
+        *ran = it_local + 1;
+    }
 }
 
 // x64 += norm_c * x32
@@ -1429,10 +1566,11 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     auto sl = [&](int i) { return s->scal.p + (int64_t)(i % R) * 3 * K; };
     double *bn2 = cs.p, *rn2 = bn2 + K, *scale = rn2 + K, *norm = scale + K, *thr = norm + K;
     // flags[0]: all columns below their thresholds; flags[1 + c]: breakdown
-    // (p^T A p <= 0) in column c
-    s->flags.reserve(1 + K);
-    int *stop = s->flags.p, *err = s->flags.p + 1;
-    std::vector<int> hflags(1 + K), nbreak(K), fallback(K), nstall(K);
+    // (p^T A p <= 0) in column c; flags[1 + K]: iterations of the current
+    // check interval that ran before flags[0] was set (0: all of them)
+    s->flags.reserve(2 + K);
+    int *stop = s->flags.p, *err = s->flags.p + 1, *ran = s->flags.p + 1 + K;
+    std::vector<int> hflags(2 + K), nbreak(K), fallback(K), nstall(K);
     int n_fallback = 0;
     const bool debug = std::getenv("SFC_DEBUG_SOLVER") != nullptr;
     const unsigned gw = (unsigned)(ctx->sm_count * 8);  // warp-per-row kernels: 8 warps/block
@@ -1442,6 +1580,10 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
     const bool two = two_any && crs.dof == 3;   // block Jacobi + rigid-body modes
     const bool two1 = two_any && crs.dof == 1;  // point Jacobi + constant modes (scalar mesh)
     const bool bj = bsr && (o.precond == SFC_PRECOND_BLOCK_JACOBI || two) && s->bdinv32.p;
+    // two-level with block Jacobi: the r update and the coarse restriction in
+    // one pass over r (SFC_RESTRICT=separate keeps the two kernels)
+    const char *fenv = std::getenv("SFC_RESTRICT");
+    const bool fuse_restrict = two && bj && !(fenv && std::string(fenv) == "separate");
     // R = B - S X (FP64) and Q = S P (FP32), node-block kernels for 3-dof meshes
     // the true residual on the lattice view unless SFC_RESID=bsr
     const char *renv = std::getenv("SFC_RESID");
@@ -1516,16 +1658,29 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         SFC_CK(cudaMemsetAsync(nxt, 0, (size_t)3 * K * 8, ctx->stream));
         double *pqi = nxt, *rz0 = cur + K, *rr0 = cur + 2 * K, *rz1 = nxt + K, *rr1 = nxt + 2 * K;
         spmm(pp, qq, pqi);
-        {
-            ProfScope ps(ctx, "bupdate32", (bj ? 3.0 : 6.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N);
-            if (bj)
-                k_nupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes, pqi,
-                                                                   rz0, rr0, thr, rz1, rr1, stop, err);
-            else
-                k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pqi, rz0,
-                                                            rr0, thr, rz1, rr1, stop, err);
+        if (fuse_restrict) {
+            coarse_block_reserve(s, K);  // no-op once reserved (always, inside a capture)
+            {
+                ProfScope ps(ctx, "nrupdate32", 3.0 * N * K * 4 + 52.0 * s->nodes + 4.0 * crs.nc * K);
+                k_nrupdate32<V><<<(unsigned)(crs.nagg * kNrSplit), 256, 0, ctx->stream>>>(
+                    rr32, qq, s->bdinv32.p, crs.agg_ptr.p, crs.agg_nodes.p, crs.mode.p, crs.c32.p, pqi, rz0, rr0,
+                    thr, rz1, rr1, stop, err);
+            }
+            count_launch(ctx);
+            coarse_block_gemm<V>(s, rz1, stop);
+        } else {
+            {
+                ProfScope ps(ctx, "bupdate32", (bj ? 3.0 : 6.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N);
+                if (bj)
+                    k_nupdate32<V, false><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->bdinv32.p, s->nodes,
+                                                                       pqi, rz0, rr0, thr, rz1, rr1, stop, err);
+                else
+                    k_bupdate32<V><<<gw, 256, 0, ctx->stream>>>(xr, rr32, pp, qq, s->dinv32.p, N, pqi, rz0,
+                                                                rr0, thr, rz1, rr1, stop, err);
+            }
+            count_launch(ctx);
+            if (two_any) coarse_block_apply<V>(s, rr32, rz1, stop);
         }
-        if (two_any) coarse_block_apply<V>(s, rr32, rz1, stop);
         {
             ProfScope ps(ctx, "bpupdate32",
                          (bj ? 5.0 : 3.0) * N * K * 4 + (bj ? 12.0 : 4.0) * N + (two ? 8.0 * s->nodes : 0.0));
@@ -1545,6 +1700,9 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                 k_bpupdate32<V><<<gw, 256, 0, ctx->stream>>>(pp, rr32, s->dinv32.p, N, rz0, rz1, rr1,
                                                              thr, stop, err);
         }
+        // convergence after every iteration: the rest of the interval returns
+        // at once when all columns are below their thresholds
+        k_bcheck_it<K><<<1, 128, 0, ctx->stream>>>(rr1, thr, stop, ran, it % check);
         count_launch(ctx, 2);
     };
     // A whole check interval as one CUDA graph: the ring's zeroing, `check`
@@ -1564,7 +1722,8 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         if (bsr && s->has_lattice && s->lat_mode == 2) xline_prepare(K);
         const std::vector<uintptr_t> key = {
             (uintptr_t)K, (uintptr_t)check, (uintptr_t)N, (uintptr_t)s->nodes, (uintptr_t)gw,
-            (uintptr_t)(bsr | (bj << 1) | (two << 2) | (two1 << 3) | (lattice << 4)), (uintptr_t)s->scal.p,
+            (uintptr_t)(bsr | (bj << 1) | (two << 2) | (two1 << 3) | (lattice << 4) | (fuse_restrict << 5)),
+            (uintptr_t)s->scal.p,
             (uintptr_t)s->blk32.p, (uintptr_t)s->colsc.p, (uintptr_t)s->flags.p, (uintptr_t)s->bdinv32.p,
             (uintptr_t)s->dinv32.p, (uintptr_t)s->bptr.p, (uintptr_t)s->bcol.p, (uintptr_t)s->bval32.p,
             (uintptr_t)s->row_ptr.p, (uintptr_t)s->col.p, (uintptr_t)s->a_op32.p, (uintptr_t)s->bq.p, (uintptr_t)s->bq64.p,
@@ -1586,8 +1745,6 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
                 ctx->stream = st;
                 try {
                     for (int j = 0; j < check; ++j) iterate(j);
-                    k_bcheck<K><<<1, 128, 0, ctx->stream>>>(sl(check) + 2 * K, thr, stop);
-                    count_launch(ctx);
                 } catch (...) {
                     ctx->stream = keep;
                     cudaStreamEndCapture(st, &graph);
@@ -1647,7 +1804,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         SFC_CK(cudaMemsetAsync(x64.p, 0, N * K * 8, ctx->stream));
         SFC_CK(cudaMemsetAsync(cs.p, 0, 6 * K * 8, ctx->stream));
         SFC_CK(cudaMemsetAsync(s->scal.p, 0, nsc * 8, ctx->stream));
-        SFC_CK(cudaMemsetAsync(s->flags.p, 0, (1 + K) * sizeof(int), ctx->stream));
+        SFC_CK(cudaMemsetAsync(s->flags.p, 0, (2 + K) * sizeof(int), ctx->stream));
         std::fill(nbreak.begin(), nbreak.end(), 0);
         std::fill(fallback.begin(), fallback.end(), 0);
         std::fill(nstall.begin(), nstall.end(), 0);
@@ -1672,7 +1829,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             rn[c] = active[c] ? bn : 0.0;
             hrestart[c] = 1;
         }
-        int it = 0, updates = 0;
+        int it = 0, updates = 0, real_it = 0;
         if (nactive > 0) {
             SFC_CK(cudaMemcpyAsync(scale, hs.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(norm, hn.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
@@ -1681,6 +1838,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             init32(sl(0) + K, sl(0) + 2 * K);
         }
         while (nactive > 0) {
+            const int it0 = it - it % check;  // first iteration of this check interval
             bool ran_graph = false;
             if (it % check == 0 && use_graph && it + check <= max_iter && launch_chunk_graph()) {
                 it += check;
@@ -1691,13 +1849,14 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             }
             double *rz1 = sl(it) + K, *rr1 = sl(it) + 2 * K;
             const bool at_cap = it >= max_iter;
-            if (!ran_graph) {
-                if (it % check != 0 && !at_cap) continue;
-                k_bcheck<K><<<1, 128, 0, ctx->stream>>>(rr1, thr, stop);
-                count_launch(ctx);
-            }
-            download(ctx, hflags.data(), s->flags.p, 1 + K);
-            download(ctx, rr_now.data(), rr1, K);
+            if (!ran_graph && it % check != 0 && !at_cap) continue;
+            download(ctx, hflags.data(), s->flags.p, 2 + K);
+            // `it` counts whole intervals (the ring and the captured graph
+            // follow it); the iterations that ran end at it0 + ran, whose
+            // slot no later (returning) iteration of the interval zeroes
+            const int ran_now = hflags[1 + K] > 0 ? hflags[1 + K] : it - it0;
+            real_it += ran_now;
+            download(ctx, rr_now.data(), sl(it0 + ran_now) + 2 * K, K);
             bool update = hflags[0] || at_cap;
             for (int c = 0; c < K; ++c)
                 if (active[c] && hflags[1 + c]) {
@@ -1780,7 +1939,7 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             SFC_CK(cudaMemcpyAsync(thr, ht.data(), K * 8, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemcpyAsync(restart.p, hrestart.data(), K * 4, cudaMemcpyHostToDevice, ctx->stream));
             SFC_CK(cudaMemsetAsync(sl(it), 0, (size_t)3 * K * 8, ctx->stream));
-            SFC_CK(cudaMemsetAsync(s->flags.p, 0, (1 + K) * sizeof(int), ctx->stream));
+            SFC_CK(cudaMemsetAsync(s->flags.p, 0, (2 + K) * sizeof(int), ctx->stream));
             // r32 <- scaled true residual, x32 <- 0, p kept (restarted columns: p = z)
             init32(rz1, rr1);
         }
@@ -1818,11 +1977,11 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
         if (nactive > 0) {
             all_conv = false;
             if (debug)
-                std::fprintf(stderr, "[sfc block %d] %d columns still open after %d iterations\n", c0, nactive, it);
+                std::fprintf(stderr, "[sfc block %d] %d columns still open after %d iterations\n", c0, nactive, real_it);
         }
         k_scatter_cols<<<grid_for(N * kb, 256), 256, 0, ctx->stream>>>(x64.p, ld, c0, kb, K, N, X);
         count_launch(ctx);
-        max_inner = std::max(max_inner, it);
+        max_inner = std::max(max_inner, real_it);
         max_updates = std::max(max_updates, updates);
     }
     SFC_CK(cudaStreamSynchronize(ctx->stream));

@@ -69,6 +69,36 @@ def test_transpose_mixed_two_level(ctx, bw):
     assert st["iterations"] < it_bj, (st["iterations"], it_bj)
 
 
+@pytest.mark.parametrize("amount,bw", [(0.0, 128), (0.3, 64), (0.3, 32)])
+def test_fused_r_update_and_restriction(ctx, amount, bw):
+    """The r update fused with the coarse restriction (the default) and the
+    two separate kernels (SFC_RESTRICT=separate) both give the direct solve's
+    answer; their FP32 sums differ only in order, so the iteration counts
+    stay close."""
+    import os
+
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 11, 6, amount)
+    rng = np.random.default_rng(2)
+    Rhs = rng.standard_normal((70, mesh.num_dofs))
+    refs = np.stack([ds.solve_transpose(r) for r in Rhs])
+    out = {}
+    for mode in ("fused", "separate"):
+        if mode == "separate":
+            os.environ["SFC_RESTRICT"] = "separate"
+        try:
+            s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-10, block_width=bw,
+                          precond=api.SFC_PRECOND_TWO_LEVEL, coarse_size=4)
+            out[mode] = (s.solveSystemTranspose(Rhs), s.last_stats())
+        finally:
+            os.environ.pop("SFC_RESTRICT", None)
+    for U, st in out.values():
+        assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
+        assert st["coarse_dofs"] > 0
+        assert np.abs(U - refs).max() <= 1e-7 * np.abs(refs).max()
+    itf, its = out["fused"][1]["iterations"], out["separate"][1]["iterations"]
+    assert abs(itf - its) <= max(8, its // 5), (itf, its)
+
+
 def test_multi_rhs_inhomogeneous_two_level(ctx):
     rng = np.random.default_rng(8)
     mesh = small_mesh(EL, 10)
