@@ -472,9 +472,13 @@ __global__ void __launch_bounds__(256, 2)
     double dacc[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) dacc[v] = 0.0;
-    const int64_t end = min(nodes, (run + 1) * per_run);
     const int64_t row = (int64_t)nx * RS;
-    for (int64_t a = run * per_run; a < end;) {
+    // chunks of per_run nodes, run r taking chunks r, r + nruns, ...: the
+    // chunks in flight at one time are a contiguous band of x-lines, so the
+    // nine neighbour lines of a line are mostly read while L2 still holds them
+    const int64_t nruns = (int64_t)gridDim.x * (8 / H);
+    for (int64_t chunk = run; chunk * per_run < nodes; chunk += nruns)
+    for (int64_t a = chunk * per_run, end = min(nodes, (chunk + 1) * per_run); a < end;) {
         const int64_t line = a / nx;
         const int x0 = (int)(a - line * nx);
         const int x1 = (int)(min(end, (line + 1) * nx) - 1 - line * nx);
@@ -748,9 +752,26 @@ template <int V, int H>
 void xresid_launch(sfc_system *s, const double *X, const double *B, double *R, double *rr)
 {
     sfc_ctx *ctx = s->ctx;
-    const int64_t runs = (int64_t)xresid_occ<V, H>() * ctx->sm_count * (8 / H);
-    const int64_t per_run = (s->nodes + runs - 1) / runs;
-    const unsigned grid = (unsigned)((s->nodes + per_run * (8 / H) - 1) / (per_run * (8 / H)));
+    // Chunks of nx .. nx + 2 nodes (about one x-line), dealt round-robin to
+    // at most the resident runs, every run taking the same number of chunks:
+    // the y and z neighbours of a node then lie in chunks that other runs
+    // walk at nearly the same time, so the nine reads of an X row come close
+    // together and mostly from L2.  (With the node range split evenly over
+    // the resident runs, each run walked more than one line, and a row's
+    // y neighbour was read by the same run one line later, after the FP64
+    // rows in flight had outgrown L2: 2.6x the algorithmic DRAM bytes.)
+    const int64_t cap = (int64_t)xresid_occ<V, H>() * ctx->sm_count * (8 / H);
+    const int64_t nx = s->lat[0], nodes = s->nodes;
+    int64_t per_run = nx, nrun = 0;
+    for (int64_t len = nx; len <= nx + 2; ++len) {
+        const int64_t passes = (nodes + cap * len - 1) / (cap * len);
+        const int64_t r = (nodes + passes * len - 1) / (passes * len);
+        if (r > nrun) {
+            nrun = r;
+            per_run = len;
+        }
+    }
+    const unsigned grid = (unsigned)((nrun + (8 / H) - 1) / (8 / H));
     k_xresid64<V, H><<<grid, 256, xrsmem<V, H>(), ctx->stream>>>(s->bq64.p, X, B, R, s->lat[0], s->lat[1], s->lat[2],
                                                                    s->nodes, per_run, rr);
     count_launch(ctx);
