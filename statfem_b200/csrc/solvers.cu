@@ -833,27 +833,25 @@ __global__ void __launch_bounds__(256, 4) k_nupdate32(float *__restrict__ x, flo
 // r.r with z the nodal block-Jacobi share (k_nupdate32<V, false>), and the
 // restriction c[6a + m][col] = (P^T r)[6a + m][col] of the updated r
 // (k_coarse_restrict32), so r is read once per iteration instead of twice.
-// The nodes are visited by aggregate: a cluster of kNrSplit CTAs per
+// The nodes are visited by aggregate: a cluster of S CTAs of W warps per
 // aggregate, a warp per node, node ids and modes fetched one per lane ahead
 // of the trips; the restriction's partial sums are added in rank order
 // through distributed shared memory (no atomics, the same sums on every
 // run), the dots as in k_nupdate32.
-constexpr int kNrSplit = 2;
-
-template <int V>
-__global__ void __cluster_dims__(kNrSplit, 1, 1) __launch_bounds__(256, 3)
+template <int V, int W, int S>
+__global__ void __cluster_dims__(S, 1, 1) __launch_bounds__(32 * W, 24 / W)
     k_nrupdate32(float *__restrict__ r, const float *__restrict__ q, const float *__restrict__ bdinv,
                  const int32_t *__restrict__ agg_ptr, const int32_t *__restrict__ agg_nodes,
                  const float4 *__restrict__ mode, float *__restrict__ c, const double *pq, const double *rz,
                  const double *rr, const double *thr, double *rz_next, double *rr_next, const int *stop, int *err)
 {
     constexpr int K = 32 * V;
-    __shared__ float red[8][6][K];
-    __shared__ double sh[8 * K];
+    __shared__ float red[W][6][K];
+    __shared__ double sh[W * K];
     if (*stop) return;  // uniform: stop changes only between launches
     cg::cluster_group cl = cg::this_cluster();
     const unsigned rank = cl.block_rank();
-    const int a = blockIdx.x / kNrSplit;
+    const int a = blockIdx.x / S;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     float alpha[V];
 #pragma unroll
@@ -875,8 +873,8 @@ __global__ void __cluster_dims__(kNrSplit, 1, 1) __launch_bounds__(256, 3)
     for (int m = 0; m < 6; ++m)
 #pragma unroll
         for (int v = 0; v < V; ++v) red[w][m][lane * V + v] = 0.f;
-    const int32_t step = 8 * kNrSplit, end = agg_ptr[a + 1];
-    const int32_t first = agg_ptr[a] + (int32_t)rank * 8 + w;  // this warp's nodes: first + k step
+    const int32_t step = W * S, end = agg_ptr[a + 1];
+    const int32_t first = agg_ptr[a] + (int32_t)rank * W + w;  // this warp's nodes: first + k step
     const int mine = first < end ? (end - 1 - first) / step + 1 : 0;
     for (int base = 0; base < mine; base += 32) {
         int32_t li = 0;
@@ -947,13 +945,13 @@ __global__ void __cluster_dims__(kNrSplit, 1, 1) __launch_bounds__(256, 3)
         const int m = t / K, col = t % K;
         float sum = 0.f;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) sum += red[j][m][col];
+        for (int j = 0; j < W; ++j) sum += red[j][m][col];
         red[0][m][col] = sum;  // entry (m, col) is read and written by this thread only
     }
     cl.sync();
-    for (int t = (int)rank * blockDim.x + threadIdx.x; t < 6 * K; t += kNrSplit * blockDim.x) {
+    for (int t = (int)rank * blockDim.x + threadIdx.x; t < 6 * K; t += S * blockDim.x) {
         float sum = 0.f;
-        for (unsigned j = 0; j < kNrSplit; ++j) sum += cl.map_shared_rank(&red[0][0][0], j)[t];
+        for (unsigned j = 0; j < S; ++j) sum += cl.map_shared_rank(&red[0][0][0], j)[t];
         c[(6 * (int64_t)a + t / K) * K + t % K] = sum;
     }
     cl.sync();  // the other CTAs' shared memory stays alive until every read is done
@@ -1662,7 +1660,8 @@ void block_mixed(sfc_system *s, const double *B, double *X, int nrhs, int ld, sf
             coarse_block_reserve(s, K);  // no-op once reserved (always, inside a capture)
             {
                 ProfScope ps(ctx, "nrupdate32", 3.0 * N * K * 4 + 52.0 * s->nodes + 4.0 * crs.nc * K);
-                k_nrupdate32<V><<<(unsigned)(crs.nagg * kNrSplit), 256, 0, ctx->stream>>>(
+                constexpr int W = 8, S = 2;  // 16 warps per aggregate
+                k_nrupdate32<V, W, S><<<(unsigned)(crs.nagg * S), 32 * W, 0, ctx->stream>>>(
                     rr32, qq, s->bdinv32.p, crs.agg_ptr.p, crs.agg_nodes.p, crs.mode.p, crs.c32.p, pqi, rz0, rr0,
                     thr, rz1, rr1, stop, err);
             }
