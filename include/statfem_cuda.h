@@ -73,7 +73,11 @@ typedef struct sfc_solver_options {
     double tol;            /* relative residual ||b-Ax||/||b|| (true, FP64)    */
     double inner_tol;      /* FP32 inner reduction per refinement cycle        */
     int32_t block_width;   /* RHS per block for SFC_SOLVER_PCG_MIXED (0: auto) */
-    int32_t check_every;   /* iterations between convergence checks (0: auto)  */
+    int32_t check_every;   /* iterations between the host's convergence checks
+                              (0: auto); the mixed block solver also tests
+                              convergence on the device after every iteration
+                              and skips the rest of an interval once all
+                              columns are below their thresholds             */
     int32_t precond;       /* SFC_PRECOND_*                                    */
     int32_t coarse_size;   /* SFC_PRECOND_TWO_LEVEL: nodes per aggregate along
                               each axis (0: 8)                                */

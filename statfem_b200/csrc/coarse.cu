@@ -268,8 +268,9 @@ __global__ void k_to_f32_sym(const double *__restrict__ a, float *__restrict__ b
 // c[6a + m][col] = (P^T r)[6a + m][col] for K = 32 V interleaved columns: a
 // cluster of kRestrictSplit CTAs per aggregate (warp per node), partial sums
 // added in rank order through distributed shared memory.  Two CTAs per
-// aggregate keep the c2 grid (216 aggregates) within one wave of resident
-// CTAs; four left a half-empty second wave (52 against 50 us per launch).
+// aggregate keep the 48^3 elasticity grid (216 aggregates) within one wave
+// of resident CTAs; four left a half-empty second wave (52 against 50 us per
+// launch).
 constexpr int kRestrictSplit = 2;
 
 template <int V>

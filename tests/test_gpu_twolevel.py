@@ -99,6 +99,38 @@ def test_fused_r_update_and_restriction(ctx, amount, bw):
     assert abs(itf - its) <= max(8, its // 5), (itf, its)
 
 
+@pytest.mark.parametrize("precond", [api.SFC_PRECOND_BLOCK_JACOBI, api.SFC_PRECOND_TWO_LEVEL])
+def test_convergence_inside_a_check_interval(ctx, precond):
+    """With a check interval longer than a whole FP32 stretch, the
+    per-iteration convergence test stops each captured interval where the
+    columns' recurrence converges (the reliable update then follows): the
+    iteration count is the one that ran, not a multiple of the interval, close
+    between the graph and separate launches (their FP64 column sums add in
+    different orders), and the answer is the direct solve's."""
+    import os
+
+    mesh, gm, s, ds, F, f = elastic_system(ctx, 8, 9)
+    rng = np.random.default_rng(5)
+    Rhs = rng.standard_normal((40, mesh.num_dofs))
+    refs = np.stack([ds.solve_transpose(r) for r in Rhs])
+    check = 400
+    out = {}
+    for mode in ("graph", "eager"):
+        if mode == "eager":
+            os.environ["SFC_BLOCK_GRAPH"] = "0"
+        try:
+            s.set_options(method=api.SFC_SOLVER_PCG_MIXED, tol=1e-9, block_width=64, precond=precond,
+                          coarse_size=4, check_every=check)
+            out[mode] = (s.solveSystemTranspose(Rhs), s.last_stats())
+        finally:
+            os.environ.pop("SFC_BLOCK_GRAPH", None)
+    for U, st in out.values():
+        assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-9, st
+        assert st["iterations"] > 0 and st["iterations"] % check != 0, st
+        assert np.abs(U - refs).max() <= 1e-6 * np.abs(refs).max()
+    assert abs(out["graph"][1]["iterations"] - out["eager"][1]["iterations"]) <= 4
+
+
 def test_multi_rhs_inhomogeneous_two_level(ctx):
     rng = np.random.default_rng(8)
     mesh = small_mesh(EL, 10)
